@@ -1,0 +1,126 @@
+/*
+ * ob.h — C ABI of the B200-native OutbreakLab storm-model time step.
+ *
+ * Every entry point is plain C: opaque handles, pointers and sizes, int status codes. A JavaScript (Node) host binds
+ * it through N-API / node-ffi; Python binds it through ctypes (outbreaklab_b200/model.py).
+ *
+ * Each declaration names the reference interface it replaces (file:line in Julianfinnerty/outbreakLab). The
+ * reference has no FFI: its boundary is the JS class API of RegionalModel (model.js), PoissonDirect (solver.js)
+ * and RadarSim (radar.js).
+ *
+ * Ownership: the library owns all device memory. Host arrays passed in are copied (the semantics of WebGPU's
+ * queue.writeBuffer, util.js:190). Readbacks go into caller-owned buffers.
+ * Threading: one host thread per handle. Work runs on the handle's in-order CUDA stream (the WebGPU queue).
+ * Errors: every call returns OB_OK or an OB_ERR_* code; ob_last_error() returns the message of the last failure on
+ * the calling thread (model.js:1194-1200 turns such failures into a thrown JS Error).
+ */
+#ifndef OB_H_
+#define OB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define OB_OK 0
+#define OB_ERR_OOM 1        /* device allocation failed (model.js:1172-1174 "not enough GPU memory") */
+#define OB_ERR_INVALID 2    /* bad argument, unsupported mode or size */
+#define OB_ERR_DEVICE 3     /* a CUDA call failed, or no CUDA device */
+#define OB_ERR_TIMEOUT 4    /* a bounded device-side wait gave up */
+#define OB_ERR_NAN 5        /* the state holds NaN/Inf after a step (the reference resets such cells, model.js:904) */
+
+/* ---- fields, in the texel layouts of model.js:1208-1233 ---- */
+#define OB_FIELD_V 0    /* (nx+1)(ny+1)(nz+1) x float4 (u at x-face, v at y-face, w at z-face, theta), x fastest */
+#define OB_FIELD_Q1 1   /* nx*ny*nz x float4 (qv, qc, qi, qr) */
+#define OB_FIELD_Q2 2   /* nx*ny*nz x float4 (qs, qg, Nr per kg, spare) */
+#define OB_FIELD_AUX 3  /* nx*ny*nz x float2 (nu_h, nu_v) */
+#define OB_FIELD_PHI 4  /* (nx+2p)(ny+2p)nz float: the pressure solve's phi on the padded grid */
+#define OB_FIELD_RAIN 5 /* nx*ny double: accumulated surface precipitation (kg/m^2); no counterpart in the reference */
+
+/* Physics and numerics knobs: RegionalModel.params (model.js:1176-1180) with the outbreak-mode overrides of
+ * app.js:1613. ob_params_default() fills the outbreak defaults. */
+typedef struct ObParams {
+  float cs, nu0, drag, z0;               /* Smagorinsky cs, background viscosity, semi-slip drag on/off, z0 (m) */
+  float spongeW, spongeTau, dampZ, dampTau;
+  float autoc, qc0, freeze, noise;       /* Kessler rate, threshold, freezing factor, INIT noise amplitude (K) */
+  float mc, vcap, evap, sortQ;           /* MacCormack strength, speed cap, rain evaporation factor, size sorting */
+  float ciRate, nudgeTau, lat, moistMix;
+  float mcFloor, scheme, evapT, dtScale; /* scheme: 0 Lin-type, 1 Thompson-style; dtScale (app.js:1666) */
+} ObParams;
+
+/* Grid: dx (m), nx, ny, nz. dz = 20000/nz and the solver padding gridPad(dx) follow model.js:1122, 1203. */
+typedef struct ObGrid {
+  int nx, ny, nz;
+  float dx;
+} ObGrid;
+
+/* one moving boundary (air mass), 148 floats, the packing of RegionalModel.setBoundaries (model.js:1371-1380) */
+#define OB_BOUNDARY_FLOATS 148
+#define OB_MAX_BOUNDS 8
+/* one updraft-nudging event, 12 floats (model.js:1383-1389) */
+#define OB_CI_FLOATS 12
+#define OB_MAX_CI 256
+
+typedef struct ObModel ObModel;
+typedef struct ObPoisson ObPoisson;
+
+/* message of the last failed call on this thread ("" if none) */
+const char* ob_last_error(void);
+/* library version string */
+const char* ob_version(void);
+/* fills the outbreak-mode defaults of model.js:1176-1180 + app.js:1613 */
+void ob_params_default(ObParams* p);
+/* padding of the pressure solve, gridPad (model.js:1122) */
+int ob_grid_pad(float dx);
+
+/* ---- RegionalModel (model.js:1156-1496) ---- */
+/* replaces RegionalModel.allocate / allocTextures (model.js:1186-1238); scheme is chosen by params */
+int ob_model_create(const ObGrid* grid, ObModel** out);
+/* replaces RegionalModel.destroy (model.js:1239-1247) */
+int ob_model_destroy(ObModel* m);
+/* replaces the base-state upload of setSounding (model.js:1276-1288): B = (nz+1)*8 floats, sounding.js:139-142 */
+int ob_model_set_base_state(ObModel* m, const float* B, int nz);
+/* replaces RegionalModel.params assignment (model.js:1176, app.js:1613) */
+int ob_model_set_params(ObModel* m, const ObParams* p);
+/* replaces setBoundaries (model.js:1371); n boundaries x OB_BOUNDARY_FLOATS */
+int ob_model_set_boundaries(ObModel* m, const float* packed, int n);
+/* replaces setCI (model.js:1383); n events x OB_CI_FLOATS, already filtered to the active ones */
+int ob_model_set_ci(ObModel* m, const float* events, int n);
+/* replaces RegionalModel.reset (model.js:1427-1440): LSF + INIT, phi/rhs cleared, time = steps = parity = 0 */
+int ob_model_reset(ObModel* m);
+/* replaces encStep (model.js:1442-1476) nsteps times with the same dt; runs on the model's stream */
+int ob_model_step(ObModel* m, float dt, int nsteps);
+/* waits for the model's stream; returns OB_ERR_NAN if the last step's NaN/Inf counter is non-zero */
+int ob_model_sync(ObModel* m);
+/* replaces requestMaps (model.js:1478-1494): 16 floats per column, 4 maps of nx*ny float4 */
+int ob_model_maps(ObModel* m, float* out16xN2);
+/* field up/download in the texel layouts above (bytes must match exactly) */
+int ob_model_get_field(ObModel* m, int field, void* host, size_t bytes);
+int ob_model_set_field(ObModel* m, int field, const void* host, size_t bytes);
+/* model time (s), steps and parity (model.js:1156-1158, 1448-1450) */
+int ob_model_time(ObModel* m, double* time, int* steps, int* parity);
+/* domain budgets in FP64 on the device: sum rho*q_total*dV (kg), sum rho*dV (kg), accumulated surface rain (kg);
+ * no counterpart in the reference (it keeps no budgets) */
+int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain);
+/* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
+void* ob_model_stream(ObModel* m);
+
+/* ---- PoissonDirect (solver.js:105-165) ---- */
+/* replaces new PoissonDirect(nx, ny, nz, dx, dz) (solver.js:106-137); precision 0 = FP32 SIMT transforms,
+ * 1 = bf16x3 tensor-core transforms (FP32 accumulate) */
+int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out);
+int ob_poisson_destroy(ObPoisson* p);
+/* replaces setDensity (solver.js:139-146): rhoC[nz] at centres, rhoW[nz+1] at bottom faces */
+int ob_poisson_set_density(ObPoisson* p, const float* rhoC, const float* rhoW);
+/* replaces bind + enc (solver.js:147-163): solves on host arrays of nx*ny*nz floats (x fastest) */
+int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi);
+/* the same on device pointers, on the given stream (cudaStream_t, may be NULL) */
+int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OB_H_ */
