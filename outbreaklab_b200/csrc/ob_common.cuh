@@ -1,0 +1,188 @@
+// ob_common.cuh — device-side layout, uniforms and physics helpers of the B200 storm-model step.
+//
+// Layout in HBM (structure of arrays): every 3-D field is one fp32 array over the staggered texel box
+// (nx+1) x (ny+1) x (nz+1), x fastest, rows padded to a pitch that is a multiple of 32 floats (128 B), so that a warp
+// reading a row segment issues whole 128-byte lines and every field shares one index i + px*(j + py*k). Cell-centred
+// fields (Q, aux, phT) use the same index and leave the i = nx, j = ny, k = nz planes unused. One channel per array
+// means a semi-Lagrangian gather of u touches only u bytes (a float4 texel would drag v, w, theta through L1/L2).
+//
+// The physics formulas restate the reference's WGSL (model.js:41-134, 578-907) in fp32 with IEEE division and
+// square root; the hurricane-mode branches are not built (outbreak mode only, model.js:1412).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ob {
+
+// uniform block (model.js:23-37), packed on the host per step (model.js:1391-1425)
+struct Uni {
+  float4 dims, dzv, step, sponge, turb, micro, misc, cor, ci, pad, micro2, hur, hur2, hur3, hur4, hur5, vtx, vtx2, cn;
+};
+
+struct Grid {
+  int nx, ny, nz;
+  int px;        // row pitch in floats (>= nx+1, multiple of 32)
+  int py;        // rows per plane (= ny+1)
+  int plane;     // px*py
+  int pad, nxp, nyp;  // pressure-solve padding and padded extents (model.js:1220-1223)
+  __host__ __device__ __forceinline__ int at(int i, int j, int k) const { return i + px * (j + py * k); }
+  __host__ __device__ __forceinline__ int pidx(int i, int j, int k) const { return (i + pad) + nxp * ((j + pad) + nyp * k); }
+};
+
+// device pointers of one model's state
+struct Fields {
+  float* V[2][4];   // (u, v, w, theta) ping-pong
+  float* Vt[4];     // advection scratch (ADVV1 output)
+  float* Q[2][8];   // (qv, qc, qi, qr, qs, qg, Nr, spare): slot 0 = state, slot 1 = after advection
+  float* Qt[8];     // advection scratch (ADVQ1 output)
+  float* aux[2];    // nu_h, nu_v
+  float* phT;       // target hydrostatic phi
+  float4* lsfA;     // 2-D nx*ny
+  float4* lsfB;
+  float4* ciMap;
+  float4* sfc;
+  const float* B;   // base state (nz+1)*8
+  float* rhs;       // padded solve grid nxp*nyp*nz
+  float* phi;
+  double* rain;     // nx*ny accumulated surface precipitation
+  const float* bnd; // OB_MAX_BOUNDS x 148
+  const float* ci;  // events x 12
+  unsigned int* flags;  // [0] NaN/Inf counter
+};
+
+constexpr float T0K = 273.15f;
+constexpr double CPDd = 1005.7, RVCd = 461.5, LVCd = 2.501e6, LFCd = 3.337e5, LSCd = 2.834e6;
+
+__device__ __forceinline__ int clampi(int x, int a, int b) { return x < a ? a : (x > b ? b : x); }
+__device__ __forceinline__ float clampf(float x, float a, float b) { return fminf(fmaxf(x, a), b); }
+__device__ __forceinline__ float sstep(float a, float b, float x) {
+  float t = clampf((x - a) / (b - a), 0.f, 1.f);
+  return t * t * (3.f - 2.f * t);
+}
+__device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.f - t) + b * t; }
+
+// base state per level: A = (theta0, qv0, rho_c, rho_w bottom), B = (pi0, p0, u0, v0)
+__device__ __forceinline__ float4 bsA(const float* B, int nz, int k) {
+  return __ldg(reinterpret_cast<const float4*>(B) + clampi(k, 0, nz - 1) * 2);
+}
+__device__ __forceinline__ float4 bsB(const float* B, int nz, int k) {
+  return __ldg(reinterpret_cast<const float4*>(B) + clampi(k, 0, nz - 1) * 2 + 1);
+}
+__device__ __forceinline__ float rhoW(const float* B, int nz, int k) { return __ldg(B + clampi(k, 0, nz) * 8 + 3); }
+
+// ---- noise.js:4-27 ----
+__device__ __forceinline__ uint32_t pcg(uint32_t v) {
+  uint32_t s = v * 747796405u + 2891336453u;
+  uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+__device__ __forceinline__ uint32_t hash2i(int x, int y) { return pcg(uint32_t(x) ^ pcg(uint32_t(y) + 0x9e3779b9u)); }
+__device__ __forceinline__ uint32_t hash3i(int x, int y, int z) {
+  return pcg(uint32_t(x) ^ pcg(uint32_t(y) ^ pcg(uint32_t(z) + 0x7f4a7c15u)));
+}
+__device__ __forceinline__ float rnd3(int x, int y, int z) { return float(hash3i(x, y, z) >> 8u) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ float fadef(float t) { return t * t * t * (t * (t * 6.f - 15.f) + 10.f); }
+__device__ __forceinline__ float gdot(int ix, int iy, float fx, float fy) {
+  float a = float(hash2i(ix, iy) >> 8u) * (6.2831853f / 16777216.0f);
+  return cosf(a) * fx + sinf(a) * fy;
+}
+__device__ __forceinline__ float gnoise2(float px, float py) {
+  float fx0 = floorf(px), fy0 = floorf(py);
+  int ix = int(fx0), iy = int(fy0);
+  float fx = px - fx0, fy = py - fy0;
+  float ux = fadef(fx), uy = fadef(fy);
+  float a = gdot(ix, iy, fx, fy), b = gdot(ix + 1, iy, fx - 1.f, fy);
+  float c = gdot(ix, iy + 1, fx, fy - 1.f), d = gdot(ix + 1, iy + 1, fx - 1.f, fy - 1.f);
+  return mixf(mixf(a, b, ux), mixf(c, d, ux), uy) * 1.4142f;
+}
+__device__ __forceinline__ float fbm2(float px, float py, int oct) {
+  float a = 0.5f, s = 0.f;
+  for (int i = 0; i < oct; i++) {
+    s += a * gnoise2(px, py);
+    float nx = 1.6f * px - 1.2f * py + 17.1f, ny = 1.2f * px + 1.6f * py + 3.7f;
+    px = nx;
+    py = ny;
+    a *= 0.5f;
+  }
+  return s;
+}
+
+// ---- saturation and fall speeds (model.js:59-101) ----
+__device__ __forceinline__ float esl(float T) { return 611.2f * expf(17.67f * (T - T0K) / (T - 29.65f)); }
+__device__ __forceinline__ float esi(float T) { return 611.2f * expf(21.8745584f * (T - 273.16f) / (T - 7.66f)); }
+__device__ __forceinline__ float fIce(float T) { return clampf((T0K - T) / 40.f, 0.f, 1.f); }
+__device__ __forceinline__ float qvsat(float T, float p, float f) {
+  float e = mixf(esl(T), esi(T), f);
+  return 0.622f * e / fmaxf(p - e, 100.f);
+}
+struct Fall {
+  float rsfc;   // surface density (step.z)
+  bool thm;     // Thompson-style scheme
+  __device__ __forceinline__ float vtR(float q, float rho) const {
+    float f = sqrtf(rsfc / rho);
+    return fminf(36.34f * powf(fmaxf(0.001f * rho * q, 0.f), 0.1364f) * f, 10.f * f);
+  }
+  __device__ __forceinline__ float vtS(float q, float rho) const {
+    return clampf(1.1f * powf(fmaxf(1000.f * rho * q, 1e-6f), 0.11f), 0.3f, 2.2f) * sqrtf(rsfc / rho);
+  }
+  __device__ __forceinline__ float vtG(float q, float rho) const {
+    float v = clampf(9.f * powf(fmaxf(1000.f * rho * q, 1e-6f), 0.42f), 1.f, 55.f) * sqrtf(rsfc / rho);
+    float r = q / 0.009f;
+    return fminf(v * (1.f + r * r), 65.f);
+  }
+  static __device__ __forceinline__ float lamR(float q, float n) {
+    return clampf(powf(float(3.14159 * 1000.0) * fmaxf(n, 1e-3f) / fmaxf(q, 1e-12f), 0.33333f), 1000.f, 1.0e5f);
+  }
+  static __device__ __forceinline__ float n0G(float q, float rho) { return clampf(200.f / fmaxf(rho * q, 1e-9f), 1e4f, 3e6f); }
+  static __device__ __forceinline__ float lamG(float q, float rho) {
+    return powf(float(3.14159 * 500.0) * n0G(q, rho) / fmaxf(rho * q, 1e-12f), 0.25f);
+  }
+  __device__ __forceinline__ float vtGT(float q, float rho) const {
+    return fminf(1503.f * powf(lamG(q, rho), -0.89f), 25.f) * sqrtf(rsfc / rho);
+  }
+  // rain fall speed (mass-weighted, number-weighted)
+  __device__ __forceinline__ float2 vtRain(float qr, float nr, float rho) const {
+    if (thm) {
+      float l = powf(lamR(qr, nr), -0.8f), s = sqrtf(rsfc / rho);
+      return make_float2(fminf(2503.f * l, 10.f) * s, fminf(784.f * l, 10.f) * s);
+    }
+    float v = vtR(qr, rho);
+    return make_float2(v, v);
+  }
+  __device__ __forceinline__ float vtGrau(float qg, float rho) const { return thm ? vtGT(qg, rho) : vtG(qg, rho); }
+  // equivalent reflectivity (mm^6/m^3), model.js:103-116
+  __device__ __forceinline__ float zRain(float qr, float nr, float rho) const {
+    if (!thm) return 3.63e9f * powf(fmaxf(rho * qr, 0.f), 1.75f);
+    if (qr < 1e-9f) return 0.f;
+    float l = lamR(qr, nr);
+    float nb = qr * l * l * l / 3141.59f;
+    return 720e18f * rho * nb / (l * l * l * l * l * l);
+  }
+  __device__ __forceinline__ float zGrau(float qg, float rho, float T) const {
+    if (!thm) return (T < T0K ? 1.2e10f : 4.33e10f) * powf(fmaxf(rho * qg, 0.f), 1.75f);
+    if (qg < 1e-9f) return 0.f;
+    float l = lamG(qg, rho), l2 = l * l;
+    return 720e18f * n0G(qg, rho) / (l2 * l2 * l2 * l) * (T < T0K ? 0.0666f : 0.24f);
+  }
+};
+
+// linear filter with clamp-to-edge on an (X, Y, Z) box stored at pitch (px, py); x, y, z in texel units
+__device__ __forceinline__ float trilerp(const float* __restrict__ f, const Grid& g, int X, int Y, int Z, float x, float y, float z) {
+  float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  int i0 = int(fx), j0 = int(fy), k0 = int(fz);
+  float ax = x - fx, ay = y - fy, az = z - fz;
+  int i1 = clampi(i0 + 1, 0, X - 1), j1 = clampi(j0 + 1, 0, Y - 1), k1 = clampi(k0 + 1, 0, Z - 1);
+  i0 = clampi(i0, 0, X - 1);
+  j0 = clampi(j0, 0, Y - 1);
+  k0 = clampi(k0, 0, Z - 1);
+  const int r00 = g.px * (j0 + g.py * k0), r10 = g.px * (j1 + g.py * k0), r01 = g.px * (j0 + g.py * k1), r11 = g.px * (j1 + g.py * k1);
+  float c00 = __ldg(f + r00 + i0) * (1.f - ax) + __ldg(f + r00 + i1) * ax;
+  float c10 = __ldg(f + r10 + i0) * (1.f - ax) + __ldg(f + r10 + i1) * ax;
+  float c01 = __ldg(f + r01 + i0) * (1.f - ax) + __ldg(f + r01 + i1) * ax;
+  float c11 = __ldg(f + r11 + i0) * (1.f - ax) + __ldg(f + r11 + i1) * ax;
+  float c0 = c00 * (1.f - ay) + c10 * ay;
+  float c1 = c01 * (1.f - ay) + c11 * ay;
+  return c0 * (1.f - az) + c1 * az;
+}
+
+}  // namespace ob

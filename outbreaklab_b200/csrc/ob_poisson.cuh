@@ -1,0 +1,39 @@
+// ob_poisson.cuh — the pressure-solve plan (solver.js:105-165) shared by the model and the standalone C ABI.
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "../../include/ob.h"
+
+namespace ob {
+
+void set_error(const char* fmt, ...);
+
+struct PoissonPlan {
+  int nx = 0, ny = 0, nz = 0, precision = 0;
+  double dx = 0, dz = 0;
+  float* mats = nullptr;  // qix | qx | qiy | qy (fp32, solver.js:115-125)
+  size_t ofs_qix = 0, ofs_qx = 0, ofs_qiy = 0, ofs_qy = 0;
+  float* lam = nullptr;   // eigenvalues (nx + ny)
+  float4* zop = nullptr;  // (lo, up, diag, rho_c) per level
+  float* tmp = nullptr;
+  float* hat = nullptr;
+  float* cpf = nullptr;   // Thomas scratch for nz without a register specialisation
+  double* cpd = nullptr;  // FP64 low-mode scratch
+  // bf16x3 tensor-core path (ob_dst_tc.cu)
+  void* tc = nullptr;
+
+  int create(int nx, int ny, int nz, double dx, double dz, int precision);
+  int set_density(const float* rhoC, const float* rhoW);
+  int solve(const float* rhs, float* phi, cudaStream_t s);
+  void destroy();
+
+  void gemm_x(const float* Mx, const float* src, float* dst, cudaStream_t s) const;
+  void gemm_y(const float* My, const float* src, float* dst, cudaStream_t s) const;
+  void tri(float* h, cudaStream_t s) const;
+  int tc_create();
+  int tc_solve(const float* rhs, float* phi, cudaStream_t s);
+  void tc_destroy();
+};
+
+}  // namespace ob

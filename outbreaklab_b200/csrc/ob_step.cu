@@ -1,0 +1,915 @@
+// ob_step.cu — the storm-model step kernels for sm_100a (one kernel per pass of model.js:1457-1472).
+//
+// Each kernel restates one WGSL pass of the reference (citations per kernel) over the structure-of-arrays layout of
+// ob_common.cuh: one thread per texel, x fastest within a warp so that every stencil row is a coalesced 128-byte
+// read, neighbours served from L1/L2. Semi-Lagrangian sampling is a software trilinear filter in fp32 (exact
+// weights; WebGPU's hardware filter uses low-precision fixed-point weights, which are not reproduced).
+#include "ob_common.cuh"
+#include "ob_step.cuh"
+
+namespace ob {
+
+#define OB_TEXEL_LOOP_BEGIN(XMAX, YMAX, ZMAX)             \
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x;   \
+  const int cj = blockIdx.y * blockDim.y + threadIdx.y;   \
+  const int ck = blockIdx.z;                              \
+  if (ci > (XMAX) || cj > (YMAX) || ck > (ZMAX)) return;
+
+// ---------------------------------------------------------------------------------------------------------------
+// target state (model.js:121-134)
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float tprof(float z, float H) { return 1.f - sstep(0.7f * H, 1.15f * H, z); }
+__device__ __forceinline__ float4 l2d(const float4* __restrict__ m, const Grid& g, int i, int j) {
+  return __ldg(m + clampi(j, 0, g.ny - 1) * g.nx + clampi(i, 0, g.nx - 1));
+}
+__device__ __forceinline__ float tgtTh(const float* B, const Grid& g, float dz, float4 A, int k) {
+  float z = (float(k) + 0.5f) * dz;
+  return bsA(B, g.nz, k).x + A.x / bsB(B, g.nz, k).x * tprof(z, A.y);
+}
+__device__ __forceinline__ float tgtQv(const float* B, const Grid& g, float dz, float4 A, int k) {
+  float z = (float(k) + 0.5f) * dz;
+  return bsA(B, g.nz, k).y * (1.f - A.z * tprof(z, A.w));
+}
+__device__ __forceinline__ float tgtU(const Fields& F, const Grid& g, float dz, int i, int j, int k) {
+  float z = (float(k) + 0.5f) * dz;
+  float4 a = l2d(F.lsfB, g, i - 1, j), b = l2d(F.lsfB, g, i, j);
+  return bsB(F.B, g.nz, k).z + 0.5f * (a.x * tprof(z, a.z) + b.x * tprof(z, b.z));
+}
+__device__ __forceinline__ float tgtV(const Fields& F, const Grid& g, float dz, int i, int j, int k) {
+  float z = (float(k) + 0.5f) * dz;
+  float4 a = l2d(F.lsfB, g, i, j - 1), b = l2d(F.lsfB, g, i, j);
+  return bsB(F.B, g.nz, k).w + 0.5f * (a.y * tprof(z, a.z) + b.y * tprof(z, b.z));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_LSF (model.js:142-244): per column, target anomalies of the boundaries' air masses + hydrostatic phi_t
+// ---------------------------------------------------------------------------------------------------------------
+__device__ void bpt(const float* bd, int i, float t, float& x, float& y) {
+  const float* q = bd + 20 + 4 * i;
+  x = q[0] + q[2] * t;
+  y = q[1] + q[3] * t;
+}
+__global__ void k_lsf(Grid g, Uni U, Fields F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const float dx = U.dims.w, t = U.step.y;
+  const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
+  float sT = 0, sH = 0, sQ = 0, sHq = 0, sU = 0, sV = 0, sHw = 0, sw = 0, nud = 0;
+  const int nb = int(U.cor.z);
+  for (int b = 0; b < nb; b++) {
+    const float* bd = F.bnd + b * 148;
+    // signed distance to the moving polyline (model.js:157-179)
+    const int np = int(bd[0]);
+    float best = 1e30f, sg = 1.f, over = 0.f, along = 0.f, s0 = 0.f;
+    for (int s = 0; s < np - 1; s++) {
+      float ax, ay, ex, ey;
+      bpt(bd, s, t, ax, ay);
+      bpt(bd, s + 1, t, ex, ey);
+      float abx = ex - ax, aby = ey - ay;
+      float la = fmaxf(sqrtf(abx * abx + aby * aby), 1.f);
+      float t0 = ((x - ax) * abx + (y - ay) * aby) / (la * la);
+      float tt = t0;
+      if (s > 0) tt = fmaxf(tt, 0.f);
+      if (s < np - 2) tt = fminf(tt, 1.f);
+      float ddx = x - (ax + tt * abx), ddy = y - (ay + tt * aby);
+      float d = sqrtf(ddx * ddx + ddy * ddy);
+      if (d < best) {
+        best = d;
+        sg = (abx * (y - ay) - aby * (x - ax) > 0.f) ? 1.f : -1.f;
+        over = (s == 0 ? fmaxf(-t0, 0.f) * la : 0.f) + (s == np - 2 ? fmaxf(t0 - 1.f, 0.f) * la : 0.f);
+        along = s0 + tt * la;
+      }
+      s0 += la;
+    }
+    const float d = best * sg * bd[15];
+    const float w = sstep(-bd[3], bd[3], d) * (1.f - sstep(0.f, 60000.f, over));
+    if (w <= 0.f) continue;
+    const float vr = bd[16];
+    const float fade = 1.f - sstep(30000.f, 90000.f, d);
+    // along-front variation (model.js:183-187) and hot spots (model.js:191-206)
+    float avv = 0.f;
+    if (bd[16] > 0.f) avv = clampf(fbm2(along / bd[18], bd[17] + t / 5400.f, 2) * 1.6f, -1.f, 1.f);
+    const float av = vr * avv * fade;
+    float lift = 1.f;
+    if (vr > 0.f) {
+      const float L = bd[18];
+      const int sd = int(bd[17] * 1000.f);
+      const float ph = t / 4800.f;
+      const int e = int(floorf(ph));
+      const float fe = sstep(0.f, 1.f, ph - floorf(ph));
+      const int k0 = int(floorf(along / L));
+      float acc = 0.f;
+      for (int k = k0 - 1; k <= k0 + 1; k++)
+        for (int q = 0; q < 2; q++) {
+          uint32_t h = hash3i(k, e + q, sd);
+          float r1 = float(h & 0xffffu) / 65535.f, r2 = float((h >> 16u) & 0xffffu) / 65535.f;
+          float z = (along - (float(k) + 0.5f + 0.7f * (r1 - 0.5f)) * L) / (0.17f * L);
+          acc += (q == 1 ? fe : 1.f - fe) * (0.35f + 0.65f * r2) * expf(-z * z);
+        }
+      lift = mixf(1.f, mixf(1.f - 0.85f * vr, 1.f + 1.3f * vr, clampf(acc, 0.f, 1.f)), fade);
+    }
+    const float Hmin = bd[7] * clampf(lift, 0.15f, 3.f);
+    const float H = fminf(fmaxf(bd[6] * fmaxf(d + bd[3], 0.f) * (1.f + 0.4f * av), Hmin), bd[5]);
+    sT += w * bd[4] * expf(0.5f * av);
+    sQ += w * bd[8];
+    sU += w * bd[10] * lift;
+    sV += w * bd[11] * lift;
+    sH += w * H;
+    sHq += w * H * bd[9];
+    sHw += w * H * bd[12];
+    sw += w;
+    nud = fmaxf(nud, bd[13] * sstep(bd[14], bd[14] + 40000.f, d) * (1.f - sstep(0.f, 60000.f, over)));
+  }
+  const float iw = 1.f / fmaxf(sw, 1e-6f);
+  const float4 A = make_float4(clampf(sT, -20.f, 10.f), fmaxf(sH * iw, 100.f), clampf(sQ, 0.f, 0.92f), fmaxf(sHq * iw, 100.f));
+  F.lsfA[j * g.nx + i] = A;
+  F.lsfB[j * g.nx + i] = make_float4(sU, sV, fmaxf(sHw * iw, 100.f), nud);
+  const float dz = U.dzv.x;
+  float ph = 0.f, bprev = 0.f;
+  for (int k = g.nz - 1; k >= 0; k--) {
+    const float z = (float(k) + 0.5f) * dz;
+    const float4 a = bsA(F.B, g.nz, k), bb = bsB(F.B, g.nz, k);
+    const float dth = A.x / bb.x * tprof(z, A.y);
+    const float dqv = -a.y * A.z * tprof(z, A.w);
+    const float bt = 9.81f * (dth / a.x + 0.608f * dqv);
+    if (k == g.nz - 1) ph = -bt * 0.5f * dz;
+    else ph -= 0.5f * (bt + bprev) * dz;
+    bprev = bt;
+    F.phT[g.at(i, j, k)] = ph;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_CI (model.js:249-281): strongest active updraft-nudging event per column
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_ci(Grid g, Uni U, Fields F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const float dx = U.dims.w, t = U.step.y;
+  const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
+  float4 best = make_float4(0.f, 0.f, 1500.f, 1500.f);
+  const int ne = int(U.ci.x);
+  for (int e = 0; e < ne; e++) {
+    const float* E = F.ci + e * 12;
+    if (t < E[6] || t > E[7]) continue;
+    const float dxv = x - (E[0] + E[8] * (t - E[6])), dyv = y - (E[1] + E[9] * (t - E[6]));
+    const float ang = atan2f(dyv, dxv);
+    const float wob = 1.f + 0.25f * gnoise2(cosf(ang) * 1.6f + E[10], sinf(ang) * 1.6f + 3.7f * E[10]);
+    const float gg = sstep(E[6], E[6] + fmaxf(E[11], 60.f), t);
+    const float r = sqrtf(dxv * dxv + dyv * dyv) / (E[3] * wob * (0.35f + 0.65f * gg));
+    if (r >= 1.f) continue;
+    const float Lx = float(g.nx) * dx, Ly = float(g.ny) * dx;
+    const float edge = fminf(fminf(x, Lx - x), fminf(y, Ly - y));
+    const float h = sstep(E[6], E[6] + 60.f, t) * (1.f - sstep(E[7] - 180.f, E[7], t)) * sstep(U.sponge.x, U.sponge.x + 10000.f, edge);
+    const float wt = E[5] * (0.4f + 0.6f * gg) * cosf(1.5707963f * r);
+    if (h * wt > best.x * best.y) best = make_float4(h, wt, E[2], E[4]);
+  }
+  F.ciMap[j * g.nx + i] = best;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_INIT (model.js:284-339), outbreak mode (no vortex)
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_init(Grid g, Uni U, Fields F) {
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const int k = min(ck, g.nz - 1);
+  const float dz = U.dzv.x;
+  const float4 A = l2d(F.lsfA, g, ci, cj);
+  const float z = (float(k) + 0.5f) * dz;
+  const float nz0 = sstep(800.f, 1500.f, z);
+  const float noise = U.misc.z * (rnd3(ci + 17, cj + 3, ck + 5) - 0.5f) * 2.f * (1.f - nz0);
+  const float th = tgtTh(F.B, g, dz, A, k) + noise;
+  const float u = (cj < g.ny && ck < g.nz) ? tgtU(F, g, dz, ci, cj, k) : 0.f;
+  const float v = (ci < g.nx && ck < g.nz) ? tgtV(F, g, dz, ci, cj, k) : 0.f;
+  const float T = th * bsB(F.B, g.nz, k).x;
+  const float qv = fminf(tgtQv(F.B, g, dz, A, k), 0.95f * qvsat(T, bsB(F.B, g.nz, k).y, fIce(T)));
+  const int o = g.at(ci, cj, ck);
+  for (int p = 0; p < 2; p++) {  // both ping-pong slots (reset copies V0 to V1, model.js:1437)
+    F.V[p][0][o] = u;
+    F.V[p][1][o] = v;
+    F.V[p][2][o] = 0.f;
+    F.V[p][3][o] = th;
+  }
+  if (ci < g.nx && cj < g.ny && ck < g.nz) {
+    F.Q[0][0][o] = qv;
+#pragma unroll
+    for (int c = 1; c < 8; c++) F.Q[0][c][o] = 0.f;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_NUT (model.js:342-389): Smagorinsky-Lilly viscosities with the Richardson correction
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_nut(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
+  const float* __restrict__ u = F.V[par][0];
+  const float* __restrict__ v = F.V[par][1];
+  const float* __restrict__ w = F.V[par][2];
+  const float* __restrict__ th = F.V[par][3];
+  auto L = [&](const float* f, int a, int b, int c) { return __ldg(f + g.at(clampi(a, 0, g.nx), clampi(b, 0, g.ny), clampi(c, 0, g.nz))); };
+  auto uc = [&](int a, int b, int c) { return 0.5f * (L(u, a, b, c) + L(u, a + 1, b, c)) - bsB(F.B, g.nz, c).z; };
+  auto vc = [&](int a, int b, int c) { return 0.5f * (L(v, a, b, c) + L(v, a, b + 1, c)) - bsB(F.B, g.nz, c).w; };
+  auto wc = [&](int a, int b, int c) { return 0.5f * (L(w, a, b, c) + L(w, a, b, c + 1)); };
+  const float dx = U.dims.w, dz = U.dzv.x;
+  const float dudx = (L(u, ci + 1, cj, ck) - L(u, ci, cj, ck)) / dx;
+  const float dvdy = (L(v, ci, cj + 1, ck) - L(v, ci, cj, ck)) / dx;
+  const float dwdz = (L(w, ci, cj, ck + 1) - L(w, ci, cj, ck)) / dz;
+  const float dudy = (uc(ci, cj + 1, ck) - uc(ci, cj - 1, ck)) / (2.f * dx), dudz = (uc(ci, cj, ck + 1) - uc(ci, cj, ck - 1)) / (2.f * dz);
+  const float dvdx = (vc(ci + 1, cj, ck) - vc(ci - 1, cj, ck)) / (2.f * dx), dvdz = (vc(ci, cj, ck + 1) - vc(ci, cj, ck - 1)) / (2.f * dz);
+  const float dwdx = (wc(ci + 1, cj, ck) - wc(ci - 1, cj, ck)) / (2.f * dx), dwdy = (wc(ci, cj + 1, ck) - wc(ci, cj - 1, ck)) / (2.f * dx);
+  const float s12 = 0.5f * (dudy + dvdx), s13 = 0.5f * (dudz + dwdx), s23 = 0.5f * (dvdz + dwdy);
+  const float S2 = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + 4.f * (s12 * s12 + s13 * s13 + s23 * s23);
+  const int kz0 = max(ck - 1, 0), kz1 = min(ck + 1, g.nz - 1);
+  float N2 = 9.81f / bsA(F.B, g.nz, ck).x * (L(th, ci, cj, kz1) - L(th, ci, cj, kz0)) / (float(kz1 - kz0) * dz);
+  const int o = g.at(ci, cj, ck);
+  if (U.cor.w > 0.5f && __ldg(F.Q[0][1] + o) + __ldg(F.Q[0][2] + o) > 1e-5f) N2 = fminf(N2, 0.f);
+  const float Ri = N2 / fmaxf(S2, 1e-10f);
+  const float fst = sqrtf(fmaxf(0.f, 1.f - Ri / 0.33f));
+  const float sS = sqrtf(fmaxf(S2, 0.f));
+  const float lh = U.turb.x * dx, lv = 0.18f * dz;
+  const float dtc = fmaxf(U.step.x, 0.1f);
+  F.aux[0][o] = fminf(lh * lh * sS * fst, 0.08f * dx * dx / dtc);
+  F.aux[1][o] = fminf(lv * lv * sS * fst, 0.15f * dz * dz / dtc);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// advection of the winds and theta (model.js:391-481)
+// ---------------------------------------------------------------------------------------------------------------
+struct Loc {
+  float vu[3], vv[3], vw[3], vc[3];
+};
+__device__ __forceinline__ Loc localVel(const Fields& F, const Grid& g, int par, int i, int j, int k) {
+  const float* __restrict__ u = F.V[par][0];
+  const float* __restrict__ v = F.V[par][1];
+  const float* __restrict__ w = F.V[par][2];
+  auto L = [&](const float* f, int a, int b, int c) { return __ldg(f + g.at(clampi(a, 0, g.nx), clampi(b, 0, g.ny), clampi(c, 0, g.nz))); };
+  Loc o;
+  const float pu = L(u, i, j, k), pv = L(v, i, j, k), pw = L(w, i, j, k);
+  const float xpu = L(u, i + 1, j, k), ypv = L(v, i, j + 1, k), zpw = L(w, i, j, k + 1);
+  o.vu[0] = pu;
+  o.vu[1] = 0.25f * (L(v, i - 1, j, k) + pv + L(v, i - 1, j + 1, k) + ypv);
+  o.vu[2] = 0.25f * (L(w, i - 1, j, k) + pw + L(w, i - 1, j, k + 1) + zpw);
+  o.vv[0] = 0.25f * (L(u, i, j - 1, k) + pu + L(u, i + 1, j - 1, k) + xpu);
+  o.vv[1] = pv;
+  o.vv[2] = 0.25f * (L(w, i, j - 1, k) + pw + L(w, i, j - 1, k + 1) + zpw);
+  o.vw[0] = 0.25f * (L(u, i, j, k - 1) + pu + L(u, i + 1, j, k - 1) + xpu);
+  o.vw[1] = 0.25f * (L(v, i, j, k - 1) + pv + L(v, i, j + 1, k - 1) + ypv);
+  o.vw[2] = pw;
+  o.vc[0] = 0.5f * (pu + xpu);
+  o.vc[1] = 0.5f * (pv + ypv);
+  o.vc[2] = 0.5f * (pw + zpw);
+  return o;
+}
+// departure (s = 1) or forward (s = -1) point, first-order trace clamped to the box (model.js:428-432)
+__device__ __forceinline__ void traceV(const Grid& g, const float k[3], float px, float py, float pz, const float v[3], float s,
+                                       float& x, float& y, float& z) {
+  x = clampf(px - s * k[0] * v[0], 0.f, float(g.nx));
+  y = clampf(py - s * k[1] * v[1], 0.f, float(g.ny));
+  z = clampf(pz - s * k[2] * v[2], 0.f, float(g.nz));
+}
+// channel sample at a point in grid units (texel offsets of u, v, w, theta: model.js:419-422)
+__device__ __forceinline__ float sampleVch(const float* f, const Grid& g, int ch, float x, float y, float z) {
+  const float ox = ch == 0 ? 0.f : 0.5f, oy = ch == 1 ? 0.f : 0.5f, oz = ch == 2 ? 0.f : 0.5f;
+  return trilerp(f, g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz);
+}
+
+__global__ void k_advv1(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const Loc L = localVel(F, g, par, ci, cj, ck);
+  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float fi = float(ci), fj = float(cj), fk = float(ck);
+  const int o = g.at(ci, cj, ck);
+  float x, y, z;
+  traceV(g, kk, fi, fj + 0.5f, fk + 0.5f, L.vu, 1.f, x, y, z);
+  F.Vt[0][o] = sampleVch(F.V[par][0], g, 0, x, y, z);
+  traceV(g, kk, fi + 0.5f, fj, fk + 0.5f, L.vv, 1.f, x, y, z);
+  F.Vt[1][o] = sampleVch(F.V[par][1], g, 1, x, y, z);
+  traceV(g, kk, fi + 0.5f, fj + 0.5f, fk, L.vw, 1.f, x, y, z);
+  F.Vt[2][o] = sampleVch(F.V[par][2], g, 2, x, y, z);
+  traceV(g, kk, fi + 0.5f, fj + 0.5f, fk + 0.5f, L.vc, 1.f, x, y, z);
+  F.Vt[3][o] = sampleVch(F.V[par][3], g, 3, x, y, z);
+}
+
+__device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Grid& g, float x, float y, float z, float ox, float oy, float oz) {
+  const int i0 = int(floorf(x - ox)), j0 = int(floorf(y - oy)), k0 = int(floorf(z - oz));
+  float lo = 1e30f, hi = -1e30f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const float s = __ldg(f + g.at(clampi(i0 + (q & 1), 0, g.nx), clampi(j0 + ((q >> 1) & 1), 0, g.ny), clampi(k0 + (q >> 2), 0, g.nz)));
+    lo = fminf(lo, s);
+    hi = fmaxf(hi, s);
+  }
+  return make_float2(lo, hi);
+}
+
+__global__ void k_advv2(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const Loc L = localVel(F, g, par, ci, cj, ck);
+  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float fi = float(ci), fj = float(cj), fk = float(ck);
+  const float P[4][3] = {{fi, fj + 0.5f, fk + 0.5f}, {fi + 0.5f, fj, fk + 0.5f}, {fi + 0.5f, fj + 0.5f, fk}, {fi + 0.5f, fj + 0.5f, fk + 0.5f}};
+  const float* vel[4] = {L.vu, L.vv, L.vw, L.vc};
+  const float cx = L.vc[0] * kk[0], cy = L.vc[1] * kk[1], cz = L.vc[2] * kk[2];
+  const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
+  const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
+  const int o = g.at(ci, cj, ck);
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float ox = c == 0 ? 0.f : 0.5f, oy = c == 1 ? 0.f : 0.5f, oz = c == 2 ? 0.f : 0.5f;
+    float x, y, z;
+    traceV(g, kk, P[c][0], P[c][1], P[c][2], vel[c], -1.f, x, y, z);
+    const float b = sampleVch(F.Vt[c], g, c, x, y, z);
+    const float hat = __ldg(F.Vt[c] + o), old = __ldg(F.V[par][c] + o);
+    const float r = hat + sm * (old - b);
+    traceV(g, kk, P[c][0], P[c][1], P[c][2], vel[c], 1.f, x, y, z);
+    const float2 m = minmax8V(F.V[par][c], g, x, y, z, ox, oy, oz);
+    F.V[1 - par][c][o] = clampf(r, m.x, m.y);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// scalar advection with fall speeds (model.js:482-576)
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cellVel(const Fields& F, const Grid& g, int par, int i, int j, int k, float v[3]) {
+  const int o = g.at(i, j, k);
+  v[0] = 0.5f * (__ldg(F.V[par][0] + o) + __ldg(F.V[par][0] + o + 1));
+  v[1] = 0.5f * (__ldg(F.V[par][1] + o) + __ldg(F.V[par][1] + o + g.px));
+  v[2] = 0.5f * (__ldg(F.V[par][2] + o) + __ldg(F.V[par][2] + o + g.plane));
+}
+__device__ __forceinline__ void traceQ(const Grid& g, const float k[3], const float p[3], const float v[3], float fall, float s,
+                                       float& x, float& y, float& z) {
+  x = clampf(p[0] - s * k[0] * v[0], 0.5f, float(g.nx) - 0.5f);
+  y = clampf(p[1] - s * k[1] * v[1], 0.5f, float(g.ny) - 0.5f);
+  z = clampf(p[2] - s * k[2] * (v[2] - fall), 0.5f, float(g.nz) - 0.5f);
+}
+__device__ __forceinline__ float sampleQ(const float* f, const Grid& g, float x, float y, float z) {
+  return trilerp(f, g, g.nx, g.ny, g.nz, x - 0.5f, y - 0.5f, z - 0.5f);
+}
+__device__ __forceinline__ float2 minmax8Q(const float* __restrict__ f, const Grid& g, float x, float y, float z) {
+  const int i0 = int(floorf(x - 0.5f)), j0 = int(floorf(y - 0.5f)), k0 = int(floorf(z - 0.5f));
+  float lo = 1e30f, hi = -1e30f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const float s = __ldg(f + g.at(clampi(i0 + (q & 1), 0, g.nx - 1), clampi(j0 + ((q >> 1) & 1), 0, g.ny - 1), clampi(k0 + (q >> 2), 0, g.nz - 1)));
+    lo = fminf(lo, s);
+    hi = fmaxf(hi, s);
+  }
+  return make_float2(lo, hi);
+}
+
+__global__ void k_advq1(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
+  float v[3];
+  cellVel(F, g, par, ci, cj, ck, v);
+  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
+  const int o = g.at(ci, cj, ck);
+  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  const float rho = bsA(F.B, g.nz, ck).z;
+  const float2 fv = fl.vtRain(__ldg(F.Q[0][3] + o), __ldg(F.Q[0][6] + o), rho);
+  const float fs = fl.vtS(__ldg(F.Q[0][4] + o), rho), fg = fl.vtGrau(__ldg(F.Q[0][5] + o), rho);
+  float x, y, z;
+  traceQ(g, kk, p, v, 0.f, 1.f, x, y, z);
+  F.Qt[0][o] = sampleQ(F.Q[0][0], g, x, y, z);
+  F.Qt[1][o] = sampleQ(F.Q[0][1], g, x, y, z);
+  F.Qt[2][o] = sampleQ(F.Q[0][2], g, x, y, z);
+  F.Qt[7][o] = sampleQ(F.Q[0][7], g, x, y, z);
+  const float nr0 = sampleQ(F.Q[0][6], g, x, y, z);
+  traceQ(g, kk, p, v, fv.x, 1.f, x, y, z);
+  F.Qt[3][o] = sampleQ(F.Q[0][3], g, x, y, z);
+  traceQ(g, kk, p, v, fs, 1.f, x, y, z);
+  F.Qt[4][o] = sampleQ(F.Q[0][4], g, x, y, z);
+  traceQ(g, kk, p, v, fg, 1.f, x, y, z);
+  F.Qt[5][o] = sampleQ(F.Q[0][5], g, x, y, z);
+  if (fl.thm) {
+    traceQ(g, kk, p, v, fv.y, 1.f, x, y, z);
+    F.Qt[6][o] = sampleQ(F.Q[0][6], g, x, y, z);
+  } else {
+    F.Qt[6][o] = nr0;
+  }
+}
+
+__global__ void k_advq2(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
+  float v[3];
+  cellVel(F, g, par, ci, cj, ck, v);
+  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
+  const int o = g.at(ci, cj, ck);
+  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  const float rho = bsA(F.B, g.nz, ck).z;
+  float q[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) q[c] = __ldg(F.Q[0][c] + o);
+  const float2 fv = fl.vtRain(q[3], q[6], rho);
+  const float fs = fl.vtS(q[4], rho), fg = fl.vtGrau(q[5], rho);
+  const float fn = fl.thm ? fv.y : 0.f;
+  const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
+  const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
+  const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
+  // per channel: the fall speed of its trace (qv, qc, qi, qr, qs, qg, Nr, spare)
+  const float fall[8] = {0.f, 0.f, 0.f, fv.x, fs, fg, fn, 0.f};
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    float x, y, z;
+    traceQ(g, kk, p, v, fall[c], -1.f, x, y, z);
+    const float b = sampleQ(F.Qt[c], g, x, y, z);
+    const float r = __ldg(F.Qt[c] + o) + sm * (q[c] - b);
+    traceQ(g, kk, p, v, fall[c], 1.f, x, y, z);
+    const float2 m = minmax8Q(F.Q[0][c], g, x, y, z);
+    F.Q[1][c][o] = fmaxf(clampf(r, m.x, m.y), 0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_PHYS (model.js:578-907): forcing stencils + microphysics, outbreak mode
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float spongeLat(const Uni& U, const Grid& g, float xmx, float xmy) {
+  const float Lx = float(g.nx) * U.dims.w, Ly = float(g.ny) * U.dims.w;
+  const float e = fminf(fminf(xmx, Lx - xmx), fminf(xmy, Ly - xmy));
+  const float d = clampf(1.f - e / U.sponge.x, 0.f, 1.f);
+  return d * (0.3f + 0.7f * d) / U.sponge.y;
+}
+__device__ __forceinline__ float spongeTop(const Uni& U, const Grid& g, float z) {
+  const float ztop = float(g.nz) * U.dzv.x;
+  if (z < U.sponge.z) return 0.f;
+  const float s = sinf(1.5707963f * (z - U.sponge.z) / (ztop - U.sponge.z));
+  return s * s / U.sponge.w;
+}
+__device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
+  const int kk = clampi(k, 0, nz - 1);
+  if (ch == 0) return bsB(B, nz, kk).z;
+  if (ch == 1) return bsB(B, nz, kk).w;
+  if (ch == 3) return bsA(B, nz, kk).x;
+  return 0.f;
+}
+
+__global__ void k_phys(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const float* __restrict__ Vin[4] = {F.V[1 - par][0], F.V[1 - par][1], F.V[1 - par][2], F.V[1 - par][3]};
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  auto L = [&](int ch, int a, int b, int c) { return __ldg(Vin[ch] + g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz))); };
+  auto LQ = [&](int ch, int a, int b, int c) { return __ldg(F.Q[1][ch] + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
+  auto LA = [&](int ch, int a, int b, int c) { return __ldg(F.aux[ch] + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
+  auto LP = [&](int a, int b, int c) { return __ldg(F.phT + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
+  const float dx = U.dims.w, dz = U.dzv.x, dt = U.step.x;
+  const int o = g.at(ci, cj, ck);
+  float V[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) V[c] = __ldg(Vin[c] + o);
+  float out[4] = {V[0], V[1], V[2], V[3]};
+  const float ix2 = 1.f / (dx * dx), iz2 = 1.f / (dz * dz);
+  const float fc = U.cor.x, nudR = 1.f / U.cor.y;
+  auto lapH = [&](int ch, float me) { return L(ch, ci + 1, cj, ck) + L(ch, ci - 1, cj, ck) + L(ch, ci, cj + 1, ck) + L(ch, ci, cj - 1, ck) - 4.f * me; };
+  auto lapZp = [&](int ch, float me, bool lo, bool hi) {
+    const float m0 = me - bsV(F.B, nz, ck, ch);
+    const float a = lo ? m0 : L(ch, ci, cj, ck - 1) - bsV(F.B, nz, ck - 1, ch);
+    const float b = hi ? m0 : L(ch, ci, cj, ck + 1) - bsV(F.B, nz, ck + 1, ch);
+    return a + b - 2.f * m0;
+  };
+  // u
+  if (cj < ny && ck < nz) {
+    const float xmx = float(ci) * dx, xmy = (float(cj) + 0.5f) * dx, z = (float(ck) + 0.5f) * dz;
+    const float nux = 0.5f * (LA(0, ci - 1, cj, ck) + LA(0, ci, cj, ck)) + U.turb.y;
+    const float nuy = 0.5f * (LA(1, ci - 1, cj, ck) + LA(1, ci, cj, ck)) + U.turb.y;
+    float du = nux * lapH(0, V[0]) * ix2 + nuy * lapZp(0, V[0], ck == 0, ck == nz - 1) * iz2;
+    const float ut = tgtU(F, g, dz, ci, cj, ck);
+    const float vbar = 0.25f * (L(1, ci - 1, cj, ck) + V[1] + L(1, ci - 1, cj + 1, ck) + L(1, ci, cj + 1, ck));
+    const float vtb = 0.5f * (tgtV(F, g, dz, ci - 1, cj, ck) + tgtV(F, g, dz, ci, cj + 1, ck));
+    const float nw = 0.5f * (l2d(F.lsfB, g, ci - 1, cj).w + l2d(F.lsfB, g, ci, cj).w);
+    du += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (ut - V[0]);
+    du += fc * (vbar - vtb);
+    if (ci > 0 && ci < nx) du -= (LP(ci, cj, ck) - LP(ci - 1, cj, ck)) / dx;
+    if (ck == 0 && U.turb.w > 0.5f) {
+      const float cd = U.micro.w;
+      du += cd * (-sqrtf(V[0] * V[0] + vbar * vbar) * V[0] + sqrtf(ut * ut + vtb * vtb) * ut) / dz;
+    }
+    out[0] = V[0] + dt * du;
+  } else out[0] = 0.f;
+  // v
+  if (ci < nx && ck < nz) {
+    const float xmx = (float(ci) + 0.5f) * dx, xmy = float(cj) * dx, z = (float(ck) + 0.5f) * dz;
+    const float nux = 0.5f * (LA(0, ci, cj - 1, ck) + LA(0, ci, cj, ck)) + U.turb.y;
+    const float nuy = 0.5f * (LA(1, ci, cj - 1, ck) + LA(1, ci, cj, ck)) + U.turb.y;
+    float dv = nux * lapH(1, V[1]) * ix2 + nuy * lapZp(1, V[1], ck == 0, ck == nz - 1) * iz2;
+    const float vt = tgtV(F, g, dz, ci, cj, ck);
+    const float ubar = 0.25f * (L(0, ci, cj - 1, ck) + V[0] + L(0, ci + 1, cj - 1, ck) + L(0, ci + 1, cj, ck));
+    const float utb = 0.5f * (tgtU(F, g, dz, ci, cj - 1, ck) + tgtU(F, g, dz, ci + 1, cj, ck));
+    const float nw = 0.5f * (l2d(F.lsfB, g, ci, cj - 1).w + l2d(F.lsfB, g, ci, cj).w);
+    dv += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (vt - V[1]);
+    dv -= fc * (ubar - utb);
+    if (cj > 0 && cj < ny) dv -= (LP(ci, cj, ck) - LP(ci, cj - 1, ck)) / dx;
+    if (ck == 0 && U.turb.w > 0.5f) {
+      const float cd = U.micro.w;
+      dv += cd * (-sqrtf(ubar * ubar + V[1] * V[1]) * V[1] + sqrtf(utb * utb + vt * vt) * vt) / dz;
+    }
+    out[1] = V[1] + dt * dv;
+  } else out[1] = 0.f;
+  // w
+  if (ci < nx && cj < ny && ck > 0 && ck < nz) {
+    const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx, z = float(ck) * dz;
+    const float nux = 0.5f * (LA(0, ci, cj, ck - 1) + LA(0, ci, cj, ck)) + U.turb.y;
+    const float nuy = 0.5f * (LA(1, ci, cj, ck - 1) + LA(1, ci, cj, ck)) + U.turb.y;
+    float dw = nux * lapH(2, V[2]) * ix2 + nuy * (L(2, ci, cj, ck - 1) + L(2, ci, cj, ck + 1) - 2.f * V[2]) * iz2;
+    auto buoy = [&](int kk) {
+      const float4 A = bsA(F.B, nz, kk);
+      const int q = g.at(ci, cj, kk);
+      return 9.81f * ((__ldg(Vin[3] + q) - A.x) / A.x + 0.608f * (__ldg(F.Q[1][0] + q) - A.y) -
+                      (__ldg(F.Q[1][1] + q) + __ldg(F.Q[1][2] + q) + __ldg(F.Q[1][3] + q) + __ldg(F.Q[1][4] + q) + __ldg(F.Q[1][5] + q)));
+    };
+    dw += 0.5f * (buoy(ck - 1) + buoy(ck)) - (LP(ci, cj, ck) - LP(ci, cj, ck - 1)) / dz;
+    dw += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z)) * (0.f - V[2]);
+    const float4 civ = __ldg(F.ciMap + cj * nx + ci);
+    if (civ.x > 0.f) {
+      const float zz = fabsf(z - civ.z) / civ.w;
+      if (zz < 1.f) {
+        const float cv = cosf(1.5707963f * zz);
+        dw += U.misc.w * civ.x * cv * fmaxf(civ.y * cv - V[2], 0.f);
+      }
+    }
+    out[2] = V[2] + dt * dw;
+  } else out[2] = 0.f;
+  // theta + microphysics at cell centres
+  if (ci < nx && cj < ny && ck < nz) {
+    const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx, z = (float(ck) + 0.5f) * dz;
+    const float4 A = bsA(F.B, nz, ck), Bb = bsB(F.B, nz, ck);
+    const float4 LAv = l2d(F.lsfA, g, ci, cj);
+    const float nw = l2d(F.lsfB, g, ci, cj).w;
+    const float tth = tgtTh(F.B, g, dz, LAv, ck), tqv = tgtQv(F.B, g, dz, LAv, ck);
+    const float sl = spongeLat(U, g, xmx, xmy);
+    const float relax = sl + nw * nudR;
+    const float nux = LA(0, ci, cj, ck) * 3.f + U.turb.y, nuy = LA(1, ci, cj, ck) * 3.f + U.turb.y;
+    float th = V[3] + dt * (nux * lapH(3, V[3]) * ix2 + nuy * lapZp(3, V[3], ck == 0, ck == nz - 1) * iz2 + (relax + spongeTop(U, g, z)) * (tth - V[3]));
+    float q1[4], q2[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      q1[c] = __ldg(F.Q[1][c] + o);
+      q2[c] = __ldg(F.Q[1][4 + c] + o);
+    }
+    float l1[3], l1z[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      l1[c] = LQ(c, ci + 1, cj, ck) + LQ(c, ci - 1, cj, ck) + LQ(c, ci, cj + 1, ck) + LQ(c, ci, cj - 1, ck) - 4.f * q1[c];
+      l1z[c] = (ck == 0 ? q1[c] : LQ(c, ci, cj, ck - 1)) + (ck == nz - 1 ? q1[c] : LQ(c, ci, cj, ck + 1)) - 2.f * q1[c];
+    }
+    const float qvb = (ck == 0 ? A.y : bsA(F.B, nz, ck - 1).y) + (ck == nz - 1 ? A.y : bsA(F.B, nz, ck + 1).y) - 2.f * A.y;
+    l1z[0] -= qvb;
+#pragma unroll
+    for (int c = 0; c < 3; c++) q1[c] = q1[c] + dt * (nux * l1[c] * ix2 + nuy * l1z[c] * iz2);
+    q1[0] += dt * relax * (tqv - q1[0]);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      q1[c] = fmaxf(q1[c], 0.f);
+      q2[c] = fmaxf(q2[c], 0.f);
+    }
+    const float pi0 = Bb.x, p0 = Bb.y, rho = A.z;
+    float T = th * pi0;
+    float qv = q1[0], qc = q1[1], qi = q1[2], qr = q1[3], qs = q2[0], qg = q2[1];
+    const bool thm = U.micro2.z > 0.5f;
+    float nr = fmaxf(q2[2], 0.f);
+    const float rq = 1000.f * rho;
+    const float rs = sqrtf(U.step.z / rho);
+    // warm rain (model.js:791-799)
+    const float pauto = U.micro.x * fmaxf(qc - U.micro.y, 0.f);
+    float accr = 2.2f * qc * powf(qr, 0.875f);
+    if (thm && qr > 1e-9f) {
+      const float l = Fall::lamR(qr, nr);
+      accr = 3100.f * rho * nr * powf(l, -2.8f) * qc * rs;
+    }
+    const float da = fminf(pauto * dt, qc);
+    const float dc = fminf(accr * dt, qc - da);
+    qc -= da + dc;
+    qr += da + dc;
+    nr += da / 2.68e-10f;
+    const float dTc = T - T0K;
+    if (dTc < 0.f) {  // ice-phase conversions (model.js:801-829)
+      const float psaut = 1e-3f * expf(0.025f * dTc) * fmaxf(qi - 6e-4f, 0.f);
+      const float psacw = 5.4e-3f * qc * powf(fmaxf(rq * qs, 0.f), 0.81f) * rs;
+      const float psaci = 5.4e-3f * qi * powf(fmaxf(rq * qs, 0.f), 0.81f) * expf(0.025f * dTc) * rs;
+      const float ewet = 1.f / (1.f + qg / 0.008f);
+      const float pgq = powf(fmaxf(rq * qg, 0.f), 0.875f);
+      const float pgacw = 3.1e-3f * qc * pgq * rs * ewet;
+      const float pgaci = 3.0e-4f * qi * pgq * rs;
+      const float pgacr = 3.1e-3f * qr * pgq * rs * ewet;
+      const float pgfr = fminf(2e-4f * U.micro.z * (expf(0.66f * fminf(-dTc, 20.f)) - 1.f), 0.08f) * qr;
+      const float pgaut = 1e-3f * expf(0.09f * dTc) * fmaxf(qs - 6e-4f, 0.f) * (thm ? 0.25f : 1.f);
+      const float a1 = fminf((psaut + psaci + pgaci) * dt, qi);
+      const float fs1 = (psaut + psaci) / fmaxf(psaut + psaci + pgaci, 1e-20f);
+      qi -= a1;
+      qs += a1 * fs1;
+      qg += a1 * (1.f - fs1);
+      const float a2 = fminf((psacw + pgacw) * dt, qc);
+      const float fs2 = psacw / fmaxf(psacw + pgacw, 1e-20f);
+      const float rimeS = thm ? 0.95f : 0.7f;
+      qc -= a2;
+      qs += a2 * fs2 * rimeS;
+      qg += a2 * (1.f - fs2 * rimeS);
+      float a3 = fminf((pgacr + pgfr) * dt, qr);
+      if (T < 235.f) a3 = qr;
+      if (qr > 1e-12f) nr *= (qr - a3) / qr;
+      qr -= a3;
+      qg += a3;
+      const float a4 = fminf(pgaut * dt, qs);
+      qs -= a4;
+      qg += a4;
+      T += float(LFCd / CPDd) * (a2 + a3);
+    } else {  // melting (model.js:830-848)
+      const float m1 = fminf(0.012f * dTc * qs * dt, qs);
+      float m2 = fminf(0.0022f * dTc * qg * dt, qg);
+      if (thm) {
+        if (qg > 1e-9f) {
+          const float l = Fall::lamG(qg, rho), n0 = Fall::n0G(qg, rho);
+          const float vent = 0.78f / (l * l) + float(0.31 * 0.843 * 1.89 * 5430.0) * powf(U.step.z / rho, 0.25f) * powf(l, -2.945f);
+          const float heat = 2.4e-2f * dTc - float(LVCd * 2.26e-5) * rho * (qvsat(T0K, p0, 0.f) - qv);
+          m2 = clampf(6.2832f / (rho * float(LFCd)) * heat * n0 * vent * dt, 0.f, qg);
+          nr += m2 / qg * n0 / (rho * l);
+        }
+        if (qs > 1e-9f) {
+          const float ls = powf(float(3.14159 * 100.0 * 2e6) / (rho * qs), 0.25f);
+          nr += m1 / qs * 2e6f / (rho * ls);
+        }
+      }
+      qs -= m1;
+      qg -= m2;
+      qr += m1 + m2;
+      T -= float(LFCd / CPDd) * (m1 + m2);
+    }
+    // rain evaporation (model.js:850-872)
+    const float qvsl = qvsat(T, p0, 0.f);
+    if (qr > 0.f && qv < qvsl) {
+      const float rc = 0.001f * rho * qr;
+      const float ern = ((1.6f + 124.9f * powf(rc, 0.2046f)) * powf(rc, 0.525f) / (2.55e8f / (p0 * qvsl) + 5.4e5f)) *
+                        ((qvsl - qv) / (0.001f * rho * qvsl));
+      const float srt = U.micro2.y > 0.f ? sqrtf(rc / (rc + 0.001f * rho * U.micro2.y)) : 1.f;
+      float e = ern * srt * dt * U.turb.z;
+      if (thm) {
+        const float l = Fall::lamR(qr, nr), n0 = rho * nr * l;
+        const float Ap = float(LVCd * LVCd) / (float(2.4e-2 * RVCd) * T * T);
+        const float Bp = 1.f / (rho * qvsl * 2.26e-5f);
+        const float vent = 0.78f / (l * l) + float(0.31 * 0.843 * 1.827 * 7492.0) * powf(U.step.z / rho, 0.25f) * powf(l, -2.9f);
+        e = 6.2832f * (1.f - qv / qvsl) * n0 * vent / (rho * (Ap + Bp)) * dt * U.micro2.w;
+      }
+      e = clampf(e, 0.f, fminf(qr, qvsl - qv));
+      if (thm && qr > 1e-12f) nr *= (qr - e) / qr;
+      qr -= e;
+      qv += e;
+      T -= float(LVCd / CPDd) * e;
+    }
+    // Thompson: self-collection / breakup (model.js:874-884)
+    if (thm) {
+      if (qr > 1e-9f) {
+        const float dm = 1.817f / Fall::lamR(qr, nr);
+        const float fb = clampf(1.f - expf(2300.f * (dm - 1.1e-3f)), -2.f, 1.f);
+        nr *= expf(-7.12f * rho * qr * fb * dt);
+        nr = clampf(nr, qr * 3.183e5f, qr * 3.183e11f);
+      } else nr = 0.f;
+    }
+    // sublimation (model.js:885-892)
+    const float qvsi = qvsat(T, p0, 1.f);
+    if (dTc < 0.f && qv < qvsi) {
+      const float sub = fmaxf(1.f - qv / qvsi, 0.f);
+      float e = fminf((2e-3f * qs + 5e-4f * qg) * sub * dt, (qvsi - qv) * 0.5f);
+      const float fsn = qs / fmaxf(qs + qg, 1e-20f);
+      e = fminf(e, qs + qg);
+      qs -= e * fsn;
+      qg -= e * (1.f - fsn);
+      qv += e;
+      T -= float(LSCd / CPDd) * e;
+    }
+    // mixed-phase saturation adjustment, 3 iterations (model.js:893-905)
+    const float qi0 = qi;
+    float qcl = qc + qi, dsum = 0.f;
+#pragma unroll
+    for (int it = 0; it < 3; it++) {
+      const float f = fIce(T);
+      const float qs_ = qvsat(T, p0, f);
+      const float Lh = mixf(float(LVCd), float(LSCd), f);
+      float d = (qv - qs_) / (1.f + Lh * Lh * qs_ / (float(CPDd * RVCd) * T * T));
+      d = fmaxf(d, -qcl);
+      qv -= d;
+      qcl += d;
+      T += Lh / float(CPDd) * d;
+      dsum += d;
+    }
+    const float f = fIce(T);
+    qi = f * qcl;
+    qc = qcl - qi;
+    T += float(LFCd / CPDd) * (qi - qi0 - f * dsum);
+    th = T / pi0;
+    const float keep = 1.f / (1.f + 2.f * dt * sl);
+    qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
+    F.Q[0][0][o] = fmaxf(qv, 0.f);
+    F.Q[0][1][o] = fmaxf(qc, 0.f);
+    F.Q[0][2][o] = fmaxf(qi, 0.f);
+    F.Q[0][3][o] = fmaxf(qr, 0.f);
+    F.Q[0][4][o] = fmaxf(qs, 0.f);
+    F.Q[0][5][o] = fmaxf(qg, 0.f);
+    F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
+    F.Q[0][7][o] = q2[3];
+    out[3] = th;
+  }
+  const float sp = sqrtf(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
+  if (sp > U.misc.x) {
+    const float s = U.misc.x / sp;
+    out[0] *= s; out[1] *= s; out[2] *= s;
+  }
+  if (!(out[0] == out[0]) || !(out[1] == out[1]) || !(out[2] == out[2]) || !(out[3] == out[3])) {
+    out[0] = bsB(F.B, nz, ck).z; out[1] = bsB(F.B, nz, ck).w; out[2] = 0.f; out[3] = bsA(F.B, nz, ck).x;
+    atomicAdd(F.flags, 1u);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) F.V[par][c][o] = out[c];
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_DIV (model.js:909-925): density-weighted divergence / dt on the padded solve grid
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_div(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
+  const int o = g.at(ci, cj, ck);
+  const float* __restrict__ u = F.V[par][0];
+  const float* __restrict__ v = F.V[par][1];
+  const float* __restrict__ w = F.V[par][2];
+  const float rc = bsA(F.B, g.nz, ck).z;
+  const float wt = ck == g.nz - 1 ? 0.f : __ldg(w + o + g.plane);
+  const float wb = ck == 0 ? 0.f : __ldg(w + o);
+  const float d = rc * (__ldg(u + o + 1) - __ldg(u + o) + __ldg(v + o + g.px) - __ldg(v + o)) / U.dims.w +
+                  (rhoW(F.B, g.nz, ck + 1) * wt - rhoW(F.B, g.nz, ck) * wb) / U.dzv.x;
+  F.rhs[g.pidx(ci, cj, ck)] = d / U.step.x;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_PROJ (model.js:927-946): u -= dt grad(phi), phi from the padded solve
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_proj(Grid g, Uni U, Fields F, int par) {
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  auto P = [&](int a, int b, int c) {
+    return __ldg(F.phi + g.pidx(clampi(a, -g.pad, g.nx + g.pad - 1), clampi(b, -g.pad, g.ny + g.pad - 1), clampi(c, 0, g.nz - 1)));
+  };
+  const int o = g.at(ci, cj, ck);
+  const float kx = U.step.x / U.dims.w, kz = U.step.x / U.dzv.x;
+  const float pc = P(ci, cj, ck);
+  float u = __ldg(F.V[par][0] + o), v = __ldg(F.V[par][1] + o), w = __ldg(F.V[par][2] + o);
+  if (cj < g.ny && ck < g.nz) u = u - kx * (pc - P(ci - 1, cj, ck));
+  if (ci < g.nx && ck < g.nz) v = v - kx * (pc - P(ci, cj - 1, ck));
+  if (ci < g.nx && cj < g.ny && ck > 0 && ck < g.nz) w = w - kz * (pc - P(ci, cj, ck - 1));
+  else w = 0.f;
+  F.V[1 - par][0][o] = u;
+  F.V[1 - par][1][o] = v;
+  F.V[1 - par][2][o] = w;
+  F.V[1 - par][3][o] = __ldg(F.V[par][3] + o);
+}
+
+// accumulated surface precipitation (no counterpart in the reference): rho(0) sum_x q_x vt_x at the lowest level
+__global__ void k_rain(Grid g, Uni U, Fields F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int o = g.at(i, j, 0);
+  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  const float rho = bsA(F.B, g.nz, 0).z;
+  const float qr = F.Q[0][3][o], qs = F.Q[0][4][o], qg = F.Q[0][5][o];
+  const float2 fv = fl.vtRain(qr, F.Q[0][6][o], rho);
+  const double flux = double(rho) * (double(qr) * double(fv.x) + double(qs) * double(fl.vtS(qs, rho)) + double(qg) * double(fl.vtGrau(qg, rho)));
+  F.rain[j * g.nx + i] += flux * double(U.step.x);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// WGSL_M_MAP (model.js:1028-1100): 16 diagnostics per column
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_maps(Grid g, Uni U, Fields F, int par, float4* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const float* const* V = F.V[par];
+  auto L = [&](int ch, int a, int b, int c) { return __ldg(V[ch] + g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz))); };
+  auto cvel = [&](int a, int b, int c, float v[3]) {
+    v[0] = 0.5f * (L(0, a, b, c) + L(0, a + 1, b, c));
+    v[1] = 0.5f * (L(1, a, b, c) + L(1, a, b + 1, c));
+    v[2] = 0.5f * (L(2, a, b, c) + L(2, a, b, c + 1));
+  };
+  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  auto dbz = [&](int k) {
+    const int o = g.at(i, j, k);
+    const float rho = bsA(F.B, nz, k).z;
+    const float T = __ldg(V[3] + o) * bsB(F.B, nz, k).x;
+    const float Zr = fl.zRain(__ldg(F.Q[0][3] + o), __ldg(F.Q[0][6] + o), rho);
+    const float Zs = 9.80e8f * powf(fmaxf(rho * __ldg(F.Q[0][4] + o), 0.f), 1.75f) * 0.224f * 4.f;
+    const float Zg = fl.zGrau(__ldg(F.Q[0][5] + o), rho, T);
+    const float Z = Zr + Zs + Zg;
+    return Z > 1e-3f ? 10.f * logf(Z) / 2.302585f : -30.f;
+  };
+  auto zeta = [&](int k) {
+    float a[3], b[3], c[3], d[3];
+    cvel(i + 1, j, k, a);
+    cvel(i - 1, j, k, b);
+    cvel(i, j + 1, k, c);
+    cvel(i, j - 1, k, d);
+    return (a[1] - b[1] - c[0] + d[0]) / (2.f * U.dims.w);
+  };
+  const float dz = U.dzv.x;
+  float comp = -30.f, wmx = 0.f, uh = 0.f;
+  const int k12 = min(int(12000.f / dz), nz - 1);
+  for (int k = 0; k < k12; k++) {
+    float v[3];
+    cvel(i, j, k, v);
+    wmx = fmaxf(wmx, v[2]);
+    comp = fmaxf(comp, dbz(k));
+    const float z = (float(k) + 0.5f) * dz;
+    if (z > 2000.f && z < 5000.f && v[2] > 0.f) uh += v[2] * fmaxf(zeta(k), 0.f) * dz;
+  }
+  const int k1 = clampi(int(1000.f / dz), 1, nz - 2);
+  float v0[3], v1[3];
+  cvel(i, j, 0, v0);
+  cvel(i, j, k1, v1);
+  const float conv = -((L(0, i + 1, j, 0) - L(0, i, j, 0) + L(1, i, j + 1, 0) - L(1, i, j, 0)) / U.dims.w) * 1000.f;
+  const int idx = j * nx + i, n2 = nx * ny;
+  out[idx] = make_float4(comp, dbz(k1), L(3, i, j, 0) - bsA(F.B, nz, 0).x, zeta(k1));
+  out[idx + n2] = make_float4(wmx, uh, conv, sqrtf(v0[0] * v0[0] + v0[1] * v0[1]));
+  out[idx + 2 * n2] = make_float4(v0[0], v0[1], v1[0], v1[1]);
+  float tr = 1.f, bt = 0.f;
+  for (int k = nz - 1; k >= 0; k--) {
+    const int o = g.at(i, j, k);
+    const float dtau = (80.f * __ldg(F.Q[0][1] + o) + 60.f * __ldg(F.Q[0][2] + o) + 25.f * __ldg(F.Q[0][4] + o) + 4.f * __ldg(F.Q[0][5] + o) +
+                        1.f * __ldg(F.Q[0][3] + o)) * bsA(F.B, nz, k).z * dz;
+    const float a = 1.f - expf(-dtau);
+    bt += tr * a * __ldg(V[3] + o) * bsB(F.B, nz, k).x;
+    tr *= 1.f - a;
+    if (tr < 1e-3f) break;
+  }
+  const float sst = F.sfc[idx].y;
+  bt += tr * (sst > 200.f ? sst : L(3, i, j, 0) * bsB(F.B, nz, 0).x);
+  const float ps = bsA(F.B, nz, 0).z * U.cn.z * __ldg(F.phi + (i + g.pad) + g.nxp * (j + g.pad)) / 100.f;
+  const int k5 = clampi(int(5000.f / dz), 1, nz - 2);
+  out[idx + 3 * n2] = make_float4(ps, bt, U.hur2.w * sqrtf(v0[0] * v0[0] + v0[1] * v0[1]), zeta(k5));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// layout conversion between the texel float4 layout of the C ABI and the device SoA layout
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_pack(Grid g, Ptr8 src, int nch, int X, int Y, int Z, float* dst) {
+  OB_TEXEL_LOOP_BEGIN(X - 1, Y - 1, Z - 1)
+  const int o = g.at(ci, cj, ck);
+  const size_t t = (size_t(ck) * Y + cj) * X + ci;
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    if (c < nch) dst[t * nch + c] = src.p[c][o];
+}
+__global__ void k_unpack(Grid g, Ptr8 dst, int nch, int X, int Y, int Z, const float* src) {
+  OB_TEXEL_LOOP_BEGIN(X - 1, Y - 1, Z - 1)
+  const int o = g.at(ci, cj, ck);
+  const size_t t = (size_t(ck) * Y + cj) * X + ci;
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    if (c < nch) dst.p[c][o] = src[t * nch + c];
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------------------------------
+static inline dim3 grid3(int X, int Y, int Z, dim3 b) { return dim3((X + b.x - 1) / b.x, (Y + b.y - 1) / b.y, Z); }
+static const dim3 kB3(32, 4, 1);
+static const dim3 kB2(32, 8, 1);
+
+void launch_lsf(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
+  k_lsf<<<grid3(g.nx, g.ny, 1, kB2), kB2, 0, s>>>(g, U, F);
+}
+void launch_ci(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
+  k_ci<<<grid3(g.nx, g.ny, 1, kB2), kB2, 0, s>>>(g, U, F);
+}
+void launch_init(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
+  k_init<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F);
+}
+void launch_nut(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_nut<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_advv(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_advv1<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+  k_advv2<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_advq1<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+  k_advq2<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_phys<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_div<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_proj<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
+  k_rain<<<grid3(g.nx, g.ny, 1, kB2), kB2, 0, s>>>(g, U, F);
+}
+void launch_maps(const Grid& g, const Uni& U, const Fields& F, int par, float4* out, cudaStream_t s) {
+  k_maps<<<grid3(g.nx, g.ny, 1, kB2), kB2, 0, s>>>(g, U, F, par, out);
+}
+void launch_pack(const Grid& g, const Ptr8& src, int nch, int X, int Y, int Z, float* dst, cudaStream_t s) {
+  k_pack<<<grid3(X, Y, Z, kB3), kB3, 0, s>>>(g, src, nch, X, Y, Z, dst);
+}
+void launch_unpack(const Grid& g, const Ptr8& dst, int nch, int X, int Y, int Z, const float* src, cudaStream_t s) {
+  k_unpack<<<grid3(X, Y, Z, kB3), kB3, 0, s>>>(g, dst, nch, X, Y, Z, src);
+}
+
+}  // namespace ob
