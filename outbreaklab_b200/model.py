@@ -98,7 +98,9 @@ class RegionalModel:
         return self.analysis
 
     def set_base_state(self, B):
-        B = np.ascontiguousarray(B, np.float32)
+        B = np.ascontiguousarray(B, np.float32).reshape(-1)
+        if B.size != (self.nz + 1) * 8:
+            raise N.ObError(N.OB_ERR_INVALID, "base state: %d values, expected (nz+1)*8 = %d" % (B.size, (self.nz + 1) * 8))
         N.check(N.lib().ob_model_set_base_state(self.h, N.fptr(B), self.nz))
         self.rho_sfc = float(B[2])
 

@@ -197,3 +197,34 @@ def gaussian_rhs(nx, ny, nz, dx, corr_len=5000.0, seed=3, dtype=np.float64):
     f -= f.mean(axis=(1, 2), keepdims=True)
     f /= max(np.abs(f).max(), 1e-30)
     return f.astype(dtype)
+
+
+def hydrometeor_blob(case: StormCase, B, seed=5, thompson=False):
+    """Seeded cloud / rain / ice / snow / graupel blobs and a supersaturated core (Q1, Q2 texel arrays, float32), so
+    that one step exercises every microphysics process of both schemes: warm rain, riming, freezing, melting,
+    evaporation, sublimation, the saturation adjustment and (Thompson) the rain-number budget."""
+    nx, ny, nz, dx, dz = case.nx, case.ny, case.nz, case.dx, case.dz
+    rng = np.random.default_rng(seed)
+    z = (np.arange(nz) + 0.5) * dz
+    y = (np.arange(ny) + 0.5) * dx
+    x = (np.arange(nx) + 0.5) * dx
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    xc, yc = nx * dx / 2, ny * dx / 2
+    r = np.sqrt(((X - xc) / (nx * dx / 4)) ** 2 + ((Y - yc) / (ny * dx / 4)) ** 2)
+    blob = np.clip(1 - r, 0, 1) * (0.6 + 0.4 * rng.random((nz, ny, nx)))
+    Bz = B.reshape(-1, 8)[:nz]
+    qv0 = Bz[:, 1][:, None, None]
+    T = Bz[:, 0][:, None, None] * Bz[:, 4][:, None, None]
+    cold = (T < 268.0).astype(np.float64)
+    warm = (T > 276.0).astype(np.float64)
+    q1 = np.zeros((nz, ny, nx, 4))
+    q2 = np.zeros((nz, ny, nx, 4))
+    q1[..., 0] = qv0 * (1 + 0.08 * blob)                          # supersaturated core
+    q1[..., 1] = 1.5e-3 * blob * (Z < 9000)                        # cloud water
+    q1[..., 2] = 8e-4 * blob * cold                                # cloud ice
+    q1[..., 3] = 3e-3 * blob * (Z < 7000) + 2e-5 * (1 - blob)      # rain (light rain outside: evaporation)
+    q2[..., 0] = 1.2e-3 * blob * (Z > 4000)                        # snow (melts below the freezing level)
+    q2[..., 1] = 4e-3 * blob * (Z > 2000) + 1e-5 * warm * (1 - blob)  # graupel
+    if thompson:
+        q2[..., 2] = q1[..., 3] * 10 ** (5 + 2 * rng.random((nz, ny, nx)))  # rain number per kg
+    return q1.astype(np.float32).reshape(-1), q2.astype(np.float32).reshape(-1)
