@@ -130,6 +130,22 @@ int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi);
 /* the same on device pointers, on the given stream (cudaStream_t, may be NULL) */
 int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream);
 
+/* ---- the pressure solve for callers that cannot allocate device memory ----
+ * No counterpart in the reference. For a host that may not call cudaMalloc (work recorded into a CUDA graph while
+ * the capture is live, or a plugin living inside another runtime's fixed GPU memory budget): one fp32 solve of
+ * rhoC lap_h(phi) + d/dz(rhoW dphi/dz) = rhs on nx*ny*nz with every working buffer in a fixed file-scope device array
+ * (about 14 MB, held by each GPU that loads the library until the process exits). All pointers are device pointers
+ * owned by the caller: rhoC[nz], rhoW[nz+1], rhs and phi (nx*ny*nz, x fastest); the work is queued on `stream`
+ * (cudaStream_t, NULL = default stream). Sizes beyond the limits below return OB_ERR_INVALID. The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Calls share the one array: two calls whose work overlaps on the GPU (different streams, or different host threads)
+ * race and corrupt each other's results; serialise them on one stream. */
+#define OB_STATIC_POISSON_MAX_SIDE 256
+#define OB_STATIC_POISSON_MAX_NZ 512
+#define OB_STATIC_POISSON_MAX_CELLS (1 << 20)
+int ob_poisson_solve_static(int nx, int ny, int nz, float dx, float dz, const float* d_rhoC, const float* d_rhoW,
+                            const float* d_rhs, float* d_phi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libob_b200.so")
 OB_OK, OB_ERR_OOM, OB_ERR_INVALID, OB_ERR_DEVICE, OB_ERR_TIMEOUT, OB_ERR_NAN = 0, 1, 2, 3, 4, 5
 FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI, FIELD_RAIN = 0, 1, 2, 3, 4, 5
 BOUNDARY_FLOATS, MAX_BOUNDS, CI_FLOATS, MAX_CI = 148, 8, 12, 256
+OB_STATIC_POISSON_MAX_SIDE, OB_STATIC_POISSON_MAX_NZ, OB_STATIC_POISSON_MAX_CELLS = 256, 512, 1 << 20
 
 
 class ObError(RuntimeError):
@@ -65,6 +66,7 @@ SYMBOLS = {
     "ob_poisson_set_density": (_i, [_vp, _fp, _fp]),
     "ob_poisson_solve": (_i, [_vp, _fp, _fp]),
     "ob_poisson_solve_device": (_i, [_vp, _vp, _vp, _vp]),
+    "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
