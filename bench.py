@@ -277,7 +277,9 @@ def run_ours(args, rank, world):
             "cell_steps_per_s": cell_steps,
             "config": {"workload": "640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)",
                        "cells": case.cells, "parallelism": "replicas" if world > 1 else "single domain",
-                       "l2": "state 2.8 GB > 126 MB L2 (no flush needed)", "solver": "fp32"},
+                       "l2": "state 2.8 GB > 126 MB L2 (no flush needed)",
+                       "solver": {0: "fp32 SIMT DST", 1: "bf16x3 tensor-core DST",
+                                  2: "bf16x3 tensor-core DST + 1 refinement sweep"}[m.solver]},
             "pass_ms": {k: round(v, 4) for k, v in pass_ms.items()},
             "step_hbm": {"algorithmic_bytes": step_bytes, "gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac_of_measured_peak": step_bytes / (step_ms / 1000.0) / 1e9 / hbm},

@@ -115,12 +115,18 @@ int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms);
  * (LSF+CI, NUT, ADVV, ADVQ, PHYS, DIV, SOLVE, PROJ+RAIN). Returns the number of passes, or -status. */
 #define OB_NPASS 8
 int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
+/* pressure-solve precision of the model: 0 = fp32 SIMT transforms (the reference's arithmetic), 1 = bf16x3
+ * tensor-core transforms, 2 = bf16x3 + one refinement sweep (the default where nz is 16, 40 or 80).
+ * No counterpart in the reference. */
+int ob_model_set_solver(ObModel* m, int precision);
+int ob_model_solver(ObModel* m);
 /* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
 void* ob_model_stream(ObModel* m);
 
 /* ---- PoissonDirect (solver.js:105-165) ---- */
 /* replaces new PoissonDirect(nx, ny, nz, dx, dz) (solver.js:106-137); precision 0 = FP32 SIMT transforms,
- * 1 = bf16x3 tensor-core transforms (FP32 accumulate) */
+ * 1 = bf16x3 tensor-core transforms (FP32 accumulate), 2 = the same plus one iterative-refinement sweep on the
+ * FP64-accumulated residual (precisions 1 and 2 need nz in {16, 40, 80}) */
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out);
 int ob_poisson_destroy(ObPoisson* p);
 /* replaces setDensity (solver.js:139-146): rhoC[nz] at centres, rhoW[nz+1] at bottom faces */
@@ -129,6 +135,15 @@ int ob_poisson_set_density(ObPoisson* p, const float* rhoC, const float* rhoW);
 int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi);
 /* the same on device pointers, on the given stream (cudaStream_t, may be NULL) */
 int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream);
+/* device time of one solve on the handle's buffers (the last uploaded right-hand side), averaged over reps solves
+ * bracketed by CUDA events; no counterpart in the reference */
+int ob_poisson_time(ObPoisson* p, int reps, float* ms);
+
+/* ---- diagnostics ----
+ * One bf16x3 tensor-core transform as used by the precision-1 solve: C[p] = A * B[p]^T for p < planes, with
+ * A[M][K], B[planes][N][K], C[planes][M][N] fp32 host arrays (K a multiple of 8). No counterpart in the reference
+ * (its transforms are fp32 SIMT GEMMs, solver.js:12-68); it exists to test the tensor-core kernel in isolation. */
+int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* A, const float* B, float* C);
 
 /* ---- the pressure solve for callers that cannot allocate device memory ----
  * No counterpart in the reference. For a host that may not call cudaMalloc (work recorded into a CUDA graph while

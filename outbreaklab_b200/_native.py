@@ -59,6 +59,8 @@ SYMBOLS = {
     "ob_model_budgets": (_i, [_vp, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
     "ob_model_nan_count": (C.c_uint, [_vp]),
     "ob_model_stream": (_vp, [_vp]),
+    "ob_model_set_solver": (_i, [_vp, _i]),
+    "ob_model_solver": (_i, [_vp]),
     "ob_model_timed_steps": (_i, [_vp, _f, _i, _fp]),
     "ob_model_profile_step": (_i, [_vp, _f, _fp, _i]),
     "ob_poisson_create": (_i, [_i, _i, _i, _f, _f, _i, C.POINTER(_vp)]),
@@ -66,6 +68,8 @@ SYMBOLS = {
     "ob_poisson_set_density": (_i, [_vp, _fp, _fp]),
     "ob_poisson_solve": (_i, [_vp, _fp, _fp]),
     "ob_poisson_solve_device": (_i, [_vp, _vp, _vp, _vp]),
+    "ob_poisson_time": (_i, [_vp, _i, _fp]),
+    "ob_dst_tc_selftest": (_i, [_i, _i, _i, _i, _fp, _fp, _fp]),
     "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),
 }
 

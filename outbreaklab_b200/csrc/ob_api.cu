@@ -84,6 +84,7 @@ struct ObModel {
   float4* d_2d = nullptr;
   double* d_red = nullptr;
   float* d_qptr = nullptr;
+  float* rhs32 = nullptr;  // the fp32 right-hand side buffer (F.rhs points here when a solver reads it)
   PoissonPlan solver;
   std::vector<float> Bh;
   double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
@@ -92,10 +93,22 @@ struct ObModel {
   int steps = 0, parity = 0;
 };
 
+// where the divergence pass writes the solve's right-hand side for the current solver precision
+static void model_bind_solver(ObModel* m) {
+  m->F.rhs_hi = m->F.rhs_lo = nullptr;
+  m->F.rhs_ld = 0;
+  m->F.rhs = m->rhs32;
+  if (m->solver.precision >= 1) {
+    m->solver.tc_rhs_split(&m->F.rhs_hi, &m->F.rhs_lo, &m->F.rhs_ld);
+    m->solver.presplit = true;
+    if (m->solver.precision == 1) m->F.rhs = nullptr;  // no fp32 copy needed
+  }
+}
+
 static void model_free(ObModel* m) {
   if (!m) return;
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -195,12 +208,14 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   alloc((void**)&m->d_maps, n2 * 4 * sizeof(float4), "maps");
   alloc((void**)&m->d_2d, n2 * 4 * sizeof(float4), "2-D fields");
   alloc((void**)&m->d_red, 8 * sizeof(double), "reductions");
-  alloc((void**)&m->F.rhs, np * sizeof(float), "rhs");
+  alloc((void**)&m->rhs32, np * sizeof(float), "rhs");
   alloc((void**)&m->F.phi, np * sizeof(float), "phi");
   m->stage_bytes = std::max(size_t(nx + 1) * (ny + 1) * (nz + 1) * 4, np) * sizeof(float);
   alloc((void**)&m->stage, m->stage_bytes, "staging");
   alloc((void**)&m->d_qptr, 8 * sizeof(float*), "pointer table");
-  if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, 0);
+  // the refined bf16x3 tensor-core solve where its tridiagonal kernel is specialised, else fp32
+  const int prec = (nz == 16 || nz == 40 || nz == 80) ? 2 : 0;
+  if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, prec);
   if (rc != OB_OK) {
     if (rc == OB_ERR_OOM) {
       const double gb = (fs * 39.0 * 4 + np * 4.0 * 5 + n2 * 200.0) / 1e9;
@@ -226,6 +241,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->F.sfc = m->d_2d + 3 * n2;
   m->F.B = m->d_B;
   m->F.rain = m->d_rain;
+  model_bind_solver(m);
   m->F.bnd = m->d_bnd;
   m->F.ci = m->d_ci;
   m->F.flags = m->d_flags;
@@ -297,7 +313,7 @@ int ob_model_reset(ObModel* m) {
   launch_init(g, m->U, m->F, m->stream);
   const size_t np = size_t(g.nxp) * g.nyp * g.nz;
   cudaMemsetAsync(m->F.phi, 0, np * sizeof(float), m->stream);
-  cudaMemsetAsync(m->F.rhs, 0, np * sizeof(float), m->stream);
+  cudaMemsetAsync(m->rhs32, 0, np * sizeof(float), m->stream);
   cudaMemsetAsync(m->d_rain, 0, size_t(g.nx) * g.ny * sizeof(double), m->stream);
   cudaMemsetAsync(m->d_flags, 0, 64 * sizeof(unsigned), m->stream);
   m->lsfT = 0;
@@ -336,7 +352,8 @@ int ob_model_step(ObModel* m, float dt, int nsteps) {
 
 int ob_model_sync(ObModel* m) {
   if (!m) { set_error("ob_model_sync: null model"); return OB_ERR_INVALID; }
-  return cuda_status(cudaStreamSynchronize(m->stream), "step");
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "step"));
+  return m->solver.tc_check();
 }
 
 int ob_model_maps(ObModel* m, float* out) {
@@ -484,6 +501,26 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   return rc == OB_OK ? e - 1 : -rc;
 }
 
+int ob_model_set_solver(ObModel* m, int precision) {
+  if (!m || precision < 0 || precision > 2) { set_error("ob_model_set_solver: precision must be 0, 1 or 2"); return OB_ERR_INVALID; }
+  const Grid& g = m->g;
+  if (precision >= 1 && g.nz != 16 && g.nz != 40 && g.nz != 80) {
+    set_error("ob_model_set_solver: the tensor-core solve supports nz in {16, 40, 80}");
+    return OB_ERR_INVALID;
+  }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set solver"));
+  m->solver.destroy();
+  OB_TRY(m->solver.create(g.nxp, g.nyp, g.nz, m->dx, m->dz, precision));
+  std::vector<float> rc(g.nz), rw(g.nz + 1);
+  for (int k = 0; k < g.nz; k++) rc[k] = m->Bh[k * 8 + 2];
+  for (int k = 0; k <= g.nz; k++) rw[k] = m->Bh[k * 8 + 3];
+  OB_TRY(m->solver.set_density(rc.data(), rw.data()));
+  model_bind_solver(m);
+  return OB_OK;
+}
+
+int ob_model_solver(ObModel* m) { return m ? m->solver.precision : -1; }
+
 unsigned ob_model_nan_count(ObModel* m) {
   unsigned h = 0;
   if (m && cudaMemcpy(&h, m->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) h = 0;
@@ -501,7 +538,7 @@ struct ObPoisson {
 };
 
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out) {
-  if (!out || (precision != 0 && precision != 1)) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
+  if (!out || precision < 0 || precision > 2) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
   *out = nullptr;
   ObPoisson* p = new ObPoisson();
   int rc = p->plan.create(nx, ny, nz, dx, dz, precision);
@@ -536,8 +573,28 @@ int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi) {
   OB_TRY(cuda_status(cudaMemcpyAsync(p->d_rhs, rhs, n, cudaMemcpyHostToDevice, p->stream), "poisson upload"));
   OB_TRY(p->plan.solve(p->d_rhs, p->d_phi, p->stream));
   OB_TRY(cuda_status(cudaMemcpyAsync(phi, p->d_phi, n, cudaMemcpyDeviceToHost, p->stream), "poisson download"));
-  return cuda_status(cudaStreamSynchronize(p->stream), "poisson solve");
+  OB_TRY(cuda_status(cudaStreamSynchronize(p->stream), "poisson solve"));
+  return p->plan.tc_check();
 }
+int ob_poisson_time(ObPoisson* p, int reps, float* ms) {
+  if (!p || reps < 1 || !ms) { set_error("ob_poisson_time: bad arguments"); return OB_ERR_INVALID; }
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int rc = p->plan.solve(p->d_rhs, p->d_phi, p->stream);  // warm-up
+  cudaEventRecord(a, p->stream);
+  for (int r = 0; r < reps && rc == OB_OK; r++) rc = p->plan.solve(p->d_rhs, p->d_phi, p->stream);
+  cudaEventRecord(b, p->stream);
+  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "poisson timing");
+  float t = 0.f;
+  if (rc == OB_OK) cudaEventElapsedTime(&t, a, b);
+  *ms = t / reps;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc == OB_OK) rc = p->plan.tc_check();
+  return rc;
+}
+
 int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream) {
   if (!p || !d_rhs || !d_phi) { set_error("ob_poisson_solve_device: null argument"); return OB_ERR_INVALID; }
   return p->plan.solve(d_rhs, d_phi, stream ? (cudaStream_t)stream : p->stream);

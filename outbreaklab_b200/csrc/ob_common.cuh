@@ -11,6 +11,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 
 namespace ob {
 
@@ -43,6 +44,9 @@ struct Fields {
   float4* sfc;
   const float* B;   // base state (nz+1)*8
   float* rhs;       // padded solve grid nxp*nyp*nz
+  __nv_bfloat16* rhs_hi;  // tensor-core solve: the right-hand side split into bf16 hi/lo, row pitch rhs_ld
+  __nv_bfloat16* rhs_lo;
+  int rhs_ld;
   float* phi;
   double* rain;     // nx*ny accumulated surface precipitation
   const float* bnd; // OB_MAX_BOUNDS x 148
@@ -113,6 +117,15 @@ __device__ __forceinline__ float esi(float T) { return 611.2f * expf(21.8745584f
 __device__ __forceinline__ float fIce(float T) { return clampf((T0K - T) / 40.f, 0.f, 1.f); }
 __device__ __forceinline__ float qvsat(float T, float p, float f) {
   float e = mixf(esl(T), esi(T), f);
+  return 0.622f * e / fmaxf(p - e, 100.f);
+}
+// qvsat with one exponential where the ice fraction is exactly 0 or 1: mix(a, b, 0) == a and mix(a, b, 1) == b for
+// finite a, b, so the result is bit-identical to qvsat
+__device__ __forceinline__ float qvsat1(float T, float p, float f) {
+  float e;
+  if (f == 0.f) e = esl(T);
+  else if (f == 1.f) e = esi(T);
+  else e = mixf(esl(T), esi(T), f);
   return 0.622f * e / fmaxf(p - e, 100.f);
 }
 struct Fall {

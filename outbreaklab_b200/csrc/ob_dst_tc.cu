@@ -1,16 +1,578 @@
-// ob_dst_tc.cu — bf16x3 tensor-core sine transforms (tcgen05, TMEM accumulators) for the pressure solve.
+// ob_dst_tc.cu — bf16x3 tensor-core sine transforms for the pressure solve (tcgen05 + TMA + TMEM), sm_100a.
+//
+// Each of the four horizontal transforms of solver.js:155-163 is a batched GEMM C = Q B^T per z-plane, with Q the
+// orthonormal DST-II matrix (M x K, K-major) and B the field (N x K, K-major). fp32 operands are split into bf16
+// pairs (x = hi + lo) and the product is accumulated in fp32 TMEM as  Q_hi B_hi + Q_hi B_lo + Q_lo B_hi  (the lo*lo
+// term, ~2^-16 relative, is dropped): three tcgen05.mma per K step on the same staged tiles.
+//
+// Layouts (x fastest unless stated) chain the transforms so that every GEMM reads K-major tiles by TMA:
+//   rhs split  S_x[k][j][i]   --X-fwd-->  S_y[k][l][j]  --Y-fwd-->  T2[k][m][l] (fp32)
+//   --tridiagonal (transposes through shared memory)-->  S_y[k][l][m]  --Y-inv-->  S_x[k][j][l]  --X-inv-->  phi[k][j][i]
+// Kernel: one 128 x 128 output tile per CTA, 6 warps: warp 0 issues TMA loads into a 3-stage ring (4 tiles of
+// 128 x 64 bf16 per stage, 128-byte swizzle), warp 1 owns TMEM and issues the MMAs from one thread, warps 2-5 drain
+// the accumulator (tcgen05.ld) and write the tile. Every mbarrier wait is bounded (ob_tc.cuh).
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "ob_poisson.cuh"
+#include "ob_tc.cuh"
 
 namespace ob {
 
+namespace {
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3;
+constexpr int TILE_BYTES = BM * BK * 2;  // 16 KB per operand tile (BN == BM)
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int kThreads = 192;
+constexpr uint32_t kTmemCols = 128;
+
+enum OutMode { OUT_ROW_BF16X2 = 0, OUT_ROW_F32 = 1, OUT_COL_F32 = 2, OUT_COL_F32_ADD = 3 };
+
+struct TcOut {
+  __nv_bfloat16* hi;
+  __nv_bfloat16* lo;
+  float* f;
+  long ldo;      // row pitch of the output (elements)
+  int M, N;      // valid rows / columns per plane
+};
+}  // namespace
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_dst_tc(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+             const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, int K, TcOut out,
+             unsigned int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accum = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, plane = blockIdx.z;
+  const int nk = (K + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(accum, 1);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tc::prefetch_tmap(&tA_hi);
+    tc::prefetch_tmap(&tA_lo);
+    tc::prefetch_tmap(&tB_hi);
+    tc::prefetch_tmap(&tB_lo);
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(tmem_slot, kTmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      for (int kt = 0; kt < nk; kt++) {
+        const int s = kt % STAGES;
+        const uint32_t ph = (kt / STAGES) & 1;
+        if (!tc::mbar_wait(&empty[s], ph ^ 1, err, 1u)) break;
+        uint8_t* st = smem + s * STAGE_BYTES;
+        tc::mbar_expect_tx(&full[s], STAGE_BYTES);
+        tc::tma_load_2d(st, &tA_hi, &full[s], kt * BK, m0);
+        tc::tma_load_2d(st + TILE_BYTES, &tA_lo, &full[s], kt * BK, m0);
+        tc::tma_load_3d(st + 2 * TILE_BYTES, &tB_hi, &full[s], kt * BK, n0, plane);
+        tc::tma_load_3d(st + 3 * TILE_BYTES, &tB_lo, &full[s], kt * BK, n0, plane);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+      bool ok = true;
+      for (int kt = 0; kt < nk && ok; kt++) {
+        const int s = kt % STAGES;
+        const uint32_t ph = (kt / STAGES) & 1;
+        if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
+        tc::tc_fence_after();
+        const uint8_t* st = smem + s * STAGE_BYTES;
+        const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
+        const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + TILE_BYTES));
+        const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * TILE_BYTES));
+        const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 3 * TILE_BYTES));
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; kk++) {
+          const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
+          tc::mma_bf16(tmem, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+          tc::mma_bf16(tmem, dah + o, dbl + o, idesc, 1u);
+          tc::mma_bf16(tmem, dal + o, dbh + o, idesc, 1u);
+        }
+        tc::mma_commit(&empty[s]);
+      }
+      tc::mma_commit(accum);  // arrives when every MMA issued above has completed
+      if (!ok) tc::mbar_wait(accum, 0, err, 4u);
+    }
+  } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
+    const int q = warp & 3;
+    const int r = m0 + q * 32 + lane;
+    if (tc::mbar_wait(accum, 0, err, 8u)) {
+      tc::tc_fence_after();
+#pragma unroll 1
+      for (int ch = 0; ch < BN / 32; ch++) {
+        float v[32];
+        tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
+        const int c0 = n0 + ch * 32;
+        if (c0 >= out.N) break;
+        if (MODE == OUT_COL_F32 || MODE == OUT_COL_F32_ADD) {
+          if (r < out.M) {
+            float* dst = out.f + (long(plane) * out.N + c0) * out.ldo + r;
+#pragma unroll
+            for (int t = 0; t < 32; t++)
+              if (c0 + t < out.N) {
+                if (MODE == OUT_COL_F32_ADD) dst[long(t) * out.ldo] += v[t];
+                else dst[long(t) * out.ldo] = v[t];
+              }
+          }
+        } else if (r < out.M) {
+          const long base = (long(plane) * out.M + r) * out.ldo + c0;
+          if (MODE == OUT_ROW_F32) {
+            float* dst = out.f + base;
+#pragma unroll
+            for (int t = 0; t < 32; t++)
+              if (c0 + t < out.N) dst[t] = v[t];
+          } else {
+            __align__(16) __nv_bfloat16 h[32], l[32];
+#pragma unroll
+            for (int t = 0; t < 32; t++) tc::split_bf16(v[t], h[t], l[t]);
+            if (c0 + 32 <= out.ldo) {  // whole 64-byte rows fit in the padded pitch
+              uint4* dh = reinterpret_cast<uint4*>(out.hi + base);
+              uint4* dl = reinterpret_cast<uint4*>(out.lo + base);
+#pragma unroll
+              for (int t = 0; t < 4; t++) {
+                dh[t] = reinterpret_cast<const uint4*>(h)[t];
+                dl[t] = reinterpret_cast<const uint4*>(l)[t];
+              }
+            } else {
+              for (int t = 0; t < 32 && c0 + t < out.ldo; t++) {
+                out.hi[base + t] = h[t];
+                out.lo[base + t] = l[t];
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// fp32 field -> bf16 hi/lo planes with a padded row pitch (rows of `cols` values, pitch ld), zero in the padding
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_split_rows(const float* __restrict__ src, long rows, int cols, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo, int ld) {
+  const long n = rows * ld;
+  for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < n; t += long(gridDim.x) * blockDim.x) {
+    const long r = t / ld;
+    const int c = int(t - r * ld);
+    const float x = c < cols ? src[r * cols + c] : 0.f;
+    tc::split_bf16(x, hi[t], lo[t]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// residual of the solved field, accumulated in FP64: r = rhs - [rho_c lap_h(phi) + lo phi(k-1) + diag phi + up phi(k+1)]
+// with phi = 0 on the faces beyond the grid (antisymmetric ghosts, the operator the sine transforms diagonalise) and
+// Neumann in z (lo = 0 at the ground, up = 0 at the lid); written split for the correction solve
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __restrict__ zop, const float* __restrict__ rhs,
+                        const float* __restrict__ phi, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= nx) return;
+  const long pl = long(nx) * ny;
+  const long o = long(k) * pl + long(j) * nx + i;
+  const double p = phi[o];
+  const double xm = i > 0 ? double(phi[o - 1]) : -p, xp = i < nx - 1 ? double(phi[o + 1]) : -p;
+  const double ym = j > 0 ? double(phi[o - nx]) : -p, yp = j < ny - 1 ? double(phi[o + nx]) : -p;
+  const float4 z = __ldg(zop + k);
+  const double zm = k > 0 ? double(phi[o - pl]) : 0.0, zp = k < nz - 1 ? double(phi[o + pl]) : 0.0;
+  const double Lp = double(z.w) * (xm + xp + ym + yp - 4.0 * p) * idx2 + double(z.x) * zm + double(z.z) * p + double(z.y) * zp;
+  const float r = float(double(rhs[o]) - Lp);
+  const long t = (long(k) * ny + j) * ld + i;
+  tc::split_bf16(r, hi[t], lo[t]);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// tridiagonal solves in z per mode (l, m) (solver.js:70-103): T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi/lo out.
+// Block = 32 modes in l x 8 in m; forward-sweep coefficients and the right-hand side stay in registers; the result
+// goes out through a shared-memory transpose so that the stores run along m. The lowest 2 x 2 modes (near-singular:
+// Neumann in z, shift ~ -(pi/L)^2) use FP64 factors precomputed on the host at set_density.
+// ---------------------------------------------------------------------------------------------------------------
+template <int NZ>
+__global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
+                                                const double* __restrict__ low, const float* __restrict__ T2,
+                                                __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo) {
+  __shared__ float tile[8][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.x * 32 + tx, m = blockIdx.y * 8 + ty;
+  const bool act = l < nxp && m < nyp;
+  const bool lowm = l < 2 && m < 2;
+  const long sxy = long(nxp) * nyp;
+  float x[NZ];
+  if (act && !lowm) {
+    const float shift = __ldg(lam + l) + __ldg(lam + nxp + m);
+    const float* h = T2 + long(m) * nxp + l;
+    float cp[NZ];
+    float cprev = 0.f, dprev = 0.f;
+#pragma unroll
+    for (int k = 0; k < NZ; k++) {
+      const float4 o = __ldg(zop + k);
+      const float den = o.z + shift * o.w - o.x * cprev;
+      cprev = o.y / den;
+      dprev = (__ldg(h + sxy * k) - o.x * dprev) / den;
+      cp[k] = cprev;
+      x[k] = dprev;
+    }
+#pragma unroll
+    for (int k = NZ - 2; k >= 0; k--) x[k] = x[k] - cp[k] * x[k + 1];
+  } else if (act) {
+    // low mode: low[(mode*2 + 0)*NZ + k] = 1/den_k, low[(mode*2 + 1)*NZ + k] = c'_k (FP64, host-factored)
+    const int mode = m * 2 + l;
+    const double* rd = low + (mode * 2) * NZ;
+    const double* cpd = rd + NZ;
+    const float* h = T2 + long(m) * nxp + l;
+    double d[NZ];
+    double dprev = 0.0;
+    for (int k = 0; k < NZ; k++) {
+      const double lo = double(__ldg(zop + k).x);
+      dprev = (double(h[sxy * k]) - lo * dprev) * rd[k];
+      d[k] = dprev;
+    }
+    for (int k = NZ - 2; k >= 0; k--) d[k] = d[k] - cpd[k] * d[k + 1];
+#pragma unroll
+    for (int k = 0; k < NZ; k++) x[k] = float(d[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NZ; k++) x[k] = 0.f;
+  }
+  // transposed store: per level, 32 (l) rows of 8 consecutive m
+  const int lo_l = blockIdx.x * 32 + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NZ; k++) {
+    tile[ty][tx] = x[k];
+    __syncthreads();
+    if (ty == 0 && lo_l < nxp) {
+      __align__(16) __nv_bfloat16 h8[8], l8[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++) tc::split_bf16(tile[t][tx], h8[t], l8[t]);
+      const long o = (long(k) * nxp + lo_l) * ldy + blockIdx.y * 8;
+      *reinterpret_cast<uint4*>(ohi + o) = *reinterpret_cast<const uint4*>(h8);
+      *reinterpret_cast<uint4*>(olo + o) = *reinterpret_cast<const uint4*>(l8);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------------------------
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                    const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode() {
+  static PFN_encodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_encodeTiled>(p);
+  }
+  return fn;
+}
+
+// 2-D [rows][cols] bf16 with pitch ld (elements), box 64 x 128, 128-byte swizzle
+static bool make_map_2d(CUtensorMap* m, void* base, long rows, long cols, long ld) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(ld * 2)};
+  cuuint32_t box[2] = {BK, BM};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// 3-D [planes][rows][cols] bf16 with pitch ld, box 64 x 128 x 1
+static bool make_map_3d(CUtensorMap* m, void* base, long planes, long rows, long cols, long ld) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[3] = {cuuint64_t(cols), cuuint64_t(rows), cuuint64_t(planes)};
+  cuuint64_t strides[2] = {cuuint64_t(ld * 2), cuuint64_t(ld * 2 * rows)};
+  cuuint32_t box[3] = {BK, BN, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static inline long pad8(long n) { return (n + 7) / 8 * 8; }
+
+struct TcPlan {
+  int nx, ny, nz;
+  long ldx, ldy;
+  __nv_bfloat16* mat = nullptr;  // 8 matrices hi/lo: qix, qiy, qy, qx
+  __nv_bfloat16 *sx_hi = nullptr, *sx_lo = nullptr, *sy_hi = nullptr, *sy_lo = nullptr;
+  __nv_bfloat16 *rx_hi = nullptr, *rx_lo = nullptr;  // the right-hand side, split (zero outside what is written)
+  float* t2 = nullptr;
+  double* low = nullptr;  // FP64 factors of the 4 lowest modes
+  unsigned int* err = nullptr;
+  CUtensorMap A[4][2];    // [transform][hi/lo]
+  CUtensorMap Bx[2], By[2], Br[2];
+};
+
+static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
+  hi.assign(size_t(N) * ld, __float2bfloat16_rn(0.f));
+  lo.assign(size_t(N) * ld, __float2bfloat16_rn(0.f));
+  for (int r = 0; r < N; r++)
+    for (int c = 0; c < N; c++) {
+      const float x = src[size_t(r) * N + c];
+      const __nv_bfloat16 h = __float2bfloat16_rn(x);
+      hi[size_t(r) * ld + c] = h;
+      lo[size_t(r) * ld + c] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+}
+
 int PoissonPlan::tc_create() {
-  set_error("poisson: the bf16x3 tensor-core path is not available in this build");
-  return OB_ERR_INVALID;
+  if (!get_encode()) {
+    set_error("poisson: cuTensorMapEncodeTiled is unavailable");
+    return OB_ERR_DEVICE;
+  }
+  TcPlan* T = new TcPlan();
+  tc = T;
+  T->nx = nx; T->ny = ny; T->nz = nz;
+  T->ldx = pad8(nx);
+  T->ldy = pad8(ny);
+  const size_t mx = size_t(nx) * T->ldx, my = size_t(ny) * T->ldy;
+  const size_t nsx = size_t(nz) * ny * T->ldx, nsy = size_t(nz) * nx * T->ldy;
+  auto al = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess && cudaMemset(*p, 0, bytes) == cudaSuccess; };
+  bool ok = al((void**)&T->mat, (4 * mx + 4 * my) * 2) && al((void**)&T->sx_hi, nsx * 2) && al((void**)&T->sx_lo, nsx * 2) &&
+            al((void**)&T->rx_hi, nsx * 2) && al((void**)&T->rx_lo, nsx * 2) &&
+            al((void**)&T->sy_hi, nsy * 2) && al((void**)&T->sy_lo, nsy * 2) && al((void**)&T->t2, size_t(nz) * nx * ny * 4) &&
+            al((void**)&T->low, size_t(8) * nz * 8) && al((void**)&T->err, 16);
+  if (!ok) {
+    set_error("poisson: out of device memory for the tensor-core path");
+    return OB_ERR_OOM;
+  }
+  // DST matrices in hi/lo bf16 (the fp32 matrices of PoissonPlan::create, split)
+  std::vector<float> M(2 * size_t(nx) * nx + 2 * size_t(ny) * ny);
+  cudaMemcpy(M.data(), mats, M.size() * 4, cudaMemcpyDeviceToHost);
+  // order: qix (x fwd), qiy (y fwd), qy (y inv), qx (x inv)
+  const float* src[4] = {M.data() + ofs_qix, M.data() + ofs_qiy, M.data() + ofs_qy, M.data() + ofs_qx};
+  const int dim[4] = {nx, ny, ny, nx};
+  const long ld[4] = {T->ldx, T->ldy, T->ldy, T->ldx};
+  size_t off = 0;
+  __nv_bfloat16* mp[4][2];
+  for (int t = 0; t < 4; t++) {
+    std::vector<__nv_bfloat16> hi, lo;
+    split_host(src[t], dim[t], ld[t], hi, lo);
+    const size_t n = size_t(dim[t]) * ld[t];
+    mp[t][0] = T->mat + off;
+    mp[t][1] = T->mat + off + n;
+    cudaMemcpy(mp[t][0], hi.data(), n * 2, cudaMemcpyHostToDevice);
+    cudaMemcpy(mp[t][1], lo.data(), n * 2, cudaMemcpyHostToDevice);
+    off += 2 * n;
+  }
+  ok = true;
+  for (int t = 0; t < 4; t++)
+    for (int h = 0; h < 2; h++) ok = ok && make_map_2d(&T->A[t][h], mp[t][h], dim[t], dim[t], ld[t]);
+  // B operands: S_x [nz][ny][nx] pitch ldx ; S_y [nz][nx][ny] pitch ldy
+  ok = ok && make_map_3d(&T->Bx[0], T->sx_hi, nz, ny, nx, T->ldx) && make_map_3d(&T->Bx[1], T->sx_lo, nz, ny, nx, T->ldx);
+  ok = ok && make_map_3d(&T->Br[0], T->rx_hi, nz, ny, nx, T->ldx) && make_map_3d(&T->Br[1], T->rx_lo, nz, ny, nx, T->ldx);
+  ok = ok && make_map_3d(&T->By[0], T->sy_hi, nz, nx, ny, T->ldy) && make_map_3d(&T->By[1], T->sy_lo, nz, nx, ny, T->ldy);
+  if (!ok) {
+    set_error("poisson: tensor map encoding failed");
+    return OB_ERR_DEVICE;
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_COL_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_COL_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  return tc_factor_low();
 }
-int PoissonPlan::tc_solve(const float*, float*, cudaStream_t) {
-  set_error("poisson: the bf16x3 tensor-core path is not available in this build");
-  return OB_ERR_INVALID;
+
+// FP64 LU factors of the lowest 2 x 2 modes (rhs independent), from the fp32 eigenvalues and z-operator
+int PoissonPlan::tc_factor_low() {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) return OB_OK;
+  std::vector<float> lamh(nx + ny);
+  std::vector<float4> zo(nz);
+  cudaMemcpy(lamh.data(), lam, lamh.size() * 4, cudaMemcpyDeviceToHost);
+  cudaMemcpy(zo.data(), zop, zo.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+  std::vector<double> f(size_t(8) * nz);
+  for (int mode = 0; mode < 4; mode++) {
+    const int l = mode & 1, m = mode >> 1;
+    const double shift = double(lamh[l]) + double(lamh[nx + m]);
+    double* rd = f.data() + size_t(mode * 2) * nz;
+    double* cp = rd + nz;
+    double cprev = 0.0;
+    for (int k = 0; k < nz; k++) {
+      const double den = double(zo[k].z) + shift * double(zo[k].w) - double(zo[k].x) * cprev;
+      rd[k] = 1.0 / den;
+      cprev = double(zo[k].y) / den;
+      cp[k] = cprev;
+    }
+  }
+  if (cudaMemcpy(T->low, f.data(), f.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_error("poisson: low-mode factor upload failed");
+    return OB_ERR_DEVICE;
+  }
+  return OB_OK;
 }
-void PoissonPlan::tc_destroy() {}
+
+void PoissonPlan::tc_destroy() {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) return;
+  for (void* p : {(void*)T->mat, (void*)T->sx_hi, (void*)T->sx_lo, (void*)T->rx_hi, (void*)T->rx_lo, (void*)T->sy_hi, (void*)T->sy_lo,
+                  (void*)T->t2, (void*)T->low, (void*)T->err})
+    if (p) cudaFree(p);
+  delete T;
+  tc = nullptr;
+}
+
+template <int MODE>
+static void launch_tc(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh, const CUtensorMap& bl, int M, int N,
+                      int K, int planes, const TcOut& o, unsigned int* err, cudaStream_t s) {
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, planes);
+  k_dst_tc<MODE><<<grid, kThreads, SMEM_BYTES, s>>>(ah, al, bh, bl, K, o, err);
+}
+
+// the four transforms and the tridiagonals; rhs == nullptr: the right-hand side was written split by the caller
+// (the model's divergence pass, via tc_rhs_split)
+// the four transforms and the tridiagonals from the split right-hand side in rx to phi (stored, or added when add)
+static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  TcOut o{};
+  // X-fwd: rows l (nx), cols j (ny), K = i  -> S_y[k][l][j]
+  o = TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, nx, ny};
+  launch_tc<OUT_ROW_BF16X2>(T->A[0][0], T->A[0][1], T->Br[0], T->Br[1], nx, ny, nx, nz, o, T->err, s);
+  // Y-fwd: rows m (ny), cols l (nx), K = j  -> T2[k][m][l] fp32
+  o = TcOut{nullptr, nullptr, T->t2, nx, ny, nx};
+  launch_tc<OUT_ROW_F32>(T->A[1][0], T->A[1][1], T->By[0], T->By[1], ny, nx, ny, nz, o, T->err, s);
+  // tridiagonals -> S_y[k][l][m]
+  dim3 tg((nx + 31) / 32, (ny + 7) / 8);
+  switch (nz) {
+    case 16: k_tri_tc<16><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+    case 40: k_tri_tc<40><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+    default: k_tri_tc<80><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+  }
+  // Y-inv: rows j (ny), cols l (nx), K = m  -> S_x[k][j][l]
+  o = TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, ny, nx};
+  launch_tc<OUT_ROW_BF16X2>(T->A[2][0], T->A[2][1], T->By[0], T->By[1], ny, nx, ny, nz, o, T->err, s);
+  // X-inv: rows i (nx), cols j (ny), K = l  -> phi[k][j][i]
+  o = TcOut{nullptr, nullptr, phi, nx, nx, ny};
+  if (add) launch_tc<OUT_COL_F32_ADD>(T->A[3][0], T->A[3][1], T->Bx[0], T->Bx[1], nx, ny, nx, nz, o, T->err, s);
+  else launch_tc<OUT_COL_F32>(T->A[3][0], T->A[3][1], T->Bx[0], T->Bx[1], nx, ny, nx, nz, o, T->err, s);
+}
+
+// precision 1: one bf16x3 pass; precision 2: a second pass on the FP64-accumulated residual (iterative refinement).
+// rhs: the fp32 right-hand side (nx*ny*nz), needed by precision 2 and by either when the split is not pre-made
+// (presplit: the model's divergence pass writes the split into rx itself).
+int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) { set_error("poisson: tensor-core plan missing"); return OB_ERR_INVALID; }
+  if (nz != 16 && nz != 40 && nz != 80) { set_error("poisson: the tensor-core path supports nz in {16, 40, 80}"); return OB_ERR_INVALID; }
+  if (!presplit || precision == 2) {
+    if (!rhs) { set_error("poisson: right-hand side missing"); return OB_ERR_INVALID; }
+  }
+  if (!presplit) k_split_rows<<<1184, 256, 0, s>>>(rhs, long(nz) * ny, nx, T->rx_hi, T->rx_lo, int(T->ldx));
+  tc_pass(*this, T, lam, zop, phi, false, s);
+  if (precision == 2) {
+    k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rx_hi, T->rx_lo, int(T->ldx));
+    tc_pass(*this, T, lam, zop, phi, true, s);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("poisson tensor-core launch: %s", cudaGetErrorString(e));
+    return OB_ERR_DEVICE;
+  }
+  return OB_OK;
+}
+
+void PoissonPlan::tc_rhs_split(__nv_bfloat16** hi, __nv_bfloat16** lo, int* ld) const {
+  const TcPlan* T = static_cast<const TcPlan*>(tc);
+  *hi = T ? T->rx_hi : nullptr;
+  *lo = T ? T->rx_lo : nullptr;
+  *ld = T ? int(T->ldx) : 0;
+}
+
+int PoissonPlan::tc_check() {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) return OB_OK;
+  unsigned int h = 0;
+  cudaMemcpy(&h, T->err, sizeof(h), cudaMemcpyDeviceToHost);
+  if (h) {
+    cudaMemset(T->err, 0, sizeof(unsigned int));
+    set_error("poisson: a tensor-core pipeline wait timed out (code %u)", h);
+    return OB_ERR_TIMEOUT;
+  }
+  return OB_OK;
+}
 
 }  // namespace ob
+
+// ---- diagnostic: one bf16x3 batched transform C[p] = A B[p]^T, host arrays ----
+extern "C" int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* A, const float* B, float* C) {
+  using namespace ob;
+  if (M < 1 || N < 1 || K < 8 || K % 8 || planes < 1) { set_error("ob_dst_tc_selftest: bad sizes"); return OB_ERR_INVALID; }
+  if (!get_encode()) { set_error("ob_dst_tc_selftest: no tensor map encoder"); return OB_ERR_DEVICE; }
+  const long ld = K;
+  std::vector<__nv_bfloat16> ah(size_t(M) * ld), al(size_t(M) * ld), bh(size_t(planes) * N * ld), bl(size_t(planes) * N * ld);
+  for (size_t i = 0; i < ah.size(); i++) { ah[i] = __float2bfloat16_rn(A[i]); al[i] = __float2bfloat16_rn(A[i] - __bfloat162float(ah[i])); }
+  for (size_t i = 0; i < bh.size(); i++) { bh[i] = __float2bfloat16_rn(B[i]); bl[i] = __float2bfloat16_rn(B[i] - __bfloat162float(bh[i])); }
+  __nv_bfloat16 *dah, *dal, *dbh, *dbl;
+  float* dc;
+  unsigned int* derr;
+  cudaMalloc(&dah, ah.size() * 2); cudaMalloc(&dal, al.size() * 2); cudaMalloc(&dbh, bh.size() * 2); cudaMalloc(&dbl, bl.size() * 2);
+  cudaMalloc(&dc, size_t(planes) * M * N * 4); cudaMalloc(&derr, 16);
+  cudaMemset(derr, 0, 16);
+  cudaMemset(dc, 0, size_t(planes) * M * N * 4);
+  cudaMemcpy(dah, ah.data(), ah.size() * 2, cudaMemcpyHostToDevice);
+  cudaMemcpy(dal, al.data(), al.size() * 2, cudaMemcpyHostToDevice);
+  cudaMemcpy(dbh, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice);
+  cudaMemcpy(dbl, bl.data(), bl.size() * 2, cudaMemcpyHostToDevice);
+  CUtensorMap tah, tal, tbh, tbl;
+  bool ok = make_map_2d(&tah, dah, M, K, ld) && make_map_2d(&tal, dal, M, K, ld) && make_map_3d(&tbh, dbh, planes, N, K, ld) &&
+            make_map_3d(&tbl, dbl, planes, N, K, ld);
+  int rc = OB_OK;
+  if (!ok) { set_error("ob_dst_tc_selftest: tensor map encoding failed"); rc = OB_ERR_DEVICE; }
+  if (rc == OB_OK) {
+    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    TcOut o{nullptr, nullptr, dc, N, M, N};  // C[p][r][c], row pitch N
+    launch_tc<OUT_ROW_F32>(tah, tal, tbh, tbl, M, N, K, planes, o, derr, nullptr);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { set_error("ob_dst_tc_selftest: %s", cudaGetErrorString(e)); rc = OB_ERR_DEVICE; }
+    unsigned int h = 0;
+    cudaMemcpy(&h, derr, 4, cudaMemcpyDeviceToHost);
+    if (rc == OB_OK && h) { set_error("ob_dst_tc_selftest: pipeline wait timed out (code %u)", h); rc = OB_ERR_TIMEOUT; }
+    if (rc == OB_OK) cudaMemcpy(C, dc, size_t(planes) * M * N * 4, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dah); cudaFree(dal); cudaFree(dbh); cudaFree(dbl); cudaFree(dc); cudaFree(derr);
+  return rc;
+}

@@ -200,7 +200,7 @@ int PoissonPlan::create(int nx_, int ny_, int nz_, double dx_, double dz_, int p
   if ((rc = ck(cudaMemcpy(lam, lamh.data(), lamh.size() * sizeof(float), cudaMemcpyHostToDevice), "poisson upload"))) return rc;
   std::vector<float> rc1(nz, 1.f), rw1(nz + 1, 1.f);
   if ((rc = set_density(rc1.data(), rw1.data()))) return rc;
-  if (precision == 1) {
+  if (precision >= 1) {
     if ((rc = tc_create())) return rc;
   }
   return OB_OK;
@@ -213,7 +213,9 @@ int PoissonPlan::set_density(const float* rhoC, const float* rhoW) {  // solver.
     const double lo = k > 0 ? double(rhoW[k]) * a : 0.0, up = k < nz - 1 ? double(rhoW[k + 1]) * a : 0.0;
     zo[k] = make_float4(float(lo), float(up), float(-(lo + up)), rhoC[k]);
   }
-  return ck(cudaMemcpy(zop, zo.data(), zo.size() * sizeof(float4), cudaMemcpyHostToDevice), "poisson setDensity");
+  const int rc = ck(cudaMemcpy(zop, zo.data(), zo.size() * sizeof(float4), cudaMemcpyHostToDevice), "poisson setDensity");
+  if (rc != OB_OK || !tc) return rc;
+  return tc_factor_low();
 }
 
 void PoissonPlan::destroy() {
@@ -249,7 +251,7 @@ void PoissonPlan::tri(float* h, cudaStream_t s) const {
 }
 
 int PoissonPlan::solve(const float* rhs, float* phi, cudaStream_t s) {
-  if (precision == 1) return tc_solve(rhs, phi, s);
+  if (precision >= 1) return tc_solve(rhs, phi, s);
   gemm_x(mats + ofs_qix, rhs, tmp, s);
   gemm_y(mats + ofs_qiy, tmp, hat, s);
   tri(hat, s);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 
 #include "../../include/ob.h"
 
@@ -10,7 +11,8 @@ namespace ob {
 void set_error(const char* fmt, ...);
 
 struct PoissonPlan {
-  int nx = 0, ny = 0, nz = 0, precision = 0;
+  int nx = 0, ny = 0, nz = 0, precision = 0;  // 0 fp32 SIMT, 1 bf16x3 tensor core, 2 bf16x3 + one refinement
+  bool presplit = false;  // precision >= 1: the caller writes the split right-hand side (tc_rhs_split) itself
   double dx = 0, dz = 0;
   float* mats = nullptr;  // qix | qx | qiy | qy (fp32, solver.js:115-125)
   size_t ofs_qix = 0, ofs_qx = 0, ofs_qiy = 0, ofs_qy = 0;
@@ -25,14 +27,18 @@ struct PoissonPlan {
 
   int create(int nx, int ny, int nz, double dx, double dz, int precision);
   int set_density(const float* rhoC, const float* rhoW);
-  int solve(const float* rhs, float* phi, cudaStream_t s);
+  int solve(const float* rhs, float* phi, cudaStream_t s);  // precision 1: rhs == nullptr -> pre-split input
   void destroy();
 
   void gemm_x(const float* Mx, const float* src, float* dst, cudaStream_t s) const;
   void gemm_y(const float* My, const float* src, float* dst, cudaStream_t s) const;
   void tri(float* h, cudaStream_t s) const;
   int tc_create();
+  int tc_factor_low();
   int tc_solve(const float* rhs, float* phi, cudaStream_t s);
+  int tc_check();  // OB_ERR_TIMEOUT if a tensor-core pipeline wait gave up since the last check
+  // where a producer writes the split right-hand side (bf16 hi/lo, [nz][ny][ld], x fastest) for tc_solve(nullptr, ...)
+  void tc_rhs_split(__nv_bfloat16** hi, __nv_bfloat16** lo, int* ld) const;
   void tc_destroy();
 };
 

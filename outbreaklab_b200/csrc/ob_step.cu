@@ -570,11 +570,16 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
     const float rq = 1000.f * rho;
     const float rs = sqrtf(U.step.z / rho);
     // warm rain (model.js:791-799)
+    // Clear-air shortcuts below skip only work whose result is exactly zero or a no-op in the reference's
+    // arithmetic (every product with a zero mixing ratio is +0), so they change no bit of the output.
     const float pauto = U.micro.x * fmaxf(qc - U.micro.y, 0.f);
-    float accr = 2.2f * qc * powf(qr, 0.875f);
-    if (thm && qr > 1e-9f) {
-      const float l = Fall::lamR(qr, nr);
-      accr = 3100.f * rho * nr * powf(l, -2.8f) * qc * rs;
+    float accr = 0.f;
+    if (qc > 0.f) {
+      accr = 2.2f * qc * powf(qr, 0.875f);
+      if (thm && qr > 1e-9f) {
+        const float l = Fall::lamR(qr, nr);
+        accr = 3100.f * rho * nr * powf(l, -2.8f) * qc * rs;
+      }
     }
     const float da = fminf(pauto * dt, qc);
     const float dc = fminf(accr * dt, qc - da);
@@ -582,7 +587,7 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
     qr += da + dc;
     nr += da / 2.68e-10f;
     const float dTc = T - T0K;
-    if (dTc < 0.f) {  // ice-phase conversions (model.js:801-829)
+    if (dTc < 0.f && qc + qi + qr + qs + qg > 0.f) {  // ice-phase conversions (model.js:801-829)
       const float psaut = 1e-3f * expf(0.025f * dTc) * fmaxf(qi - 6e-4f, 0.f);
       const float psacw = 5.4e-3f * qc * powf(fmaxf(rq * qs, 0.f), 0.81f) * rs;
       const float psaci = 5.4e-3f * qi * powf(fmaxf(rq * qs, 0.f), 0.81f) * expf(0.025f * dTc) * rs;
@@ -613,7 +618,7 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
       qs -= a4;
       qg += a4;
       T += float(LFCd / CPDd) * (a2 + a3);
-    } else {  // melting (model.js:830-848)
+    } else if (dTc >= 0.f && (qs > 0.f || qg > 0.f)) {  // melting (model.js:830-848)
       const float m1 = fminf(0.012f * dTc * qs * dt, qs);
       float m2 = fminf(0.0022f * dTc * qg * dt, qg);
       if (thm) {
@@ -635,7 +640,7 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
       T -= float(LFCd / CPDd) * (m1 + m2);
     }
     // rain evaporation (model.js:850-872)
-    const float qvsl = qvsat(T, p0, 0.f);
+    const float qvsl = qr > 0.f ? qvsat1(T, p0, 0.f) : 0.f;
     if (qr > 0.f && qv < qvsl) {
       const float rc = 0.001f * rho * qr;
       const float ern = ((1.6f + 124.9f * powf(rc, 0.2046f)) * powf(rc, 0.525f) / (2.55e8f / (p0 * qvsl) + 5.4e5f)) *
@@ -665,8 +670,9 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
       } else nr = 0.f;
     }
     // sublimation (model.js:885-892)
-    const float qvsi = qvsat(T, p0, 1.f);
-    if (dTc < 0.f && qv < qvsi) {
+    const bool sub_on = dTc < 0.f && (qs > 0.f || qg > 0.f);
+    const float qvsi = sub_on ? qvsat1(T, p0, 1.f) : 0.f;
+    if (sub_on && qv < qvsi) {
       const float sub = fmaxf(1.f - qv / qvsi, 0.f);
       float e = fminf((2e-3f * qs + 5e-4f * qg) * sub * dt, (qvsi - qv) * 0.5f);
       const float fsn = qs / fmaxf(qs + qg, 1e-20f);
@@ -679,13 +685,13 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
     // mixed-phase saturation adjustment, 3 iterations (model.js:893-905)
     const float qi0 = qi;
     float qcl = qc + qi, dsum = 0.f;
-#pragma unroll
     for (int it = 0; it < 3; it++) {
       const float f = fIce(T);
-      const float qs_ = qvsat(T, p0, f);
+      const float qs_ = qvsat1(T, p0, f);
       const float Lh = mixf(float(LVCd), float(LSCd), f);
       float d = (qv - qs_) / (1.f + Lh * Lh * qs_ / (float(CPDd * RVCd) * T * T));
       d = fmaxf(d, -qcl);
+      if (d == 0.f) break;  // nothing changes: the remaining iterations would repeat this one exactly
       qv -= d;
       qcl += d;
       T += Lh / float(CPDd) * d;
@@ -735,7 +741,14 @@ __global__ void k_div(Grid g, Uni U, Fields F, int par) {
   const float wb = ck == 0 ? 0.f : __ldg(w + o);
   const float d = rc * (__ldg(u + o + 1) - __ldg(u + o) + __ldg(v + o + g.px) - __ldg(v + o)) / U.dims.w +
                   (rhoW(F.B, g.nz, ck + 1) * wt - rhoW(F.B, g.nz, ck) * wb) / U.dzv.x;
-  F.rhs[g.pidx(ci, cj, ck)] = d / U.step.x;
+  const float r = d / U.step.x;
+  if (F.rhs_hi) {  // tensor-core solve: write the split directly in its [z][y][x] layout with pitch rhs_ld
+    const long o2 = (long(ck) * g.nyp + (cj + g.pad)) * F.rhs_ld + (ci + g.pad);
+    const __nv_bfloat16 h = __float2bfloat16_rn(r);
+    F.rhs_hi[o2] = h;
+    F.rhs_lo[o2] = __float2bfloat16_rn(r - __bfloat162float(h));
+  }
+  if (F.rhs) F.rhs[g.pidx(ci, cj, ck)] = r;  // fp32 solve, or the residual of the refined solve
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -173,6 +173,14 @@ class RegionalModel:
         N.check(N.lib().ob_model_time(self.h, C.byref(t), C.byref(s), C.byref(p)))
         return p.value
 
+    def set_solver(self, precision: int):
+        """Pressure-solve precision: 0 = fp32 transforms, 1 = bf16x3 tensor-core transforms."""
+        N.check(N.lib().ob_model_set_solver(self.h, int(precision)))
+
+    @property
+    def solver(self):
+        return int(N.lib().ob_model_solver(self.h))
+
     @property
     def nan_count(self):
         return int(N.lib().ob_model_nan_count(self.h))
@@ -237,6 +245,12 @@ class PoissonDirect:
         out = np.empty_like(r)
         N.check(N.lib().ob_poisson_solve(self.h, N.fptr(r), N.fptr(out)))
         return out
+
+    def device_ms(self, reps=10):
+        """Device time of one solve (CUDA events) on the last right-hand side."""
+        t = C.c_float()
+        N.check(N.lib().ob_poisson_time(self.h, int(reps), C.byref(t)))
+        return t.value
 
     def destroy(self):
         if getattr(self, "h", None):

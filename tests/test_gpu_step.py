@@ -44,16 +44,30 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("solver", [2, 0])
 @pytest.mark.parametrize("name", list(CASES))
-def test_one_step_parity(oracle_lib, native, name):
+def test_one_step_parity(oracle_lib, native, name, solver):
+    """Solver 2 (refined bf16x3 tensor-core solve, the default) and 0 (fp32 transforms) both within the envelope."""
     case = CASES[name]()
     g, f, d = _setup(oracle_lib, case, blob="blob" in name)
+    g.set_solver(solver)
     for m in (g, f, d):
         m.step(case.dt, 1)
     g.sync()
     bad, rep = _compare(g, f, d)
     assert not bad, "\n".join(bad)
     assert g.nan_count == 0
+
+
+def test_one_step_unrefined_bf16x3_stated_error(oracle_lib, native):
+    """Solver 1 (bf16x3 without refinement): its stated one-step error bound, 5e-4 of each field's maximum."""
+    case = CASES["small-lin-blob"]()
+    g, f, d = _setup(oracle_lib, case, blob=True)
+    g.set_solver(1)
+    for m in (g, f, d):
+        m.step(case.dt, 1)
+    bad, _ = _compare(g, f, d, tol=5e-4, envelope=0.0)
+    assert not bad, "\n".join(bad)
 
 
 @pytest.mark.parametrize("name", ["small-lin-blob", "small-thompson-blob"])

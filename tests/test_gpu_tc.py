@@ -1,0 +1,71 @@
+"""The bf16x3 tcgen05 transform kernel in isolation, and the precision-1 pressure solve."""
+import numpy as np
+import pytest
+
+from outbreaklab_b200 import _native as N, model as M, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _tc(A, B):
+    Mr, K = A.shape
+    P, Nn, K2 = B.shape
+    assert K == K2
+    C = np.empty((P, Mr, Nn), np.float32)
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    N.check(N.lib().ob_dst_tc_selftest(Mr, Nn, K, P, N.fptr(A), N.fptr(B.reshape(-1)), N.fptr(C.reshape(-1))))
+    return C
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 64, 1), (128, 128, 128, 2), (200, 136, 72, 3), (656, 96, 656, 2)])
+def test_tc_transform_matches_fp64(native, shape):
+    Mr, Nn, K, P = shape
+    rng = np.random.default_rng(Mr + K)
+    A = rng.standard_normal((Mr, K)).astype(np.float32)
+    B = rng.standard_normal((P, Nn, K)).astype(np.float32)
+    C = _tc(A, B)
+    ref = np.einsum("mk,pnk->pmn", A.astype(np.float64), B.astype(np.float64))
+    # bf16x3 keeps ~16 significant bits per product; the error of a K-term sum is ~2^-16 sqrt(K) of the sum's scale
+    err = np.abs(C - ref).max() / np.abs(ref).max()
+    assert err < 2e-4, err
+
+
+def test_tc_transform_identity_exact(native):
+    """With the identity as A (exact in bf16), C = hi(B) + lo(B) reproduces B to bf16x2 precision."""
+    K = 64
+    A = np.eye(128, K, dtype=np.float32)
+    rng = np.random.default_rng(3)
+    B = rng.standard_normal((1, 128, K)).astype(np.float32)
+    C = _tc(A, B)[0]
+    ref = B[0].T[:128]
+    assert np.abs(C[:K] - B[0].T).max() <= 1e-5 * np.abs(B).max()
+
+
+def _density(nz, dz):
+    rc = 1.15 * np.exp(-(np.arange(nz) + 0.5) * dz / 9000.0)
+    rw = np.concatenate([[rc[0] * 1.02], 0.5 * (rc[1:] + rc[:-1]), [rc[-1] * 0.94]])
+    return rc.astype(np.float32), rw.astype(np.float32)
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+@pytest.mark.parametrize("shape", [(96, 80, 40), (150, 130, 16), (256, 200, 80)])
+def test_poisson_bf16x3_vs_fp64(oracle_lib, native, shape, precision):
+    nx, ny, nz = shape
+    dx, dz = 1000.0, 20000.0 / nz
+    rc, rw = _density(nz, dz)
+    rhs = W.gaussian_rhs(nx, ny, nz, dx, corr_len=5000.0, seed=nx).astype(np.float32)
+    P = M.PoissonDirect(nx, ny, nz, dx, dz, precision)
+    P.set_density(rc, rw)
+    phi = P.solve(rhs)
+    r64, w64 = rc.astype(np.float64), rw.astype(np.float64)
+    ref = oracle_lib.poisson_solve(rhs.astype(np.float64), dx, dz, r64, w64, 8)
+    f32 = oracle_lib.poisson_solve(rhs, dx, dz, rc, rw, 4)
+    err = np.abs(phi - ref).max() / np.abs(ref).max()
+    err32 = np.abs(f32 - ref).max() / np.abs(ref).max()
+    res = np.abs(oracle_lib.poisson_apply(phi.astype(np.float64), dx, dz, r64, w64) - rhs).max() / np.abs(rhs).max()
+    if precision == 1:
+        assert err < 5e-4, err                     # stated error of the unrefined bf16x3 solve
+    else:
+        assert err <= max(1e-5, 2 * err32), (err, err32)   # refined: at least as accurate as the fp32 restatement
+        assert res < 3e-4, res                     # one sweep cuts the ~1e-2 residual of a single pass ~100x
