@@ -85,6 +85,7 @@ struct ObModel {
   double* d_red = nullptr;
   float* d_qptr = nullptr;
   float* rhs32 = nullptr;  // the fp32 right-hand side buffer (F.rhs points here when a solver reads it)
+  unsigned int* d_act = nullptr;  // 4 brick-flag arrays (clear-air skip of the scalar advection)
   PoissonPlan solver;
   std::vector<float> Bh;
   double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
@@ -108,7 +109,7 @@ static void model_bind_solver(ObModel* m) {
 static void model_free(ObModel* m) {
   if (!m) return;
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -213,6 +214,9 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->stage_bytes = std::max(size_t(nx + 1) * (ny + 1) * (nz + 1) * 4, np) * sizeof(float);
   alloc((void**)&m->stage, m->stage_bytes, "staging");
   alloc((void**)&m->d_qptr, 8 * sizeof(float*), "pointer table");
+  const int nbx = (nx + 31) / 32, nby = (ny + 3) / 4;
+  const size_t nbr = size_t(nbx) * nby * nz;
+  alloc((void**)&m->d_act, 4 * nbr * sizeof(unsigned int), "activity flags");
   // the refined bf16x3 tensor-core solve where its tridiagonal kernel is specialised, else fp32
   const int prec = (nz == 16 || nz == 40 || nz == 80) ? 2 : 0;
   if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, prec);
@@ -245,6 +249,13 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->F.bnd = m->d_bnd;
   m->F.ci = m->d_ci;
   m->F.flags = m->d_flags;
+  m->F.nbx = nbx;
+  m->F.nby = nby;
+  m->F.actQ0 = m->d_act;
+  m->F.actQt = m->d_act + nbr;
+  m->F.zeroQt = m->d_act + 2 * nbr;
+  m->F.zeroQ1 = m->d_act + 3 * nbr;
+  m->F.fallmax = 100.f;
   cudaMemcpy(m->d_qptr, m->F.Q[0], 8 * sizeof(float*), cudaMemcpyHostToDevice);
   // a neutral base state until one is set
   m->Bh.assign(size_t(nz + 1) * 8, 0.f);
@@ -268,6 +279,14 @@ int ob_model_set_base_state(ObModel* m, const float* B, int nz) {
   if (!m || !B || nz != m->g.nz) { set_error("ob_model_set_base_state: expected nz = %d", m ? m->g.nz : -1); return OB_ERR_INVALID; }
   m->Bh.assign(B, B + size_t(nz + 1) * 8);
   m->rhoSfc = B[2];
+  {
+    // the largest fall speed any hydrometeor can reach (model.js:63-99): rain <= 10, snow <= 2.2, Thompson graupel
+    // <= 25 m/s, each times sqrt(rho_sfc / rho), Lin graupel <= 65 m/s; bounds the vertical reach of a fall trace
+    double rmin = 1e30;
+    for (int k = 0; k < nz; k++) rmin = std::min(rmin, double(B[k * 8 + 2]));
+    const double s = std::sqrt(std::max(double(m->rhoSfc), 1e-6) / std::max(rmin, 1e-6));
+    m->F.fallmax = float(std::max(65.0, 25.0 * s) * 1.01 + 1.0);
+  }
   OB_TRY(cuda_status(cudaMemcpyAsync(m->d_B, m->Bh.data(), m->Bh.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream), "base state"));
   std::vector<float> rc(nz), rw(nz + 1);
   for (int k = 0; k < nz; k++) rc[k] = B[k * 8 + 2];
@@ -316,6 +335,7 @@ int ob_model_reset(ObModel* m) {
   cudaMemsetAsync(m->rhs32, 0, np * sizeof(float), m->stream);
   cudaMemsetAsync(m->d_rain, 0, size_t(g.nx) * g.ny * sizeof(double), m->stream);
   cudaMemsetAsync(m->d_flags, 0, 64 * sizeof(unsigned), m->stream);
+  launch_activity(g, m->F, m->stream);
   m->lsfT = 0;
   return cuda_status(cudaGetLastError(), "reset");
 }
@@ -420,6 +440,7 @@ int ob_model_set_field(ObModel* m, int field, const void* host, size_t bytes) {
   if (bytes != need) { set_error("ob_model_set_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
   OB_TRY(cuda_status(cudaMemcpyAsync(m->stage, host, bytes, cudaMemcpyHostToDevice, m->stream), "set field"));
   launch_unpack(g, p, nch, X, Y, Z, m->stage, m->stream);
+  if (field == OB_FIELD_Q1 || field == OB_FIELD_Q2) launch_activity(g, m->F, m->stream);
   return cuda_status(cudaStreamSynchronize(m->stream), "set field");
 }
 

@@ -357,67 +357,247 @@ __device__ __forceinline__ float2 minmax8Q(const float* __restrict__ f, const Gr
   return make_float2(lo, hi);
 }
 
-__global__ void k_advq1(Grid g, Uni U, Fields F, int par) {
-  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
-  float v[3];
-  cellVel(F, g, par, ci, cj, ck, v);
+// A trilinear tap on the cell-centred box: base offsets of the 2 x 2 x 2 neighbourhood (clamp-to-edge) and the
+// weights; the same footprint is the 8-texel min/max window of the MacCormack limiter (model.js:537-540).
+struct Tap {
+  int i0, i1, r00, r10, r01, r11;
+  float ax, ay, az;
+};
+__device__ __forceinline__ Tap tapQ(const Grid& g, float x, float y, float z) {
+  const float tx = x - 0.5f, ty = y - 0.5f, tz = z - 0.5f;
+  const float fx = floorf(tx), fy = floorf(ty), fz = floorf(tz);
+  int i0 = int(fx), j0 = int(fy), k0 = int(fz);
+  Tap t;
+  t.ax = tx - fx;
+  t.ay = ty - fy;
+  t.az = tz - fz;
+  const int j1 = clampi(j0 + 1, 0, g.ny - 1), k1 = clampi(k0 + 1, 0, g.nz - 1);
+  t.i1 = clampi(i0 + 1, 0, g.nx - 1);
+  t.i0 = clampi(i0, 0, g.nx - 1);
+  j0 = clampi(j0, 0, g.ny - 1);
+  k0 = clampi(k0, 0, g.nz - 1);
+  t.r00 = g.px * (j0 + g.py * k0);
+  t.r10 = g.px * (j1 + g.py * k0);
+  t.r01 = g.px * (j0 + g.py * k1);
+  t.r11 = g.px * (j1 + g.py * k1);
+  return t;
+}
+__device__ __forceinline__ float gatherQ(const float* __restrict__ f, const Tap& t) {
+  const float c00 = __ldg(f + t.r00 + t.i0) * (1.f - t.ax) + __ldg(f + t.r00 + t.i1) * t.ax;
+  const float c10 = __ldg(f + t.r10 + t.i0) * (1.f - t.ax) + __ldg(f + t.r10 + t.i1) * t.ax;
+  const float c01 = __ldg(f + t.r01 + t.i0) * (1.f - t.ax) + __ldg(f + t.r01 + t.i1) * t.ax;
+  const float c11 = __ldg(f + t.r11 + t.i0) * (1.f - t.ax) + __ldg(f + t.r11 + t.i1) * t.ax;
+  const float c0 = c00 * (1.f - t.ay) + c10 * t.ay;
+  const float c1 = c01 * (1.f - t.ay) + c11 * t.ay;
+  return c0 * (1.f - t.az) + c1 * t.az;
+}
+__device__ __forceinline__ float2 minmaxQ(const float* __restrict__ f, const Tap& t) {
+  const float a = __ldg(f + t.r00 + t.i0), b = __ldg(f + t.r00 + t.i1), c = __ldg(f + t.r10 + t.i0), d = __ldg(f + t.r10 + t.i1);
+  const float e = __ldg(f + t.r01 + t.i0), h = __ldg(f + t.r01 + t.i1), k = __ldg(f + t.r11 + t.i0), l = __ldg(f + t.r11 + t.i1);
+  return make_float2(fminf(fminf(fminf(a, b), fminf(c, d)), fminf(fminf(e, h), fminf(k, l))),
+                     fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), fmaxf(fmaxf(e, h), fmaxf(k, l))));
+}
+
+// Clear-air skip of the hydrometeor channels (qc, qi, qr, qs, qg, Nr). A block (one brick of 32 x 4 x 1 cells) reads
+// those channels only inside the footprints of its departure points; if every brick touching that region holds no
+// hydrometeor, the semi-Lagrangian samples, the MacCormack correction, the limiter and the clip all give exactly +0,
+// so the block writes zeros (once) instead of gathering. Falling hydrometeors shift a departure point vertically by
+// at most dt/dz * fallmax, which widens the region in z.
+struct Region {
+  int x0, x1, y0, y1, z0, z1;
+};
+__device__ __forceinline__ bool region_active(const Grid& g, const Fields& F, Region r, const unsigned int* flagsA,
+                                              const unsigned int* flagsB) {
+  __shared__ int red[6];
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    red[0] = red[2] = red[4] = 1 << 30;
+    red[1] = red[3] = red[5] = -(1 << 30);
+  }
+  __syncthreads();
+  // warp-level min/max, then one shared atomic per warp
+  const unsigned m = 0xffffffffu;
+  const int a0 = __reduce_min_sync(m, r.x0), a1 = __reduce_max_sync(m, r.x1);
+  const int b0 = __reduce_min_sync(m, r.y0), b1 = __reduce_max_sync(m, r.y1);
+  const int c0 = __reduce_min_sync(m, r.z0), c1 = __reduce_max_sync(m, r.z1);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&red[0], a0); atomicMax(&red[1], a1);
+    atomicMin(&red[2], b0); atomicMax(&red[3], b1);
+    atomicMin(&red[4], c0); atomicMax(&red[5], c1);
+  }
+  __syncthreads();
+  const int bx0 = clampi(red[0], 0, g.nx - 1) / 32, bx1 = clampi(red[1], 0, g.nx - 1) / 32;
+  const int by0 = clampi(red[2], 0, g.ny - 1) / 4, by1 = clampi(red[3], 0, g.ny - 1) / 4;
+  const int bz0 = clampi(red[4], 0, g.nz - 1), bz1 = clampi(red[5], 0, g.nz - 1);
+  const int nxb = bx1 - bx0 + 1, nyb = by1 - by0 + 1, nzb = bz1 - bz0 + 1;
+  const int count = nxb * nyb * nzb;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  unsigned any = 0;
+  for (int t = tid; t < count; t += blockDim.x * blockDim.y) {
+    const int bx = bx0 + t % nxb, by = by0 + (t / nxb) % nyb, bz = bz0 + t / (nxb * nyb);
+    const int b = bx + F.nbx * (by + F.nby * bz);
+    any |= __ldg(flagsA + b);
+    if (flagsB) any |= __ldg(flagsB + b);
+  }
+  return __syncthreads_or(any != 0u) != 0;
+}
+
+// ---- ADVQ1 (model.js:500-529): semi-Lagrangian step of the 8 scalars, channels grouped by the fall speed of
+// their trace (qv, qc, qi, spare [and Nr for Lin] at the air's speed; qr, qs, qg, Nr (Thompson) each their own) ----
+__global__ void __launch_bounds__(128) k_advq1(Grid g, Uni U, Fields F, int par) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
+  const int o = in ? g.at(ci, cj, ck) : 0;
   const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  float v[3] = {0.f, 0.f, 0.f};
   const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
-  const int o = g.at(ci, cj, ck);
-  const Fall fl{U.step.z, U.micro2.z > 0.5f};
-  const float rho = bsA(F.B, g.nz, ck).z;
-  const float2 fv = fl.vtRain(__ldg(F.Q[0][3] + o), __ldg(F.Q[0][6] + o), rho);
-  const float fs = fl.vtS(__ldg(F.Q[0][4] + o), rho), fg = fl.vtGrau(__ldg(F.Q[0][5] + o), rho);
-  float x, y, z;
-  traceQ(g, kk, p, v, 0.f, 1.f, x, y, z);
-  F.Qt[0][o] = sampleQ(F.Q[0][0], g, x, y, z);
-  F.Qt[1][o] = sampleQ(F.Q[0][1], g, x, y, z);
-  F.Qt[2][o] = sampleQ(F.Q[0][2], g, x, y, z);
-  F.Qt[7][o] = sampleQ(F.Q[0][7], g, x, y, z);
-  const float nr0 = sampleQ(F.Q[0][6], g, x, y, z);
-  traceQ(g, kk, p, v, fv.x, 1.f, x, y, z);
-  F.Qt[3][o] = sampleQ(F.Q[0][3], g, x, y, z);
-  traceQ(g, kk, p, v, fs, 1.f, x, y, z);
-  F.Qt[4][o] = sampleQ(F.Q[0][4], g, x, y, z);
-  traceQ(g, kk, p, v, fg, 1.f, x, y, z);
-  F.Qt[5][o] = sampleQ(F.Q[0][5], g, x, y, z);
-  if (fl.thm) {
-    traceQ(g, kk, p, v, fv.y, 1.f, x, y, z);
-    F.Qt[6][o] = sampleQ(F.Q[0][6], g, x, y, z);
-  } else {
-    F.Qt[6][o] = nr0;
+  float x = 0.5f, y = 0.5f, z = 0.5f;
+  Region r{ci, ci, cj, cj, ck, ck};
+  if (in) {
+    cellVel(F, g, par, ci, cj, ck, v);
+    traceQ(g, kk, p, v, 0.f, 1.f, x, y, z);
+    r.x0 = min(r.x0, int(floorf(x - 0.5f)));
+    r.x1 = max(r.x1, int(floorf(x - 0.5f)) + 1);
+    r.y0 = min(r.y0, int(floorf(y - 0.5f)));
+    r.y1 = max(r.y1, int(floorf(y - 0.5f)) + 1);
+    r.z0 = min(r.z0, int(floorf(z - 0.5f)));
+    r.z1 = max(r.z1, int(floorf(fminf(z + kk[2] * F.fallmax, float(g.nz) - 0.5f) - 0.5f)) + 1);
+  }
+  const bool active = region_active(g, F, r, F.actQ0, nullptr);
+  const int brick = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+  if (in) {
+    const Tap t0 = tapQ(g, x, y, z);
+    F.Qt[0][o] = gatherQ(F.Q[0][0], t0);
+    F.Qt[7][o] = gatherQ(F.Q[0][7], t0);
+    if (active) {
+      F.Qt[1][o] = gatherQ(F.Q[0][1], t0);
+      F.Qt[2][o] = gatherQ(F.Q[0][2], t0);
+      const float nr0 = gatherQ(F.Q[0][6], t0);
+      const Fall fl{U.step.z, U.micro2.z > 0.5f};
+      const float rho = bsA(F.B, g.nz, ck).z;
+      const float2 fv = fl.vtRain(__ldg(F.Q[0][3] + o), __ldg(F.Q[0][6] + o), rho);
+      const float fs = fl.vtS(__ldg(F.Q[0][4] + o), rho), fg = fl.vtGrau(__ldg(F.Q[0][5] + o), rho);
+      traceQ(g, kk, p, v, fv.x, 1.f, x, y, z);
+      F.Qt[3][o] = gatherQ(F.Q[0][3], tapQ(g, x, y, z));
+      traceQ(g, kk, p, v, fs, 1.f, x, y, z);
+      F.Qt[4][o] = gatherQ(F.Q[0][4], tapQ(g, x, y, z));
+      traceQ(g, kk, p, v, fg, 1.f, x, y, z);
+      F.Qt[5][o] = gatherQ(F.Q[0][5], tapQ(g, x, y, z));
+      if (fl.thm) {
+        traceQ(g, kk, p, v, fv.y, 1.f, x, y, z);
+        F.Qt[6][o] = gatherQ(F.Q[0][6], tapQ(g, x, y, z));
+      } else {
+        F.Qt[6][o] = nr0;
+      }
+    } else if (!F.zeroQt[brick]) {
+#pragma unroll
+      for (int c = 1; c < 7; c++) F.Qt[c][o] = 0.f;
+    }
+  }
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    F.actQt[brick] = active ? 1u : 0u;
+    F.zeroQt[brick] = active ? 0u : 1u;
   }
 }
 
-__global__ void k_advq2(Grid g, Uni U, Fields F, int par) {
-  OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
-  float v[3];
-  cellVel(F, g, par, ci, cj, ck, v);
+// ---- ADVQ2 (model.js:530-576): MacCormack correction, limiter on the departure cell's 8 texels, clip >= 0 ----
+__device__ __forceinline__ float advq2_channel(const Fields& F, const Grid& g, const float kk[3], const float p[3], const float v[3],
+                                               float fall, float sm, float qc_, int c, int o) {
+  float x, y, z;
+  traceQ(g, kk, p, v, fall, -1.f, x, y, z);
+  const float b = gatherQ(F.Qt[c], tapQ(g, x, y, z));
+  const float r = __ldg(F.Qt[c] + o) + sm * (qc_ - b);
+  traceQ(g, kk, p, v, fall, 1.f, x, y, z);
+  const float2 m = minmaxQ(F.Q[0][c], tapQ(g, x, y, z));
+  return fmaxf(clampf(r, m.x, m.y), 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_advq2(Grid g, Uni U, Fields F, int par) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
+  const int o = in ? g.at(ci, cj, ck) : 0;
   const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  float v[3] = {0.f, 0.f, 0.f};
   const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
-  const int o = g.at(ci, cj, ck);
-  const Fall fl{U.step.z, U.micro2.z > 0.5f};
-  const float rho = bsA(F.B, g.nz, ck).z;
-  float q[8];
+  float xb = 0.5f, yb = 0.5f, zb = 0.5f, xf = 0.5f, yf = 0.5f, zf = 0.5f;
+  Region r{ci, ci, cj, cj, ck, ck};
+  if (in) {
+    cellVel(F, g, par, ci, cj, ck, v);
+    traceQ(g, kk, p, v, 0.f, -1.f, xb, yb, zb);
+    traceQ(g, kk, p, v, 0.f, 1.f, xf, yf, zf);
+    r.x0 = min(r.x0, int(floorf(fminf(xb, xf) - 0.5f)));
+    r.x1 = max(r.x1, int(floorf(fmaxf(xb, xf) - 0.5f)) + 1);
+    r.y0 = min(r.y0, int(floorf(fminf(yb, yf) - 0.5f)));
+    r.y1 = max(r.y1, int(floorf(fmaxf(yb, yf) - 0.5f)) + 1);
+    const float dzf = kk[2] * F.fallmax;
+    r.z0 = min(r.z0, int(floorf(fmaxf(fminf(zb, zf) - dzf, 0.5f) - 0.5f)));
+    r.z1 = max(r.z1, int(floorf(fminf(fmaxf(zb, zf) + dzf, float(g.nz) - 0.5f) - 0.5f)) + 1);
+  }
+  const bool active = region_active(g, F, r, F.actQ0, F.actQt);
+  const int brick = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+  if (in) {
+    const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
+    const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
+    const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
+    {  // the air-speed group: qv and the spare channel always
+      const Tap tb = tapQ(g, xb, yb, zb), tf = tapQ(g, xf, yf, zf);
 #pragma unroll
-  for (int c = 0; c < 8; c++) q[c] = __ldg(F.Q[0][c] + o);
-  const float2 fv = fl.vtRain(q[3], q[6], rho);
-  const float fs = fl.vtS(q[4], rho), fg = fl.vtGrau(q[5], rho);
-  const float fn = fl.thm ? fv.y : 0.f;
-  const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
-  const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
-  const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
-  // per channel: the fall speed of its trace (qv, qc, qi, qr, qs, qg, Nr, spare)
-  const float fall[8] = {0.f, 0.f, 0.f, fv.x, fs, fg, fn, 0.f};
+      for (int c = 0; c < 8; c += 7) {
+        const float b = gatherQ(F.Qt[c], tb);
+        const float rr = __ldg(F.Qt[c] + o) + sm * (__ldg(F.Q[0][c] + o) - b);
+        const float2 m = minmaxQ(F.Q[0][c], tf);
+        F.Q[1][c][o] = fmaxf(clampf(rr, m.x, m.y), 0.f);
+      }
+      if (active) {
+        const Fall fl{U.step.z, U.micro2.z > 0.5f};
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    float x, y, z;
-    traceQ(g, kk, p, v, fall[c], -1.f, x, y, z);
-    const float b = sampleQ(F.Qt[c], g, x, y, z);
-    const float r = __ldg(F.Qt[c] + o) + sm * (q[c] - b);
-    traceQ(g, kk, p, v, fall[c], 1.f, x, y, z);
-    const float2 m = minmax8Q(F.Q[0][c], g, x, y, z);
-    F.Q[1][c][o] = fmaxf(clampf(r, m.x, m.y), 0.f);
+        for (int c = 1; c < 3; c++) {
+          const float b = gatherQ(F.Qt[c], tb);
+          const float rr = __ldg(F.Qt[c] + o) + sm * (__ldg(F.Q[0][c] + o) - b);
+          const float2 m = minmaxQ(F.Q[0][c], tf);
+          F.Q[1][c][o] = fmaxf(clampf(rr, m.x, m.y), 0.f);
+        }
+        if (!fl.thm) {
+          const float b = gatherQ(F.Qt[6], tb);
+          const float rr = __ldg(F.Qt[6] + o) + sm * (__ldg(F.Q[0][6] + o) - b);
+          const float2 m = minmaxQ(F.Q[0][6], tf);
+          F.Q[1][6][o] = fmaxf(clampf(rr, m.x, m.y), 0.f);
+        }
+      }
+    }
+    if (active) {
+      const Fall fl{U.step.z, U.micro2.z > 0.5f};
+      const float rho = bsA(F.B, g.nz, ck).z;
+      const float q3 = __ldg(F.Q[0][3] + o), q4 = __ldg(F.Q[0][4] + o), q5 = __ldg(F.Q[0][5] + o), q6 = __ldg(F.Q[0][6] + o);
+      const float2 fv = fl.vtRain(q3, q6, rho);
+      F.Q[1][3][o] = advq2_channel(F, g, kk, p, v, fv.x, sm, q3, 3, o);
+      F.Q[1][4][o] = advq2_channel(F, g, kk, p, v, fl.vtS(q4, rho), sm, q4, 4, o);
+      F.Q[1][5][o] = advq2_channel(F, g, kk, p, v, fl.vtGrau(q5, rho), sm, q5, 5, o);
+      if (fl.thm) F.Q[1][6][o] = advq2_channel(F, g, kk, p, v, fv.y, sm, q6, 6, o);
+    } else if (!F.zeroQ1[brick]) {
+#pragma unroll
+      for (int c = 1; c < 7; c++) F.Q[1][c][o] = 0.f;
+    }
+  }
+  if (threadIdx.x == 0 && threadIdx.y == 0) F.zeroQ1[brick] = active ? 0u : 1u;
+}
+
+// hydrometeor flags of Q slot 0 per brick, from scratch (after a reset or a host upload of Q); the scratch-known-zero
+// flags are cleared because the host may have written anywhere
+__global__ void __launch_bounds__(128) k_activity(Grid g, Fields F) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  bool act = false;
+  if (ci < g.nx && cj < g.ny && ck < g.nz) {
+    const int o = g.at(ci, cj, ck);
+#pragma unroll
+    for (int c = 1; c < 7; c++) act |= F.Q[0][c][o] != 0.f;
+  }
+  const bool any = __syncthreads_or(act) != 0;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int b = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+    F.actQ0[b] = any ? 1u : 0u;
+    F.actQt[b] = 1u;
+    F.zeroQt[b] = 0u;
+    F.zeroQ1[b] = 0u;
   }
 }
 
@@ -444,8 +624,9 @@ __device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
   return 0.f;
 }
 
-__global__ void k_phys(Grid g, Uni U, Fields F, int par) {
-  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+// one texel of the physics pass; returns whether the cell's new state holds a hydrometeor
+__device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
+  bool hyd = false;
   const float* __restrict__ Vin[4] = {F.V[1 - par][0], F.V[1 - par][1], F.V[1 - par][2], F.V[1 - par][3]};
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   auto L = [&](int ch, int a, int b, int c) { return __ldg(Vin[ch] + g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz))); };
@@ -713,6 +894,7 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
     F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
     F.Q[0][7][o] = q2[3];
     out[3] = th;
+    hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f;
   }
   const float sp = sqrtf(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
   if (sp > U.misc.x) {
@@ -725,6 +907,17 @@ __global__ void k_phys(Grid g, Uni U, Fields F, int par) {
   }
 #pragma unroll
   for (int c = 0; c < 4; c++) F.V[par][c][o] = out[c];
+  return hyd;
+}
+
+__global__ void __launch_bounds__(128) k_phys(Grid g, Uni U, Fields F, int par) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  bool hyd = false;
+  if (ci <= g.nx && cj <= g.ny && ck <= g.nz) hyd = phys_texel(g, U, F, par, ci, cj, ck);
+  // hydrometeor flag of this block's brick for the next step's scalar advection
+  const bool any = __syncthreads_or(hyd) != 0;
+  if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && ck < g.nz)
+    F.actQ0[blockIdx.x + F.nbx * (blockIdx.y + F.nby * ck)] = any ? 1u : 0u;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -902,6 +1095,9 @@ void launch_advv(const Grid& g, const Uni& U, const Fields& F, int par, cudaStre
 void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
   k_advq1<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
   k_advq2<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_activity(const Grid& g, const Fields& F, cudaStream_t s) {
+  k_activity<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, F);
 }
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
   k_phys<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);

@@ -14,6 +14,7 @@ void launch_init(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
 void launch_nut(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_advv(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
+void launch_activity(const Grid& g, const Fields& F, cudaStream_t s);
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
