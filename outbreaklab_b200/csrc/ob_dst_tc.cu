@@ -123,49 +123,69 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
     const int q = warp & 3;
-    const int r = m0 + q * 32 + lane;
-    if (tc::mbar_wait(accum, 0, err, 8u)) {
-      tc::tc_fence_after();
+    const bool ok = tc::mbar_wait(accum, 0, err, 8u);
+    if (ok) tc::tc_fence_after();
+    if (MODE == OUT_COL_F32 || MODE == OUT_COL_F32_ADD) {
+      // rows are the output's fastest index: lane l of every store writes row m0 + 32q + l, one 128-byte line
+      const int r = m0 + q * 32 + lane;
+      if (ok) {
 #pragma unroll 1
-      for (int ch = 0; ch < BN / 32; ch++) {
-        float v[32];
-        tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
-        const int c0 = n0 + ch * 32;
-        if (c0 >= out.N) break;
-        if (MODE == OUT_COL_F32 || MODE == OUT_COL_F32_ADD) {
+        for (int ch = 0; ch < BN / 32; ch++) {
+          float v[32];
+          tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
+          const int c0 = n0 + ch * 32;
+          if (c0 >= out.N) break;
           if (r < out.M) {
-            float* dst = out.f + (long(plane) * out.N + c0) * out.ldo + r;
+            float* __restrict__ dst = out.f + (long(plane) * out.N + c0) * out.ldo + r;
+            if (MODE == OUT_COL_F32_ADD) {
+              float old[32];
 #pragma unroll
-            for (int t = 0; t < 32; t++)
-              if (c0 + t < out.N) {
-                if (MODE == OUT_COL_F32_ADD) dst[long(t) * out.ldo] += v[t];
-                else dst[long(t) * out.ldo] = v[t];
-              }
-          }
-        } else if (r < out.M) {
-          const long base = (long(plane) * out.M + r) * out.ldo + c0;
-          if (MODE == OUT_ROW_F32) {
-            float* dst = out.f + base;
+              for (int t = 0; t < 32; t++) old[t] = (c0 + t < out.N) ? dst[long(t) * out.ldo] : 0.f;
 #pragma unroll
-            for (int t = 0; t < 32; t++)
-              if (c0 + t < out.N) dst[t] = v[t];
-          } else {
-            __align__(16) __nv_bfloat16 h[32], l[32];
-#pragma unroll
-            for (int t = 0; t < 32; t++) tc::split_bf16(v[t], h[t], l[t]);
-            if (c0 + 32 <= out.ldo) {  // whole 64-byte rows fit in the padded pitch
-              uint4* dh = reinterpret_cast<uint4*>(out.hi + base);
-              uint4* dl = reinterpret_cast<uint4*>(out.lo + base);
-#pragma unroll
-              for (int t = 0; t < 4; t++) {
-                dh[t] = reinterpret_cast<const uint4*>(h)[t];
-                dl[t] = reinterpret_cast<const uint4*>(l)[t];
-              }
+              for (int t = 0; t < 32; t++)
+                if (c0 + t < out.N) dst[long(t) * out.ldo] = old[t] + v[t];
             } else {
-              for (int t = 0; t < 32 && c0 + t < out.ldo; t++) {
-                out.hi[base + t] = h[t];
-                out.lo[base + t] = l[t];
-              }
+#pragma unroll
+              for (int t = 0; t < 32; t++)
+                if (c0 + t < out.N) dst[long(t) * out.ldo] = v[t];
+            }
+          }
+        }
+      }
+    } else {
+      // columns are the output's fastest index: stage the 128 x 128 tile in the drained pipeline ring (all TMA
+      // writes and MMA reads of it are complete once the accumulator barrier has fired), then write whole rows
+      constexpr int LDS = BN + 1;
+      float* stage = reinterpret_cast<float*>(smem);
+      if (ok) {
+#pragma unroll 1
+        for (int ch = 0; ch < BN / 32; ch++) {
+          float v[32];
+          tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
+          float* srow = stage + (q * 32 + lane) * LDS + ch * 32;
+#pragma unroll
+          for (int t = 0; t < 32; t++) srow[t] = v[t];
+        }
+      }
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
+      if (ok) {
+        const int ew = warp - 2;
+#pragma unroll 1
+        for (int rr = ew; rr < BM; rr += 4) {
+          const int r = m0 + rr;
+          if (r >= out.M) break;
+          const long base = (long(plane) * out.M + r) * out.ldo + n0;
+#pragma unroll
+          for (int s4 = 0; s4 < BN / 32; s4++) {
+            const int c = s4 * 32 + lane;
+            const float val = stage[rr * LDS + c];
+            if (MODE == OUT_ROW_F32) {
+              if (n0 + c < out.N) out.f[base + c] = val;
+            } else if (n0 + c < out.ldo) {
+              __nv_bfloat16 h, l;
+              tc::split_bf16(val, h, l);
+              out.hi[base + c] = h;
+              out.lo[base + c] = l;
             }
           }
         }
@@ -226,8 +246,9 @@ template <int NZ>
 __global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
                                                 const double* __restrict__ low, const float* __restrict__ T2,
                                                 __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo) {
-  __shared__ float tile[8][33];
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  constexpr int KC = 16;  // levels per transpose chunk
+  __shared__ float tile[KC][8][33];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
   const int l = blockIdx.x * 32 + tx, m = blockIdx.y * 8 + ty;
   const bool act = l < nxp && m < nyp;
   const bool lowm = l < 2 && m < 2;
@@ -236,14 +257,17 @@ __global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const
   if (act && !lowm) {
     const float shift = __ldg(lam + l) + __ldg(lam + nxp + m);
     const float* h = T2 + long(m) * nxp + l;
+    float rhs[NZ];
+#pragma unroll
+    for (int k = 0; k < NZ; k++) rhs[k] = __ldg(h + sxy * k);  // all loads issued up front
     float cp[NZ];
     float cprev = 0.f, dprev = 0.f;
 #pragma unroll
     for (int k = 0; k < NZ; k++) {
       const float4 o = __ldg(zop + k);
-      const float den = o.z + shift * o.w - o.x * cprev;
-      cprev = o.y / den;
-      dprev = (__ldg(h + sxy * k) - o.x * dprev) / den;
+      const float rd = __frcp_rn(o.z + shift * o.w - o.x * cprev);
+      cprev = o.y * rd;
+      dprev = (rhs[k] - o.x * dprev) * rd;
       cp[k] = cprev;
       x[k] = dprev;
     }
@@ -269,19 +293,25 @@ __global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const
 #pragma unroll
     for (int k = 0; k < NZ; k++) x[k] = 0.f;
   }
-  // transposed store: per level, 32 (l) rows of 8 consecutive m
-  const int lo_l = blockIdx.x * 32 + threadIdx.x;
+  // transposed store, KC levels at a time: every thread then writes 8 consecutive m of one (level, l) row
 #pragma unroll
-  for (int k = 0; k < NZ; k++) {
-    tile[ty][tx] = x[k];
+  for (int kc = 0; kc < NZ; kc += KC) {
+#pragma unroll
+    for (int kk = 0; kk < KC; kk++)
+      if (kc + kk < NZ) tile[kk][ty][tx] = x[kc + kk];
     __syncthreads();
-    if (ty == 0 && lo_l < nxp) {
-      __align__(16) __nv_bfloat16 h8[8], l8[8];
+    const int nkc = NZ - kc < KC ? NZ - kc : KC;
+    for (int t = tid; t < nkc * 32; t += 256) {
+      const int kk = t >> 5, lx = t & 31;
+      const int ll = blockIdx.x * 32 + lx;
+      if (ll < nxp) {
+        __align__(16) __nv_bfloat16 h8[8], l8[8];
 #pragma unroll
-      for (int t = 0; t < 8; t++) tc::split_bf16(tile[t][tx], h8[t], l8[t]);
-      const long o = (long(k) * nxp + lo_l) * ldy + blockIdx.y * 8;
-      *reinterpret_cast<uint4*>(ohi + o) = *reinterpret_cast<const uint4*>(h8);
-      *reinterpret_cast<uint4*>(olo + o) = *reinterpret_cast<const uint4*>(l8);
+        for (int u = 0; u < 8; u++) tc::split_bf16(tile[kk][u][lx], h8[u], l8[u]);
+        const long o = (long(kc + kk) * nxp + ll) * ldy + blockIdx.y * 8;
+        *reinterpret_cast<uint4*>(ohi + o) = *reinterpret_cast<const uint4*>(h8);
+        *reinterpret_cast<uint4*>(olo + o) = *reinterpret_cast<const uint4*>(l8);
+      }
     }
     __syncthreads();
   }
