@@ -30,6 +30,13 @@ __device__ __forceinline__ float tgtQv(const float* B, const Grid& g, float dz, 
   float z = (float(k) + 0.5f) * dz;
   return bsA(B, g.nz, k).y * (1.f - A.z * tprof(z, A.w));
 }
+// with no boundary air masses (LSF over zero boundaries gives lsfA = (0, 100, 0, 100), lsfB = (0, 0, 100, 0) and
+// phi_t = +-0), every target expression below reduces exactly to the base state: x + 0 * t == x, qv0 * (1 - 0 * t)
+// == qv0, and +-0 differences of phi_t change nothing. The BND = false instantiations skip those loads.
+template <bool BND>
+__device__ __forceinline__ float tgtUb(const Fields& F, const Grid& g, float dz, int i, int j, int k);
+template <bool BND>
+__device__ __forceinline__ float tgtVb(const Fields& F, const Grid& g, float dz, int i, int j, int k);
 __device__ __forceinline__ float tgtU(const Fields& F, const Grid& g, float dz, int i, int j, int k) {
   float z = (float(k) + 0.5f) * dz;
   float4 a = l2d(F.lsfB, g, i - 1, j), b = l2d(F.lsfB, g, i, j);
@@ -40,6 +47,15 @@ __device__ __forceinline__ float tgtV(const Fields& F, const Grid& g, float dz, 
   float4 a = l2d(F.lsfB, g, i, j - 1), b = l2d(F.lsfB, g, i, j);
   return bsB(F.B, g.nz, k).w + 0.5f * (a.y * tprof(z, a.z) + b.y * tprof(z, b.z));
 }
+
+template <>
+__device__ __forceinline__ float tgtUb<true>(const Fields& F, const Grid& g, float dz, int i, int j, int k) { return tgtU(F, g, dz, i, j, k); }
+template <>
+__device__ __forceinline__ float tgtUb<false>(const Fields& F, const Grid& g, float, int, int, int k) { return bsB(F.B, g.nz, k).z; }
+template <>
+__device__ __forceinline__ float tgtVb<true>(const Fields& F, const Grid& g, float dz, int i, int j, int k) { return tgtV(F, g, dz, i, j, k); }
+template <>
+__device__ __forceinline__ float tgtVb<false>(const Fields& F, const Grid& g, float, int, int, int k) { return bsB(F.B, g.nz, k).w; }
 
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_LSF (model.js:142-244): per column, target anomalies of the boundaries' air masses + hydrostatic phi_t
@@ -625,14 +641,26 @@ __device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
 }
 
 // one texel of the physics pass; returns whether the cell's new state holds a hydrometeor
+// CL: clamp neighbour indices to the box (edge blocks); interior blocks index without clamps, which reads the same
+// texels. BND: boundary air masses present (else the target state is the base state, see tgtUb).
+template <bool CL, bool BND>
 __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
   bool hyd = false;
   const float* __restrict__ Vin[4] = {F.V[1 - par][0], F.V[1 - par][1], F.V[1 - par][2], F.V[1 - par][3]};
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  auto L = [&](int ch, int a, int b, int c) { return __ldg(Vin[ch] + g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz))); };
-  auto LQ = [&](int ch, int a, int b, int c) { return __ldg(F.Q[1][ch] + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
-  auto LA = [&](int ch, int a, int b, int c) { return __ldg(F.aux[ch] + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
-  auto LP = [&](int a, int b, int c) { return __ldg(F.phT + g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1))); };
+  auto L = [&](int ch, int a, int b, int c) {
+    return __ldg(Vin[ch] + (CL ? g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz)) : g.at(a, b, c)));
+  };
+  auto LQ = [&](int ch, int a, int b, int c) {
+    return __ldg(F.Q[1][ch] + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
+  };
+  auto LA = [&](int ch, int a, int b, int c) {
+    return __ldg(F.aux[ch] + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
+  };
+  auto LP = [&](int a, int b, int c) {
+    if (!BND) return 0.f;
+    return __ldg(F.phT + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
+  };
   const float dx = U.dims.w, dz = U.dzv.x, dt = U.step.x;
   const int o = g.at(ci, cj, ck);
   float V[4];
@@ -654,10 +682,10 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     const float nux = 0.5f * (LA(0, ci - 1, cj, ck) + LA(0, ci, cj, ck)) + U.turb.y;
     const float nuy = 0.5f * (LA(1, ci - 1, cj, ck) + LA(1, ci, cj, ck)) + U.turb.y;
     float du = nux * lapH(0, V[0]) * ix2 + nuy * lapZp(0, V[0], ck == 0, ck == nz - 1) * iz2;
-    const float ut = tgtU(F, g, dz, ci, cj, ck);
+    const float ut = tgtUb<BND>(F, g, dz, ci, cj, ck);
     const float vbar = 0.25f * (L(1, ci - 1, cj, ck) + V[1] + L(1, ci - 1, cj + 1, ck) + L(1, ci, cj + 1, ck));
-    const float vtb = 0.5f * (tgtV(F, g, dz, ci - 1, cj, ck) + tgtV(F, g, dz, ci, cj + 1, ck));
-    const float nw = 0.5f * (l2d(F.lsfB, g, ci - 1, cj).w + l2d(F.lsfB, g, ci, cj).w);
+    const float vtb = 0.5f * (tgtVb<BND>(F, g, dz, ci - 1, cj, ck) + tgtVb<BND>(F, g, dz, ci, cj + 1, ck));
+    const float nw = BND ? 0.5f * (l2d(F.lsfB, g, ci - 1, cj).w + l2d(F.lsfB, g, ci, cj).w) : 0.f;
     du += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (ut - V[0]);
     du += fc * (vbar - vtb);
     if (ci > 0 && ci < nx) du -= (LP(ci, cj, ck) - LP(ci - 1, cj, ck)) / dx;
@@ -673,10 +701,10 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     const float nux = 0.5f * (LA(0, ci, cj - 1, ck) + LA(0, ci, cj, ck)) + U.turb.y;
     const float nuy = 0.5f * (LA(1, ci, cj - 1, ck) + LA(1, ci, cj, ck)) + U.turb.y;
     float dv = nux * lapH(1, V[1]) * ix2 + nuy * lapZp(1, V[1], ck == 0, ck == nz - 1) * iz2;
-    const float vt = tgtV(F, g, dz, ci, cj, ck);
+    const float vt = tgtVb<BND>(F, g, dz, ci, cj, ck);
     const float ubar = 0.25f * (L(0, ci, cj - 1, ck) + V[0] + L(0, ci + 1, cj - 1, ck) + L(0, ci + 1, cj, ck));
-    const float utb = 0.5f * (tgtU(F, g, dz, ci, cj - 1, ck) + tgtU(F, g, dz, ci + 1, cj, ck));
-    const float nw = 0.5f * (l2d(F.lsfB, g, ci, cj - 1).w + l2d(F.lsfB, g, ci, cj).w);
+    const float utb = 0.5f * (tgtUb<BND>(F, g, dz, ci, cj - 1, ck) + tgtUb<BND>(F, g, dz, ci + 1, cj, ck));
+    const float nw = BND ? 0.5f * (l2d(F.lsfB, g, ci, cj - 1).w + l2d(F.lsfB, g, ci, cj).w) : 0.f;
     dv += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (vt - V[1]);
     dv -= fc * (ubar - utb);
     if (cj > 0 && cj < ny) dv -= (LP(ci, cj, ck) - LP(ci, cj - 1, ck)) / dx;
@@ -714,9 +742,9 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   if (ci < nx && cj < ny && ck < nz) {
     const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx, z = (float(ck) + 0.5f) * dz;
     const float4 A = bsA(F.B, nz, ck), Bb = bsB(F.B, nz, ck);
-    const float4 LAv = l2d(F.lsfA, g, ci, cj);
-    const float nw = l2d(F.lsfB, g, ci, cj).w;
-    const float tth = tgtTh(F.B, g, dz, LAv, ck), tqv = tgtQv(F.B, g, dz, LAv, ck);
+    const float4 LAv = BND ? l2d(F.lsfA, g, ci, cj) : make_float4(0.f, 100.f, 0.f, 100.f);
+    const float nw = BND ? l2d(F.lsfB, g, ci, cj).w : 0.f;
+    const float tth = BND ? tgtTh(F.B, g, dz, LAv, ck) : A.x, tqv = BND ? tgtQv(F.B, g, dz, LAv, ck) : A.y;
     const float sl = spongeLat(U, g, xmx, xmy);
     const float relax = sl + nw * nudR;
     const float nux = LA(0, ci, cj, ck) * 3.f + U.turb.y, nuy = LA(1, ci, cj, ck) * 3.f + U.turb.y;
@@ -913,7 +941,15 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
 __global__ void __launch_bounds__(128) k_phys(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   bool hyd = false;
-  if (ci <= g.nx && cj <= g.ny && ck <= g.nz) hyd = phys_texel(g, U, F, par, ci, cj, ck);
+  // interior block: every texel's +-1 neighbours of every field lie inside the cell box (1 <= i <= nx - 2 etc.)
+  const int bx0 = blockIdx.x * blockDim.x, by0 = blockIdx.y * blockDim.y;
+  const bool interior = bx0 >= 1 && bx0 + int(blockDim.x) - 1 <= g.nx - 2 && by0 >= 1 && by0 + int(blockDim.y) - 1 <= g.ny - 2 &&
+                        ck >= 1 && ck <= g.nz - 2;
+  const bool bnd = U.cor.z > 0.5f;
+  if (ci <= g.nx && cj <= g.ny && ck <= g.nz) {
+    if (interior) hyd = bnd ? phys_texel<false, true>(g, U, F, par, ci, cj, ck) : phys_texel<false, false>(g, U, F, par, ci, cj, ck);
+    else hyd = bnd ? phys_texel<true, true>(g, U, F, par, ci, cj, ck) : phys_texel<true, false>(g, U, F, par, ci, cj, ck);
+  }
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && ck < g.nz)
