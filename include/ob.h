@@ -139,6 +139,47 @@ int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void
  * bracketed by CUDA events; no counterpart in the reference */
 int ob_poisson_time(ObPoisson* p, int reps, float* ms);
 
+/* ---- RadarSim (radar.js:271-413): virtual WSR-88D gate sampling ----
+ * The host keeps RadarSim's VCP tables, volume layout and scan scheduling (radar.js:289-392); the library owns each
+ * radar's device buffers and runs the cut (WGSL_R_CUT, radar.js:80-241) and PhiDP (WGSL_R_PHI, radar.js:243-268)
+ * kernels on the model's stream, sampling the model's current state. */
+#define OB_RADAR_MAX_RADIALS 720      /* super-resolution cuts (radar.js:300) */
+#define OB_RADAR_MAX_TORNADOES 64     /* radar.js:282 */
+#define OB_RADAR_TORNADO_FLOATS 8     /* x, y, core radius, Vmax, debris top, debris dBZ, debris 0-1, 0 (radar.js:283) */
+/* one cut's uniform block RU (radar.js:36-39, filled by encCut radar.js:369-384); angles in radians unless noted */
+typedef struct ObRadarCut {
+  float site[4];   /* model x, model y, antenna height MSL (m), ke * earth radius (m) */
+  float geo[4];    /* lat0, lon0 of the projection, site lat, site lon */
+  float cut[4];    /* elevation, first azimuth (deg), azimuth step (deg), radials */
+  float gates[4];  /* REF gates, Doppler gates, first gate (m), gate spacing (m) */
+  float nyq[4];    /* Nyquist (m/s), time (s), noise seed, system PhiDP (deg) */
+  float offA[4];   /* u32 word offsets in the volume of REF, VEL, SW, ZDR */
+  float offB[4];   /* word offsets of PHI, RHO; unused; moment mask (REF 1, VEL 2, SW 4, ZDR 8, PHI 16, RHO 32) */
+  float mdl[4];    /* nx, ny, nz, dx */
+  float mdl2[4];   /* dz, ground MSL, domain x0, domain y0 (projected metres of the model's (0, 0) corner) */
+  float phys[4];   /* rho at the ground, echo floor (dBZ), microphysics (0 Lin, 1 Thompson), tornadoes in use */
+  float phys2[4];  /* maritime graupel (hurricane mode) 0/1, unused x3 */
+} ObRadarCut;
+typedef struct ObRadar ObRadar;
+/* replaces the buffers addRadar creates (radar.js:313-316): a volume of volume_bytes (every cut's moments, one
+ * byte per gate, radial-major) and the KDP scratch for up to OB_RADAR_MAX_RADIALS x ng_dop gates */
+int ob_radar_create(ObModel* m, size_t volume_bytes, int ng_dop, ObRadar** out);
+/* replaces RadarSim.destroy (radar.js:336-340) for one radar */
+int ob_radar_destroy(ObRadar* r);
+/* replaces setTornadoes (radar.js:280-286): n x OB_RADAR_TORNADO_FLOATS, the first 64 are kept */
+int ob_radar_set_tornadoes(ObRadar* r, const float* tor, int n);
+/* replaces encCut's dispatches (radar.js:385-390): samples one cut of the model's current state into the volume,
+ * on the model's stream. Rejects (OB_ERR_INVALID) cuts whose moments would fall outside the volume. */
+int ob_radar_cut(ObRadar* r, const ObRadarCut* cut);
+/* replaces the volume's copyBufferToBuffer + mapAsync readback (radar.js:360-363, 394-401): the first bytes of the
+ * volume into a caller buffer, after the queued cuts finish */
+int ob_radar_read(ObRadar* r, void* host, size_t bytes);
+/* diagnostics, no counterpart in the reference: the same cut, also returning per gate the moments it quantised
+ * (dBZ, Vr, SW, ZDR, rho_hv, KDP; NaN where the gate or moment is empty), radials x REF gates x 6 floats; and the
+ * KDP scratch of the last cut (radials x Doppler gates, -1 for empty gates) */
+int ob_radar_cut_moments(ObRadar* r, const ObRadarCut* cut, float* host, size_t count);
+int ob_radar_kdp(ObRadar* r, float* host, size_t count);
+
 /* ---- diagnostics ----
  * One bf16x3 tensor-core transform as used by the precision-1 solve: C[p] = A * B[p]^T for p < planes, with
  * A[M][K], B[planes][N][K], C[planes][M][N] fp32 host arrays (K a multiple of 8). No counterpart in the reference

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -370,13 +371,13 @@ template <class R> struct Model {
   // linear sampler, clamp-to-edge, coordinates in texel units (texel i centred at x = i)
   R sampleV(const std::vector<R>& t, R x, R y, R z, int ch) const { return sample(t, VX(), VY(), VZ(), x, y, z, ch); }
   R sampleQ(const std::vector<R>& t, R x, R y, R z, int ch) const { return sample(t, nx, ny, nz, x, y, z, ch); }
-  R sample(const std::vector<R>& t, int X, int Y, int Z, R x, R y, R z, int ch) const {
+  R sample(const std::vector<R>& t, int X, int Y, int Z, R x, R y, R z, int ch, int nch = 4) const {
     R fx = std::floor(x), fy = std::floor(y), fz = std::floor(z);
     int i0 = int(fx), j0 = int(fy), k0 = int(fz);
     R ax = x - fx, ay = y - fy, az = z - fz;
     int i1 = clampi(i0 + 1, 0, X - 1), j1 = clampi(j0 + 1, 0, Y - 1), k1 = clampi(k0 + 1, 0, Z - 1);
     i0 = clampi(i0, 0, X - 1); j0 = clampi(j0, 0, Y - 1); k0 = clampi(k0, 0, Z - 1);
-    auto at = [&](int i, int j, int k) { return t[((size_t(k) * Y + j) * X + i) * 4 + ch]; };
+    auto at = [&](int i, int j, int k) { return t[((size_t(k) * Y + j) * X + i) * nch + ch]; };
     R c00 = at(i0, j0, k0) * (R(1) - ax) + at(i1, j0, k0) * ax;
     R c10 = at(i0, j1, k0) * (R(1) - ax) + at(i1, j1, k0) * ax;
     R c01 = at(i0, j0, k1) * (R(1) - ax) + at(i1, j0, k1) * ax;
@@ -1250,6 +1251,250 @@ template <class R> struct Model {
   }
 };
 
+
+// ---------------------------------------------------------------------------------------------------------------
+// Virtual radar (radar.js:41-268): WGSL_R_CUT's gate moments and Level II codes, WGSL_R_PHI's sequential PhiDP.
+// U is the cut's uniform block (radar.js:36-39, 11 vec4 = 44 floats, the layout of ObRadarCut in ob.h):
+//   site, geo, cut, gates, nyq, offA, offB, mdl, mdl2, phys, phys2.
+// Sampling uses the model's current state V[parity], Q1/Q2 slot 0 and aux, as RadarSim.makeBind binds them
+// (radar.js:331-336); textureSampleLevel with normalised coordinates becomes a texel-unit lerp (texel i at x = i).
+// ---------------------------------------------------------------------------------------------------------------
+template <class R> struct RadarCut {
+  const Model<R>& M;
+  R U[44];
+  const float* tor;
+  explicit RadarCut(const Model<R>& m, const float* u, const float* t) : M(m), tor(t) {
+    for (int i = 0; i < 44; i++) U[i] = R(u[i]);
+  }
+  R u(int v, int c) const { return U[v * 4 + c]; }  // vec4 v, component c
+  enum { SITE, GEO, CUT, GATES, NYQ, OFFA, OFFB, MDL, MDL2, PHYS, PHYS2 };
+  static R sq(R x) { return x * x; }
+  static R db2lin(R d) { return std::pow(R(10), R(0.1) * d); }
+  // great-circle destination (bearing a, ground distance s) -> model metres (radar.js:51-64)
+  void gatePos(R a, R s, R& x, R& y) const {
+    const R RE = R(6371000.0);
+    R p1 = u(GEO, 2), l1 = u(GEO, 3), d = s / RE;
+    R sp2 = std::sin(p1) * std::cos(d) + std::cos(p1) * std::sin(d) * std::cos(a);
+    R p2 = std::asin(clampv(sp2, R(-1), R(1)));
+    R l2 = l1 + std::atan2(std::sin(a) * std::sin(d) * std::cos(p1), std::cos(d) - std::sin(p1) * sp2);
+    R p0 = u(GEO, 0), dl = l2 - u(GEO, 1);
+    R cc = clampv(std::sin(p0) * std::sin(p2) + std::cos(p0) * std::cos(p2) * std::cos(dl), R(-1), R(1));
+    R c = std::acos(cc);
+    R k = c < R(1e-6) ? R(1) : c / std::sin(c);
+    x = RE * k * std::cos(p2) * std::sin(dl) - u(MDL2, 2);
+    y = RE * k * (std::cos(p0) * std::sin(p2) - std::sin(p0) * std::cos(p2) * std::cos(dl)) - u(MDL2, 3);
+  }
+  // 4/3-earth beam: height above the antenna and ground distance at slant range r (radar.js:66-72)
+  void beam(R r, R el, R& h, R& s) const {
+    R a = u(SITE, 3);
+    R q = r * r + R(2) * r * a * std::sin(el);
+    h = q / (std::sqrt(q + a * a) + a);
+    s = a * std::asin(clampv(r * std::cos(el) / (a + h), R(-1), R(1)));
+  }
+  struct Smp { R zr, zs, zg, vt, u[3], T, qr, rho, nu, inside, lr; };
+  // radar.js:89-139
+  Smp sample(R px, R py, R z) const {
+    Smp o{};
+    const R n[3] = {u(MDL, 0), u(MDL, 1), u(MDL, 2)};
+    const R dx = u(MDL, 3), dz = u(MDL2, 0);
+    const R g[3] = {px / dx, py / dx, z / dz};
+    o.inside = (g[0] >= 0 && g[1] >= 0 && g[2] >= 0 && g[0] <= n[0] && g[1] <= n[1] && g[2] <= n[2] && z >= 0) ? R(1) : R(0);
+    R gc[3];
+    for (int c = 0; c < 3; c++) gc[c] = clampv(g[c], R(0), n[c]);
+    const std::vector<R>& Vs = M.V[M.parity];
+    auto q1 = [&](int ch) { return M.sampleQ(M.Q1[0], gc[0] - R(0.5), gc[1] - R(0.5), gc[2] - R(0.5), ch); };
+    auto q2 = [&](int ch) { return M.sampleQ(M.Q2[0], gc[0] - R(0.5), gc[1] - R(0.5), gc[2] - R(0.5), ch); };
+    const R uu = M.sampleV(Vs, gc[0], gc[1] - R(0.5), gc[2] - R(0.5), 0);
+    const R vv = M.sampleV(Vs, gc[0] - R(0.5), gc[1], gc[2] - R(0.5), 1);
+    const R ww = M.sampleV(Vs, gc[0] - R(0.5), gc[1] - R(0.5), gc[2], 2);
+    const R th = M.sampleV(Vs, gc[0] - R(0.5), gc[1] - R(0.5), gc[2] - R(0.5), 3);
+    const int k = int(clampv(std::floor(gc[2]), R(0), n[2] - R(1)));
+    const R* A = M.bsA(k);
+    const R* B = M.bsB(k);
+    const R rho = A[2], T = th * B[0];
+    const R qr = std::max(q1(3), R(0)), qs = std::max(q2(0), R(0)), qg = std::max(q2(1), R(0));
+    o.zr = R(3.63e9) * std::pow(rho * qr, R(1.75));
+    o.zs = R(9.80e8) * std::pow(rho * qs, R(1.75)) * R(0.224) * R(4.0);
+    o.zg = (T < R(273.15) ? R(1.2e10) : R(4.33e10)) * std::pow(rho * qg, R(1.75));
+    const R sqv = std::sqrt(u(PHYS, 0) / rho);
+    R vr = std::min(R(36.34) * std::pow(std::max(R(0.001) * rho * qr, R(0)), R(0.1364)) * sqv, R(10) * sqv);
+    const R vs = clampv(R(1.1) * std::pow(std::max(R(1000) * rho * qs, R(1e-6)), R(0.11)), R(0.3), R(2.2)) * sqv;
+    R vg = clampv(R(9) * std::pow(std::max(R(1000) * rho * qg, R(1e-6)), R(0.42)), R(1), R(55)) * sqv;
+    const R rr = qg / R(0.009);
+    vg = std::min(vg * (R(1) + rr * rr), R(65));
+    if (u(PHYS2, 0) > R(0.5) && u(PHYS, 2) < R(0.5)) {
+      o.zg = (T < R(273.15) ? R(1.3e9) : R(1.0e10)) * std::pow(rho * qg, R(1.75));
+      vg = clampv(R(5) * std::pow(std::max(R(1000) * rho * qg, R(1e-6)), R(0.25)), R(1), R(9)) * sqv;
+    }
+    o.lr = std::pow(R(3.14159 * 1000.0 * 8e6) / std::max(rho * qr, R(1e-9)), R(0.25));
+    if (u(PHYS, 2) > R(0.5)) {
+      const R nr = std::max(q2(2), R(0));
+      if (qr > R(1e-9)) {
+        const R l = clampv(std::pow(R(3.14159 * 1000.0) * std::max(nr, R(1e-3)) / qr, R(0.33333)), R(1000), R(1.0e5));
+        const R nb = qr * l * l * l / R(3141.59);
+        o.zr = R(720e18) * rho * nb / std::pow(l, R(6));
+        o.lr = l;
+        vr = std::min(R(3949) * std::pow(l, R(-0.8)), R(10)) * sqv;
+      } else {
+        o.zr = R(0);
+      }
+      if (qg > R(1e-9)) {
+        const R n0 = clampv(R(200) / (rho * qg), R(1e4), R(3e6));
+        const R l = std::pow(R(3.14159 * 500.0) * n0 / (rho * qg), R(0.25));
+        o.zg = R(720e18) * n0 / std::pow(l, R(7)) * (T < R(273.15) ? R(0.0666) : R(0.24));
+        vg = std::min(R(2483) * std::pow(l, R(-0.89)), R(30)) * sqv;
+      } else {
+        o.zg = R(0);
+      }
+    }
+    const R zt = o.zr + o.zs + o.zg;
+    o.vt = zt > R(1e-6) ? (o.zr * vr + o.zs * vs + o.zg * vg) / zt : R(0);
+    o.u[0] = uu; o.u[1] = vv; o.u[2] = ww;
+    o.T = T; o.qr = qr; o.rho = rho;
+    o.nu = M.sample(M.aux, M.nx, M.ny, M.nz, gc[0] - R(0.5), gc[1] - R(0.5), gc[2] - R(0.5), 0, 2);
+    return o;
+  }
+  // WGSL code(): u32(clamp(round(v*sc + ofs), 2, 255)); WGSL round is half-to-even
+  static uint32_t code(R v, R sc, R ofs) {
+    R t = std::nearbyint(v * sc + ofs);
+    return uint32_t(clampv(t, R(2), R(255)));
+  }
+  // one gate (radar.js:144-227). mom = (dBZ, Vr, SW, ZDR, rho_hv, KDP), NaN where the gate or moment is empty.
+  void gate(int ri, int gi, uint8_t cd[5], R& kdp, R mom[6]) const {
+    for (int i = 0; i < 5; i++) cd[i] = 0;
+    kdp = R(-1);
+    for (int i = 0; i < 6; i++) mom[i] = std::numeric_limits<R>::quiet_NaN();
+    const R r = u(GATES, 2) + u(GATES, 3) * R(gi);
+    const R el = u(CUT, 0);
+    const R az = (u(CUT, 1) + u(CUT, 2) * R(ri)) * R(0.017453293);
+    const R bw = R(0.0165);
+    R hch, hcs;
+    beam(r, el, hch, hcs);
+    R px, py, qx, qy;
+    gatePos(az, hcs, px, py);
+    gatePos(az, hcs + R(200), qx, qy);
+    R ex = qx - px, ey = qy - py;
+    const R el_ = std::sqrt(ex * ex + ey * ey);
+    ex /= el_; ey /= el_;
+    const R zAnt = u(SITE, 2) - u(MDL2, 1);
+    const R zc = zAnt + hch;
+    if (zc > u(MDL, 2) * u(MDL2, 0) - R(200)) return;
+    R hl, hu, tmp;
+    beam(r, el - R(0.4) * bw, hl, tmp);
+    beam(r, el + R(0.4) * bw, hu, tmp);
+    hl += zAnt; hu += zAnt;
+    const Smp s0 = sample(px, py, std::max(zc, R(5))), s1 = sample(px, py, std::max(hl, R(5))), s2 = sample(px, py, std::max(hu, R(5)));
+    if (s0.inside < R(0.5)) return;
+    const R zr = R(0.5) * s0.zr + R(0.25) * (s1.zr + s2.zr), zs = R(0.5) * s0.zs + R(0.25) * (s1.zs + s2.zs);
+    const R zg = R(0.5) * s0.zg + R(0.25) * (s1.zg + s2.zg);
+    const R zmet = zr + zs + zg;
+    R zdeb = 0, dvx = 0, dvy = 0, swt = 0;
+    const R bwm = R(0.5) * r * bw;
+    const int ntor = int(u(PHYS, 3));
+    for (int q = 0; q < ntor; q++) {
+      const float* A = tor + 8 * q;
+      const float* B = A + 4;
+      const R dxv = px - R(A[0]), dyv = py - R(A[1]);
+      const R rt = std::sqrt(dxv * dxv + dyv * dyv);
+      const R Re = std::sqrt(R(A[2]) * R(A[2]) + bwm * bwm + R(125.0 * 125.0));
+      if (rt > R(8) * Re) continue;
+      const R vmx = R(A[3]) * R(A[2]) / Re;
+      const R vt = vmx * (rt < Re ? rt / Re : Re / std::max(rt, R(1)));
+      const R etx = -dyv / std::max(rt, R(1)), ety = dxv / std::max(rt, R(1));
+      const R erx = dxv / std::max(rt, R(1)), ery = dyv / std::max(rt, R(1));
+      const R fz = R(1) - sstep(R(1200), R(3500), zc);
+      dvx += (vt * etx - R(0.25) * vt * erx) * fz;
+      dvy += (vt * ety - R(0.25) * vt * ery) * fz;
+      swt = std::max(swt, vmx * R(0.4) * std::exp(-rt * rt / (R(4) * Re * Re)) * fz);
+      if (B[2] > 0.f && zc < R(B[0])) {
+        const R rd = std::max(R(1.4) * R(A[2]), R(150));
+        zdeb += db2lin(R(B[1])) * std::min(R(1), rd * rd / (Re * Re)) * std::exp(-rt * rt / (Re * Re)) *
+                (R(1) - sstep(R(0.55) * R(B[0]), R(B[0]), zc)) * R(B[2]);
+      }
+    }
+    const R ztot = zmet + zdeb;
+    if (ztot <= R(1e-6)) return;
+    const R dbz = R(10) * std::log(ztot) / R(2.302585);
+    if (dbz < u(PHYS, 1)) return;
+    mom[0] = dbz;
+    cd[0] = uint8_t(code(dbz, R(2), R(66)));
+    if (gi >= int(u(GATES, 1))) return;
+    const R ce = std::cos(el), se = std::sin(el);
+    const R vtf = s0.vt * zmet / ztot;
+    R vr = ((s0.u[0] + dvx) * ex + (s0.u[1] + dvy) * ey) * ce + (s0.u[2] - vtf) * se;
+    const R nyq = u(NYQ, 0);
+    vr = vr - R(2) * nyq * std::floor((vr + nyq) / (R(2) * nyq));
+    mom[1] = vr;
+    cd[1] = uint8_t(code(vr, R(2), R(129)));
+    const R vru = (s2.u[0] * ex + s2.u[1] * ey) * ce, vrl = (s1.u[0] * ex + s1.u[1] * ey) * ce;
+    const R swv = std::sqrt(R(1) + sq(clampv(R(2.5) * std::sqrt(std::max(s0.nu, R(0)) / R(1000)), R(0), R(8))) +
+                            sq((vru - vrl) / R(2.5)) + sq(R(0.15) * s0.vt * se) + sq(swt));
+    mom[2] = std::min(swv, R(19.5));
+    cd[2] = uint8_t(code(mom[2], R(2), R(129)));
+    const R d0 = R(3.67) / s0.lr * R(1000);
+    const bool melt = s0.T > R(273.15);
+    const R zdrR = clampv(R(0.2) + R(1.15) * (d0 - R(0.5)), R(0.1), R(4.8));
+    const R zdrS = melt ? R(1.3) : R(0.3);
+    const R zdrG = melt ? (zg > R(3.2e5) ? R(0) : R(0.7)) : R(0.15);
+    const R zv = zr / db2lin(zdrR) + zs / db2lin(zdrS) + zg / db2lin(zdrG) + zdeb / db2lin(R(0.2));
+    const R zdr = R(10) * std::log(std::max(ztot, R(1e-9)) / std::max(zv, R(1e-9))) / R(2.302585);
+    mom[3] = clampv(zdr, R(-7.9), R(7.9));
+    cd[3] = uint8_t(code(mom[3], R(16), R(128)));
+    const R fr = zr / ztot, fs = zs / ztot, fg = zg / ztot, fd = zdeb / ztot;
+    R cc = fr * (d0 > R(2.5) ? R(0.986) : R(0.995)) + fs * (melt ? R(0.93) : R(0.985)) +
+           fg * (melt ? (zg > R(3.2e5) ? R(0.90) : R(0.94)) : R(0.985)) + fd * R(0.55);
+    cc -= R(0.24) * fr * fg;
+    mom[4] = clampv(cc, R(0.2), R(1.05));
+    cd[4] = uint8_t(code(mom[4], R(300), R(-60.5)));
+    kdp = std::pow(R(0.017) * std::pow(std::max(zr, R(0)), R(0.714)) / R(44), R(1.2165));
+    mom[5] = kdp;
+  }
+  // WGSL_R_CUT main (radar.js:229-240) over every radial, then WGSL_R_PHI (radar.js:243-268). out = the volume's
+  // bytes (codes stored little-endian, 4 per u32 word as the reference packs them); kdp = nrad*ngDop scratch;
+  // mom (optional) = nrad*ngRef*6 moments.
+  void run(uint8_t* out, R* kdp, R* mom) const {
+    const int nrad = int(u(CUT, 3)), ngR = int(u(GATES, 0)), ngD = int(u(GATES, 1));
+    const uint32_t mask = uint32_t(u(OFFB, 3));
+    const size_t oR = size_t(u(OFFA, 0)) * 4, oV = size_t(u(OFFA, 1)) * 4, oS = size_t(u(OFFA, 2)) * 4,
+                 oZ = size_t(u(OFFA, 3)) * 4, oP = size_t(u(OFFB, 0)) * 4, oH = size_t(u(OFFB, 1)) * 4;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int ri = 0; ri < nrad; ri++)
+      for (int gi = 0; gi < ngR; gi++) {
+        uint8_t cd[5];
+        R kd, m6[6];
+        gate(ri, gi, cd, kd, m6);
+        out[oR + size_t(ri) * ngR + gi] = cd[0];
+        if (gi < ngD) {
+          const size_t o = size_t(ri) * ngD + gi;
+          if (mask & 2u) out[oV + o] = cd[1];
+          if (mask & 4u) out[oS + o] = cd[2];
+          if (mask & 8u) out[oZ + o] = cd[3];
+          if (mask & 32u) out[oH + o] = cd[4];
+          kdp[o] = kd;
+        }
+        if (mom)
+          for (int c = 0; c < 6; c++) mom[(size_t(ri) * ngR + gi) * 6 + c] = m6[c];
+      }
+    if (mask & 16u) phi(out + oP, kdp, nrad, ngD);
+  }
+  // WGSL_R_PHI: fp32 accumulation in gate order, 2 * KDP * dr (km), mod 360 (radar.js:251-264)
+  void phi(uint8_t* out, const R* kdp, int nrad, int ng) const {
+    for (int ri = 0; ri < nrad; ri++) {
+      R acc = u(NYQ, 3);
+      for (int gi = 0; gi < (ng / 4) * 4; gi++) {
+        const R kd = kdp[size_t(ri) * ng + gi];
+        uint8_t c = 0;
+        if (kd >= R(0)) {
+          acc += R(2) * kd * u(GATES, 3) * R(0.001);
+          const R ph = acc - R(360) * std::floor(acc / R(360));
+          c = uint8_t(clampv(std::nearbyint(ph * R(253) / R(360) + R(2)), R(2), R(255)));
+        }
+        out[size_t(ri) * ng + gi] = c;
+      }
+    }
+  }
+};
+
 }  // namespace oro
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1389,6 +1634,26 @@ void oro_poisson_apply_f64(int nx, int ny, int nz, double dx, double dz, const d
         double lo = k > 0 ? rhoW[k] * (p - phi[(size_t(k - 1) * ny + j) * nx + i]) : 0.0;
         out[(size_t(k) * ny + j) * nx + i] = rhoC[k] * lh + (up - lo) * iz2;
       }
+}
+
+// one radar cut on the model's current state (radar.js:229-268); out = volume bytes, kdp = nrad*ngDop,
+// mom = nrad*ngRef*6 (may be null); the FP64 model writes double moments into mom64 instead
+void oro_radar_cut(OroModel* m, const float* U, const float* tor, uint8_t* out, float* kdp, float* mom) {
+  oro::Model<float>& M = *m->f;
+  oro::RadarCut<float> rc(M, U, tor);
+  rc.run(out, kdp, mom);
+}
+void oro_radar_cut_f64(OroModel* m, const float* U, const float* tor, uint8_t* out, double* kdp, double* mom) {
+  oro::Model<double>& M = *m->d;
+  oro::RadarCut<double> rc(M, U, tor);
+  rc.run(out, kdp, mom);
+}
+// WGSL code() and the PhiDP accumulation alone, for quantising given moments
+uint32_t oro_radar_code(float v, float sc, float ofs) { return oro::RadarCut<float>::code(v, sc, ofs); }
+void oro_radar_phi(const float* U, const float* kdp, int nrad, int ng, uint8_t* out) {
+  oro::Model<float> dummy;
+  oro::RadarCut<float> rc(dummy, U, nullptr);
+  rc.phi(out, kdp, nrad, ng);
 }
 
 // helpers exposed for known-answer tests

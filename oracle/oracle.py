@@ -80,6 +80,12 @@ def _declare(L):
     L.oro_gnoise2.restype = f
     L.oro_gnoise2.argtypes = [f, f]
     L.oro_dst_matrix.argtypes = [i, dp]
+    u8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+    L.oro_radar_cut.argtypes = [vp, fp, fp, u8, fp, C.c_void_p]
+    L.oro_radar_cut_f64.argtypes = [vp, fp, fp, u8, dp, C.c_void_p]
+    L.oro_radar_code.restype = C.c_uint32
+    L.oro_radar_code.argtypes = [f, f, f]
+    L.oro_radar_phi.argtypes = [fp, fp, i, i, u8]
     L.ob_params_default.argtypes = [C.POINTER(ObParams)]
     L.ob_grid_pad.restype = i
     L.ob_grid_pad.argtypes = [f]
@@ -165,6 +171,36 @@ class OracleModel:
         w, m = C.c_double(), C.c_double()
         lib().oro_budgets(self.h, C.byref(w), C.byref(m))
         return w.value, m.value
+
+    def radar_cut(self, U, tor, volume_bytes, ng_dop, moments=True):
+        """One radar cut on the current state (radar.js:229-268): returns (volume bytes, KDP (nrad, ngDop),
+        moments (nrad, ngRef, 6) or None) in this model's precision."""
+        U = np.ascontiguousarray(U, np.float32).reshape(-1)
+        assert U.size == 44
+        nrad, ngr = int(U[11]), int(U[12])
+        tor = np.ascontiguousarray(tor if tor is not None else np.zeros(8), np.float32).reshape(-1)
+        out = np.zeros(volume_bytes, np.uint8)
+        dt = np.float64 if self.precision == 8 else np.float32
+        kdp = np.zeros(720 * ng_dop, dt)
+        mom = np.zeros(nrad * ngr * 6, dt) if moments else None
+        fn = lib().oro_radar_cut_f64 if self.precision == 8 else lib().oro_radar_cut
+        fn(self.h, U, tor, out, kdp, mom.ctypes.data if moments else None)
+        return out, kdp[:nrad * ng_dop].reshape(nrad, ng_dop), (mom.reshape(nrad, ngr, 6) if moments else None)
+
+
+def radar_code(v, sc, ofs):
+    """WGSL code() of radar.js:140 on fp32 values (vectorised over v)."""
+    v = np.asarray(v, np.float32)
+    return np.array([lib().oro_radar_code(float(x), float(sc), float(ofs)) for x in v.reshape(-1)], np.uint32).reshape(v.shape)
+
+
+def radar_phi(U, kdp):
+    """WGSL_R_PHI (radar.js:243-268) on a given fp32 KDP array (nrad, ng): the PHI codes."""
+    kdp = np.ascontiguousarray(kdp, np.float32)
+    nrad, ng = kdp.shape
+    out = np.zeros(nrad * ng, np.uint8)
+    lib().oro_radar_phi(np.ascontiguousarray(U, np.float32).reshape(-1), kdp.reshape(-1), nrad, ng, out)
+    return out.reshape(nrad, ng)
 
 
 def poisson_solve(rhs, dx, dz, rhoC, rhoW, precision=4):

@@ -16,6 +16,7 @@ OB_OK, OB_ERR_OOM, OB_ERR_INVALID, OB_ERR_DEVICE, OB_ERR_TIMEOUT, OB_ERR_NAN = 0
 FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI, FIELD_RAIN = 0, 1, 2, 3, 4, 5
 BOUNDARY_FLOATS, MAX_BOUNDS, CI_FLOATS, MAX_CI = 148, 8, 12, 256
 OB_STATIC_POISSON_MAX_SIDE, OB_STATIC_POISSON_MAX_NZ, OB_STATIC_POISSON_MAX_CELLS = 256, 512, 1 << 20
+RADAR_MAX_RADIALS, RADAR_MAX_TORNADOES, RADAR_TORNADO_FLOATS = 720, 64, 8
 
 
 class ObError(RuntimeError):
@@ -71,6 +72,13 @@ SYMBOLS = {
     "ob_poisson_time": (_i, [_vp, _i, _fp]),
     "ob_dst_tc_selftest": (_i, [_i, _i, _i, _i, _fp, _fp, _fp]),
     "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),
+    "ob_radar_create": (_i, [_vp, _sz, _i, C.POINTER(_vp)]),
+    "ob_radar_destroy": (_i, [_vp]),
+    "ob_radar_set_tornadoes": (_i, [_vp, _fp, _i]),
+    "ob_radar_cut": (_i, [_vp, _vp]),
+    "ob_radar_read": (_i, [_vp, _vp, _sz]),
+    "ob_radar_cut_moments": (_i, [_vp, _vp, _fp, _sz]),
+    "ob_radar_kdp": (_i, [_vp, _fp, _sz]),
 }
 
 _lib = None

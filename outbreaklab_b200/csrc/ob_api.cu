@@ -13,6 +13,7 @@
 #include "../../include/ob.h"
 #include "ob_common.cuh"
 #include "ob_poisson.cuh"
+#include "ob_radar.cuh"
 #include "ob_step.cuh"
 
 namespace ob {
@@ -619,6 +620,133 @@ int ob_poisson_time(ObPoisson* p, int reps, float* ms) {
 int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void* stream) {
   if (!p || !d_rhs || !d_phi) { set_error("ob_poisson_solve_device: null argument"); return OB_ERR_INVALID; }
   return p->plan.solve(d_rhs, d_phi, stream ? (cudaStream_t)stream : p->stream);
+}
+
+// ---- RadarSim (radar.js:271-413): the device side of one radar ----
+struct ObRadar {
+  ObModel* m = nullptr;
+  uint8_t* d_out = nullptr;  // the volume: every cut's moments, radial-major, one byte per gate (radar.js:298-310)
+  size_t bytes = 0;
+  float* d_kdp = nullptr;    // OB_RADAR_MAX_RADIALS x ng_dop KDP of the cut being sampled (radar.js:316)
+  int ng_dop = 0;
+  float* d_tor = nullptr;    // OB_RADAR_MAX_TORNADOES x 8
+  int ntor = 0;
+  float* d_mom = nullptr;    // moments of the last cut (diagnostic path only)
+  size_t mom_count = 0;
+};
+
+int ob_radar_create(ObModel* m, size_t volume_bytes, int ng_dop, ObRadar** out) {
+  if (!m || !out || volume_bytes == 0 || volume_bytes % 4 != 0 || ng_dop <= 0 || ng_dop % 4 != 0) {
+    set_error("ob_radar_create: bad arguments (volume bytes must be a positive multiple of 4, Doppler gates of 4)");
+    return OB_ERR_INVALID;
+  }
+  *out = nullptr;
+  ObRadar* r = new ObRadar();
+  r->m = m;
+  r->bytes = volume_bytes;
+  r->ng_dop = ng_dop;
+  int rc = cuda_status(cudaMalloc(&r->d_out, volume_bytes), "radar volume");
+  if (rc == OB_OK) rc = cuda_status(cudaMemsetAsync(r->d_out, 0, volume_bytes, m->stream), "radar volume");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&r->d_kdp, size_t(OB_RADAR_MAX_RADIALS) * ng_dop * sizeof(float)), "radar KDP");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&r->d_tor, size_t(OB_RADAR_MAX_TORNADOES) * OB_RADAR_TORNADO_FLOATS * sizeof(float)), "radar tornadoes");
+  if (rc == OB_OK) rc = cuda_status(cudaMemsetAsync(r->d_tor, 0, size_t(OB_RADAR_MAX_TORNADOES) * OB_RADAR_TORNADO_FLOATS * sizeof(float), m->stream), "radar tornadoes");
+  if (rc == OB_OK) rc = cuda_status(cudaStreamSynchronize(m->stream), "radar create");
+  if (rc != OB_OK) {
+    ob_radar_destroy(r);
+    return rc;
+  }
+  *out = r;
+  return OB_OK;
+}
+
+int ob_radar_destroy(ObRadar* r) {
+  if (!r) return OB_OK;
+  if (r->m) cudaStreamSynchronize(r->m->stream);
+  for (void* p : {(void*)r->d_out, (void*)r->d_kdp, (void*)r->d_tor, (void*)r->d_mom})
+    if (p) cudaFree(p);
+  delete r;
+  return OB_OK;
+}
+
+int ob_radar_set_tornadoes(ObRadar* r, const float* tor, int n) {
+  if (!r || n < 0 || (n > 0 && !tor)) { set_error("ob_radar_set_tornadoes: bad arguments"); return OB_ERR_INVALID; }
+  r->ntor = n < OB_RADAR_MAX_TORNADOES ? n : OB_RADAR_MAX_TORNADOES;  // the first 64 (radar.js:282)
+  if (r->ntor) {
+    OB_TRY(cuda_status(cudaMemcpyAsync(r->d_tor, tor, sizeof(float) * OB_RADAR_TORNADO_FLOATS * r->ntor, cudaMemcpyHostToDevice, r->m->stream), "tornadoes"));
+    OB_TRY(cuda_status(cudaStreamSynchronize(r->m->stream), "tornadoes"));
+  }
+  return OB_OK;
+}
+
+// every region the cut writes lies inside the volume, the KDP scratch holds the cut, and the tornado count is set
+static int radar_check(const ObRadar* r, const ObRadarCut* c) {
+  auto whole = [](float v) { return v >= 0.f && v < 16777216.f && float(int(v)) == v; };
+  const float nradf = c->cut[3], ngRf = c->gates[0], ngDf = c->gates[1];
+  if (!whole(nradf) || !whole(ngRf) || !whole(ngDf) || !whole(c->offB[3])) { set_error("ob_radar_cut: radials, gates and mask must be whole numbers"); return OB_ERR_INVALID; }
+  const int nrad = int(nradf), ngR = int(ngRf), ngD = int(ngDf), mask = int(c->offB[3]);
+  if (nrad < 1 || nrad > OB_RADAR_MAX_RADIALS || ngR < 4 || ngR % 4 || ngD < 0 || ngD % 4 || ngD > ngR || ngD > r->ng_dop) {
+    set_error("ob_radar_cut: %d radials x %d REF / %d Doppler gates do not fit this radar (<= %d radials, <= %d Doppler gates, multiples of 4)",
+              nrad, ngR, ngD, OB_RADAR_MAX_RADIALS, r->ng_dop);
+    return OB_ERR_INVALID;
+  }
+  const float offs[6] = {c->offA[0], c->offA[1], c->offA[2], c->offA[3], c->offB[0], c->offB[1]};
+  const int bit[6] = {1, 2, 4, 8, 16, 32};
+  for (int i = 0; i < 6; i++) {
+    if (i > 0 && !(mask & bit[i])) continue;
+    if (!whole(offs[i])) { set_error("ob_radar_cut: moment offsets must be whole word counts"); return OB_ERR_INVALID; }
+    const size_t end = size_t(offs[i]) * 4 + size_t(nrad) * (i == 0 ? ngR : ngD);
+    if (end > r->bytes) { set_error("ob_radar_cut: moment %d ends at byte %zu, past the %zu-byte volume", i, end, r->bytes); return OB_ERR_INVALID; }
+  }
+  if (!whole(c->phys[3]) || int(c->phys[3]) > r->ntor) { set_error("ob_radar_cut: %g tornadoes requested, %d set", double(c->phys[3]), r->ntor); return OB_ERR_INVALID; }
+  if (!(c->gates[3] > 0.f) || !(c->site[3] > 0.f) || !(c->mdl[3] > 0.f) || !(c->mdl2[0] > 0.f) || !(c->nyq[0] > 0.f)) {
+    set_error("ob_radar_cut: gate spacing, earth radius, dx, dz and Nyquist must be positive");
+    return OB_ERR_INVALID;
+  }
+  return OB_OK;
+}
+
+static int radar_launch(ObRadar* r, const ObRadarCut* c, float* d_mom) {
+  RadarU U;
+  static_assert(sizeof(ObRadarCut) == sizeof(RadarU), "ObRadarCut layout");
+  std::memcpy(&U, c, sizeof(U));
+  ObModel* m = r->m;
+  launch_radar_cut(U, m->g, m->F, m->parity, r->d_tor, r->d_out, r->d_kdp, d_mom, m->stream);
+  return cuda_status(cudaGetLastError(), "radar cut launch");
+}
+
+int ob_radar_cut(ObRadar* r, const ObRadarCut* c) {
+  if (!r || !c) { set_error("ob_radar_cut: null argument"); return OB_ERR_INVALID; }
+  OB_TRY(radar_check(r, c));
+  return radar_launch(r, c, nullptr);
+}
+
+int ob_radar_cut_moments(ObRadar* r, const ObRadarCut* c, float* host, size_t count) {
+  if (!r || !c || !host) { set_error("ob_radar_cut_moments: null argument"); return OB_ERR_INVALID; }
+  OB_TRY(radar_check(r, c));
+  const size_t need = size_t(c->cut[3]) * size_t(c->gates[0]) * 6;
+  if (count != need) { set_error("ob_radar_cut_moments: %zu floats, expected %zu", count, need); return OB_ERR_INVALID; }
+  if (r->mom_count < need) {
+    if (r->d_mom) cudaFree(r->d_mom);
+    r->d_mom = nullptr;
+    r->mom_count = 0;
+    OB_TRY(cuda_status(cudaMalloc(&r->d_mom, need * sizeof(float)), "radar moments"));
+    r->mom_count = need;
+  }
+  OB_TRY(radar_launch(r, c, r->d_mom));
+  OB_TRY(cuda_status(cudaMemcpyAsync(host, r->d_mom, need * sizeof(float), cudaMemcpyDeviceToHost, r->m->stream), "radar moments"));
+  return cuda_status(cudaStreamSynchronize(r->m->stream), "radar moments");
+}
+
+int ob_radar_read(ObRadar* r, void* host, size_t bytes) {
+  if (!r || !host || bytes > r->bytes) { set_error("ob_radar_read: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaMemcpyAsync(host, r->d_out, bytes, cudaMemcpyDeviceToHost, r->m->stream), "radar read"));
+  return cuda_status(cudaStreamSynchronize(r->m->stream), "radar read");
+}
+
+int ob_radar_kdp(ObRadar* r, float* host, size_t count) {
+  if (!r || !host || count > size_t(OB_RADAR_MAX_RADIALS) * r->ng_dop) { set_error("ob_radar_kdp: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaMemcpyAsync(host, r->d_kdp, count * sizeof(float), cudaMemcpyDeviceToHost, r->m->stream), "radar KDP"));
+  return cuda_status(cudaStreamSynchronize(r->m->stream), "radar KDP");
 }
 
 }  // extern "C"
