@@ -87,6 +87,9 @@ struct ObModel {
   float* d_qptr = nullptr;
   float* rhs32 = nullptr;  // the fp32 right-hand side buffer (F.rhs points here when a solver reads it)
   unsigned int* d_act = nullptr;  // 4 brick-flag arrays (clear-air skip of the scalar advection)
+  float* d_tab = nullptr;          // sponge tables of the physics pass (Fields::spz/slx/sly)
+  float tab_key[8] = {};           // the uniforms the tables were made from; NaN = never made
+  unsigned tab_gen = ~0u, base_gen = 0;  // base-state version the tables saw / current
   PoissonPlan solver;
   std::vector<float> Bh;
   double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
@@ -110,7 +113,7 @@ static void model_bind_solver(ObModel* m) {
 static void model_free(ObModel* m) {
   if (!m) return;
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -143,6 +146,16 @@ static void write_uniforms(ObModel* m, double dt) {
   U.vtx2 = v4(1, 0, 0, 0);
   U.pad = v4(m->g.pad, m->g.nxp, m->g.nyp, 0);
   U.dzv = v4(m->dz, 1 / m->dx, 1 / m->dz, P.mcFloor);
+  // the same float expressions the kernels would evaluate per thread, once on the host (IEEE float arithmetic)
+  const float fdt = U.step.x, fdx = U.dims.w, fdz = U.dzv.x;
+  U.der = make_float4(fdt / fdx, fdt / fdz, 1.f / (fdx * fdx), 1.f / (fdz * fdz));
+  // sponge tables, remade when a uniform they read or the base state changed
+  const float key[8] = {U.sponge.x, U.sponge.y, U.sponge.z, U.sponge.w, U.step.z, fdx, fdz, 0.f};
+  if (m->tab_gen != m->base_gen || std::memcmp(key, m->tab_key, sizeof(key)) != 0) {
+    launch_tables(m->g, U, m->F, m->stream);
+    std::memcpy(m->tab_key, key, sizeof(key));
+    m->tab_gen = m->base_gen;
+  }
 }
 
 extern "C" {
@@ -218,6 +231,8 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   const int nbx = (nx + 31) / 32, nby = (ny + 3) / 4;
   const size_t nbr = size_t(nbx) * nby * nz;
   alloc((void**)&m->d_act, 4 * nbr * sizeof(unsigned int), "activity flags");
+  const size_t ntab = size_t(4) * (nz + 1) + 2 * size_t(nx + 1) + 2 * size_t(ny + 1);
+  alloc((void**)&m->d_tab, ntab * sizeof(float), "sponge tables");
   // the refined bf16x3 tensor-core solve where its tridiagonal kernel is specialised, else fp32
   const int prec = (nz == 16 || nz == 40 || nz == 80) ? 2 : 0;
   if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, prec);
@@ -257,6 +272,9 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->F.zeroQt = m->d_act + 2 * nbr;
   m->F.zeroQ1 = m->d_act + 3 * nbr;
   m->F.fallmax = 100.f;
+  m->F.spz = m->d_tab;                      // 4 floats per level: 16-byte aligned
+  m->F.slx = m->d_tab + 4 * (nz + 1);       // 2 floats per column: 8-byte aligned
+  m->F.sly = m->F.slx + 2 * (nx + 1);
   cudaMemcpy(m->d_qptr, m->F.Q[0], 8 * sizeof(float*), cudaMemcpyHostToDevice);
   // a neutral base state until one is set
   m->Bh.assign(size_t(nz + 1) * 8, 0.f);
@@ -280,6 +298,7 @@ int ob_model_set_base_state(ObModel* m, const float* B, int nz) {
   if (!m || !B || nz != m->g.nz) { set_error("ob_model_set_base_state: expected nz = %d", m ? m->g.nz : -1); return OB_ERR_INVALID; }
   m->Bh.assign(B, B + size_t(nz + 1) * 8);
   m->rhoSfc = B[2];
+  m->base_gen++;
   {
     // the largest fall speed any hydrometeor can reach (model.js:63-99): rain <= 10, snow <= 2.2, Thompson graupel
     // <= 25 m/s, each times sqrt(rho_sfc / rho), Lin graupel <= 65 m/s; bounds the vertical reach of a fall trace

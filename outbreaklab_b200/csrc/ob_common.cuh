@@ -18,6 +18,7 @@ namespace ob {
 // uniform block (model.js:23-37), packed on the host per step (model.js:1391-1425)
 struct Uni {
   float4 dims, dzv, step, sponge, turb, micro, misc, cor, ci, pad, micro2, hur, hur2, hur3, hur4, hur5, vtx, vtx2, cn;
+  float4 der;  // derived on the host per step: (dt/dx, dt/dz, 1/dx^2, 1/dz^2), so no thread divides uniforms
 };
 
 struct Grid {
@@ -59,12 +60,20 @@ struct Fields {
   unsigned int* zeroQ1;  // Q slot 1's hydrometeor channels are known to be zero there
   int nbx, nby;
   float fallmax;         // bound on every hydrometeor fall speed of the base state (m/s)
+  // sponge coefficients tabulated once per parameter set (k_tables): spz[2k] = top sponge at the cell centre height
+  // (k + 1/2) dz, spz[2k+1] at the face height k dz; slx[2i] = lateral sponge of the x distance alone at the face
+  // x = i dx, slx[2i+1] at the centre (i + 1/2) dx; sly likewise in y. The lateral sponge of a point is
+  // max(slx, sly): it is a non-increasing function of min(x distance, y distance), so the maximum of the two
+  // one-dimensional values is the same float as the formula applied to the minimum distance.
+  const float* spz;
+  const float* slx;
+  const float* sly;
 };
 
 constexpr float T0K = 273.15f;
 constexpr double CPDd = 1005.7, RVCd = 461.5, LVCd = 2.501e6, LFCd = 3.337e5, LSCd = 2.834e6;
 
-__device__ __forceinline__ int clampi(int x, int a, int b) { return x < a ? a : (x > b ? b : x); }
+__device__ __forceinline__ int clampi(int x, int a, int b) { return min(max(x, a), b); }
 __device__ __forceinline__ float clampf(float x, float a, float b) { return fminf(fmaxf(x, a), b); }
 __device__ __forceinline__ float sstep(float a, float b, float x) {
   float t = clampf((x - a) / (b - a), 0.f, 1.f);
@@ -200,6 +209,24 @@ __device__ __forceinline__ float trilerp(const float* __restrict__ f, const Grid
   float c10 = __ldg(f + r10 + i0) * (1.f - ax) + __ldg(f + r10 + i1) * ax;
   float c01 = __ldg(f + r01 + i0) * (1.f - ax) + __ldg(f + r01 + i1) * ax;
   float c11 = __ldg(f + r11 + i0) * (1.f - ax) + __ldg(f + r11 + i1) * ax;
+  float c0 = c00 * (1.f - ay) + c10 * ay;
+  float c1 = c01 * (1.f - ay) + c11 * ay;
+  return c0 * (1.f - az) + c1 * az;
+}
+
+// the same filter where the trace is already clamped to the box, so that the floor index of every axis lies in
+// [-1, extent - 1]: then max(i0, 0) and min(i0 + 1, extent - 1) are the clamped corners (same texels, fewer bounds)
+__device__ __forceinline__ float trilerpB(const float* __restrict__ f, const Grid& g, int X, int Y, int Z, float x, float y, float z) {
+  const int i0 = __float2int_rd(x), j0 = __float2int_rd(y), k0 = __float2int_rd(z);
+  const float ax = x - float(i0), ay = y - float(j0), az = z - float(k0);
+  const int ia = max(i0, 0), ib = min(i0 + 1, X - 1);
+  const int ja = max(j0, 0), jb = min(j0 + 1, Y - 1);
+  const int ka = max(k0, 0), kb = min(k0 + 1, Z - 1);
+  const int r00 = g.px * (ja + g.py * ka), r10 = g.px * (jb + g.py * ka), r01 = g.px * (ja + g.py * kb), r11 = g.px * (jb + g.py * kb);
+  float c00 = __ldg(f + r00 + ia) * (1.f - ax) + __ldg(f + r00 + ib) * ax;
+  float c10 = __ldg(f + r10 + ia) * (1.f - ax) + __ldg(f + r10 + ib) * ax;
+  float c01 = __ldg(f + r01 + ia) * (1.f - ax) + __ldg(f + r01 + ib) * ax;
+  float c11 = __ldg(f + r11 + ia) * (1.f - ax) + __ldg(f + r11 + ib) * ax;
   float c0 = c00 * (1.f - ay) + c10 * ay;
   float c1 = c01 * (1.f - ay) + c11 * ay;
   return c0 * (1.f - az) + c1 * az;

@@ -4,6 +4,8 @@
 // ob_common.cuh: one thread per texel, x fastest within a warp so that every stencil row is a coalesced 128-byte
 // read, neighbours served from L1/L2. Semi-Lagrangian sampling is a software trilinear filter in fp32 (exact
 // weights; WebGPU's hardware filter uses low-precision fixed-point weights, which are not reproduced).
+#include <algorithm>
+
 #include "ob_common.cuh"
 #include "ob_step.cuh"
 
@@ -218,26 +220,32 @@ __global__ void k_init(Grid g, Uni U, Fields F) {
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void k_nut(Grid g, Uni U, Fields F, int par) {
   OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
-  const float* __restrict__ u = F.V[par][0];
-  const float* __restrict__ v = F.V[par][1];
-  const float* __restrict__ w = F.V[par][2];
-  const float* __restrict__ th = F.V[par][3];
-  auto L = [&](const float* f, int a, int b, int c) { return __ldg(f + g.at(clampi(a, 0, g.nx), clampi(b, 0, g.ny), clampi(c, 0, g.nz))); };
-  auto uc = [&](int a, int b, int c) { return 0.5f * (L(u, a, b, c) + L(u, a + 1, b, c)) - bsB(F.B, g.nz, c).z; };
-  auto vc = [&](int a, int b, int c) { return 0.5f * (L(v, a, b, c) + L(v, a, b + 1, c)) - bsB(F.B, g.nz, c).w; };
-  auto wc = [&](int a, int b, int c) { return 0.5f * (L(w, a, b, c) + L(w, a, b, c + 1)); };
+  // a cell's +1 neighbours on the staggered box always exist; the -1 ones clamp to the edge (offset 0)
+  const int o = g.at(ci, cj, ck);
+  const int xm = ci > 0 ? -1 : 0, ym = cj > 0 ? -g.px : 0, zm = ck > 0 ? -g.plane : 0;
+  const int xp = 1, yp = g.px, zp = g.plane;
+  const float* __restrict__ u = F.V[par][0] + o;
+  const float* __restrict__ v = F.V[par][1] + o;
+  const float* __restrict__ w = F.V[par][2] + o;
+  const float* __restrict__ th = F.V[par][3] + o;
+  const float u0m = bsB(F.B, g.nz, ck - 1).z, u00 = bsB(F.B, g.nz, ck).z, u0p = bsB(F.B, g.nz, ck + 1).z;
+  const float v0m = bsB(F.B, g.nz, ck - 1).w, v00 = bsB(F.B, g.nz, ck).w, v0p = bsB(F.B, g.nz, ck + 1).w;
+  auto uc = [&](int off, float u0) { return 0.5f * (__ldg(u + off) + __ldg(u + off + xp)) - u0; };
+  auto vc = [&](int off, float v0) { return 0.5f * (__ldg(v + off) + __ldg(v + off + yp)) - v0; };
+  auto wc = [&](int off) { return 0.5f * (__ldg(w + off) + __ldg(w + off + zp)); };
   const float dx = U.dims.w, dz = U.dzv.x;
-  const float dudx = (L(u, ci + 1, cj, ck) - L(u, ci, cj, ck)) / dx;
-  const float dvdy = (L(v, ci, cj + 1, ck) - L(v, ci, cj, ck)) / dx;
-  const float dwdz = (L(w, ci, cj, ck + 1) - L(w, ci, cj, ck)) / dz;
-  const float dudy = (uc(ci, cj + 1, ck) - uc(ci, cj - 1, ck)) / (2.f * dx), dudz = (uc(ci, cj, ck + 1) - uc(ci, cj, ck - 1)) / (2.f * dz);
-  const float dvdx = (vc(ci + 1, cj, ck) - vc(ci - 1, cj, ck)) / (2.f * dx), dvdz = (vc(ci, cj, ck + 1) - vc(ci, cj, ck - 1)) / (2.f * dz);
-  const float dwdx = (wc(ci + 1, cj, ck) - wc(ci - 1, cj, ck)) / (2.f * dx), dwdy = (wc(ci, cj + 1, ck) - wc(ci, cj - 1, ck)) / (2.f * dx);
+  // differences times the correctly rounded reciprocals 1/dx, 1/dz (and their exact halves) instead of divisions
+  const float idx = U.dzv.y, idz = U.dzv.z, ih2x = 0.5f * idx, ih2z = 0.5f * idz;
+  const float dudx = (__ldg(u + xp) - __ldg(u)) * idx;
+  const float dvdy = (__ldg(v + yp) - __ldg(v)) * idx;
+  const float dwdz = (__ldg(w + zp) - __ldg(w)) * idz;
+  const float dudy = (uc(yp, u00) - uc(ym, u00)) * ih2x, dudz = (uc(zp, u0p) - uc(zm, u0m)) * ih2z;
+  const float dvdx = (vc(xp, v00) - vc(xm, v00)) * ih2x, dvdz = (vc(zp, v0p) - vc(zm, v0m)) * ih2z;
+  const float dwdx = (wc(xp) - wc(xm)) * ih2x, dwdy = (wc(yp) - wc(ym)) * ih2x;
   const float s12 = 0.5f * (dudy + dvdx), s13 = 0.5f * (dudz + dwdx), s23 = 0.5f * (dvdz + dwdy);
   const float S2 = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + 4.f * (s12 * s12 + s13 * s13 + s23 * s23);
   const int kz0 = max(ck - 1, 0), kz1 = min(ck + 1, g.nz - 1);
-  float N2 = 9.81f / bsA(F.B, g.nz, ck).x * (L(th, ci, cj, kz1) - L(th, ci, cj, kz0)) / (float(kz1 - kz0) * dz);
-  const int o = g.at(ci, cj, ck);
+  float N2 = 9.81f / bsA(F.B, g.nz, ck).x * (__ldg(th + (kz1 - ck) * g.plane) - __ldg(th + (kz0 - ck) * g.plane)) / (float(kz1 - kz0) * dz);
   if (U.cor.w > 0.5f && __ldg(F.Q[0][1] + o) + __ldg(F.Q[0][2] + o) > 1e-5f) N2 = fminf(N2, 0.f);
   const float Ri = N2 / fmaxf(S2, 1e-10f);
   const float fst = sqrtf(fmaxf(0.f, 1.f - Ri / 0.33f));
@@ -255,26 +263,30 @@ struct Loc {
   float vu[3], vv[3], vw[3], vc[3];
 };
 __device__ __forceinline__ Loc localVel(const Fields& F, const Grid& g, int par, int i, int j, int k) {
-  const float* __restrict__ u = F.V[par][0];
-  const float* __restrict__ v = F.V[par][1];
-  const float* __restrict__ w = F.V[par][2];
-  auto L = [&](const float* f, int a, int b, int c) { return __ldg(f + g.at(clampi(a, 0, g.nx), clampi(b, 0, g.ny), clampi(c, 0, g.nz))); };
-  Loc o;
-  const float pu = L(u, i, j, k), pv = L(v, i, j, k), pw = L(w, i, j, k);
-  const float xpu = L(u, i + 1, j, k), ypv = L(v, i, j + 1, k), zpw = L(w, i, j, k + 1);
-  o.vu[0] = pu;
-  o.vu[1] = 0.25f * (L(v, i - 1, j, k) + pv + L(v, i - 1, j + 1, k) + ypv);
-  o.vu[2] = 0.25f * (L(w, i - 1, j, k) + pw + L(w, i - 1, j, k + 1) + zpw);
-  o.vv[0] = 0.25f * (L(u, i, j - 1, k) + pu + L(u, i + 1, j - 1, k) + xpu);
-  o.vv[1] = pv;
-  o.vv[2] = 0.25f * (L(w, i, j - 1, k) + pw + L(w, i, j - 1, k + 1) + zpw);
-  o.vw[0] = 0.25f * (L(u, i, j, k - 1) + pu + L(u, i + 1, j, k - 1) + xpu);
-  o.vw[1] = 0.25f * (L(v, i, j, k - 1) + pv + L(v, i, j + 1, k - 1) + ypv);
-  o.vw[2] = pw;
-  o.vc[0] = 0.5f * (pu + xpu);
-  o.vc[1] = 0.5f * (pv + ypv);
-  o.vc[2] = 0.5f * (pw + zpw);
-  return o;
+  // clamp-to-edge neighbour offsets of the staggered box, once per texel
+  const int o = g.at(i, j, k);
+  const int xm = i > 0 ? -1 : 0, xp = i < g.nx ? 1 : 0;
+  const int ym = j > 0 ? -g.px : 0, yp = j < g.ny ? g.px : 0;
+  const int zm = k > 0 ? -g.plane : 0, zp = k < g.nz ? g.plane : 0;
+  const float* __restrict__ u = F.V[par][0] + o;
+  const float* __restrict__ v = F.V[par][1] + o;
+  const float* __restrict__ w = F.V[par][2] + o;
+  Loc L;
+  const float pu = __ldg(u), pv = __ldg(v), pw = __ldg(w);
+  const float xpu = __ldg(u + xp), ypv = __ldg(v + yp), zpw = __ldg(w + zp);
+  L.vu[0] = pu;
+  L.vu[1] = 0.25f * (__ldg(v + xm) + pv + __ldg(v + xm + yp) + ypv);
+  L.vu[2] = 0.25f * (__ldg(w + xm) + pw + __ldg(w + xm + zp) + zpw);
+  L.vv[0] = 0.25f * (__ldg(u + ym) + pu + __ldg(u + xp + ym) + xpu);
+  L.vv[1] = pv;
+  L.vv[2] = 0.25f * (__ldg(w + ym) + pw + __ldg(w + ym + zp) + zpw);
+  L.vw[0] = 0.25f * (__ldg(u + zm) + pu + __ldg(u + xp + zm) + xpu);
+  L.vw[1] = 0.25f * (__ldg(v + zm) + pv + __ldg(v + yp + zm) + ypv);
+  L.vw[2] = pw;
+  L.vc[0] = 0.5f * (pu + xpu);
+  L.vc[1] = 0.5f * (pv + ypv);
+  L.vc[2] = 0.5f * (pw + zpw);
+  return L;
 }
 // departure (s = 1) or forward (s = -1) point, first-order trace clamped to the box (model.js:428-432)
 __device__ __forceinline__ void traceV(const Grid& g, const float k[3], float px, float py, float pz, const float v[3], float s,
@@ -286,13 +298,13 @@ __device__ __forceinline__ void traceV(const Grid& g, const float k[3], float px
 // channel sample at a point in grid units (texel offsets of u, v, w, theta: model.js:419-422)
 __device__ __forceinline__ float sampleVch(const float* f, const Grid& g, int ch, float x, float y, float z) {
   const float ox = ch == 0 ? 0.f : 0.5f, oy = ch == 1 ? 0.f : 0.5f, oz = ch == 2 ? 0.f : 0.5f;
-  return trilerp(f, g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz);
+  return trilerpB(f, g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz);
 }
 
 __global__ void k_advv1(Grid g, Uni U, Fields F, int par) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
-  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
   const float fi = float(ci), fj = float(cj), fk = float(ck);
   const int o = g.at(ci, cj, ck);
   float x, y, z;
@@ -307,11 +319,13 @@ __global__ void k_advv1(Grid g, Uni U, Fields F, int par) {
 }
 
 __device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Grid& g, float x, float y, float z, float ox, float oy, float oz) {
-  const int i0 = int(floorf(x - ox)), j0 = int(floorf(y - oy)), k0 = int(floorf(z - oz));
+  // the trace is clamped to the box, so each floor index lies in [-1, n] and one bound per corner clamps it
+  const int i0 = __float2int_rd(x - ox), j0 = __float2int_rd(y - oy), k0 = __float2int_rd(z - oz);
+  const int ia = max(i0, 0), ib = min(i0 + 1, g.nx), ja = max(j0, 0), jb = min(j0 + 1, g.ny), ka = max(k0, 0), kb = min(k0 + 1, g.nz);
   float lo = 1e30f, hi = -1e30f;
 #pragma unroll
   for (int q = 0; q < 8; q++) {
-    const float s = __ldg(f + g.at(clampi(i0 + (q & 1), 0, g.nx), clampi(j0 + ((q >> 1) & 1), 0, g.ny), clampi(k0 + (q >> 2), 0, g.nz)));
+    const float s = __ldg(f + g.at((q & 1) ? ib : ia, ((q >> 1) & 1) ? jb : ja, (q >> 2) ? kb : ka));
     lo = fminf(lo, s);
     hi = fmaxf(hi, s);
   }
@@ -321,7 +335,7 @@ __device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Gr
 __global__ void k_advv2(Grid g, Uni U, Fields F, int par) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
-  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
   const float fi = float(ci), fj = float(cj), fk = float(ck);
   const float P[4][3] = {{fi, fj + 0.5f, fk + 0.5f}, {fi + 0.5f, fj, fk + 0.5f}, {fi + 0.5f, fj + 0.5f, fk}, {fi + 0.5f, fj + 0.5f, fk + 0.5f}};
   const float* vel[4] = {L.vu, L.vv, L.vw, L.vc};
@@ -358,21 +372,6 @@ __device__ __forceinline__ void traceQ(const Grid& g, const float k[3], const fl
   y = clampf(p[1] - s * k[1] * v[1], 0.5f, float(g.ny) - 0.5f);
   z = clampf(p[2] - s * k[2] * (v[2] - fall), 0.5f, float(g.nz) - 0.5f);
 }
-__device__ __forceinline__ float sampleQ(const float* f, const Grid& g, float x, float y, float z) {
-  return trilerp(f, g, g.nx, g.ny, g.nz, x - 0.5f, y - 0.5f, z - 0.5f);
-}
-__device__ __forceinline__ float2 minmax8Q(const float* __restrict__ f, const Grid& g, float x, float y, float z) {
-  const int i0 = int(floorf(x - 0.5f)), j0 = int(floorf(y - 0.5f)), k0 = int(floorf(z - 0.5f));
-  float lo = 1e30f, hi = -1e30f;
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const float s = __ldg(f + g.at(clampi(i0 + (q & 1), 0, g.nx - 1), clampi(j0 + ((q >> 1) & 1), 0, g.ny - 1), clampi(k0 + (q >> 2), 0, g.nz - 1)));
-    lo = fminf(lo, s);
-    hi = fmaxf(hi, s);
-  }
-  return make_float2(lo, hi);
-}
-
 // A trilinear tap on the cell-centred box: base offsets of the 2 x 2 x 2 neighbourhood (clamp-to-edge) and the
 // weights; the same footprint is the 8-texel min/max window of the MacCormack limiter (model.js:537-540).
 struct Tap {
@@ -380,18 +379,17 @@ struct Tap {
   float ax, ay, az;
 };
 __device__ __forceinline__ Tap tapQ(const Grid& g, float x, float y, float z) {
+  // x, y, z come from traceQ, clamped to [0.5, n - 0.5]: the floor indices lie in [0, n - 1], so only the upper
+  // corner needs its clamp-to-edge bound
   const float tx = x - 0.5f, ty = y - 0.5f, tz = z - 0.5f;
-  const float fx = floorf(tx), fy = floorf(ty), fz = floorf(tz);
-  int i0 = int(fx), j0 = int(fy), k0 = int(fz);
+  const int i0 = __float2int_rd(tx), j0 = __float2int_rd(ty), k0 = __float2int_rd(tz);
   Tap t;
-  t.ax = tx - fx;
-  t.ay = ty - fy;
-  t.az = tz - fz;
-  const int j1 = clampi(j0 + 1, 0, g.ny - 1), k1 = clampi(k0 + 1, 0, g.nz - 1);
-  t.i1 = clampi(i0 + 1, 0, g.nx - 1);
-  t.i0 = clampi(i0, 0, g.nx - 1);
-  j0 = clampi(j0, 0, g.ny - 1);
-  k0 = clampi(k0, 0, g.nz - 1);
+  t.ax = tx - float(i0);
+  t.ay = ty - float(j0);
+  t.az = tz - float(k0);
+  const int j1 = min(j0 + 1, g.ny - 1), k1 = min(k0 + 1, g.nz - 1);
+  t.i0 = i0;
+  t.i1 = min(i0 + 1, g.nx - 1);
   t.r00 = g.px * (j0 + g.py * k0);
   t.r10 = g.px * (j1 + g.py * k0);
   t.r01 = g.px * (j0 + g.py * k1);
@@ -463,7 +461,7 @@ __global__ void __launch_bounds__(128) k_advq1(Grid g, Uni U, Fields F, int par)
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
-  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
   float v[3] = {0.f, 0.f, 0.f};
   const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
   float x = 0.5f, y = 0.5f, z = 0.5f;
@@ -531,7 +529,7 @@ __global__ void __launch_bounds__(128) k_advq2(Grid g, Uni U, Fields F, int par)
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
-  const float kk[3] = {U.step.x / U.dims.w, U.step.x / U.dims.w, U.step.x / U.dzv.x};
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
   float v[3] = {0.f, 0.f, 0.f};
   const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
   float xb = 0.5f, yb = 0.5f, zb = 0.5f, xf = 0.5f, yf = 0.5f, zf = 0.5f;
@@ -620,9 +618,8 @@ __global__ void __launch_bounds__(128) k_activity(Grid g, Fields F) {
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_PHYS (model.js:578-907): forcing stencils + microphysics, outbreak mode
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ float spongeLat(const Uni& U, const Grid& g, float xmx, float xmy) {
-  const float Lx = float(g.nx) * U.dims.w, Ly = float(g.ny) * U.dims.w;
-  const float e = fminf(fminf(xmx, Lx - xmx), fminf(xmy, Ly - xmy));
+// lateral sponge of one distance to the nearest side wall, and the top sponge at height z (model.js:611-626)
+__device__ __forceinline__ float spongeLat1(const Uni& U, float e) {
   const float d = clampf(1.f - e / U.sponge.x, 0.f, 1.f);
   return d * (0.3f + 0.7f * d) / U.sponge.y;
 }
@@ -632,6 +629,28 @@ __device__ __forceinline__ float spongeTop(const Uni& U, const Grid& g, float z)
   const float s = sinf(1.5707963f * (z - U.sponge.z) / (ztop - U.sponge.z));
   return s * s / U.sponge.w;
 }
+// sponge tables (Fields::spz/slx/sly) and the per-level rain-speed density factor sqrt(rho_sfc / rho) (spz[4k+2])
+__global__ void k_tables(Grid g, Uni U, const float* B, float* spz, float* slx, float* sly) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const float dx = U.dims.w, dz = U.dzv.x;
+  if (t <= g.nz) {
+    spz[4 * t + 0] = spongeTop(U, g, (float(t) + 0.5f) * dz);
+    spz[4 * t + 1] = spongeTop(U, g, float(t) * dz);
+    spz[4 * t + 2] = sqrtf(U.step.z / bsA(B, g.nz, t).z);
+    spz[4 * t + 3] = 0.f;
+  }
+  const float Lx = float(g.nx) * dx, Ly = float(g.ny) * dx;
+  if (t <= g.nx) {
+    const float xf = float(t) * dx, xc = (float(t) + 0.5f) * dx;
+    slx[2 * t] = spongeLat1(U, fminf(xf, Lx - xf));
+    slx[2 * t + 1] = spongeLat1(U, fminf(xc, Lx - xc));
+  }
+  if (t <= g.ny) {
+    const float yf = float(t) * dx, yc = (float(t) + 0.5f) * dx;
+    sly[2 * t] = spongeLat1(U, fminf(yf, Ly - yf));
+    sly[2 * t + 1] = spongeLat1(U, fminf(yc, Ly - yc));
+  }
+}
 __device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
   const int kk = clampi(k, 0, nz - 1);
   if (ch == 0) return bsB(B, nz, kk).z;
@@ -640,55 +659,66 @@ __device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
   return 0.f;
 }
 
-// one texel of the physics pass; returns whether the cell's new state holds a hydrometeor
-// CL: clamp neighbour indices to the box (edge blocks); interior blocks index without clamps, which reads the same
-// texels. BND: boundary air masses present (else the target state is the base state, see tgtUb).
-template <bool CL, bool BND>
+// one texel of the physics pass; returns whether the cell's new state holds a hydrometeor.
+// Neighbour reads clamp to the edge of their texture (textureLoad with clamped coordinates, model.js:596-606): the
+// offsets below are the clamped index minus the texel's own, for the staggered box [0, n] (V) and the cell box
+// [0, n-1] (Q, aux, phi_t), computed once per texel. BND: boundary air masses present (else the target state is the
+// base state, see tgtUb).
+template <bool BND>
 __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
   bool hyd = false;
-  const float* __restrict__ Vin[4] = {F.V[1 - par][0], F.V[1 - par][1], F.V[1 - par][2], F.V[1 - par][3]};
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  auto L = [&](int ch, int a, int b, int c) {
-    return __ldg(Vin[ch] + (CL ? g.at(clampi(a, 0, nx), clampi(b, 0, ny), clampi(c, 0, nz)) : g.at(a, b, c)));
-  };
-  auto LQ = [&](int ch, int a, int b, int c) {
-    return __ldg(F.Q[1][ch] + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
-  };
-  auto LA = [&](int ch, int a, int b, int c) {
-    return __ldg(F.aux[ch] + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
-  };
-  auto LP = [&](int a, int b, int c) {
+  const int o = g.at(ci, cj, ck);
+  const float* __restrict__ Vu = F.V[1 - par][0] + o;
+  const float* __restrict__ Vv = F.V[1 - par][1] + o;
+  const float* __restrict__ Vw = F.V[1 - par][2] + o;
+  const float* __restrict__ Vth = F.V[1 - par][3] + o;
+  const float* __restrict__ A0 = F.aux[0] + o;
+  const float* __restrict__ A1 = F.aux[1] + o;
+  // staggered box
+  const int xm = ci > 0 ? -1 : 0, xp = ci < nx ? 1 : 0;
+  const int ym = cj > 0 ? -g.px : 0, yp = cj < ny ? g.px : 0;
+  const int zm = ck > 0 ? -g.plane : 0, zp = ck < nz ? g.plane : 0;
+  // cell box: own index and +-1, clamped to [0, n-1]
+  const int xc0 = ci < nx ? 0 : -1, xcp = ci < nx - 1 ? 1 : xc0;
+  const int yc0 = cj < ny ? 0 : -g.px, ycp = cj < ny - 1 ? g.px : yc0;
+  auto LP = [&](int off) {
     if (!BND) return 0.f;
-    return __ldg(F.phT + (CL ? g.at(clampi(a, 0, nx - 1), clampi(b, 0, ny - 1), clampi(c, 0, nz - 1)) : g.at(a, b, c)));
+    return __ldg(F.phT + o + off);
   };
   const float dx = U.dims.w, dz = U.dzv.x, dt = U.step.x;
-  const int o = g.at(ci, cj, ck);
-  float V[4];
-#pragma unroll
-  for (int c = 0; c < 4; c++) V[c] = __ldg(Vin[c] + o);
+  float V[4] = {__ldg(Vu), __ldg(Vv), __ldg(Vw), __ldg(Vth)};
   float out[4] = {V[0], V[1], V[2], V[3]};
-  const float ix2 = 1.f / (dx * dx), iz2 = 1.f / (dz * dz);
-  const float fc = U.cor.x, nudR = 1.f / U.cor.y;
-  auto lapH = [&](int ch, float me) { return L(ch, ci + 1, cj, ck) + L(ch, ci - 1, cj, ck) + L(ch, ci, cj + 1, ck) + L(ch, ci, cj - 1, ck) - 4.f * me; };
+  const float ix2 = U.der.z, iz2 = U.der.w;
+  const float fc = U.cor.x;
+  const float* __restrict__ Vc[4] = {Vu, Vv, Vw, Vth};
+  auto lapH = [&](int ch, float me) { return __ldg(Vc[ch] + xp) + __ldg(Vc[ch] + xm) + __ldg(Vc[ch] + yp) + __ldg(Vc[ch] + ym) - 4.f * me; };
   auto lapZp = [&](int ch, float me, bool lo, bool hi) {
     const float m0 = me - bsV(F.B, nz, ck, ch);
-    const float a = lo ? m0 : L(ch, ci, cj, ck - 1) - bsV(F.B, nz, ck - 1, ch);
-    const float b = hi ? m0 : L(ch, ci, cj, ck + 1) - bsV(F.B, nz, ck + 1, ch);
+    const float a = lo ? m0 : __ldg(Vc[ch] + zm) - bsV(F.B, nz, ck - 1, ch);
+    const float b = hi ? m0 : __ldg(Vc[ch] + zp) - bsV(F.B, nz, ck + 1, ch);
     return a + b - 2.f * m0;
   };
+  const float4 spk = __ldg(reinterpret_cast<const float4*>(F.spz) + ck);  // (top sponge centre, face, rain factor, -)
+  const float2 slx = __ldg(reinterpret_cast<const float2*>(F.slx) + ci);  // (face, centre)
+  const float2 sly = __ldg(reinterpret_cast<const float2*>(F.sly) + cj);
   // u
   if (cj < ny && ck < nz) {
-    const float xmx = float(ci) * dx, xmy = (float(cj) + 0.5f) * dx, z = (float(ck) + 0.5f) * dz;
-    const float nux = 0.5f * (LA(0, ci - 1, cj, ck) + LA(0, ci, cj, ck)) + U.turb.y;
-    const float nuy = 0.5f * (LA(1, ci - 1, cj, ck) + LA(1, ci, cj, ck)) + U.turb.y;
+    const float nux = 0.5f * (__ldg(A0 + xm) + __ldg(A0 + xc0)) + U.turb.y;
+    const float nuy = 0.5f * (__ldg(A1 + xm) + __ldg(A1 + xc0)) + U.turb.y;
     float du = nux * lapH(0, V[0]) * ix2 + nuy * lapZp(0, V[0], ck == 0, ck == nz - 1) * iz2;
     const float ut = tgtUb<BND>(F, g, dz, ci, cj, ck);
-    const float vbar = 0.25f * (L(1, ci - 1, cj, ck) + V[1] + L(1, ci - 1, cj + 1, ck) + L(1, ci, cj + 1, ck));
+    const float vbar = 0.25f * (__ldg(Vv + xm) + V[1] + __ldg(Vv + xm + yp) + __ldg(Vv + yp));
     const float vtb = 0.5f * (tgtVb<BND>(F, g, dz, ci - 1, cj, ck) + tgtVb<BND>(F, g, dz, ci, cj + 1, ck));
-    const float nw = BND ? 0.5f * (l2d(F.lsfB, g, ci - 1, cj).w + l2d(F.lsfB, g, ci, cj).w) : 0.f;
-    du += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (ut - V[0]);
+    const float sp = fmaxf(slx.x, sly.y) + spk.x;
+    if (BND) {
+      const float nw = 0.5f * (l2d(F.lsfB, g, ci - 1, cj).w + l2d(F.lsfB, g, ci, cj).w);
+      du += (sp + nw * (1.f / U.cor.y)) * (ut - V[0]);
+    } else {
+      du += sp * (ut - V[0]);
+    }
     du += fc * (vbar - vtb);
-    if (ci > 0 && ci < nx) du -= (LP(ci, cj, ck) - LP(ci - 1, cj, ck)) / dx;
+    if (BND && ci > 0 && ci < nx) du -= (LP(0) - LP(-1)) / dx;
     if (ck == 0 && U.turb.w > 0.5f) {
       const float cd = U.micro.w;
       du += cd * (-sqrtf(V[0] * V[0] + vbar * vbar) * V[0] + sqrtf(ut * ut + vtb * vtb) * ut) / dz;
@@ -697,17 +727,21 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   } else out[0] = 0.f;
   // v
   if (ci < nx && ck < nz) {
-    const float xmx = (float(ci) + 0.5f) * dx, xmy = float(cj) * dx, z = (float(ck) + 0.5f) * dz;
-    const float nux = 0.5f * (LA(0, ci, cj - 1, ck) + LA(0, ci, cj, ck)) + U.turb.y;
-    const float nuy = 0.5f * (LA(1, ci, cj - 1, ck) + LA(1, ci, cj, ck)) + U.turb.y;
+    const float nux = 0.5f * (__ldg(A0 + ym) + __ldg(A0 + yc0)) + U.turb.y;
+    const float nuy = 0.5f * (__ldg(A1 + ym) + __ldg(A1 + yc0)) + U.turb.y;
     float dv = nux * lapH(1, V[1]) * ix2 + nuy * lapZp(1, V[1], ck == 0, ck == nz - 1) * iz2;
     const float vt = tgtVb<BND>(F, g, dz, ci, cj, ck);
-    const float ubar = 0.25f * (L(0, ci, cj - 1, ck) + V[0] + L(0, ci + 1, cj - 1, ck) + L(0, ci + 1, cj, ck));
+    const float ubar = 0.25f * (__ldg(Vu + ym) + V[0] + __ldg(Vu + xp + ym) + __ldg(Vu + xp));
     const float utb = 0.5f * (tgtUb<BND>(F, g, dz, ci, cj - 1, ck) + tgtUb<BND>(F, g, dz, ci + 1, cj, ck));
-    const float nw = BND ? 0.5f * (l2d(F.lsfB, g, ci, cj - 1).w + l2d(F.lsfB, g, ci, cj).w) : 0.f;
-    dv += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z) + nw * nudR) * (vt - V[1]);
+    const float sp = fmaxf(slx.y, sly.x) + spk.x;
+    if (BND) {
+      const float nw = 0.5f * (l2d(F.lsfB, g, ci, cj - 1).w + l2d(F.lsfB, g, ci, cj).w);
+      dv += (sp + nw * (1.f / U.cor.y)) * (vt - V[1]);
+    } else {
+      dv += sp * (vt - V[1]);
+    }
     dv -= fc * (ubar - utb);
-    if (cj > 0 && cj < ny) dv -= (LP(ci, cj, ck) - LP(ci, cj - 1, ck)) / dx;
+    if (BND && cj > 0 && cj < ny) dv -= (LP(0) - LP(-g.px)) / dx;
     if (ck == 0 && U.turb.w > 0.5f) {
       const float cd = U.micro.w;
       dv += cd * (-sqrtf(ubar * ubar + V[1] * V[1]) * V[1] + sqrtf(utb * utb + vt * vt) * vt) / dz;
@@ -716,20 +750,21 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   } else out[1] = 0.f;
   // w
   if (ci < nx && cj < ny && ck > 0 && ck < nz) {
-    const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx, z = float(ck) * dz;
-    const float nux = 0.5f * (LA(0, ci, cj, ck - 1) + LA(0, ci, cj, ck)) + U.turb.y;
-    const float nuy = 0.5f * (LA(1, ci, cj, ck - 1) + LA(1, ci, cj, ck)) + U.turb.y;
-    float dw = nux * lapH(2, V[2]) * ix2 + nuy * (L(2, ci, cj, ck - 1) + L(2, ci, cj, ck + 1) - 2.f * V[2]) * iz2;
-    auto buoy = [&](int kk) {
+    const float nux = 0.5f * (__ldg(A0 - g.plane) + __ldg(A0)) + U.turb.y;
+    const float nuy = 0.5f * (__ldg(A1 - g.plane) + __ldg(A1)) + U.turb.y;
+    float dw = nux * lapH(2, V[2]) * ix2 + nuy * (__ldg(Vw - g.plane) + __ldg(Vw + g.plane) - 2.f * V[2]) * iz2;
+    auto buoy = [&](int kk, int off) {
       const float4 A = bsA(F.B, nz, kk);
-      const int q = g.at(ci, cj, kk);
-      return 9.81f * ((__ldg(Vin[3] + q) - A.x) / A.x + 0.608f * (__ldg(F.Q[1][0] + q) - A.y) -
-                      (__ldg(F.Q[1][1] + q) + __ldg(F.Q[1][2] + q) + __ldg(F.Q[1][3] + q) + __ldg(F.Q[1][4] + q) + __ldg(F.Q[1][5] + q)));
+      return 9.81f * ((__ldg(Vth + off) - A.x) / A.x + 0.608f * (__ldg(F.Q[1][0] + o + off) - A.y) -
+                      (__ldg(F.Q[1][1] + o + off) + __ldg(F.Q[1][2] + o + off) + __ldg(F.Q[1][3] + o + off) +
+                       __ldg(F.Q[1][4] + o + off) + __ldg(F.Q[1][5] + o + off)));
     };
-    dw += 0.5f * (buoy(ck - 1) + buoy(ck)) - (LP(ci, cj, ck) - LP(ci, cj, ck - 1)) / dz;
-    dw += (spongeLat(U, g, xmx, xmy) + spongeTop(U, g, z)) * (0.f - V[2]);
+    dw += 0.5f * (buoy(ck - 1, -g.plane) + buoy(ck, 0));
+    if (BND) dw -= (LP(0) - LP(-g.plane)) / dz;
+    dw += (fmaxf(slx.y, sly.y) + spk.y) * (0.f - V[2]);
     const float4 civ = __ldg(F.ciMap + cj * nx + ci);
     if (civ.x > 0.f) {
+      const float z = float(ck) * dz;
       const float zz = fabsf(z - civ.z) / civ.w;
       if (zz < 1.f) {
         const float cv = cosf(1.5707963f * zz);
@@ -740,15 +775,13 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   } else out[2] = 0.f;
   // theta + microphysics at cell centres
   if (ci < nx && cj < ny && ck < nz) {
-    const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx, z = (float(ck) + 0.5f) * dz;
     const float4 A = bsA(F.B, nz, ck), Bb = bsB(F.B, nz, ck);
     const float4 LAv = BND ? l2d(F.lsfA, g, ci, cj) : make_float4(0.f, 100.f, 0.f, 100.f);
-    const float nw = BND ? l2d(F.lsfB, g, ci, cj).w : 0.f;
     const float tth = BND ? tgtTh(F.B, g, dz, LAv, ck) : A.x, tqv = BND ? tgtQv(F.B, g, dz, LAv, ck) : A.y;
-    const float sl = spongeLat(U, g, xmx, xmy);
-    const float relax = sl + nw * nudR;
-    const float nux = LA(0, ci, cj, ck) * 3.f + U.turb.y, nuy = LA(1, ci, cj, ck) * 3.f + U.turb.y;
-    float th = V[3] + dt * (nux * lapH(3, V[3]) * ix2 + nuy * lapZp(3, V[3], ck == 0, ck == nz - 1) * iz2 + (relax + spongeTop(U, g, z)) * (tth - V[3]));
+    const float sl = fmaxf(slx.y, sly.y);
+    const float relax = BND ? sl + l2d(F.lsfB, g, ci, cj).w * (1.f / U.cor.y) : sl;
+    const float nux = __ldg(A0) * 3.f + U.turb.y, nuy = __ldg(A1) * 3.f + U.turb.y;
+    float th = V[3] + dt * (nux * lapH(3, V[3]) * ix2 + nuy * lapZp(3, V[3], ck == 0, ck == nz - 1) * iz2 + (relax + spk.x) * (tth - V[3]));
     float q1[4], q2[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) {
@@ -758,8 +791,9 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     float l1[3], l1z[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      l1[c] = LQ(c, ci + 1, cj, ck) + LQ(c, ci - 1, cj, ck) + LQ(c, ci, cj + 1, ck) + LQ(c, ci, cj - 1, ck) - 4.f * q1[c];
-      l1z[c] = (ck == 0 ? q1[c] : LQ(c, ci, cj, ck - 1)) + (ck == nz - 1 ? q1[c] : LQ(c, ci, cj, ck + 1)) - 2.f * q1[c];
+      const float* __restrict__ q = F.Q[1][c] + o;
+      l1[c] = __ldg(q + xcp) + __ldg(q + xm) + __ldg(q + ycp) + __ldg(q + ym) - 4.f * q1[c];
+      l1z[c] = (ck == 0 ? q1[c] : __ldg(q + zm)) + (ck == nz - 1 ? q1[c] : __ldg(q + g.plane)) - 2.f * q1[c];
     }
     const float qvb = (ck == 0 ? A.y : bsA(F.B, nz, ck - 1).y) + (ck == nz - 1 ? A.y : bsA(F.B, nz, ck + 1).y) - 2.f * A.y;
     l1z[0] -= qvb;
@@ -777,7 +811,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     const bool thm = U.micro2.z > 0.5f;
     float nr = fmaxf(q2[2], 0.f);
     const float rq = 1000.f * rho;
-    const float rs = sqrtf(U.step.z / rho);
+    const float rs = spk.z;  // sqrt(rho_sfc / rho) of this level
     // warm rain (model.js:791-799)
     // Clear-air shortcuts below skip only work whose result is exactly zero or a no-op in the reference's
     // arithmetic (every product with a zero mixing ratio is +0), so they change no bit of the output.
@@ -941,15 +975,8 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
 __global__ void __launch_bounds__(128) k_phys(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   bool hyd = false;
-  // interior block: every texel's +-1 neighbours of every field lie inside the cell box (1 <= i <= nx - 2 etc.)
-  const int bx0 = blockIdx.x * blockDim.x, by0 = blockIdx.y * blockDim.y;
-  const bool interior = bx0 >= 1 && bx0 + int(blockDim.x) - 1 <= g.nx - 2 && by0 >= 1 && by0 + int(blockDim.y) - 1 <= g.ny - 2 &&
-                        ck >= 1 && ck <= g.nz - 2;
-  const bool bnd = U.cor.z > 0.5f;
-  if (ci <= g.nx && cj <= g.ny && ck <= g.nz) {
-    if (interior) hyd = bnd ? phys_texel<false, true>(g, U, F, par, ci, cj, ck) : phys_texel<false, false>(g, U, F, par, ci, cj, ck);
-    else hyd = bnd ? phys_texel<true, true>(g, U, F, par, ci, cj, ck) : phys_texel<true, false>(g, U, F, par, ci, cj, ck);
-  }
+  if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
+    hyd = U.cor.z > 0.5f ? phys_texel<true>(g, U, F, par, ci, cj, ck) : phys_texel<false>(g, U, F, par, ci, cj, ck);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && ck < g.nz)
@@ -989,7 +1016,7 @@ __global__ void k_proj(Grid g, Uni U, Fields F, int par) {
     return __ldg(F.phi + g.pidx(clampi(a, -g.pad, g.nx + g.pad - 1), clampi(b, -g.pad, g.ny + g.pad - 1), clampi(c, 0, g.nz - 1)));
   };
   const int o = g.at(ci, cj, ck);
-  const float kx = U.step.x / U.dims.w, kz = U.step.x / U.dzv.x;
+  const float kx = U.der.x, kz = U.der.y;
   const float pc = P(ci, cj, ck);
   float u = __ldg(F.V[par][0] + o), v = __ldg(F.V[par][1] + o), w = __ldg(F.V[par][2] + o);
   if (cj < g.ny && ck < g.nz) u = u - kx * (pc - P(ci - 1, cj, ck));
@@ -1134,6 +1161,10 @@ void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStre
 }
 void launch_activity(const Grid& g, const Fields& F, cudaStream_t s) {
   k_activity<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, F);
+}
+void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
+  const int n = std::max(g.nz, std::max(g.nx, g.ny)) + 1;
+  k_tables<<<(n + 127) / 128, 128, 0, s>>>(g, U, F.B, const_cast<float*>(F.spz), const_cast<float*>(F.slx), const_cast<float*>(F.sly));
 }
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
   k_phys<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);

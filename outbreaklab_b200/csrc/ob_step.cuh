@@ -15,6 +15,8 @@ void launch_nut(const Grid& g, const Uni& U, const Fields& F, int par, cudaStrea
 void launch_advv(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_activity(const Grid& g, const Fields& F, cudaStream_t s);
+// sponge tables of the physics pass (Fields::spz/slx/sly) for the uniforms' sponge parameters and the base state
+void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
