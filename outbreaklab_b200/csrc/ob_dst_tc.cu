@@ -1,19 +1,25 @@
 // ob_dst_tc.cu — bf16x3 tensor-core sine transforms for the pressure solve (tcgen05 + TMA + TMEM), sm_100a.
 //
-// Each of the four horizontal transforms of solver.js:155-163 is a batched GEMM C = Q B^T per z-plane, with Q the
-// orthonormal DST-II matrix (M x K, K-major) and B the field (N x K, K-major). fp32 operands are split into bf16
-// pairs (x = hi + lo) and the product is accumulated in fp32 TMEM as  Q_hi B_hi + Q_hi B_lo + Q_lo B_hi  (the lo*lo
-// term, ~2^-16 relative, is dropped): three tcgen05.mma per K step on the same staged tiles.
+// Each of the four horizontal transforms of solver.js:155-163 is one batched GEMM over all z-planes at once,
+// C[m][n] = sum_k F[m][k] Q[n][k]: F is the field with its planes' rows stacked (m = plane * rows + row, K-major) and Q
+// the orthonormal DST-II matrix (N x K, K-major). fp32 operands are split into bf16 pairs (x = hi + lo) and the
+// product is accumulated in fp32 TMEM as  F_hi Q_hi + F_hi Q_lo + F_lo Q_hi  (the lo*lo term, ~2^-16 relative, is
+// dropped): three tcgen05.mma per K step on the same staged tiles.
 //
 // Layouts (x fastest unless stated) chain the transforms so that every GEMM reads K-major tiles by TMA:
 //   rhs split  S_x[k][j][i]   --X-fwd-->  S_y[k][l][j]  --Y-fwd-->  T2[k][m][l] (fp32)
 //   --tridiagonal (transposes through shared memory)-->  S_y[k][l][m]  --Y-inv-->  S_x[k][j][l]  --X-inv-->  phi[k][j][i]
-// Kernel: one 128 x 128 output tile per CTA, 6 warps: warp 0 issues TMA loads into a 3-stage ring (4 tiles of
-// 128 x 64 bf16 per stage, 128-byte swizzle), warp 1 owns TMEM and issues the MMAs from one thread, warps 2-5 drain
-// the accumulator (tcgen05.ld) and write the tile. Every mbarrier wait is bounded (ob_tc.cuh).
+// The first three transforms write the field's row index fastest (lane = row: coalesced column stores straight from
+// TMEM); the last writes phi row-major.
+// Kernel: persistent, one CTA per SM, tiles of 128 field rows x BN outputs (BN <= 256 chosen per transform so the
+// output width divides with little padding: 656 -> 3 x 224), 6 warps: warp 0 issues TMA loads into a 2-stage ring
+// (hi/lo tiles of both operands, 128-byte swizzle), warp 1 owns TMEM (two 256-column accumulators) and issues the
+// MMAs from one thread, warps 2-5 drain one accumulator (tcgen05.ld) while the MMAs fill the other. No TMA
+// multicast. Every mbarrier wait is bounded (ob_tc.cuh).
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -24,53 +30,70 @@
 namespace ob {
 
 namespace {
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3;
-constexpr int TILE_BYTES = BM * BK * 2;  // 16 KB per operand tile (BN == BM)
-constexpr int STAGE_BYTES = 4 * TILE_BYTES;
+constexpr int BM = 128;                 // tile rows: rows of the field operand (plane x row)
+constexpr int BNMAX = 256;              // tile columns: transform outputs (the DST matrix's rows), runtime <= 256
+constexpr int BK = 64;                  // K per pipeline stage: one 128-byte swizzled row of bf16
+constexpr int STAGES = 2;
+constexpr int A_TILE = BM * BK * 2;     // 16 KB per A operand tile (hi or lo)
+constexpr int B_TILE = BNMAX * BK * 2;  // 32 KB per B operand tile slot
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int kThreads = 192;
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 512;     // two accumulators of 256 columns: the epilogue of one tile overlaps the next
 
-enum OutMode { OUT_ROW_BF16X2 = 0, OUT_ROW_F32 = 1, OUT_COL_F32 = 2, OUT_COL_F32_ADD = 3 };
+// OUT_T_*: element (m, n) of the product goes to out[(plane * N + n) * ld + r], m = plane * R + r (the field's row
+// index is the output's fastest index: the layout the next transform reads K-major). OUT_R_*: out[m * ld + n].
+enum OutMode { OUT_T_BF16X2 = 0, OUT_T_F32 = 1, OUT_R_F32 = 2, OUT_R_F32_ADD = 3 };
 
 struct TcOut {
   __nv_bfloat16* hi;
   __nv_bfloat16* lo;
   float* f;
-  long ldo;      // row pitch of the output (elements)
-  int M, N;      // valid rows / columns per plane
+  long ld;   // output pitch (elements)
+  int R;     // field rows per plane
+  int M;     // valid field rows (planes x R)
+  int N;     // valid transform outputs
 };
 }  // namespace
 
+// Persistent batched transform C[m][n] = sum_k F[m][k] Q[n][k] in bf16x3: F (the field, M x K, K-major) and Q (the
+// DST matrix, N x K, K-major) are each given as bf16 hi/lo planes by TMA maps; tiles of BM x BN are taken round-robin
+// (n fastest, so that CTAs working at the same time share the field tile through L2).
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_dst_tc(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
-             const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, int K, TcOut out,
+    k_dst_tc(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
+             const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
              unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* accum = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* tfull = empty + STAGES;  // [2] accumulator b holds a finished tile
+  uint64_t* tempty = tfull + 2;      // [2] the epilogue has drained accumulator b
+  uint64_t* done = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, plane = blockIdx.z;
   const int nk = (K + BK - 1) / BK;
+  const int mt = (out.M + BM - 1) / BM, ntn = (out.N + BN - 1) / BN, ntiles = mt * ntn;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    tc::mbar_init(accum, 1);
+    for (int b = 0; b < 2; b++) {
+      tc::mbar_init(&tfull[b], 1);
+      tc::mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
+    tc::mbar_init(done, 1);
     tc::fence_mbar_init();
   }
   if (warp == 0 && lane == 0) {
-    tc::prefetch_tmap(&tA_hi);
-    tc::prefetch_tmap(&tA_lo);
-    tc::prefetch_tmap(&tB_hi);
-    tc::prefetch_tmap(&tB_lo);
+    tc::prefetch_tmap(&tF_hi);
+    tc::prefetch_tmap(&tF_lo);
+    tc::prefetch_tmap(&tQ_hi);
+    tc::prefetch_tmap(&tQ_lo);
   }
   if (warp == 1) {
     tc::tmem_alloc(tmem_slot, kTmemCols);
@@ -83,113 +106,120 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
-      for (int kt = 0; kt < nk; kt++) {
-        const int s = kt % STAGES;
-        const uint32_t ph = (kt / STAGES) & 1;
-        if (!tc::mbar_wait(&empty[s], ph ^ 1, err, 1u)) break;
-        uint8_t* st = smem + s * STAGE_BYTES;
-        tc::mbar_expect_tx(&full[s], STAGE_BYTES);
-        tc::tma_load_2d(st, &tA_hi, &full[s], kt * BK, m0);
-        tc::tma_load_2d(st + TILE_BYTES, &tA_lo, &full[s], kt * BK, m0);
-        tc::tma_load_3d(st + 2 * TILE_BYTES, &tB_hi, &full[s], kt * BK, n0, plane);
-        tc::tma_load_3d(st + 3 * TILE_BYTES, &tB_lo, &full[s], kt * BK, n0, plane);
+      const uint32_t bytes = uint32_t(2 * A_TILE + 2 * BN * BK * 2);
+      int g = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+        for (int kt = 0; kt < nk; kt++, g++) {
+          const int s = g % STAGES;
+          const uint32_t ph = (g / STAGES) & 1;
+          if (!(ok = tc::mbar_wait(&empty[s], ph ^ 1, err, 1u))) break;
+          uint8_t* st = smem + s * STAGE_BYTES;
+          tc::mbar_expect_tx(&full[s], bytes);
+          tc::tma_load_2d(st, &tF_hi, &full[s], kt * BK, m0);
+          tc::tma_load_2d(st + A_TILE, &tF_lo, &full[s], kt * BK, m0);
+          tc::tma_load_2d(st + 2 * A_TILE, &tQ_hi, &full[s], kt * BK, n0);
+          tc::tma_load_2d(st + 2 * A_TILE + B_TILE, &tQ_lo, &full[s], kt * BK, n0);
+        }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+      const uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+      int g = 0, it = 0;
       bool ok = true;
-      for (int kt = 0; kt < nk && ok; kt++) {
-        const int s = kt % STAGES;
-        const uint32_t ph = (kt / STAGES) & 1;
-        if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, it++) {
+        const int b = it & 1;
+        if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
         tc::tc_fence_after();
-        const uint8_t* st = smem + s * STAGE_BYTES;
-        const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
-        const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + TILE_BYTES));
-        const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * TILE_BYTES));
-        const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 3 * TILE_BYTES));
-#pragma unroll
-        for (int kk = 0; kk < BK / 16; kk++) {
-          const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
-          tc::mma_bf16(tmem, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
-          tc::mma_bf16(tmem, dah + o, dbl + o, idesc, 1u);
-          tc::mma_bf16(tmem, dal + o, dbh + o, idesc, 1u);
+        const uint32_t acc = tmem + uint32_t(b * 256);
+        for (int kt = 0; kt < nk; kt++, g++) {
+          const int s = g % STAGES;
+          const uint32_t ph = (g / STAGES) & 1;
+          if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
+          tc::tc_fence_after();
+          const uint8_t* st = smem + s * STAGE_BYTES;
+          const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
+          const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
+          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
+          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + B_TILE));
+          const int ksub = min(BK, K - kt * BK + 15) / 16;  // 16-wide steps holding data (the rest is zero fill)
+          for (int kk = 0; kk < ksub; kk++) {
+            const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
+            tc::mma_bf16(acc, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+            tc::mma_bf16(acc, dah + o, dbl + o, idesc, 1u);
+            tc::mma_bf16(acc, dal + o, dbh + o, idesc, 1u);
+          }
+          tc::mma_commit(&empty[s]);
         }
-        tc::mma_commit(&empty[s]);
+        if (ok) tc::mma_commit(&tfull[b]);
       }
-      tc::mma_commit(accum);  // arrives when every MMA issued above has completed
-      if (!ok) tc::mbar_wait(accum, 0, err, 4u);
+      tc::mma_commit(done);  // arrives when every MMA issued above has completed
+      tc::mbar_wait(done, 0, err, 4u);
     }
   } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
     const int q = warp & 3;
-    const bool ok = tc::mbar_wait(accum, 0, err, 8u);
-    if (ok) tc::tc_fence_after();
-    if (MODE == OUT_COL_F32 || MODE == OUT_COL_F32_ADD) {
-      // rows are the output's fastest index: lane l of every store writes row m0 + 32q + l, one 128-byte line
-      const int r = m0 + q * 32 + lane;
-      if (ok) {
-#pragma unroll 1
-        for (int ch = 0; ch < BN / 32; ch++) {
-          float v[32];
-          tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
-          const int c0 = n0 + ch * 32;
-          if (c0 >= out.N) break;
-          if (r < out.M) {
-            float* __restrict__ dst = out.f + (long(plane) * out.N + c0) * out.ldo + r;
-            if (MODE == OUT_COL_F32_ADD) {
-              float old[32];
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+      const int b = it & 1;
+      const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+      if (!tc::mbar_wait(&tfull[b], (it >> 1) & 1, err, 8u)) break;
+      tc::tc_fence_after();
+      const int m = m0 + q * 32 + lane;  // this thread's row of the tile
+      const bool mv = m < out.M;
+      const int cend = min(out.N, n0 + BN);  // columns past BN belong to the next tile (BN need not be a multiple of 32)
+      const int plane = m / out.R, r = m - plane * out.R;
+      for (int ch = 0; ch * 32 < BN; ch++) {
+        float v[32];
+        tc::tmem_ld32(tmem + uint32_t(b * 256) + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
+        const int c0 = n0 + ch * 32;
+        if (c0 >= cend) continue;
+        if (MODE == OUT_T_BF16X2 || MODE == OUT_T_F32) {
+          // column by column: the warp's 32 lanes write 32 consecutive field rows of one output row
+          if (mv) {
+            const long base = long(plane) * out.N * out.ld + r;
 #pragma unroll
-              for (int t = 0; t < 32; t++) old[t] = (c0 + t < out.N) ? dst[long(t) * out.ldo] : 0.f;
+            for (int c = 0; c < 32; c++) {
+              if (c0 + c < cend) {
+                const long a = base + long(c0 + c) * out.ld;
+                if (MODE == OUT_T_F32) {
+                  out.f[a] = v[c];
+                } else {
+                  __nv_bfloat16 h, l;
+                  tc::split_bf16(v[c], h, l);
+                  out.hi[a] = h;
+                  out.lo[a] = l;
+                }
+              }
+            }
+          }
+        } else {
+          // row-major output: each thread writes 32 consecutive values of its own row, 16 bytes at a time
+          if (mv) {
+            float* __restrict__ dst = out.f + long(m) * out.ld + c0;
+            const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
 #pragma unroll
-              for (int t = 0; t < 32; t++)
-                if (c0 + t < out.N) dst[long(t) * out.ldo] = old[t] + v[t];
-            } else {
-#pragma unroll
-              for (int t = 0; t < 32; t++)
-                if (c0 + t < out.N) dst[long(t) * out.ldo] = v[t];
+            for (int c = 0; c < 32; c += 4) {
+              if (vec && c0 + c + 3 < cend) {
+                float4 w = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                if (MODE == OUT_R_F32_ADD) {
+                  const float4 o4 = *reinterpret_cast<const float4*>(dst + c);
+                  w.x += o4.x; w.y += o4.y; w.z += o4.z; w.w += o4.w;
+                }
+                *reinterpret_cast<float4*>(dst + c) = w;
+              } else {
+                for (int e = 0; e < 4; e++)
+                  if (c0 + c + e < cend) dst[c + e] = (MODE == OUT_R_F32_ADD ? dst[c + e] : 0.f) + v[c + e];
+              }
             }
           }
         }
       }
-    } else {
-      // columns are the output's fastest index: stage the 128 x 128 tile in the drained pipeline ring (all TMA
-      // writes and MMA reads of it are complete once the accumulator barrier has fired), then write whole rows
-      constexpr int LDS = BN + 1;
-      float* stage = reinterpret_cast<float*>(smem);
-      if (ok) {
-#pragma unroll 1
-        for (int ch = 0; ch < BN / 32; ch++) {
-          float v[32];
-          tc::tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
-          float* srow = stage + (q * 32 + lane) * LDS + ch * 32;
-#pragma unroll
-          for (int t = 0; t < 32; t++) srow[t] = v[t];
-        }
-      }
-      asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
-      if (ok) {
-        const int ew = warp - 2;
-#pragma unroll 1
-        for (int rr = ew; rr < BM; rr += 4) {
-          const int r = m0 + rr;
-          if (r >= out.M) break;
-          const long base = (long(plane) * out.M + r) * out.ldo + n0;
-#pragma unroll
-          for (int s4 = 0; s4 < BN / 32; s4++) {
-            const int c = s4 * 32 + lane;
-            const float val = stage[rr * LDS + c];
-            if (MODE == OUT_ROW_F32) {
-              if (n0 + c < out.N) out.f[base + c] = val;
-            } else if (n0 + c < out.ldo) {
-              __nv_bfloat16 h, l;
-              tc::split_bf16(val, h, l);
-              out.hi[base + c] = h;
-              out.lo[base + c] = l;
-            }
-          }
-        }
-      }
+      // the accumulator is free again once every lane's tcgen05.ld of it has completed
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&tempty[b]);
     }
   }
   tc::tc_fence_before();
@@ -335,27 +365,44 @@ static PFN_encodeTiled get_encode() {
   return fn;
 }
 
-// 2-D [rows][cols] bf16 with pitch ld (elements), box 64 x 128, 128-byte swizzle
-static bool make_map_2d(CUtensorMap* m, void* base, long rows, long cols, long ld) {
+// 2-D [rows][cols] bf16 with pitch ld (elements), box 64 x box_rows, 128-byte swizzle; reads past cols or rows are
+// zero-filled
+static bool make_map_2d(CUtensorMap* m, void* base, long rows, long cols, long ld, int box_rows) {
   PFN_encodeTiled enc = get_encode();
   if (!enc) return false;
   cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
   cuuint64_t strides[1] = {cuuint64_t(ld * 2)};
-  cuuint32_t box[2] = {BK, BM};
+  cuuint32_t box[2] = {BK, cuuint32_t(box_rows)};
   cuuint32_t es[2] = {1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
-// 3-D [planes][rows][cols] bf16 with pitch ld, box 64 x 128 x 1
-static bool make_map_3d(CUtensorMap* m, void* base, long planes, long rows, long cols, long ld) {
-  PFN_encodeTiled enc = get_encode();
-  if (!enc) return false;
-  cuuint64_t dims[3] = {cuuint64_t(cols), cuuint64_t(rows), cuuint64_t(planes)};
-  cuuint64_t strides[2] = {cuuint64_t(ld * 2), cuuint64_t(ld * 2 * rows)};
-  cuuint32_t box[3] = {BK, BN, 1};
-  cuuint32_t es[3] = {1, 1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+
+// tile width for N transform outputs: the fewest tiles of at most 256, then the smallest multiple of 16 covering N
+static int pick_bn(int N) {
+  const int nt = (N + BNMAX - 1) / BNMAX;
+  return ((N + nt - 1) / nt + 15) / 16 * 16;
+}
+
+static int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
+static void set_smem_attrs() {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_dst_tc<OUT_T_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_R_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
 }
 
 static inline long pad8(long n) { return (n + 7) / 8 * 8; }
@@ -369,8 +416,9 @@ struct TcPlan {
   float* t2 = nullptr;
   double* low = nullptr;  // FP64 factors of the 4 lowest modes
   unsigned int* err = nullptr;
-  CUtensorMap A[4][2];    // [transform][hi/lo]
-  CUtensorMap Bx[2], By[2], Br[2];
+  int bnx = 0, bny = 0;   // tile widths of the x and y transforms
+  CUtensorMap Q[4][2];    // DST matrices, the B operand: [transform][hi/lo]
+  CUtensorMap Fx[2], Fy[2], Fr[2];  // fields, the A operand: S_x, S_y and the split right-hand side
 };
 
 static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
@@ -425,25 +473,21 @@ int PoissonPlan::tc_create() {
     cudaMemcpy(mp[t][1], lo.data(), n * 2, cudaMemcpyHostToDevice);
     off += 2 * n;
   }
+  T->bnx = pick_bn(nx);
+  T->bny = pick_bn(ny);
+  const int bn[4] = {T->bnx, T->bny, T->bny, T->bnx};
   ok = true;
   for (int t = 0; t < 4; t++)
-    for (int h = 0; h < 2; h++) ok = ok && make_map_2d(&T->A[t][h], mp[t][h], dim[t], dim[t], ld[t]);
-  // B operands: S_x [nz][ny][nx] pitch ldx ; S_y [nz][nx][ny] pitch ldy
-  ok = ok && make_map_3d(&T->Bx[0], T->sx_hi, nz, ny, nx, T->ldx) && make_map_3d(&T->Bx[1], T->sx_lo, nz, ny, nx, T->ldx);
-  ok = ok && make_map_3d(&T->Br[0], T->rx_hi, nz, ny, nx, T->ldx) && make_map_3d(&T->Br[1], T->rx_lo, nz, ny, nx, T->ldx);
-  ok = ok && make_map_3d(&T->By[0], T->sy_hi, nz, nx, ny, T->ldy) && make_map_3d(&T->By[1], T->sy_lo, nz, nx, ny, T->ldy);
+    for (int h = 0; h < 2; h++) ok = ok && make_map_2d(&T->Q[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t]);
+  // A operands, planes stacked: S_x and the split rhs [nz * ny][nx] pitch ldx; S_y [nz * nx][ny] pitch ldy
+  ok = ok && make_map_2d(&T->Fx[0], T->sx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fx[1], T->sx_lo, long(nz) * ny, nx, T->ldx, BM);
+  ok = ok && make_map_2d(&T->Fr[0], T->rx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fr[1], T->rx_lo, long(nz) * ny, nx, T->ldx, BM);
+  ok = ok && make_map_2d(&T->Fy[0], T->sy_hi, long(nz) * nx, ny, T->ldy, BM) && make_map_2d(&T->Fy[1], T->sy_lo, long(nz) * nx, ny, T->ldy, BM);
   if (!ok) {
     set_error("poisson: tensor map encoding failed");
     return OB_ERR_DEVICE;
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaFuncSetAttribute(k_dst_tc<OUT_COL_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaFuncSetAttribute(k_dst_tc<OUT_COL_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  set_smem_attrs();
   return tc_factor_low();
 }
 
@@ -487,24 +531,18 @@ void PoissonPlan::tc_destroy() {
 }
 
 template <int MODE>
-static void launch_tc(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh, const CUtensorMap& bl, int M, int N,
-                      int K, int planes, const TcOut& o, unsigned int* err, cudaStream_t s) {
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, planes);
-  k_dst_tc<MODE><<<grid, kThreads, SMEM_BYTES, s>>>(ah, al, bh, bl, K, o, err);
+static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn, const TcOut& o, unsigned int* err, cudaStream_t s) {
+  const int tiles = ((o.M + BM - 1) / BM) * ((o.N + bn - 1) / bn);
+  k_dst_tc<MODE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
 }
 
-// the four transforms and the tridiagonals; rhs == nullptr: the right-hand side was written split by the caller
-// (the model's divergence pass, via tc_rhs_split)
 // the four transforms and the tridiagonals from the split right-hand side in rx to phi (stored, or added when add)
 static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s) {
   const int nx = P.nx, ny = P.ny, nz = P.nz;
-  TcOut o{};
-  // X-fwd: rows l (nx), cols j (ny), K = i  -> S_y[k][l][j]
-  o = TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, nx, ny};
-  launch_tc<OUT_ROW_BF16X2>(T->A[0][0], T->A[0][1], T->Br[0], T->Br[1], nx, ny, nx, nz, o, T->err, s);
-  // Y-fwd: rows m (ny), cols l (nx), K = j  -> T2[k][m][l] fp32
-  o = TcOut{nullptr, nullptr, T->t2, nx, ny, nx};
-  launch_tc<OUT_ROW_F32>(T->A[1][0], T->A[1][1], T->By[0], T->By[1], ny, nx, ny, nz, o, T->err, s);
+  // X-fwd: field rows (k, j), K = i, outputs l  -> S_y[k][l][j]
+  launch_tc<OUT_T_BF16X2>(T->Fr, T->Q[0], nx, T->bnx, TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, T->err, s);
+  // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
+  launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, T->err, s);
   // tridiagonals -> S_y[k][l][m]
   dim3 tg((nx + 31) / 32, (ny + 7) / 8);
   switch (nz) {
@@ -512,13 +550,12 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
     case 40: k_tri_tc<40><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
     default: k_tri_tc<80><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
   }
-  // Y-inv: rows j (ny), cols l (nx), K = m  -> S_x[k][j][l]
-  o = TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, ny, nx};
-  launch_tc<OUT_ROW_BF16X2>(T->A[2][0], T->A[2][1], T->By[0], T->By[1], ny, nx, ny, nz, o, T->err, s);
-  // X-inv: rows i (nx), cols j (ny), K = l  -> phi[k][j][i]
-  o = TcOut{nullptr, nullptr, phi, nx, nx, ny};
-  if (add) launch_tc<OUT_COL_F32_ADD>(T->A[3][0], T->A[3][1], T->Bx[0], T->Bx[1], nx, ny, nx, nz, o, T->err, s);
-  else launch_tc<OUT_COL_F32>(T->A[3][0], T->A[3][1], T->Bx[0], T->Bx[1], nx, ny, nx, nz, o, T->err, s);
+  // Y-inv: field rows (k, l), K = m, outputs j  -> S_x[k][j][l]
+  launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny}, T->err, s);
+  // X-inv: field rows (k, j), K = l, outputs i  -> phi[k][j][i]
+  const TcOut o{nullptr, nullptr, phi, nx, ny, nz * ny, nx};
+  if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
+  else launch_tc<OUT_R_F32>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
 }
 
 // precision 1: one bf16x3 pass; precision 2: a second pass on the FP64-accumulated residual (iterative refinement).
@@ -587,15 +624,17 @@ extern "C" int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* 
   cudaMemcpy(dal, al.data(), al.size() * 2, cudaMemcpyHostToDevice);
   cudaMemcpy(dbh, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice);
   cudaMemcpy(dbl, bl.data(), bl.size() * 2, cudaMemcpyHostToDevice);
-  CUtensorMap tah, tal, tbh, tbl;
-  bool ok = make_map_2d(&tah, dah, M, K, ld) && make_map_2d(&tal, dal, M, K, ld) && make_map_3d(&tbh, dbh, planes, N, K, ld) &&
-            make_map_3d(&tbl, dbl, planes, N, K, ld);
+  // the test's A (M x K) is the transform matrix (the kernel's B operand); its B planes (planes x N x K) are the field
+  const int bn = pick_bn(M);
+  CUtensorMap tq[2], tf[2];
+  bool ok = make_map_2d(&tq[0], dah, M, K, ld, bn) && make_map_2d(&tq[1], dal, M, K, ld, bn) &&
+            make_map_2d(&tf[0], dbh, long(planes) * N, K, ld, BM) && make_map_2d(&tf[1], dbl, long(planes) * N, K, ld, BM);
   int rc = OB_OK;
   if (!ok) { set_error("ob_dst_tc_selftest: tensor map encoding failed"); rc = OB_ERR_DEVICE; }
   if (rc == OB_OK) {
-    cudaFuncSetAttribute(k_dst_tc<OUT_ROW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    TcOut o{nullptr, nullptr, dc, N, M, N};  // C[p][r][c], row pitch N
-    launch_tc<OUT_ROW_F32>(tah, tal, tbh, tbl, M, N, K, planes, o, derr, nullptr);
+    set_smem_attrs();
+    const TcOut o{nullptr, nullptr, dc, N, N, planes * N, M};  // C[p][m][n] = out[(p * M + m) * N + n]
+    launch_tc<OUT_T_F32>(tf, tq, K, bn, o, derr, nullptr);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { set_error("ob_dst_tc_selftest: %s", cudaGetErrorString(e)); rc = OB_ERR_DEVICE; }
     unsigned int h = 0;
