@@ -186,6 +186,48 @@ int ob_radar_kdp(ObRadar* r, float* host, size_t count);
  * (its transforms are fp32 SIMT GEMMs, solver.js:12-68); it exists to test the tensor-core kernel in isolation. */
 int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* A, const float* B, float* C);
 
+/* ---- microphysics surrogate (no counterpart in the reference) ----
+ * A per-cell MLP (12 inputs -> 3 x 128 GELU -> 10 tendencies) that emulates the Thompson-style microphysics block
+ * of the physics pass (model.js:775-905, micro2.z = 1). Inputs: (T, p, rho, qv, qc, qr, qi, qs, qg, Nr, Ni, w) of a
+ * cell before the block; outputs: its change over one step of (T, qv, qc, qi, qr, qs, qg, Nr, Ni, w). The reference
+ * has no ice number (the fourth Q2 channel is a spare) and the block leaves w alone, so those two outputs are never
+ * applied. Training pairs come from the model's own plain-scheme steps (ob_model_record_micro); training runs on
+ * the GPU (fp32 forward/backward kernels, Adam); inference runs inside the step on the tensor cores (BF16 weights,
+ * FP32 accumulation) for the cells the scheme can change, with positivity and total-water conservation enforced
+ * and the scheme itself as the fallback for inputs outside the training range. */
+#define OB_MLP_NIN 12
+#define OB_MLP_NOUT 10
+#define OB_MLP_NPARAM 35978  /* W1[128][12] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[10][128] b4[10] */
+#define OB_MLP_PAIR 24       /* floats per recorded pair: 12 inputs, 10 tendencies, 2 pad */
+#define OB_MLP_NNORM 59      /* in_mean[12] in_scale[12] out_scale[10] in_lo[12] in_hi[12] dt */
+typedef struct ObMlp ObMlp;
+int ob_mlp_create(unsigned seed, ObMlp** out);  /* He-initialised weights from the seed */
+int ob_mlp_destroy(ObMlp* n);
+int ob_mlp_set_params(ObMlp* n, const float* host, int count);  /* count = OB_MLP_NPARAM; resets Adam */
+int ob_mlp_get_params(ObMlp* n, float* host, int count);
+/* normalisation: inputs x' = (f(x) - in_mean) * in_scale with f = log(q + 1e-9) for the mixing ratios,
+ * log(Nr + 1) for Nr, identity otherwise; outputs y = y' * out_scale; [in_lo, in_hi] is the raw input range the
+ * surrogate is trusted on; dt the step of the training pairs */
+int ob_mlp_set_norm(ObMlp* n, const float* host, int count);
+int ob_mlp_get_norm(ObMlp* n, float* host, int count);
+int ob_mlp_reserve_pairs(ObMlp* n, long long capacity);  /* device buffer for recorded pairs; clears the count */
+int ob_mlp_pair_count(ObMlp* n, long long* count);
+int ob_mlp_read_pairs(ObMlp* n, long long first, long long count, float* host);
+int ob_mlp_write_pairs(ObMlp* n, const float* host, long long count);  /* replaces the buffer's pairs */
+/* forward + backward on `count` host pairs (in order): the loss (mean squared error of the 8 scheme tendencies in
+ * normalised units) and its gradient with respect to every parameter (OB_MLP_NPARAM floats) */
+int ob_mlp_grad(ObMlp* n, const float* pairs, int count, double* loss, float* grad);
+int ob_mlp_eval(ObMlp* n, const float* pairs, int count, float* out);  /* count x OB_MLP_NOUT tendencies */
+/* `steps` Adam steps on batches of `batch` pairs drawn from the recorded pairs; mean loss over the steps */
+int ob_mlp_train(ObMlp* n, int batch, int steps, float lr, unsigned seed, double* mean_loss);
+/* record pairs of the plain scheme into net's buffer on every following step, each candidate cell (one the scheme
+ * can change) with probability rate; rate 0 stops */
+int ob_model_record_micro(ObModel* m, ObMlp* net, float rate);
+/* run the microphysics through a copy of net's current weights from the next step on (NULL: the plain scheme) */
+int ob_model_set_surrogate(ObModel* m, const ObMlp* net);
+/* cells the last step queued for the surrogate and how many of them fell back to the scheme */
+int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks);
+
 /* ---- the pressure solve for callers that cannot allocate device memory ----
  * No counterpart in the reference. For a host that may not call cudaMalloc (work recorded into a CUDA graph while
  * the capture is live, or a plugin living inside another runtime's fixed GPU memory budget): one fp32 solve of

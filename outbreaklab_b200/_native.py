@@ -79,7 +79,24 @@ SYMBOLS = {
     "ob_radar_read": (_i, [_vp, _vp, _sz]),
     "ob_radar_cut_moments": (_i, [_vp, _vp, _fp, _sz]),
     "ob_radar_kdp": (_i, [_vp, _fp, _sz]),
+    "ob_mlp_create": (_i, [C.c_uint, C.POINTER(_vp)]),
+    "ob_mlp_destroy": (_i, [_vp]),
+    "ob_mlp_set_params": (_i, [_vp, _fp, _i]),
+    "ob_mlp_get_params": (_i, [_vp, _fp, _i]),
+    "ob_mlp_set_norm": (_i, [_vp, _fp, _i]),
+    "ob_mlp_get_norm": (_i, [_vp, _fp, _i]),
+    "ob_mlp_reserve_pairs": (_i, [_vp, C.c_longlong]),
+    "ob_mlp_pair_count": (_i, [_vp, C.POINTER(C.c_longlong)]),
+    "ob_mlp_read_pairs": (_i, [_vp, C.c_longlong, C.c_longlong, _fp]),
+    "ob_mlp_write_pairs": (_i, [_vp, _fp, C.c_longlong]),
+    "ob_mlp_grad": (_i, [_vp, _fp, _i, C.POINTER(_d), _fp]),
+    "ob_mlp_eval": (_i, [_vp, _fp, _i, _fp]),
+    "ob_mlp_train": (_i, [_vp, _i, _i, _f, C.c_uint, C.POINTER(_d)]),
+    "ob_model_record_micro": (_i, [_vp, _vp, _f]),
+    "ob_model_set_surrogate": (_i, [_vp, _vp]),
+    "ob_model_surrogate_stats": (_i, [_vp, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
 }
+MLP_NIN, MLP_NOUT, MLP_NPARAM, MLP_PAIR, MLP_NNORM = 12, 10, 35978, 24, 59
 
 _lib = None
 

@@ -12,6 +12,7 @@
 
 #include "../../include/ob.h"
 #include "ob_common.cuh"
+#include "ob_mlp.cuh"
 #include "ob_poisson.cuh"
 #include "ob_radar.cuh"
 #include "ob_step.cuh"
@@ -90,6 +91,15 @@ struct ObModel {
   float* d_tab = nullptr;          // sponge tables of the physics pass (Fields::spz/slx/sly)
   float tab_key[8] = {};           // the uniforms the tables were made from; NaN = never made
   unsigned tab_gen = ~0u, base_gen = 0;  // base-state version the tables saw / current
+  // microphysics surrogate: queue of cells for it, its counters (queued, fallbacks), its inference copy
+  unsigned* d_queue = nullptr;
+  unsigned* d_mlpc = nullptr;
+  unsigned queue_cap = 0;
+  void* d_surr = nullptr;
+  mlp::Norm surr_norm{};
+  bool surrogate = false;
+  ObMlp* rec = nullptr;  // recording (state, tendency) pairs into this network's buffer, at rate rec_rate
+  float rec_rate = 0.f;
   PoissonPlan solver;
   std::vector<float> Bh;
   double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
@@ -113,7 +123,7 @@ static void model_bind_solver(ObModel* m) {
 static void model_free(ObModel* m) {
   if (!m) return;
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_queue, (void*)m->d_mlpc, m->d_surr, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -360,6 +370,36 @@ int ob_model_reset(ObModel* m) {
   return cuda_status(cudaGetLastError(), "reset");
 }
 
+extern "C++" {
+namespace ob {
+int surrogate_prepare(const ObMlp* net, void** d_image, mlp::Norm* norm);
+void launch_surrogate(const Grid& g, const Uni& U, const Fields& F, int par, const void* d_image, const mlp::Norm& nm,
+                      unsigned int* err, cudaStream_t s);
+void mlp_record_target(ObMlp* n, float** buf, unsigned** count, unsigned* cap);
+}  // namespace ob
+}
+
+// the physics pass with the model's microphysics mode: the scheme, the scheme while recording pairs, or the surrogate
+static int physics_pass(ObModel* m, int par, cudaStream_t s) {
+  const Grid& g = m->g;
+  if (m->surrogate) {
+    if (m->P.scheme < 0.5f) { set_error("the microphysics surrogate emulates the Thompson-style scheme (params.scheme = 1)"); return OB_ERR_INVALID; }
+    m->F.mlp_buf = reinterpret_cast<float*>(m->d_queue);
+    m->F.mlp_count = m->d_mlpc;
+    m->F.mlp_cap = m->queue_cap;
+    OB_TRY(cuda_status(cudaMemsetAsync(m->d_mlpc, 0, 2 * sizeof(unsigned), s), "surrogate counters"));
+    launch_phys(g, m->U, m->F, par, s, kMicroSurrogate);
+    launch_surrogate(g, m->U, m->F, par, m->d_surr, m->surr_norm, m->d_flags + 1, s);
+  } else if (m->rec && m->rec_rate > 0.f) {
+    mlp_record_target(m->rec, &m->F.mlp_buf, &m->F.mlp_count, &m->F.mlp_cap);
+    m->F.mlp_rate = m->rec_rate;
+    launch_phys(g, m->U, m->F, par, s, m->F.mlp_buf ? kMicroRecord : kMicroPlain);
+  } else {
+    launch_phys(g, m->U, m->F, par, s, kMicroPlain);
+  }
+  return OB_OK;
+}
+
 static int model_step_once(ObModel* m, double dt) {
   write_uniforms(m, dt);
   const Grid& g = m->g;
@@ -373,7 +413,7 @@ static int model_step_once(ObModel* m, double dt) {
   launch_nut(g, m->U, m->F, par, s);
   launch_advv(g, m->U, m->F, par, s);
   launch_advq(g, m->U, m->F, par, s);
-  launch_phys(g, m->U, m->F, par, s);
+  OB_TRY(physics_pass(m, par, s));
   launch_div(g, m->U, m->F, par, s);
   OB_TRY(m->solver.solve(m->F.rhs, m->F.phi, s));
   launch_proj(g, m->U, m->F, par, s);
@@ -524,11 +564,12 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   cudaEventRecord(ev[e++], s);
   launch_advq(g, m->U, m->F, par, s);
   cudaEventRecord(ev[e++], s);
-  launch_phys(g, m->U, m->F, par, s);
+  const int prc = physics_pass(m, par, s);
   cudaEventRecord(ev[e++], s);
   launch_div(g, m->U, m->F, par, s);
   cudaEventRecord(ev[e++], s);
   int rc = m->solver.solve(m->F.rhs, m->F.phi, s);
+  if (rc == OB_OK) rc = prc;
   cudaEventRecord(ev[e++], s);
   launch_proj(g, m->U, m->F, par, s);
   launch_rain(g, m->U, m->F, s);
@@ -540,6 +581,47 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   for (int i = 0; i + 1 < e && rc == OB_OK; i++) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
   for (int i = 0; i <= OB_NPASS; i++) cudaEventDestroy(ev[i]);
   return rc == OB_OK ? e - 1 : -rc;
+}
+
+int ob_model_record_micro(ObModel* m, ObMlp* net, float rate) {
+  if (!m || rate < 0.f || rate > 1.f) { set_error("ob_model_record_micro: bad arguments"); return OB_ERR_INVALID; }
+  m->rec = rate > 0.f ? net : nullptr;
+  m->rec_rate = rate;
+  return OB_OK;
+}
+
+int ob_model_set_surrogate(ObModel* m, const ObMlp* net) {
+  if (!m) { set_error("ob_model_set_surrogate: null model"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set surrogate"));
+  if (!net) { m->surrogate = false; return OB_OK; }
+  if (!m->d_queue) {
+    const size_t cells = size_t(m->g.nx) * m->g.ny * m->g.nz;
+    OB_TRY(cuda_status(cudaMalloc(&m->d_queue, cells * sizeof(unsigned)), "surrogate queue"));
+    OB_TRY(cuda_status(cudaMalloc(&m->d_mlpc, 2 * sizeof(unsigned)), "surrogate counters"));
+    OB_TRY(cuda_status(cudaMemset(m->d_mlpc, 0, 2 * sizeof(unsigned)), "surrogate counters"));
+    m->queue_cap = unsigned(cells);
+  }
+  OB_TRY(surrogate_prepare(net, &m->d_surr, &m->surr_norm));
+  m->surrogate = true;
+  return OB_OK;
+}
+
+int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks) {
+  if (!m || !queued || !fallbacks) { set_error("ob_model_surrogate_stats: null argument"); return OB_ERR_INVALID; }
+  unsigned h[2] = {0, 0}, e = 0;
+  if (m->d_mlpc) {
+    OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "surrogate stats"));
+    OB_TRY(cuda_status(cudaMemcpy(h, m->d_mlpc, sizeof(h), cudaMemcpyDeviceToHost), "surrogate stats"));
+    OB_TRY(cuda_status(cudaMemcpy(&e, m->d_flags + 1, sizeof(e), cudaMemcpyDeviceToHost), "surrogate stats"));
+  }
+  *queued = h[0];
+  *fallbacks = h[1];
+  if (e) {
+    cudaMemset(m->d_flags + 1, 0, sizeof(unsigned));
+    set_error("surrogate: a tensor-core pipeline wait timed out (code %u)", e);
+    return OB_ERR_TIMEOUT;
+  }
+  return OB_OK;
 }
 
 int ob_model_set_solver(ObModel* m, int precision) {

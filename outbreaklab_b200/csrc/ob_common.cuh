@@ -68,6 +68,12 @@ struct Fields {
   const float* spz;
   const float* slx;
   const float* sly;
+  // microphysics surrogate: in record mode mlp_buf holds sampled (state, tendency) pairs (24 floats each, cells
+  // drawn with probability mlp_rate), in surrogate mode the queue of cell offsets; mlp_count is the append counter
+  float* mlp_buf;
+  unsigned* mlp_count;
+  unsigned mlp_cap;
+  float mlp_rate;
 };
 
 constexpr float T0K = 273.15f;

@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "ob_common.cuh"
+#include "ob_micro.cuh"
 #include "ob_step.cuh"
 
 namespace ob {
@@ -659,12 +660,24 @@ __device__ __forceinline__ float bsV(const float* B, int nz, int k, int ch) {
   return 0.f;
 }
 
-// one texel of the physics pass; returns whether the cell's new state holds a hydrometeor.
+// one slot of an append-only list per calling thread: one atomic per warp, slots in lane order
+__device__ __forceinline__ unsigned warp_append(unsigned* ctr) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(ctr, unsigned(__popc(mask)));
+  base = __shfl_sync(mask, base, leader);
+  return base + unsigned(__popc(mask & ((1u << lane) - 1u)));
+}
+
+// one texel of the physics pass; returns whether the cell's new state holds a hydrometeor. MM: microphysics as the
+// scheme (kMicroPlain), the scheme plus sampled (state, tendency) pairs (kMicroRecord), or queued for the surrogate
+// kernel where it can act (kMicroSurrogate).
 // Neighbour reads clamp to the edge of their texture (textureLoad with clamped coordinates, model.js:596-606): the
 // offsets below are the clamped index minus the texel's own, for the staggered box [0, n] (V) and the cell box
 // [0, n-1] (Q, aux, phi_t), computed once per texel. BND: boundary air masses present (else the target state is the
 // base state, see tgtUb).
-template <bool BND>
+template <bool BND, int MM>
 __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
   bool hyd = false;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -809,154 +822,56 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     float T = th * pi0;
     float qv = q1[0], qc = q1[1], qi = q1[2], qr = q1[3], qs = q2[0], qg = q2[1];
     const bool thm = U.micro2.z > 0.5f;
-    float nr = fmaxf(q2[2], 0.f);
-    const float rq = 1000.f * rho;
-    const float rs = spk.z;  // sqrt(rho_sfc / rho) of this level
-    // warm rain (model.js:791-799)
-    // Clear-air shortcuts below skip only work whose result is exactly zero or a no-op in the reference's
-    // arithmetic (every product with a zero mixing ratio is +0), so they change no bit of the output.
-    const float pauto = U.micro.x * fmaxf(qc - U.micro.y, 0.f);
-    float accr = 0.f;
-    if (qc > 0.f) {
-      accr = 2.2f * qc * powf(qr, 0.875f);
-      if (thm && qr > 1e-9f) {
-        const float l = Fall::lamR(qr, nr);
-        accr = 3100.f * rho * nr * powf(l, -2.8f) * qc * rs;
+    MCell mc{T, qv, qc, qi, qr, qs, qg, fmaxf(q2[2], 0.f)};
+    bool done = false;
+    if (MM == kMicroSurrogate && micro_active(mc, p0)) {
+      // surrogate cell: store the state before the microphysics and queue the cell; the surrogate kernel applies
+      // the tendencies, the sponge removal and the clips (a full queue falls through to the scheme here)
+      const unsigned slot = warp_append(F.mlp_count);
+      if (slot < F.mlp_cap) {
+        reinterpret_cast<unsigned*>(F.mlp_buf)[slot] = unsigned(o);
+        F.Q[0][0][o] = mc.qv; F.Q[0][1][o] = mc.qc; F.Q[0][2][o] = mc.qi; F.Q[0][3][o] = mc.qr;
+        F.Q[0][4][o] = mc.qs; F.Q[0][5][o] = mc.qg; F.Q[0][6][o] = mc.nr; F.Q[0][7][o] = q2[3];
+        out[3] = mc.T / pi0;
+        hyd = true;
+        done = true;
       }
     }
-    const float da = fminf(pauto * dt, qc);
-    const float dc = fminf(accr * dt, qc - da);
-    qc -= da + dc;
-    qr += da + dc;
-    nr += da / 2.68e-10f;
-    const float dTc = T - T0K;
-    if (dTc < 0.f && qc + qi + qr + qs + qg > 0.f) {  // ice-phase conversions (model.js:801-829)
-      const float psaut = 1e-3f * expf(0.025f * dTc) * fmaxf(qi - 6e-4f, 0.f);
-      const float psacw = 5.4e-3f * qc * powf(fmaxf(rq * qs, 0.f), 0.81f) * rs;
-      const float psaci = 5.4e-3f * qi * powf(fmaxf(rq * qs, 0.f), 0.81f) * expf(0.025f * dTc) * rs;
-      const float ewet = 1.f / (1.f + qg / 0.008f);
-      const float pgq = powf(fmaxf(rq * qg, 0.f), 0.875f);
-      const float pgacw = 3.1e-3f * qc * pgq * rs * ewet;
-      const float pgaci = 3.0e-4f * qi * pgq * rs;
-      const float pgacr = 3.1e-3f * qr * pgq * rs * ewet;
-      const float pgfr = fminf(2e-4f * U.micro.z * (expf(0.66f * fminf(-dTc, 20.f)) - 1.f), 0.08f) * qr;
-      const float pgaut = 1e-3f * expf(0.09f * dTc) * fmaxf(qs - 6e-4f, 0.f) * (thm ? 0.25f : 1.f);
-      const float a1 = fminf((psaut + psaci + pgaci) * dt, qi);
-      const float fs1 = (psaut + psaci) / fmaxf(psaut + psaci + pgaci, 1e-20f);
-      qi -= a1;
-      qs += a1 * fs1;
-      qg += a1 * (1.f - fs1);
-      const float a2 = fminf((psacw + pgacw) * dt, qc);
-      const float fs2 = psacw / fmaxf(psacw + pgacw, 1e-20f);
-      const float rimeS = thm ? 0.95f : 0.7f;
-      qc -= a2;
-      qs += a2 * fs2 * rimeS;
-      qg += a2 * (1.f - fs2 * rimeS);
-      float a3 = fminf((pgacr + pgfr) * dt, qr);
-      if (T < 235.f) a3 = qr;
-      if (qr > 1e-12f) nr *= (qr - a3) / qr;
-      qr -= a3;
-      qg += a3;
-      const float a4 = fminf(pgaut * dt, qs);
-      qs -= a4;
-      qg += a4;
-      T += float(LFCd / CPDd) * (a2 + a3);
-    } else if (dTc >= 0.f && (qs > 0.f || qg > 0.f)) {  // melting (model.js:830-848)
-      const float m1 = fminf(0.012f * dTc * qs * dt, qs);
-      float m2 = fminf(0.0022f * dTc * qg * dt, qg);
-      if (thm) {
-        if (qg > 1e-9f) {
-          const float l = Fall::lamG(qg, rho), n0 = Fall::n0G(qg, rho);
-          const float vent = 0.78f / (l * l) + float(0.31 * 0.843 * 1.89 * 5430.0) * powf(U.step.z / rho, 0.25f) * powf(l, -2.945f);
-          const float heat = 2.4e-2f * dTc - float(LVCd * 2.26e-5) * rho * (qvsat(T0K, p0, 0.f) - qv);
-          m2 = clampf(6.2832f / (rho * float(LFCd)) * heat * n0 * vent * dt, 0.f, qg);
-          nr += m2 / qg * n0 / (rho * l);
-        }
-        if (qs > 1e-9f) {
-          const float ls = powf(float(3.14159 * 100.0 * 2e6) / (rho * qs), 0.25f);
-          nr += m1 / qs * 2e6f / (rho * ls);
+    if (!done) {
+      const MCell pre = mc;
+      micro_plain(U, dt, p0, rho, spk.z, mc);
+      if (MM == kMicroRecord && micro_active(pre, p0) &&
+          float(hash3i(ci, cj, ck ^ int(__float_as_uint(U.step.y) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
+        // one (state, tendency) pair of the scheme: 12 inputs, 10 tendencies, 2 pad (24 floats)
+        const unsigned slot = warp_append(F.mlp_count);
+        if (slot < F.mlp_cap) {
+          float* r = F.mlp_buf + size_t(slot) * 24;
+          const float x[12] = {pre.T, p0, rho, pre.qv, pre.qc, pre.qr, pre.qi, pre.qs, pre.qg, pre.nr, q2[3], V[2]};
+          const float y[12] = {mc.T - pre.T, mc.qv - pre.qv, mc.qc - pre.qc, mc.qi - pre.qi, mc.qr - pre.qr, mc.qs - pre.qs,
+                               mc.qg - pre.qg, mc.nr - pre.nr, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int e = 0; e < 12; e++) {
+            r[e] = x[e];
+            r[12 + e] = y[e];
+          }
         }
       }
-      qs -= m1;
-      qg -= m2;
-      qr += m1 + m2;
-      T -= float(LFCd / CPDd) * (m1 + m2);
+      T = mc.T; qv = mc.qv; qc = mc.qc; qi = mc.qi; qr = mc.qr; qs = mc.qs; qg = mc.qg;
+      float nr = mc.nr;
+      th = T / pi0;
+      const float keep = 1.f / (1.f + 2.f * dt * sl);
+      qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
+      F.Q[0][0][o] = fmaxf(qv, 0.f);
+      F.Q[0][1][o] = fmaxf(qc, 0.f);
+      F.Q[0][2][o] = fmaxf(qi, 0.f);
+      F.Q[0][3][o] = fmaxf(qr, 0.f);
+      F.Q[0][4][o] = fmaxf(qs, 0.f);
+      F.Q[0][5][o] = fmaxf(qg, 0.f);
+      F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
+      F.Q[0][7][o] = q2[3];
+      out[3] = th;
+      hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f;
     }
-    // rain evaporation (model.js:850-872)
-    const float qvsl = qr > 0.f ? qvsat1(T, p0, 0.f) : 0.f;
-    if (qr > 0.f && qv < qvsl) {
-      const float rc = 0.001f * rho * qr;
-      const float ern = ((1.6f + 124.9f * powf(rc, 0.2046f)) * powf(rc, 0.525f) / (2.55e8f / (p0 * qvsl) + 5.4e5f)) *
-                        ((qvsl - qv) / (0.001f * rho * qvsl));
-      const float srt = U.micro2.y > 0.f ? sqrtf(rc / (rc + 0.001f * rho * U.micro2.y)) : 1.f;
-      float e = ern * srt * dt * U.turb.z;
-      if (thm) {
-        const float l = Fall::lamR(qr, nr), n0 = rho * nr * l;
-        const float Ap = float(LVCd * LVCd) / (float(2.4e-2 * RVCd) * T * T);
-        const float Bp = 1.f / (rho * qvsl * 2.26e-5f);
-        const float vent = 0.78f / (l * l) + float(0.31 * 0.843 * 1.827 * 7492.0) * powf(U.step.z / rho, 0.25f) * powf(l, -2.9f);
-        e = 6.2832f * (1.f - qv / qvsl) * n0 * vent / (rho * (Ap + Bp)) * dt * U.micro2.w;
-      }
-      e = clampf(e, 0.f, fminf(qr, qvsl - qv));
-      if (thm && qr > 1e-12f) nr *= (qr - e) / qr;
-      qr -= e;
-      qv += e;
-      T -= float(LVCd / CPDd) * e;
-    }
-    // Thompson: self-collection / breakup (model.js:874-884)
-    if (thm) {
-      if (qr > 1e-9f) {
-        const float dm = 1.817f / Fall::lamR(qr, nr);
-        const float fb = clampf(1.f - expf(2300.f * (dm - 1.1e-3f)), -2.f, 1.f);
-        nr *= expf(-7.12f * rho * qr * fb * dt);
-        nr = clampf(nr, qr * 3.183e5f, qr * 3.183e11f);
-      } else nr = 0.f;
-    }
-    // sublimation (model.js:885-892)
-    const bool sub_on = dTc < 0.f && (qs > 0.f || qg > 0.f);
-    const float qvsi = sub_on ? qvsat1(T, p0, 1.f) : 0.f;
-    if (sub_on && qv < qvsi) {
-      const float sub = fmaxf(1.f - qv / qvsi, 0.f);
-      float e = fminf((2e-3f * qs + 5e-4f * qg) * sub * dt, (qvsi - qv) * 0.5f);
-      const float fsn = qs / fmaxf(qs + qg, 1e-20f);
-      e = fminf(e, qs + qg);
-      qs -= e * fsn;
-      qg -= e * (1.f - fsn);
-      qv += e;
-      T -= float(LSCd / CPDd) * e;
-    }
-    // mixed-phase saturation adjustment, 3 iterations (model.js:893-905)
-    const float qi0 = qi;
-    float qcl = qc + qi, dsum = 0.f;
-    for (int it = 0; it < 3; it++) {
-      const float f = fIce(T);
-      const float qs_ = qvsat1(T, p0, f);
-      const float Lh = mixf(float(LVCd), float(LSCd), f);
-      float d = (qv - qs_) / (1.f + Lh * Lh * qs_ / (float(CPDd * RVCd) * T * T));
-      d = fmaxf(d, -qcl);
-      if (d == 0.f) break;  // nothing changes: the remaining iterations would repeat this one exactly
-      qv -= d;
-      qcl += d;
-      T += Lh / float(CPDd) * d;
-      dsum += d;
-    }
-    const float f = fIce(T);
-    qi = f * qcl;
-    qc = qcl - qi;
-    T += float(LFCd / CPDd) * (qi - qi0 - f * dsum);
-    th = T / pi0;
-    const float keep = 1.f / (1.f + 2.f * dt * sl);
-    qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
-    F.Q[0][0][o] = fmaxf(qv, 0.f);
-    F.Q[0][1][o] = fmaxf(qc, 0.f);
-    F.Q[0][2][o] = fmaxf(qi, 0.f);
-    F.Q[0][3][o] = fmaxf(qr, 0.f);
-    F.Q[0][4][o] = fmaxf(qs, 0.f);
-    F.Q[0][5][o] = fmaxf(qg, 0.f);
-    F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
-    F.Q[0][7][o] = q2[3];
-    out[3] = th;
-    hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f;
   }
   const float sp = sqrtf(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
   if (sp > U.misc.x) {
@@ -972,11 +887,12 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   return hyd;
 }
 
-__global__ void __launch_bounds__(128) k_phys(Grid g, Uni U, Fields F, int par) {
+template <int MM>
+__global__ void __launch_bounds__(128, 8) k_phys(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
-    hyd = U.cor.z > 0.5f ? phys_texel<true>(g, U, F, par, ci, cj, ck) : phys_texel<false>(g, U, F, par, ci, cj, ck);
+    hyd = U.cor.z > 0.5f ? phys_texel<true, MM>(g, U, F, par, ci, cj, ck) : phys_texel<false, MM>(g, U, F, par, ci, cj, ck);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && ck < g.nz)
@@ -1166,8 +1082,10 @@ void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s)
   const int n = std::max(g.nz, std::max(g.nx, g.ny)) + 1;
   k_tables<<<(n + 127) / 128, 128, 0, s>>>(g, U, F.B, const_cast<float*>(F.spz), const_cast<float*>(F.slx), const_cast<float*>(F.sly));
 }
-void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
-  k_phys<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s, int micro_mode) {
+  if (micro_mode == kMicroRecord) k_phys<kMicroRecord><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+  else if (micro_mode == kMicroSurrogate) k_phys<kMicroSurrogate><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+  else k_phys<kMicroPlain><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
 }
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
   k_div<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);

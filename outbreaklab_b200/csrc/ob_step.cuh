@@ -17,7 +17,9 @@ void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStre
 void launch_activity(const Grid& g, const Fields& F, cudaStream_t s);
 // sponge tables of the physics pass (Fields::spz/slx/sly) for the uniforms' sponge parameters and the base state
 void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
-void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
+// microphysics modes of the physics pass
+enum { kMicroPlain = 0, kMicroRecord = 1, kMicroSurrogate = 2 };
+void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s, int micro_mode = kMicroPlain);
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
