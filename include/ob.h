@@ -198,7 +198,7 @@ int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* A, const fl
 #define OB_MLP_NIN 12
 #define OB_MLP_NOUT 10
 #define OB_MLP_NPARAM 35978  /* W1[128][12] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[10][128] b4[10] */
-#define OB_MLP_PAIR 24       /* floats per recorded pair: 12 inputs, 10 tendencies, 2 pad */
+#define OB_MLP_PAIR 24       /* floats per recorded pair: 12 inputs, 10 tendencies, texel offset (uint32 bits), pad */
 #define OB_MLP_NNORM 59      /* in_mean[12] in_scale[12] out_scale[10] in_lo[12] in_hi[12] dt */
 typedef struct ObMlp ObMlp;
 int ob_mlp_create(unsigned seed, ObMlp** out);  /* He-initialised weights from the seed */

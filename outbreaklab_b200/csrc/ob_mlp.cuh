@@ -17,7 +17,7 @@ constexpr int NIN = 12, NH = 128, NOUT = 10, NLOSS = 8;  // NLOSS: outputs that 
 // fp32 master parameters, packed: W1[NH][NIN] b1[NH] W2[NH][NH] b2[NH] W3[NH][NH] b3[NH] W4[NOUT][NH] b4[NOUT]
 constexpr int OW1 = 0, OB1 = OW1 + NH * NIN, OW2 = OB1 + NH, OB2 = OW2 + NH * NH, OW3 = OB2 + NH, OB3 = OW3 + NH * NH,
               OW4 = OB3 + NH, OB4 = OW4 + NOUT * NH, NPARAM = OB4 + NOUT;
-constexpr int PAIR = 24;  // floats per recorded pair: 12 inputs, 10 tendencies, 2 pad
+constexpr int PAIR = 24;  // floats per recorded pair: 12 inputs, 10 tendencies, texel offset (uint bits), pad
 constexpr float QEPS = 1e-9f;
 
 // normalisation, the raw input range seen in training (inputs outside it fall back to the scheme) and the time step

@@ -181,6 +181,18 @@ class RegionalModel:
     def solver(self):
         return int(N.lib().ob_model_solver(self.h))
 
+    # ---- microphysics surrogate (no counterpart in the reference; see surrogate.py) ----
+    def set_surrogate(self, net=None):
+        """From the next step on, the microphysics of queued cells runs through a copy of net's current weights on
+        the tensor cores (None: the plain scheme)."""
+        N.check(N.lib().ob_model_set_surrogate(self.h, net.h if net is not None else None))
+
+    def surrogate_stats(self):
+        """(cells the last step queued for the surrogate, how many of them fell back to the scheme)."""
+        q, f = C.c_uint(), C.c_uint()
+        N.check(N.lib().ob_model_surrogate_stats(self.h, C.byref(q), C.byref(f)))
+        return q.value, f.value
+
     @property
     def nan_count(self):
         return int(N.lib().ob_model_nan_count(self.h))
