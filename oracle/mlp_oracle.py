@@ -111,20 +111,53 @@ def loss_and_grad(params, pairs, norm):
     return loss, pack(g)
 
 
+CPD, RV, LV, LF, LS, T0 = 1005.7, 461.5, 2.501e6, 3.337e5, 2.834e6, 273.15
+NEW_SPECIES_FLOOR = 1e-8
+
+
+def sat_adjust(T, qv, qc, qi, p):
+    """The scheme's 3-iteration mixed-phase saturation adjustment (model.js:893-905), vectorised in float64."""
+    T, qv, qc, qi = (np.array(a, np.float64) for a in (T, qv, qc, qi))
+    fice = lambda t: np.clip((T0 - t) / 40.0, 0.0, 1.0)
+    esl = lambda t: 611.2 * np.exp(17.67 * (t - T0) / (t - 29.65))
+    esi = lambda t: 611.2 * np.exp(21.8745584 * (t - 273.16) / (t - 7.66))
+    qi0 = qi.copy()
+    qcl = qc + qi
+    dsum = np.zeros_like(T)
+    for _ in range(3):
+        f = fice(T)
+        e = esl(T) * (1 - f) + esi(T) * f
+        qs = 0.622 * e / np.maximum(p - e, 100.0)
+        Lh = LV * (1 - f) + LS * f
+        d = (qv - qs) / (1.0 + Lh * Lh * qs / (CPD * RV * T * T))
+        d = np.maximum(d, -qcl)
+        qv, qcl, T, dsum = qv - d, qcl + d, T + Lh / CPD * d, dsum + d
+    f = fice(T)
+    qi = f * qcl
+    qc = qcl - qi
+    T = T + LF / CPD * (qi - qi0 - f * dsum)
+    return T, qv, qc, qi
+
+
 def apply(pairs, outputs, norm, dt):
-    """The surrogate kernel's use of the outputs on each recorded cell: scaled tendencies, positivity, total water.
-    Returns the new (T, qv, qc, qi, qr, qs, qg, Nr) before the sponge factor and the final clips."""
+    """The surrogate kernel's use of the outputs on each recorded cell: scaled process tendencies, the noise floor of
+    empty species, positivity, total water, the rain-number bounds, then the saturation adjustment. Returns the new
+    (T, qv, qc, qi, qr, qs, qg, Nr) before the sponge factor and the final clips."""
     n = split_norm(norm)
     x = np.asarray(pairs, np.float64)
     scale = dt / n["dt"] if n["dt"] > 0 else 1.0
     d = outputs[:, :NLOSS] * n["out_scale"][:NLOSS] * scale
     q = np.stack([x[:, 3], x[:, 4], x[:, 6], x[:, 5], x[:, 7], x[:, 8]], 1)  # qv, qc, qi, qr, qs, qg
-    dq = np.maximum(d[:, 1:7], -q)
+    dq = np.where((q == 0) & (d[:, 1:7] < NEW_SPECIES_FLOOR), 0.0, d[:, 1:7])
+    dq = np.maximum(dq, -q)
     gain = np.where(dq > 0, dq, 0).sum(1)
     loss = -np.where(dq < 0, dq, 0).sum(1)
     fg = np.where(gain > loss, loss / np.where(gain > 0, gain, 1), 1.0)
     fl = np.where(loss > gain, gain / np.where(loss > 0, loss, 1), 1.0)
     qn = q + dq * np.where(dq > 0, fg[:, None], fl[:, None])
     T = x[:, 0] + d[:, 0]
-    nr = np.maximum(x[:, 9] + d[:, 7], 0.0)
-    return np.column_stack([T, qn, nr])
+    nr = x[:, 9] + d[:, 7]
+    qr = qn[:, 3]
+    nr = np.where(qr > 1e-9, np.clip(nr, qr * 3.183e5, qr * 3.183e11), 0.0)
+    T, qv, qc, qi = sat_adjust(T, qn[:, 0], qn[:, 1], qn[:, 2], x[:, 1])
+    return np.column_stack([T, qv, qc, qi, qn[:, 3], qn[:, 4], qn[:, 5], nr])

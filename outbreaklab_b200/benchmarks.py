@@ -2,6 +2,7 @@
 
   python -m outbreaklab_b200.benchmarks solve --nx 1024 --ny 1024 --nz 80 --precision 2 --reps 20
   python -m outbreaklab_b200.benchmarks step --case c4 --steps 50
+  python -m outbreaklab_b200.benchmarks surrogate [--nx 512] [--minutes 60] [--pairs 100000000]
 
 The solve benchmark's right-hand side is the 5 km-correlated Gaussian random field of the 1024 x 1024 x 80 case
 (zero horizontal mean per level), with the Weisman-Klemp densities; errors and residuals are computed in FP64 on the
@@ -65,6 +66,76 @@ def step(args):
                       "sim_s_per_wall_s": args.steps * case.dt / (t.value / 1000.0), "solver": m.solver}), flush=True)
 
 
+def _storm_metrics(m):
+    """Accumulated surface rain (kg), maximum composite reflectivity (dBZ), maximum updraft (m/s), and the cells
+    holding any condensate / at least the surrogate's 1e-5 kg/kg of it."""
+    from . import _native as N
+    mp = m.request_maps()
+    q1 = m.get_field(N.FIELD_Q1).reshape(-1, 4)
+    q2 = m.get_field(N.FIELD_Q2).reshape(-1, 4)
+    cond = q1[:, 1:4].astype(np.float64).sum(1) + q2[:, 0:2].astype(np.float64).sum(1)
+    return {"rain_kg": m.budgets()["rain"], "max_dbz": float(mp["m0"][..., 0].max()), "max_w": float(mp["m1"][..., 0].max()),
+            "cells_with_condensate": int((cond > 0).sum()), "cells_above_1e-5": int((cond >= 1e-5).sum())}
+
+
+def surrogate(args):
+    """Plain Thompson-style microphysics vs the MLP surrogate on the 512 x 512 x 40 (500 m, dt 3 s) case: training
+    pairs recorded from a plain run of the same grid and step with other seeded bubbles, training on the GPU, then
+    two runs of the evaluation case from the same initial state, timed on the device (CUDA events)."""
+    import ctypes as C
+    from . import _native as N, surrogate as S
+    nx = args.nx
+    dx, dt = 500.0, 3.0
+    steps = int(round(args.minutes * 60 / dt))
+    L = nx * dx
+    edge = min(40000.0, 0.15 * L)
+    sep = min(35000.0, 0.2 * L)
+    mk = lambda name, seed: W.StormCase(name, nx, nx, 40, dx, dt, steps, scheme=1,
+                                        bubbles=W.place_bubbles(8, L, L, seed=seed, min_sep=sep, edge=edge))
+    out = {"bench": "microphysics surrogate", "grid": [nx, nx, 40], "dx": dx, "dt": dt, "minutes": args.minutes}
+    net = S.MicroSurrogate(seed=args.seed)
+    net.reserve(args.pairs)
+    # training data: a plain run with another bubble draw (one-step tendencies of an instantaneous saturation
+    # adjustment do not scale with dt, so the pairs come from the same time step as the runs they serve)
+    tm, _ = M.setup_case(mk("train", args.seed + 100))
+    t0 = time.time()
+    S.record(tm, net, steps, dt, args.rate)
+    tm.sync()
+    out["record_s"] = time.time() - t0
+    tm.destroy()
+    out["pairs"] = net.count()
+    net.fit_norm(dt, margin=args.margin)
+    out["range_margin"] = args.margin
+    t0 = time.time()
+    losses = []
+    for lr, frac in ((args.lr, 0.6), (args.lr * 0.3, 0.25), (args.lr * 0.1, 0.15)):
+        losses.append(net.train(args.batch, max(1, int(args.train_steps * frac)), lr))
+    out["train_s"] = time.time() - t0
+    out["train_loss"] = losses
+    out["train_steps"] = args.train_steps
+    out["batch"] = args.batch
+    res = {}
+    for mode in ("plain", "surrogate"):
+        m, _ = M.setup_case(mk("eval", 4))
+        if mode == "surrogate":
+            m.set_surrogate(net)
+        t = C.c_float()
+        N.check(N.lib().ob_model_timed_steps(m.h, dt, steps, C.byref(t)))
+        r = {"ms_per_step": t.value / steps, "sim_s_per_wall_s": steps * dt / (t.value / 1000.0),
+             "cell_steps_per_s": m.nx * m.ny * m.nz * steps / (t.value / 1000.0)}
+        r.update(_storm_metrics(m))
+        if mode == "surrogate":
+            r["queued_last_step"], r["fallbacks_last_step"] = m.surrogate_stats()
+        res[mode] = r
+        m.destroy()
+    out.update(res)
+    p, q = res["plain"], res["surrogate"]
+    out["speedup"] = q["sim_s_per_wall_s"] / p["sim_s_per_wall_s"]
+    out["rain_rel_diff"] = (q["rain_kg"] - p["rain_kg"]) / max(abs(p["rain_kg"]), 1e-30)
+    out["max_dbz_diff"] = q["max_dbz"] - p["max_dbz"]
+    print(json.dumps(out), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -81,8 +152,18 @@ def main(argv=None):
     b.add_argument("--steps", type=int, default=50)
     b.add_argument("--warmup", type=int, default=5)
     b.add_argument("--solver", type=int, default=None)
+    c = sub.add_parser("surrogate")
+    c.add_argument("--nx", type=int, default=512)
+    c.add_argument("--minutes", type=float, default=60.0)
+    c.add_argument("--pairs", type=int, default=100_000_000)
+    c.add_argument("--rate", type=float, default=0.3)
+    c.add_argument("--batch", type=int, default=16384)
+    c.add_argument("--train-steps", type=int, default=20000)
+    c.add_argument("--lr", type=float, default=1e-3)
+    c.add_argument("--seed", type=int, default=1)
+    c.add_argument("--margin", type=float, default=0.05, help="trusted input range: training range widened by this share")
     args = ap.parse_args(argv)
-    {"solve": solve, "step": step}[args.cmd](args)
+    {"solve": solve, "step": step, "surrogate": surrogate}[args.cmd](args)
 
 
 if __name__ == "__main__":

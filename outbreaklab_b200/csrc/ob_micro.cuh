@@ -10,10 +10,10 @@ struct MCell {
   float T, qv, qc, qi, qr, qs, qg, nr;
 };
 
-// Lin-type (micro2.z = 0) or Thompson-style (micro2.z = 1) microphysics on one cell: warm rain, ice-phase
-// conversions, melting, rain evaporation, Thompson self-collection, sublimation and the 3-iteration mixed-phase
-// saturation adjustment. p0 and rho are the level's base-state pressure and density, rs = sqrt(rho_sfc / rho).
-__device__ __forceinline__ void micro_plain(const Uni& U, float dt, float p0, float rho, float rs, MCell& m) {
+// The process rates of the Lin-type (micro2.z = 0) or Thompson-style (micro2.z = 1) microphysics on one cell: warm
+// rain, ice-phase conversions, melting, rain evaporation, Thompson self-collection and sublimation (model.js:791-892).
+// p0 and rho are the level's base-state pressure and density, rs = sqrt(rho_sfc / rho).
+__device__ __forceinline__ void micro_processes(const Uni& U, float dt, float p0, float rho, float rs, MCell& m) {
   const bool thm = U.micro2.z > 0.5f;
   float T = m.T, qv = m.qv, qc = m.qc, qi = m.qi, qr = m.qr, qs = m.qs, qg = m.qg, nr = m.nr;
   const float rq = 1000.f * rho;
@@ -130,6 +130,12 @@ __device__ __forceinline__ void micro_plain(const Uni& U, float dt, float p0, fl
     qv += e;
     T -= float(LSCd / CPDd) * e;
   }
+  m.T = T; m.qv = qv; m.qc = qc; m.qi = qi; m.qr = qr; m.qs = qs; m.qg = qg; m.nr = nr;
+}
+
+// the 3-iteration mixed-phase saturation adjustment that closes the block (model.js:893-905)
+__device__ __forceinline__ void sat_adjust(float p0, MCell& m) {
+  float T = m.T, qv = m.qv, qc = m.qc, qi = m.qi;
   // mixed-phase saturation adjustment, 3 iterations (model.js:893-905)
   const float qi0 = qi;
   float qcl = qc + qi, dsum = 0.f;
@@ -149,7 +155,24 @@ __device__ __forceinline__ void micro_plain(const Uni& U, float dt, float p0, fl
   qi = f * qcl;
   qc = qcl - qi;
   T += float(LFCd / CPDd) * (qi - qi0 - f * dsum);
-  m.T = T; m.qv = qv; m.qc = qc; m.qi = qi; m.qr = qr; m.qs = qs; m.qg = qg; m.nr = nr;
+  m.T = T; m.qv = qv; m.qc = qc; m.qi = qi;
+}
+
+// the whole block (model.js:775-905)
+__device__ __forceinline__ void micro_plain(const Uni& U, float dt, float p0, float rho, float rs, MCell& m) {
+  micro_processes(U, dt, p0, rho, rs, m);
+  sat_adjust(p0, m);
+}
+
+// a cell the process rates can change: it holds a hydrometeor (without one, every rate is exactly zero)
+__device__ __forceinline__ bool micro_has_hydrometeor(const MCell& m) { return m.qc + m.qi + m.qr + m.qs + m.qg > 0.f; }
+
+// The surrogate's domain: cells holding at least this much condensate (kg/kg). Cells with only traces run the scheme,
+// which removes traces exactly (complete evaporation or sublimation, the rain-number reset); a network's small
+// errors on them would otherwise leave traces everywhere that never vanish.
+constexpr float kSurrogateMinCondensate = 1e-5f;
+__device__ __forceinline__ bool surrogate_cell(const MCell& m) {
+  return m.qc + m.qi + m.qr + m.qs + m.qg >= kSurrogateMinCondensate;
 }
 
 // a cell the microphysics can change: it holds a hydrometeor or is supersaturated. Elsewhere micro_plain only sets

@@ -1,7 +1,8 @@
 // ob_mlp_tc.cu — the microphysics surrogate inside the model step (sm_100a): a persistent tcgen05 kernel that runs
-// the 12 -> 3 x 128 GELU -> 10 MLP on the cells the physics pass queued (those holding a hydrometeor or
-// supersaturated), enforces positivity and total-water conservation on its tendencies, and falls back to the scheme
-// (micro_plain) for cells whose inputs lie outside the training range.
+// the 12 -> 3 x 128 GELU -> 10 MLP on the cells the physics pass queued (those holding a hydrometeor), applies its
+// process tendencies with positivity and total-water conservation enforced, closes with the scheme's saturation
+// adjustment (thermodynamic equilibrium, not a process rate), and falls back to the whole scheme (micro_plain) for
+// cells whose inputs lie outside the training range.
 //
 // One CTA per SM, 256 threads in two independent groups of 4 warps; each group takes tiles of 128 queued cells (one
 // cell per thread = one TMEM lane) and runs the four layers as tcgen05.mma (M = 128 cells, BF16 operands, FP32
@@ -40,6 +41,7 @@ constexpr int WIMG_BYTES = OFF_W4 + W4_BYTES;  // 86016
 constexpr int ACT_BYTES = 2 * 128 * 128;       // one group's activation tile: 128 cells x 128 K bf16
 constexpr int SMEM_INFER = WIMG_BYTES + 2 * ACT_BYTES + 1024 + 64;
 constexpr int NBIAS = 3 * NH + W4_ROWS;
+constexpr float kNewSpeciesFloor = 1e-8f;  // kg/kg per step: gains of an empty species below this are noise
 
 // byte offset of element (row r, column k) in a K-major 128-byte-swizzled operand of `rows` rows (64 columns per
 // tile): rows of 128 bytes, the 16-byte chunk index XORed with the row index mod 8 (the layout TMA writes)
@@ -195,12 +197,13 @@ __global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, i
       float d[NLOSS];
 #pragma unroll
       for (int e = 0; e < NLOSS; e++) d[e] = (y[e] + __ldg(net.bias + 3 * NH + e)) * nm.out_scale[e] * tscale;
-      // positivity: no species loses more than it holds; total water: the six water tendencies sum to zero, by
-      // shrinking whichever side (gains or losses) is larger
+      // no species appears from below the network's noise floor; no species loses more than it holds; the six
+      // water tendencies sum to zero (total water), by shrinking whichever side, gains or losses, is larger
       float q[6] = {m.qv, m.qc, m.qi, m.qr, m.qs, m.qg};
       float gain = 0.f, loss = 0.f;
 #pragma unroll
       for (int s = 0; s < 6; s++) {
+        if (q[s] == 0.f && d[1 + s] < kNewSpeciesFloor) d[1 + s] = 0.f;
         d[1 + s] = fmaxf(d[1 + s], -q[s]);
         if (d[1 + s] > 0.f) gain += d[1 + s]; else loss -= d[1 + s];
       }
@@ -209,7 +212,12 @@ __global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, i
       for (int s = 0; s < 6; s++) q[s] += d[1 + s] * (d[1 + s] > 0.f ? fg : fl);
       m.qv = q[0]; m.qc = q[1]; m.qi = q[2]; m.qr = q[3]; m.qs = q[4]; m.qg = q[5];
       m.T += d[0];
-      m.nr = fmaxf(m.nr + d[7], 0.f);
+      // the scheme's own bounds on the rain number (model.js:874-884): none without rain, else within the
+      // mass-weighted limits
+      const float nr = m.nr + d[7];
+      m.nr = m.qr > 1e-9f ? clampf(nr, m.qr * 3.183e5f, m.qr * 3.183e11f) : 0.f;
+      // the saturation adjustment is thermodynamic equilibrium, not a process rate: it runs as in the scheme
+      sat_adjust(p0, m);
     } else {
       micro_plain(U, dt, p0, rho, rs, m);
       atomicAdd(F.mlp_count + 1, 1u);  // fallbacks of this step

@@ -824,9 +824,10 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     const bool thm = U.micro2.z > 0.5f;
     MCell mc{T, qv, qc, qi, qr, qs, qg, fmaxf(q2[2], 0.f)};
     bool done = false;
-    if (MM == kMicroSurrogate && micro_active(mc, p0)) {
+    if (MM == kMicroSurrogate && surrogate_cell(mc)) {
       // surrogate cell: store the state before the microphysics and queue the cell; the surrogate kernel applies
-      // the tendencies, the sponge removal and the clips (a full queue falls through to the scheme here)
+      // the process tendencies, the saturation adjustment, the sponge removal and the clips (a full queue falls
+      // through to the scheme here)
       const unsigned slot = warp_append(F.mlp_count);
       if (slot < F.mlp_cap) {
         reinterpret_cast<unsigned*>(F.mlp_buf)[slot] = unsigned(o);
@@ -839,10 +840,11 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     }
     if (!done) {
       const MCell pre = mc;
-      micro_plain(U, dt, p0, rho, spk.z, mc);
-      if (MM == kMicroRecord && micro_active(pre, p0) &&
+      micro_processes(U, dt, p0, rho, spk.z, mc);
+      if (MM == kMicroRecord && surrogate_cell(pre) &&
           float(hash3i(ci, cj, ck ^ int(__float_as_uint(U.step.y) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
-        // one (state, tendency) pair of the scheme: 12 inputs, 10 tendencies, the cell's texel offset (as bits), 1 pad
+        // one (state, process tendency) pair of the scheme: 12 inputs, 10 tendencies (before the saturation
+        // adjustment), the cell's texel offset (as bits), 1 pad
         const unsigned slot = warp_append(F.mlp_count);
         if (slot < F.mlp_cap) {
           float* r = F.mlp_buf + size_t(slot) * 24;
@@ -856,6 +858,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
           }
         }
       }
+      sat_adjust(p0, mc);
       T = mc.T; qv = mc.qv; qc = mc.qc; qi = mc.qi; qr = mc.qr; qs = mc.qs; qg = mc.qg;
       float nr = mc.nr;
       th = T / pi0;

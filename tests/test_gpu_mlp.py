@@ -101,7 +101,7 @@ def test_recorded_pairs_are_scheme_tendencies(native):
     i, j, k = off % px, (off // px) % (case.ny + 1), off // (px * (case.ny + 1))
     assert (i < case.nx).all() and (j < case.ny).all() and (k < case.nz).all()
     assert len(np.unique(off)) == len(off)
-    # the microphysics block conserves total water: the six water tendencies cancel to fp32 rounding
+    # the process rates conserve total water: the six water tendencies cancel to fp32 rounding
     dq = P[:, 13:19].astype(np.float64)
     q = P[:, 3:9].astype(np.float64)
     assert np.abs(dq.sum(1)).max() <= 1e-6 * q.sum(1).max()
@@ -121,8 +121,9 @@ def _cell_state(model, case, B, off):
 
 
 def test_tensor_core_inference_in_the_step(native):
-    """One surrogate step: the queued cells are exactly the recorded ones, none falls back, and each cell's T and qv
-    equal the oracle's bf16-emulating forward pass with the positivity and total-water projection applied."""
+    """One surrogate step: the queued cells are exactly the recorded ones (those holding condensate), none falls
+    back, and each cell's T and qv equal the oracle's bf16-emulating forward pass with the projection and the
+    saturation adjustment applied."""
     case, a, B, rec, P = _record_one_step()
     net = S.MicroSurrogate(seed=11)
     net.reserve(len(P))
@@ -139,12 +140,15 @@ def test_tensor_core_inference_in_the_step(native):
     Y, _ = MO.forward(net.params().astype(np.float64), X, emulate_bf16=True)
     ref = MO.apply(P, Y, norm.astype(np.float64), case.dt)
     sc = norm[24:34].astype(np.float64)
+    # compare the changes the network made: after the saturation adjustment, with its latent heat
     dT, dq = np.abs(T - ref[:, 0]), np.abs(qv - ref[:, 1])
     # bf16 activations, the hardware tanh and the summation order: a few percent of an output's spread at most;
     # a wrong operand layout would be off by the spread itself
-    assert dT.max() <= 0.05 * sc[0] + 1e-3, (dT.max(), sc[0])
-    assert dq.max() <= 0.05 * sc[1] + 1e-8, (dq.max(), sc[1])
-    assert np.median(dT) <= 0.01 * sc[0] + 1e-4
+    # (cells at the edge of saturation can condense on one side and not the other, so the bound on the largest
+    # difference is looser than on the 99th percentile)
+    for d, s_ in ((dT, sc[0]), (dq, sc[1])):
+        assert np.percentile(d, 99) <= 0.02 * s_, (np.percentile(d, 99), s_)
+        assert d.max() <= 0.3 * s_, (d.max(), s_)
 
 
 def test_out_of_range_cells_fall_back_to_the_scheme(native):
