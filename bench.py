@@ -287,8 +287,28 @@ def run_ours(args, rank, world):
             "e2e": {"value": e2e_val, "unit": "sim-s/wall-s", "h2d_bytes_per_step": int(pinned.nbytes * 0) + 304,
                     "d2h_bytes_per_step": 24, "steps": ke},
             "gpu_launches": None, "nan_guard_count": m.nan_count}
-    launches_per_step = 15  # CI, NUT, ADVV x2, ADVQ x2, PHYS, DIV, 4 transforms, 2 tridiagonal, PROJ, RAIN
-    line["gpu_launches"] = int(args.steps * launches_per_step + math.ceil(args.steps / 10))
+    # CI, NUT, ADVV x2, ADVQ x2, PHYS, DIV, the refined solve (8 transforms, 2 tridiagonals, 1 residual), PROJ, RAIN;
+    # LSF every 60 s of model time
+    launches_per_step = 20
+    line["gpu_launches"] = int(args.steps * launches_per_step + math.ceil(args.steps * case.dt / 60.0))
+    if rank == 0 and world == 1 and not args.no_mlp:
+        # the metric's second half: plain vs MLP microphysics on the 512 x 512 x 40 Thompson case, 60 minutes
+        from outbreaklab_b200 import benchmarks as BM
+        try:
+            r = BM.surrogate_compare()
+            line["mlp"] = {
+                "workload": "512x512x40 dx 500 m dz 500 m dt 3 s, Thompson-style, 8 warm bubbles, 60 min; surrogate "
+                            "12->3x128 GELU->10, BF16 weights / FP32 accumulation on tcgen05",
+                "plain_sim_s_per_wall_s": r["plain"]["sim_s_per_wall_s"],
+                "mlp_sim_s_per_wall_s": r["surrogate"]["sim_s_per_wall_s"],
+                "plain_cell_steps_per_s": r["plain"]["cell_steps_per_s"],
+                "mlp_cell_steps_per_s": r["surrogate"]["cell_steps_per_s"],
+                "speedup": r["speedup"], "rain_rel_diff": r["rain_rel_diff"], "max_dbz_diff": r["max_dbz_diff"],
+                "max_w_rel_diff": r["max_w_rel_diff"], "pairs": r["pairs"], "train_s": r["train_s"],
+                "train_loss": r["train_loss"][-1], "queued_last_step": r["surrogate"]["queued_last_step"],
+                "fallbacks_last_step": r["surrogate"]["fallbacks_last_step"]}
+        except Exception as e:  # the headline line still prints
+            line["mlp"] = {"error": str(e)[:300]}
     if rank == 0:
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(case, 1)
@@ -304,6 +324,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mlp", action="store_true", help="skip the plain vs MLP microphysics leg")
     ap.add_argument("--nx", type=int, default=0, help="smaller square domain (profiling captures); 0 = 640")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

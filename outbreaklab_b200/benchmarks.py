@@ -78,13 +78,15 @@ def _storm_metrics(m):
             "cells_with_condensate": int((cond > 0).sum()), "cells_above_1e-5": int((cond >= 1e-5).sum())}
 
 
-def surrogate(args):
+def surrogate_compare(nx=512, minutes=60.0, pairs=100_000_000, rate=0.3, batch=16384, train_steps=20000, lr=1e-3,
+                      seed=1, margin=0.05):
     """Plain Thompson-style microphysics vs the MLP surrogate on the 512 x 512 x 40 (500 m, dt 3 s) case: training
     pairs recorded from a plain run of the same grid and step with other seeded bubbles, training on the GPU, then
-    two runs of the evaluation case from the same initial state, timed on the device (CUDA events)."""
+    two runs of the evaluation case from the same initial state, timed on the device (CUDA events). Returns a dict."""
     import ctypes as C
     from . import _native as N, surrogate as S
-    nx = args.nx
+    args = argparse.Namespace(nx=nx, minutes=minutes, pairs=pairs, rate=rate, batch=batch, train_steps=train_steps, lr=lr,
+                              seed=seed, margin=margin)
     dx, dt = 500.0, 3.0
     steps = int(round(args.minutes * 60 / dt))
     L = nx * dx
@@ -133,7 +135,13 @@ def surrogate(args):
     out["speedup"] = q["sim_s_per_wall_s"] / p["sim_s_per_wall_s"]
     out["rain_rel_diff"] = (q["rain_kg"] - p["rain_kg"]) / max(abs(p["rain_kg"]), 1e-30)
     out["max_dbz_diff"] = q["max_dbz"] - p["max_dbz"]
-    print(json.dumps(out), flush=True)
+    out["max_w_rel_diff"] = (q["max_w"] - p["max_w"]) / max(abs(p["max_w"]), 1e-30)
+    return out
+
+
+def surrogate(args):
+    print(json.dumps(surrogate_compare(args.nx, args.minutes, args.pairs, args.rate, args.batch, args.train_steps, args.lr,
+                                       args.seed, args.margin)), flush=True)
 
 
 def main(argv=None):
