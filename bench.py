@@ -289,7 +289,7 @@ def run_ours(args, rank, world):
             "gpu_launches": None, "nan_guard_count": m.nan_count}
     # CI, NUT, ADVV x2, ADVQ x2, PHYS, DIV, the refined solve (8 transforms, 2 tridiagonals, 1 residual), PROJ, RAIN;
     # LSF every 60 s of model time
-    launches_per_step = 20
+    launches_per_step = 21
     line["gpu_launches"] = int(args.steps * launches_per_step + math.ceil(args.steps * case.dt / 60.0))
     if rank == 0 and world == 1 and not args.no_mlp:
         # the metric's second half: plain vs MLP microphysics on the 512 x 512 x 40 Thompson case, 60 minutes
