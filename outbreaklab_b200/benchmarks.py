@@ -3,6 +3,7 @@
   python -m outbreaklab_b200.benchmarks solve --nx 1024 --ny 1024 --nz 80 --precision 2 --reps 20
   python -m outbreaklab_b200.benchmarks step --case c4 --steps 50
   python -m outbreaklab_b200.benchmarks surrogate [--nx 512] [--minutes 60] [--pairs 100000000]
+  python -m outbreaklab_b200.benchmarks ensemble [--members 24] [--steps 50]     (torchrun: members shard over ranks)
 
 The solve benchmark's right-hand side is the 5 km-correlated Gaussian random field of the 1024 x 1024 x 80 case
 (zero horizontal mean per level), with the Weisman-Klemp densities; errors and residuals are computed in FP64 on the
@@ -144,6 +145,33 @@ def surrogate(args):
                                        args.seed, args.margin)), flush=True)
 
 
+def ensemble(args):
+    """The C5 ensemble: members drawn by seed, sharded over ranks by cell count (torchrun sets WORLD_SIZE), each
+    rank stepping its members concurrently; rank 0 prints the gathered metrics."""
+    from . import ensemble as E
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = (torch, td)
+    cases = E.draw_members(args.members, args.seed, steps=args.steps)
+    mine = [cases[i] for i in E.plan_shards(cases, world)[rank]]
+    local = E.run(mine, args.steps, args.warmup)
+    res = E.gather(local, dist)
+    if rank == 0:
+        res.update({"bench": "ensemble", "members": len(cases), "cells": sum(c.cells for c in cases), "steps": args.steps,
+                    "n_gpus": world, "host_launch_ms_rank0": local["host_launch_ms"],
+                    "device_ms_rank0": local["device_ms"], "nan_guard_count_rank0": local["nan_guard_count"],
+                    "grids": [[c.nx, c.ny, c.nz, c.dx] for c in cases]})
+        print(json.dumps(res), flush=True)
+    if dist:
+        dist[1].destroy_process_group()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -170,8 +198,13 @@ def main(argv=None):
     c.add_argument("--lr", type=float, default=1e-3)
     c.add_argument("--seed", type=int, default=1)
     c.add_argument("--margin", type=float, default=0.05, help="trusted input range: training range widened by this share")
+    e = sub.add_parser("ensemble")
+    e.add_argument("--members", type=int, default=24)
+    e.add_argument("--steps", type=int, default=50)
+    e.add_argument("--warmup", type=int, default=3)
+    e.add_argument("--seed", type=int, default=5)
     args = ap.parse_args(argv)
-    {"solve": solve, "step": step, "surrogate": surrogate}[args.cmd](args)
+    {"solve": solve, "step": step, "surrogate": surrogate, "ensemble": ensemble}[args.cmd](args)
 
 
 if __name__ == "__main__":
