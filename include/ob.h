@@ -112,9 +112,15 @@ int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain);
  * reference, whose GPUProfiler (util.js:194-230) is never instantiated) */
 int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms);
 /* one step with CUDA events between its passes; ms[i] = device time of pass i in the order
- * (LSF+CI, NUT, ADVV, ADVQ, PHYS, DIV, SOLVE, PROJ+RAIN). Returns the number of passes, or -status. */
+ * (LSF+CI, NUT, ADVV, ADVQ, PHYS, DIV, SOLVE, PROJ+RAIN). The passes run one after another on the model's stream
+ * here (ob_model_step overlaps NUT, ADVV and ADVQ on side streams). Returns the number of passes, or -status. */
 #define OB_NPASS 8
 int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
+/* replay of captured steps (on by default; no counterpart in the reference): from the second step of each variant
+ * (parity, LSF due, microphysics mode) on, ob_model_step replays a CUDA graph of the step instead of launching its
+ * ~21 kernels one by one, as long as the step's uniforms and buffers are the ones it was captured with; on = 0
+ * launches every kernel directly. Results are identical either way. */
+int ob_model_set_graphs(ObModel* m, int on);
 /* pressure-solve precision of the model: 0 = fp32 SIMT transforms (the reference's arithmetic), 1 = bf16x3
  * tensor-core transforms, 2 = bf16x3 + one refinement sweep (the default where nz is 16, 40 or 80).
  * No counterpart in the reference. */

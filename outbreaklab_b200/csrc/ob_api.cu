@@ -73,6 +73,10 @@ struct ObModel {
   ObParams P{};
   Uni U{};
   cudaStream_t stream = nullptr;
+  // NUT and ADVQ read only the previous state, as ADVV does: they run on two side streams between a fork event
+  // after CI and a join before PHYS, so the three issue-bound passes share the SMs
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   float* pool = nullptr;
   float* stage = nullptr;      // texel-layout staging for field transfers
   size_t stage_bytes = 0;
@@ -100,6 +104,16 @@ struct ObModel {
   bool surrogate = false;
   ObMlp* rec = nullptr;  // recording (state, tendency) pairs into this network's buffer, at rate rec_rate
   float rec_rate = 0.f;
+  double* d_clock = nullptr;  // model time on the device (Fields::clock)
+  // captured steps, one per (parity, LSF this step, microphysics mode); replayed while the uniforms and field
+  // pointers they were captured with are unchanged (model time is on the device)
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    Uni U{};
+    Fields F{};
+    int seen = 0;
+  } graphs[2][2][3];
+  bool use_graphs = true;
   PoissonPlan solver;
   std::vector<float> Bh;
   double rhoSfc = 1.15, dx = 0, dz = 0, Lx = 0, Ly = 0;
@@ -120,12 +134,27 @@ static void model_bind_solver(ObModel* m) {
   }
 }
 
+static void drop_graphs(ObModel* m) {
+  for (auto& a : m->graphs)
+    for (auto& b : a)
+      for (auto& G : b) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G = ObModel::StepGraph{};
+      }
+}
+
 static void model_free(ObModel* m) {
   if (!m) return;
+  drop_graphs(m);
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_queue, (void*)m->d_mlpc, m->d_surr, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_queue, (void*)m->d_mlpc, m->d_surr, (void*)m->d_clock, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
+  for (int i = 0; i < 2; i++) {
+    if (m->side[i]) cudaStreamDestroy(m->side[i]);
+    if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
+  }
+  if (m->ev_fork) cudaEventDestroy(m->ev_fork);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
 }
@@ -137,7 +166,7 @@ static void write_uniforms(ObModel* m, double dt) {
   auto v4 = [](double a, double b, double c, double d) { return make_float4(float(a), float(b), float(c), float(d)); };
   Uni& U = m->U;
   U.dims = v4(m->g.nx, m->g.ny, m->g.nz, m->dx);
-  U.step = v4(dt, m->time, m->rhoSfc, 9.81);
+  U.step = v4(dt, 0.0, m->rhoSfc, 9.81);  // model time: Fields::clock on the device
   U.sponge = v4(P.spongeW, P.spongeTau, P.dampZ, P.dampTau);
   U.turb = v4(P.cs, P.nu0, P.evap, P.drag != 0.f ? 1 : 0);
   const double cd = std::pow(0.41 / std::log(0.5 * m->dz / P.z0 + 1), 2);
@@ -224,6 +253,11 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
     if (rc == OB_OK) rc = cuda_status(cudaMemset(*p, 0, bytes), what);
   };
   rc = cuda_status(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "stream");
+  for (int i = 0; i < 2 && rc == OB_OK; i++) {
+    rc = cuda_status(cudaStreamCreateWithFlags(&m->side[i], cudaStreamNonBlocking), "side stream");
+    if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&m->ev_join[i], cudaEventDisableTiming), "event");
+  }
+  if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming), "event");
   alloc((void**)&m->pool, fs * 39 * sizeof(float), "model fields");
   alloc((void**)&m->d_B, size_t(nz + 1) * 8 * sizeof(float), "base state");
   alloc((void**)&m->d_bnd, size_t(OB_MAX_BOUNDS) * OB_BOUNDARY_FLOATS * sizeof(float), "boundaries");
@@ -233,6 +267,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   alloc((void**)&m->d_maps, n2 * 4 * sizeof(float4), "maps");
   alloc((void**)&m->d_2d, n2 * 4 * sizeof(float4), "2-D fields");
   alloc((void**)&m->d_red, 8 * sizeof(double), "reductions");
+  alloc((void**)&m->d_clock, sizeof(double), "model clock");
   alloc((void**)&m->rhs32, np * sizeof(float), "rhs");
   alloc((void**)&m->F.phi, np * sizeof(float), "phi");
   m->stage_bytes = std::max(size_t(nx + 1) * (ny + 1) * (nz + 1) * 4, np) * sizeof(float);
@@ -275,6 +310,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->F.bnd = m->d_bnd;
   m->F.ci = m->d_ci;
   m->F.flags = m->d_flags;
+  m->F.clock = m->d_clock;
   m->F.nbx = nbx;
   m->F.nby = nby;
   m->F.actQ0 = m->d_act;
@@ -356,6 +392,7 @@ int ob_model_set_ci(ObModel* m, const float* ev, int n) {
 int ob_model_reset(ObModel* m) {
   if (!m) { set_error("ob_model_reset: null model"); return OB_ERR_INVALID; }
   m->time = 0; m->steps = 0; m->parity = 0;
+  cudaMemsetAsync(m->d_clock, 0, sizeof(double), m->stream);
   write_uniforms(m, 1.0);
   const Grid& g = m->g;
   launch_lsf(g, m->U, m->F, m->stream);
@@ -380,44 +417,102 @@ void mlp_record_target(ObMlp* n, float** buf, unsigned** count, unsigned* cap);
 }
 
 // the physics pass with the model's microphysics mode: the scheme, the scheme while recording pairs, or the surrogate
-static int physics_pass(ObModel* m, int par, cudaStream_t s) {
-  const Grid& g = m->g;
-  if (m->surrogate) {
+static int micro_mode(const ObModel* m) { return m->surrogate ? kMicroSurrogate : (m->rec && m->rec_rate > 0.f) ? kMicroRecord : kMicroPlain; }
+
+// the microphysics fields of the kernel parameters for the model's mode (before a step is launched or captured)
+static int prepare_micro(ObModel* m) {
+  const int mode = micro_mode(m);
+  if (mode == kMicroSurrogate) {
     if (m->P.scheme < 0.5f) { set_error("the microphysics surrogate emulates the Thompson-style scheme (params.scheme = 1)"); return OB_ERR_INVALID; }
     m->F.mlp_buf = reinterpret_cast<float*>(m->d_queue);
     m->F.mlp_count = m->d_mlpc;
     m->F.mlp_cap = m->queue_cap;
-    OB_TRY(cuda_status(cudaMemsetAsync(m->d_mlpc, 0, 2 * sizeof(unsigned), s), "surrogate counters"));
-    launch_phys(g, m->U, m->F, par, s, kMicroSurrogate);
-    launch_surrogate(g, m->U, m->F, par, m->d_surr, m->surr_norm, m->d_flags + 1, s);
-  } else if (m->rec && m->rec_rate > 0.f) {
+    m->F.mlp_rate = 0.f;
+  } else if (mode == kMicroRecord) {
     mlp_record_target(m->rec, &m->F.mlp_buf, &m->F.mlp_count, &m->F.mlp_cap);
     m->F.mlp_rate = m->rec_rate;
-    launch_phys(g, m->U, m->F, par, s, m->F.mlp_buf ? kMicroRecord : kMicroPlain);
   } else {
-    launch_phys(g, m->U, m->F, par, s, kMicroPlain);
+    m->F.mlp_buf = nullptr;
+    m->F.mlp_count = nullptr;
+    m->F.mlp_cap = 0;
+    m->F.mlp_rate = 0.f;
   }
   return OB_OK;
 }
 
-static int model_step_once(ObModel* m, double dt) {
-  write_uniforms(m, dt);
+// the physics pass with the model's microphysics mode: the scheme, the scheme while recording pairs, or the surrogate
+static int physics_pass(ObModel* m, int par, cudaStream_t s) {
+  const Grid& g = m->g;
+  OB_TRY(prepare_micro(m));
+  const int mode = micro_mode(m);
+  if (mode == kMicroSurrogate) {
+    OB_TRY(cuda_status(cudaMemsetAsync(m->d_mlpc, 0, 2 * sizeof(unsigned), s), "surrogate counters"));
+    launch_phys(g, m->U, m->F, par, s, kMicroSurrogate);
+    launch_surrogate(g, m->U, m->F, par, m->d_surr, m->surr_norm, m->d_flags + 1, s);
+  } else {
+    launch_phys(g, m->U, m->F, par, s, m->F.mlp_buf ? mode : kMicroPlain);
+  }
+  return OB_OK;
+}
+
+// every pass of one step, queued on the model's stream (NUT and ADVQ on the side streams)
+static int enqueue_step(ObModel* m, bool lsf, cudaStream_t s) {
   const Grid& g = m->g;
   const int par = m->parity;
-  cudaStream_t s = m->stream;
-  if (m->time - m->lsfT >= 60 || m->time == 0) {
-    launch_lsf(g, m->U, m->F, s);
-    m->lsfT = m->time;
-  }
+  if (lsf) launch_lsf(g, m->U, m->F, s);
   launch_ci(g, m->U, m->F, s);
-  launch_nut(g, m->U, m->F, par, s);
+  cudaEventRecord(m->ev_fork, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(m->side[i], m->ev_fork, 0);
+  launch_nut(g, m->U, m->F, par, m->side[0]);
+  cudaEventRecord(m->ev_join[0], m->side[0]);
+  launch_advq(g, m->U, m->F, par, m->side[1]);
+  cudaEventRecord(m->ev_join[1], m->side[1]);
   launch_advv(g, m->U, m->F, par, s);
-  launch_advq(g, m->U, m->F, par, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(s, m->ev_join[i], 0);
   OB_TRY(physics_pass(m, par, s));
   launch_div(g, m->U, m->F, par, s);
   OB_TRY(m->solver.solve(m->F.rhs, m->F.phi, s));
   launch_proj(g, m->U, m->F, par, s);
   launch_rain(g, m->U, m->F, s);
+  return OB_OK;
+}
+
+// One step. With graphs on, the second occurrence of a (parity, LSF, microphysics mode) variant is captured and
+// later occurrences replay it as long as the uniforms and the kernels' field pointers are the ones it was captured
+// with (the model time lives on the device); the first occurrence runs uncaptured, so every lazy set-up (function
+// attributes, device queries) has happened before any capture.
+static int model_step_once(ObModel* m, double dt) {
+  write_uniforms(m, dt);
+  cudaStream_t s = m->stream;
+  const bool lsf = m->time - m->lsfT >= 60 || m->time == 0;
+  if (lsf) m->lsfT = m->time;
+  OB_TRY(prepare_micro(m));
+  if (!m->use_graphs) {
+    OB_TRY(enqueue_step(m, lsf, s));
+  } else {
+    ObModel::StepGraph& G = m->graphs[m->parity][lsf ? 1 : 0][micro_mode(m)];
+    const bool match = G.exec && std::memcmp(&G.U, &m->U, sizeof(Uni)) == 0 && std::memcmp(&G.F, &m->F, sizeof(Fields)) == 0;
+    if (match) {
+      OB_TRY(cuda_status(cudaGraphLaunch(G.exec, s), "step graph launch"));
+    } else if (G.seen == 0) {
+      G.seen = 1;
+      OB_TRY(enqueue_step(m, lsf, s));
+    } else {
+      if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+      OB_TRY(cuda_status(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "step capture"));
+      const int rc = enqueue_step(m, lsf, s);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      if (rc != OB_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+      OB_TRY(cuda_status(ec, "step capture"));
+      const cudaError_t ei = cudaGraphInstantiate(&G.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      OB_TRY(cuda_status(ei, "step graph instantiate"));
+      G.U = m->U;
+      G.F = m->F;
+      OB_TRY(cuda_status(cudaGraphLaunch(G.exec, s), "step graph launch"));
+    }
+  }
   m->parity = 1 - m->parity;
   m->time += dt;
   m->steps++;
@@ -583,6 +678,14 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   return rc == OB_OK ? e - 1 : -rc;
 }
 
+int ob_model_set_graphs(ObModel* m, int on) {
+  if (!m) { set_error("ob_model_set_graphs: null model"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set graphs"));
+  drop_graphs(m);
+  m->use_graphs = on != 0;
+  return OB_OK;
+}
+
 int ob_model_record_micro(ObModel* m, ObMlp* net, float rate) {
   if (!m || rate < 0.f || rate > 1.f) { set_error("ob_model_record_micro: bad arguments"); return OB_ERR_INVALID; }
   m->rec = rate > 0.f ? net : nullptr;
@@ -632,6 +735,7 @@ int ob_model_set_solver(ObModel* m, int precision) {
     return OB_ERR_INVALID;
   }
   OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set solver"));
+  drop_graphs(m);
   m->solver.destroy();
   OB_TRY(m->solver.create(g.nxp, g.nyp, g.nz, m->dx, m->dz, precision));
   std::vector<float> rc(g.nz), rw(g.nz + 1);

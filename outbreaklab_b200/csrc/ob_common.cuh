@@ -19,6 +19,7 @@ namespace ob {
 struct Uni {
   float4 dims, dzv, step, sponge, turb, micro, misc, cor, ci, pad, micro2, hur, hur2, hur3, hur4, hur5, vtx, vtx2, cn;
   float4 der;  // derived on the host per step: (dt/dx, dt/dz, 1/dx^2, 1/dz^2), so no thread divides uniforms
+  // step.y (the model time of the reference's block) stays 0 here: the kernels read the time from Fields::clock
 };
 
 struct Grid {
@@ -74,6 +75,9 @@ struct Fields {
   unsigned* mlp_count;
   unsigned mlp_cap;
   float mlp_rate;
+  // model time (s) on the device: read by the passes that move with time (LSF, CI, the record-mode draw) and
+  // advanced by the last pass of each step, so a captured step replays unchanged
+  double* clock;
 };
 
 constexpr float T0K = 273.15f;

@@ -71,7 +71,7 @@ __device__ void bpt(const float* bd, int i, float t, float& x, float& y) {
 __global__ void k_lsf(Grid g, Uni U, Fields F) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
-  const float dx = U.dims.w, t = U.step.y;
+  const float dx = U.dims.w, t = float(__ldg(F.clock));
   const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
   float sT = 0, sH = 0, sQ = 0, sHq = 0, sU = 0, sV = 0, sHw = 0, sw = 0, nud = 0;
   const int nb = int(U.cor.z);
@@ -164,7 +164,7 @@ __global__ void k_lsf(Grid g, Uni U, Fields F) {
 __global__ void k_ci(Grid g, Uni U, Fields F) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
-  const float dx = U.dims.w, t = U.step.y;
+  const float dx = U.dims.w, t = float(__ldg(F.clock));
   const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
   float4 best = make_float4(0.f, 0.f, 1500.f, 1500.f);
   const int ne = int(U.ci.x);
@@ -842,7 +842,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       const MCell pre = mc;
       micro_processes(U, dt, p0, rho, spk.z, mc);
       if (MM == kMicroRecord && surrogate_cell(pre) &&
-          float(hash3i(ci, cj, ck ^ int(__float_as_uint(U.step.y) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
+          float(hash3i(ci, cj, ck ^ int(__float_as_uint(float(__ldg(F.clock))) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
         // one (state, process tendency) pair of the scheme: 12 inputs, 10 tendencies (before the saturation
         // adjustment), the cell's texel offset (as bits), 1 pad
         const unsigned slot = warp_append(F.mlp_count);
@@ -959,6 +959,7 @@ __global__ void k_rain(Grid g, Uni U, Fields F) {
   const float2 fv = fl.vtRain(qr, F.Q[0][6][o], rho);
   const double flux = double(rho) * (double(qr) * double(fv.x) + double(qs) * double(fl.vtS(qs, rho)) + double(qg) * double(fl.vtGrau(qg, rho)));
   F.rain[j * g.nx + i] += flux * double(U.step.x);
+  if (i == 0 && j == 0) *F.clock += double(U.step.x);  // the step's last pass advances the model time
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -149,3 +149,27 @@ def test_step_errors(native):
         g.set_base_state(np.zeros(5, np.float32))
     with pytest.raises(N.ObError):
         g.set_surface(np.zeros(4, np.float32), {"ck": 1})
+
+
+def test_graph_replay_equals_direct_launches(native):
+    """25 steps (LSF due at steps 1, 11, 21; both parities): replayed CUDA graphs give the bytes of direct launches."""
+    case = CASES["small-thompson-blob"]()
+    g1, B = M.setup_case(case)
+    g2, _ = M.setup_case(case)
+    q1, q2 = W.hydrometeor_blob(case, B, thompson=True)
+    for g in (g1, g2):
+        g.set_field(N.FIELD_Q1, q1)
+        g.set_field(N.FIELD_Q2, q2)
+    N.check(N.lib().ob_model_set_graphs(g2.h, 0))
+    for _ in range(25):
+        g1.step(case.dt, 1)
+        g2.step(case.dt, 1)
+    g1.sync()
+    g2.sync()
+    assert g1.time == g2.time and g1.steps == 25
+    for f in (N.FIELD_V, N.FIELD_Q1, N.FIELD_Q2, N.FIELD_PHI):
+        assert np.array_equal(g1.get_field(f), g2.get_field(f)), f
+    # the FP64 budget sums use atomics (their order varies run to run): equal to rounding
+    b1, b2 = g1.budgets(), g2.budgets()
+    for k in b1:
+        assert np.isclose(b1[k], b2[k], rtol=1e-12, atol=0), k
