@@ -180,6 +180,32 @@ int ob_radar_cut(ObRadar* r, const ObRadarCut* cut);
 /* replaces the volume's copyBufferToBuffer + mapAsync readback (radar.js:360-363, 394-401): the first bytes of the
  * volume into a caller buffer, after the queued cuts finish */
 int ob_radar_read(ObRadar* r, void* host, size_t bytes);
+/* Level II (Archive II message 31) radial records of one volume, assembled on the GPU from the radar volume: replaces
+ * the per-sweep radial loop of the server's writer (_sweep_block, l2writer.py:91-158; encode_volume's records,
+ * l2writer.py:161-182). The host builds each sweep's radial template (everything that is equal for all radials of
+ * the sweep) and describes it below; each radial = the template with the sweep's gate codes dropped in at data_at
+ * and its sequence number, collection time, radial number, azimuth and status patched (big-endian). host_out gets
+ * every sweep's nrad x rec_len bytes at out_off; compressing the 120-radial records and framing the file stay on
+ * the host. */
+typedef struct ObL2Sweep {
+  uint64_t tpl_off;      /* byte offset of the sweep's radial template in `templates` */
+  uint64_t out_off;      /* byte offset of its radial 0 in host_out */
+  uint32_t rec_len;      /* bytes per radial record (28-byte message header + message 31) */
+  uint32_t nrad;         /* radials */
+  uint32_t nmom;         /* moments present (<= 6) */
+  uint32_t seq0;         /* message sequence number of radial 0 */
+  uint32_t ei, nsw;      /* elevation index, sweeps in the volume */
+  double t0_ms, dur_ms;  /* sweep start (epoch ms) and duration (ms) */
+  double az0;            /* azimuth of radial 0 (deg); radials step 360 / nrad clockwise */
+  uint32_t data_at[6];   /* byte offset of each moment's codes in the record */
+  uint32_t ngates[6];
+  uint64_t src_off[6];   /* byte offset of each moment's codes (nrad x ngates, radial-major) in the radar volume */
+} ObL2Sweep;
+int ob_radar_level2(ObRadar* r, const ObL2Sweep* sweeps, int nsweeps, const uint8_t* templates, size_t template_bytes,
+                    uint8_t* host_out, size_t out_bytes);
+/* upload bytes into the start of the radar volume (no counterpart in the reference: lets a host re-encode a volume
+ * it holds, and tests feed known codes) */
+int ob_radar_write(ObRadar* r, const void* host, size_t bytes);
 /* diagnostics, no counterpart in the reference: the same cut, also returning per gate the moments it quantised
  * (dBZ, Vr, SW, ZDR, rho_hv, KDP; NaN where the gate or moment is empty), radials x REF gates x 6 floats; and the
  * KDP scratch of the last cut (radials x Doppler gates, -1 for empty gates) */

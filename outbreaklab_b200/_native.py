@@ -79,6 +79,8 @@ SYMBOLS = {
     "ob_radar_read": (_i, [_vp, _vp, _sz]),
     "ob_radar_cut_moments": (_i, [_vp, _vp, _fp, _sz]),
     "ob_radar_kdp": (_i, [_vp, _fp, _sz]),
+    "ob_radar_level2": (_i, [_vp, _vp, _i, _vp, _sz, _vp, _sz]),
+    "ob_radar_write": (_i, [_vp, _vp, _sz]),
     "ob_mlp_create": (_i, [C.c_uint, C.POINTER(_vp)]),
     "ob_mlp_destroy": (_i, [_vp]),
     "ob_mlp_set_params": (_i, [_vp, _fp, _i]),

@@ -413,6 +413,8 @@ int surrogate_prepare(const ObMlp* net, void** d_image, mlp::Norm* norm);
 void launch_surrogate(const Grid& g, const Uni& U, const Fields& F, int par, const void* d_image, const mlp::Norm& nm,
                       unsigned int* err, cudaStream_t s);
 void mlp_record_target(ObMlp* n, float** buf, unsigned** count, unsigned* cap);
+void launch_level2(const uint8_t* vol, size_t vol_bytes, const ObL2Sweep* d_sweeps, int nsweeps, int max_nrad, const uint8_t* d_tpl,
+                   uint8_t* d_out, cudaStream_t s);
 }  // namespace ob
 }
 
@@ -940,6 +942,49 @@ int ob_radar_cut_moments(ObRadar* r, const ObRadarCut* c, float* host, size_t co
   OB_TRY(radar_launch(r, c, r->d_mom));
   OB_TRY(cuda_status(cudaMemcpyAsync(host, r->d_mom, need * sizeof(float), cudaMemcpyDeviceToHost, r->m->stream), "radar moments"));
   return cuda_status(cudaStreamSynchronize(r->m->stream), "radar moments");
+}
+
+int ob_radar_write(ObRadar* r, const void* host, size_t bytes) {
+  if (!r || !host || bytes > r->bytes) { set_error("ob_radar_write: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaMemcpyAsync(r->d_out, host, bytes, cudaMemcpyHostToDevice, r->m->stream), "radar write"));
+  return cuda_status(cudaStreamSynchronize(r->m->stream), "radar write");
+}
+
+int ob_radar_level2(ObRadar* r, const ObL2Sweep* sweeps, int nsweeps, const uint8_t* templates, size_t template_bytes,
+                    uint8_t* host_out, size_t out_bytes) {
+  if (!r || !sweeps || nsweeps < 1 || !templates || !host_out) { set_error("ob_radar_level2: null argument"); return OB_ERR_INVALID; }
+  int max_nrad = 0;
+  for (int i = 0; i < nsweeps; i++) {
+    const ObL2Sweep& s = sweeps[i];
+    if (s.nrad < 1 || s.nrad > OB_RADAR_MAX_RADIALS || s.nmom > 6 || s.rec_len < 64 || s.tpl_off + s.rec_len > template_bytes ||
+        s.out_off + uint64_t(s.nrad) * s.rec_len > out_bytes) {
+      set_error("ob_radar_level2: sweep %d does not fit its template or the output", i);
+      return OB_ERR_INVALID;
+    }
+    for (uint32_t m = 0; m < s.nmom; m++)
+      if (s.data_at[m] + s.ngates[m] > s.rec_len || s.src_off[m] + uint64_t(s.nrad) * s.ngates[m] > r->bytes) {
+        set_error("ob_radar_level2: sweep %d moment %u lies outside its record or the volume", i, m);
+        return OB_ERR_INVALID;
+      }
+    max_nrad = std::max(max_nrad, int(s.nrad));
+  }
+  cudaStream_t st = r->m->stream;
+  void *d_sw = nullptr, *d_tpl = nullptr, *d_o = nullptr;
+  int rc = cuda_status(cudaMalloc(&d_sw, sizeof(ObL2Sweep) * nsweeps), "level2 sweeps");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&d_tpl, template_bytes), "level2 templates");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&d_o, out_bytes), "level2 records");
+  if (rc == OB_OK) rc = cuda_status(cudaMemcpyAsync(d_sw, sweeps, sizeof(ObL2Sweep) * nsweeps, cudaMemcpyHostToDevice, st), "level2");
+  if (rc == OB_OK) rc = cuda_status(cudaMemcpyAsync(d_tpl, templates, template_bytes, cudaMemcpyHostToDevice, st), "level2");
+  if (rc == OB_OK) rc = cuda_status(cudaMemsetAsync(d_o, 0, out_bytes, st), "level2");
+  if (rc == OB_OK) {
+    launch_level2(r->d_out, r->bytes, static_cast<const ObL2Sweep*>(d_sw), nsweeps, max_nrad, static_cast<const uint8_t*>(d_tpl),
+                  static_cast<uint8_t*>(d_o), st);
+    rc = cuda_status(cudaMemcpyAsync(host_out, d_o, out_bytes, cudaMemcpyDeviceToHost, st), "level2 readback");
+  }
+  if (rc == OB_OK) rc = cuda_status(cudaStreamSynchronize(st), "level2");
+  for (void* p : {d_sw, d_tpl, d_o})
+    if (p) cudaFree(p);
+  return rc;
 }
 
 int ob_radar_read(ObRadar* r, void* host, size_t bytes) {

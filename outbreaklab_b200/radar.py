@@ -229,6 +229,20 @@ class RadarSim:
         return U
 
     # ---- radar.js:394-412 ----
+    def _volume_header(self, d, run, epoch0):
+        """The JSON header of a volume (radar.js:394-412): site, VCP, and per cut its timing and moment offsets."""
+        R = d["R"]
+        t0 = epoch0 + d["volStart"] * 1000
+        nyq = lambda c: 63.5 if R["opts"].get("aliasing") is False else c["nyquist"]
+        return {
+            "run": run, "icao": R["site"]["id"], "lat": R["site"]["lat"], "lon": R["site"]["lon"],
+            "elev": R["site"]["h"] + 20, "vcp": R["vcpId"], "epoch_ms": round(t0),
+            "sweeps": [{"angle": c["angle"], "superRes": c["superRes"], "kind": c["kind"], "az0": d["az0"],
+                        "nrad": c["nrad"], "nyquist": nyq(c), "unamb_km": 466 if c["kind"] == "surv" else 300,
+                        "start_ms": round(t0 + c["t0"] * 1000), "dur_ms": round(c["dur"] * 1000),
+                        "moments": [{"name": o["name"], "ngates": o["ngates"], "off": o["off"]} for o in c["mom"]]}
+                       for c in R["cuts"]]}
+
     def collect(self, d, run, epoch0):
         R = d["R"]
         buf = np.empty(R["bytes"], np.uint8)
@@ -237,18 +251,20 @@ class RadarSim:
         except Exception:
             R["failed"] += 1
             raise
-        t0 = epoch0 + d["volStart"] * 1000
-        nyq = lambda c: 63.5 if R["opts"].get("aliasing") is False else c["nyquist"]
-        header = {
-            "run": run, "icao": R["site"]["id"], "lat": R["site"]["lat"], "lon": R["site"]["lon"],
-            "elev": R["site"]["h"] + 20, "vcp": R["vcpId"], "epoch_ms": round(t0),
-            "sweeps": [{"angle": c["angle"], "superRes": c["superRes"], "kind": c["kind"], "az0": d["az0"],
-                        "nrad": c["nrad"], "nyquist": nyq(c), "unamb_km": 466 if c["kind"] == "surv" else 300,
-                        "start_ms": round(t0 + c["t0"] * 1000), "dur_ms": round(c["dur"] * 1000),
-                        "moments": [{"name": o["name"], "ngates": o["ngates"], "off": o["off"]} for o in c["mom"]]}
-                       for c in R["cuts"]]}
+        header = self._volume_header(d, run, epoch0)
         R["done"] += 1
         return {"R": R, "header": header, "bytes": buf}
+
+    def collect_level2(self, d, run, epoch0):
+        """The finished volume as an Archive II file, as the server would write it from collect()'s upload
+        (server.py:249-284, l2writer.py:161-188), with the radial records assembled on the GPU from the radar
+        volume (no readback of the raw codes). Returns {"R", "header", "name", "bytes"}."""
+        from . import level2 as L2
+        R = d["R"]
+        header = self._volume_header(d, run, epoch0)
+        data = L2.encode_volume_gpu(R["h"], header)
+        R["done"] += 1
+        return {"R": R, "header": header, "name": L2.archive_name(header["icao"], header["epoch_ms"]), "bytes": data}
 
     # ---- diagnostics (no counterpart in the reference) ----
     def cut_moments(self, R, U):
