@@ -268,18 +268,24 @@ __global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __res
 
 // ---------------------------------------------------------------------------------------------------------------
 // tridiagonal solves in z per mode (l, m) (solver.js:70-103): T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi/lo out.
-// Block = 32 modes in l x 8 in m; forward-sweep coefficients and the right-hand side stay in registers; the result
-// goes out through a shared-memory transpose so that the stores run along m. The lowest 2 x 2 modes (near-singular:
+// Block = 32 modes in l x 16 in m; forward-sweep coefficients and the right-hand side stay in registers; the result
+// goes out through a shared-memory transpose so that every thread stores 16 consecutive m (32 bytes per output
+// row: whole sectors). The lowest 2 x 2 modes (near-singular:
 // Neumann in z, shift ~ -(pi/L)^2) use FP64 factors precomputed on the host at set_density.
 // ---------------------------------------------------------------------------------------------------------------
+// modes in m per block: 16 (whole 32-byte sectors per output row) while a thread's NZ levels fit in the 128 registers
+// of a 512-thread block, else 8
 template <int NZ>
-__global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
+constexpr int tri_tm() { return NZ > 40 ? 8 : 16; }
+template <int NZ>
+__global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
                                                 const double* __restrict__ low, const float* __restrict__ T2,
                                                 __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo) {
   constexpr int KC = 16;  // levels per transpose chunk
-  __shared__ float tile[KC][8][33];
+  constexpr int TRI_TM = tri_tm<NZ>();
+  __shared__ float tile[KC][TRI_TM][33];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
-  const int l = blockIdx.x * 32 + tx, m = blockIdx.y * 8 + ty;
+  const int l = blockIdx.x * 32 + tx, m = blockIdx.y * TRI_TM + ty;
   const bool act = l < nxp && m < nyp;
   const bool lowm = l < 2 && m < 2;
   const long sxy = long(nxp) * nyp;
@@ -331,16 +337,22 @@ __global__ void __launch_bounds__(256) k_tri_tc(int nxp, int nyp, int ldy, const
       if (kc + kk < NZ) tile[kk][ty][tx] = x[kc + kk];
     __syncthreads();
     const int nkc = NZ - kc < KC ? NZ - kc : KC;
-    for (int t = tid; t < nkc * 32; t += 256) {
+    for (int t = tid; t < nkc * 32; t += 32 * TRI_TM) {
       const int kk = t >> 5, lx = t & 31;
       const int ll = blockIdx.x * 32 + lx;
       if (ll < nxp) {
-        __align__(16) __nv_bfloat16 h8[8], l8[8];
+        __align__(16) __nv_bfloat16 h16[TRI_TM], l16[TRI_TM];
 #pragma unroll
-        for (int u = 0; u < 8; u++) tc::split_bf16(tile[kk][u][lx], h8[u], l8[u]);
-        const long o = (long(kc + kk) * nxp + ll) * ldy + blockIdx.y * 8;
-        *reinterpret_cast<uint4*>(ohi + o) = *reinterpret_cast<const uint4*>(h8);
-        *reinterpret_cast<uint4*>(olo + o) = *reinterpret_cast<const uint4*>(l8);
+        for (int u = 0; u < TRI_TM; u++) tc::split_bf16(tile[kk][u][lx], h16[u], l16[u]);
+        // rows hold ldy (a multiple of 8) values: 16-byte aligned; columns past nyp land in the row's zero padding
+        // when the pitch has room for them, else they are skipped
+        const long o = (long(kc + kk) * nxp + ll) * ldy + blockIdx.y * TRI_TM;
+#pragma unroll
+        for (int h = 0; h < TRI_TM / 8; h++)
+          if (blockIdx.y * TRI_TM + h * 8 + 8 <= ldy) {
+            *reinterpret_cast<uint4*>(ohi + o + h * 8) = *reinterpret_cast<const uint4*>(h16 + h * 8);
+            *reinterpret_cast<uint4*>(olo + o + h * 8) = *reinterpret_cast<const uint4*>(l16 + h * 8);
+          }
       }
     }
     __syncthreads();
@@ -544,11 +556,10 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
   launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, T->err, s);
   // tridiagonals -> S_y[k][l][m]
-  dim3 tg((nx + 31) / 32, (ny + 7) / 8);
   switch (nz) {
-    case 16: k_tri_tc<16><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
-    case 40: k_tri_tc<40><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
-    default: k_tri_tc<80><<<tg, dim3(32, 8), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+    case 16: k_tri_tc<16><<<dim3((nx + 31) / 32, (ny + tri_tm<16>() - 1) / tri_tm<16>()), dim3(32, tri_tm<16>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+    case 40: k_tri_tc<40><<<dim3((nx + 31) / 32, (ny + tri_tm<40>() - 1) / tri_tm<40>()), dim3(32, tri_tm<40>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+    default: k_tri_tc<80><<<dim3((nx + 31) / 32, (ny + tri_tm<80>() - 1) / tri_tm<80>()), dim3(32, tri_tm<80>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
   }
   // Y-inv: field rows (k, l), K = m, outputs j  -> S_x[k][j][l]
   launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny}, T->err, s);

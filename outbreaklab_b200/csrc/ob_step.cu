@@ -862,7 +862,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       T = mc.T; qv = mc.qv; qc = mc.qc; qi = mc.qi; qr = mc.qr; qs = mc.qs; qg = mc.qg;
       float nr = mc.nr;
       th = T / pi0;
-      const float keep = 1.f / (1.f + 2.f * dt * sl);
+      const float keep = sl > 0.f ? 1.f / (1.f + 2.f * dt * sl) : 1.f;  // 1 / (1 + 0) == 1 exactly: no division
       qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
       F.Q[0][0][o] = fmaxf(qv, 0.f);
       F.Q[0][1][o] = fmaxf(qc, 0.f);
@@ -891,7 +891,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
 }
 
 template <int MM>
-__global__ void __launch_bounds__(128, 8) k_phys(Grid g, Uni U, Fields F, int par) {
+__global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
