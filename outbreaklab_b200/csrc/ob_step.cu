@@ -219,7 +219,7 @@ __global__ void k_init(Grid g, Uni U, Fields F) {
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_NUT (model.js:342-389): Smagorinsky-Lilly viscosities with the Richardson correction
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_nut(Grid g, Uni U, Fields F, int par) {
+__global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) {
   OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
   // a cell's +1 neighbours on the staggered box always exist; the -1 ones clamp to the edge (offset 0)
   const int o = g.at(ci, cj, ck);
@@ -333,7 +333,7 @@ __device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Gr
   return make_float2(lo, hi);
 }
 
-__global__ void k_advv2(Grid g, Uni U, Fields F, int par) {
+__global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
   const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
