@@ -458,7 +458,7 @@ __device__ __forceinline__ bool region_active(const Grid& g, const Fields& F, Re
 
 // ---- ADVQ1 (model.js:500-529): semi-Lagrangian step of the 8 scalars, channels grouped by the fall speed of
 // their trace (qv, qc, qi, spare [and Nr for Lin] at the air's speed; qr, qs, qg, Nr (Thompson) each their own) ----
-__global__ void __launch_bounds__(128) k_advq1(Grid g, Uni U, Fields F, int par) {
+__global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
@@ -526,7 +526,7 @@ __device__ __forceinline__ float advq2_channel(const Fields& F, const Grid& g, c
   return fmaxf(clampf(r, m.x, m.y), 0.f);
 }
 
-__global__ void __launch_bounds__(128) k_advq2(Grid g, Uni U, Fields F, int par) {
+__global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int par) {
   const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
