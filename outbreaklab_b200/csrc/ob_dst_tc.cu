@@ -37,7 +37,9 @@ constexpr int STAGES = 2;
 constexpr int A_TILE = BM * BK * 2;     // 16 KB per A operand tile (hi or lo)
 constexpr int B_TILE = BNMAX * BK * 2;  // 32 KB per B operand tile slot
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int STG_LD = 33;                          // row pitch (floats) of the epilogue's transpose buffer
+constexpr int STG_BYTES = 4 * 32 * STG_LD * 4;       // 32 x 32 floats per epilogue warp
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + STG_BYTES;
 constexpr int kThreads = 192;
 constexpr uint32_t kTmemCols = 512;     // two accumulators of 256 columns: the epilogue of one tile overlaps the next
 
@@ -195,25 +197,27 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
           }
         } else {
-          // row-major output: each thread writes 32 consecutive values of its own row, 16 bytes at a time
-          if (mv) {
-            float* __restrict__ dst = out.f + long(m) * out.ld + c0;
-            const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+          // row-major output: the warp's 32 rows x 32 columns go through shared memory so that each store (and,
+          // when adding, each load of the old values) covers one row's 32 consecutive columns: 128 bytes
+          float* stg = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES + 256) + q * 32 * STG_LD;
 #pragma unroll
-            for (int c = 0; c < 32; c += 4) {
-              if (vec && c0 + c + 3 < cend) {
-                float4 w = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-                if (MODE == OUT_R_F32_ADD) {
-                  const float4 o4 = *reinterpret_cast<const float4*>(dst + c);
-                  w.x += o4.x; w.y += o4.y; w.z += o4.z; w.w += o4.w;
-                }
-                *reinterpret_cast<float4*>(dst + c) = w;
-              } else {
-                for (int e = 0; e < 4; e++)
-                  if (c0 + c + e < cend) dst[c + e] = (MODE == OUT_R_F32_ADD ? dst[c + e] : 0.f) + v[c + e];
-              }
+          for (int c = 0; c < 32; c++) stg[lane * STG_LD + c] = v[c];
+          __syncwarp();
+          const bool cv = c0 + lane < cend;
+          const int mrow = m0 + q * 32;
+          float old[32];
+          if (MODE == OUT_R_F32_ADD) {
+#pragma unroll
+            for (int r = 0; r < 32; r++) old[r] = (cv && mrow + r < out.M) ? out.f[long(mrow + r) * out.ld + c0 + lane] : 0.f;
+          }
+#pragma unroll
+          for (int r = 0; r < 32; r++) {
+            if (cv && mrow + r < out.M) {
+              const float val = stg[r * STG_LD + lane];
+              out.f[long(mrow + r) * out.ld + c0 + lane] = MODE == OUT_R_F32_ADD ? old[r] + val : val;
             }
           }
+          __syncwarp();
         }
       }
       // the accumulator is free again once every lane's tcgen05.ld of it has completed
