@@ -100,6 +100,10 @@ int ob_model_sync(ObModel* m);
 unsigned ob_model_nan_count(ObModel* m);
 /* replaces requestMaps (model.js:1478-1494): 16 floats per column, 4 maps of nx*ny float4 */
 int ob_model_maps(ObModel* m, float* out16xN2);
+/* the sub-grid tornado scheme's candidates (tornadoCandidates, app.js:1457-1472), found on the GPU in the maps of the
+ * last ob_model_maps call: 7 floats each (i, j, x, y, 1-km vorticity, 2-5 km updraft helicity, max updraft), in no
+ * particular order; *count = all candidates found (only the first cap are written) */
+int ob_model_tornado_candidates(ObModel* m, float zeta_min, float* out, int cap, int* count);
 /* field up/download in the texel layouts above (bytes must match exactly) */
 int ob_model_get_field(ObModel* m, int field, void* host, size_t bytes);
 int ob_model_set_field(ObModel* m, int field, const void* host, size_t bytes);

@@ -96,6 +96,7 @@ SYMBOLS = {
     "ob_mlp_train": (_i, [_vp, _i, _i, _f, C.c_uint, C.POINTER(_d)]),
     "ob_model_record_micro": (_i, [_vp, _vp, _f]),
     "ob_model_set_graphs": (_i, [_vp, _i]),
+    "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),
     "ob_model_set_surrogate": (_i, [_vp, _vp]),
     "ob_model_surrogate_stats": (_i, [_vp, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
 }

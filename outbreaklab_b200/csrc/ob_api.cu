@@ -541,6 +541,27 @@ int ob_model_maps(ObModel* m, float* out) {
   return cuda_status(cudaStreamSynchronize(m->stream), "maps");
 }
 
+int ob_model_tornado_candidates(ObModel* m, float zeta_min, float* out, int cap, int* count) {
+  if (!m || !out || cap < 1 || !count) { set_error("ob_model_tornado_candidates: bad arguments"); return OB_ERR_INVALID; }
+  float* d_out = nullptr;
+  unsigned* d_n = nullptr;
+  int rc = cuda_status(cudaMalloc(&d_out, size_t(cap) * 7 * sizeof(float)), "tornado candidates");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&d_n, sizeof(unsigned)), "tornado candidates");
+  if (rc == OB_OK) rc = cuda_status(cudaMemsetAsync(d_n, 0, sizeof(unsigned), m->stream), "tornado candidates");
+  unsigned n = 0;
+  if (rc == OB_OK) {
+    launch_tor_candidates(m->g, float(m->dx), m->d_maps, zeta_min, d_out, cap, d_n, m->stream);
+    rc = cuda_status(cudaMemcpyAsync(&n, d_n, sizeof(unsigned), cudaMemcpyDeviceToHost, m->stream), "tornado candidates");
+  }
+  if (rc == OB_OK) rc = cuda_status(cudaStreamSynchronize(m->stream), "tornado candidates");
+  if (rc == OB_OK && n > 0)
+    rc = cuda_status(cudaMemcpy(out, d_out, size_t(std::min<unsigned>(n, unsigned(cap))) * 7 * sizeof(float), cudaMemcpyDeviceToHost), "tornado candidates");
+  *count = int(n);
+  if (d_out) cudaFree(d_out);
+  if (d_n) cudaFree(d_n);
+  return rc;
+}
+
 static int field_layout(ObModel* m, int field, Ptr8& p, int& nch, int& X, int& Y, int& Z) {
   const Grid& g = m->g;
   switch (field) {

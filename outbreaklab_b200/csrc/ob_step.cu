@@ -1103,6 +1103,44 @@ void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
 void launch_maps(const Grid& g, const Uni& U, const Fields& F, int par, float4* out, cudaStream_t s) {
   k_maps<<<grid3(g.nx, g.ny, 1, kB2), kB2, 0, s>>>(g, U, F, par, out);
 }
+
+// ---------------------------------------------------------------------------------------------------------------
+// tornado candidates of the sub-grid tornado scheme (tornadoCandidates, app.js:1457-1472) on the device maps: on the
+// stride-2 lattice 6 cells inside the edges, a point whose 1-km vorticity (map0.w) is at least zmin and whose
+// low-level theta' (map0.z) is not below -4.5 K, that has the largest vorticity of its stride-2 5 x 5 window, with a
+// window maximum of 2-5 km updraft helicity (map1.y) above 60 m2/s2 and of updraft (map1.x) above 12 m/s. Appends
+// (i, j, x, y, zeta, uh, w) per candidate; the host restores the lattice order (j, then i).
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_tor_candidates(const float4* __restrict__ maps, int nx, int ny, float dx, float zmin, float* out, int cap,
+                                 unsigned* count) {
+  const int i = 6 + 2 * (blockIdx.x * blockDim.x + threadIdx.x), j = 6 + 2 * (blockIdx.y * blockDim.y + threadIdx.y);
+  if (i >= nx - 6 || j >= ny - 6) return;
+  const float4* m0 = maps;
+  const float4* m1 = maps + size_t(nx) * ny;
+  const float4 c = __ldg(m0 + j * nx + i);
+  const float z1 = c.w;
+  if (z1 < zmin || c.z < -4.5f) return;
+  bool is_max = true;
+  float uh = 0.f, w = 0.f;
+  for (int dj = -4; dj <= 4; dj += 2)
+    for (int di = -4; di <= 4; di += 2) {
+      const int q = (i + di) + nx * (j + dj);
+      if ((di || dj) && __ldg(m0 + q).w > z1) is_max = false;
+      const float4 b = __ldg(m1 + q);
+      uh = fmaxf(uh, b.y);
+      w = fmaxf(w, b.x);
+    }
+  if (!(is_max && uh > 60.f && w > 12.f)) return;
+  const unsigned slot = atomicAdd(count, 1u);
+  if (slot >= unsigned(cap)) return;
+  float* o = out + size_t(slot) * 7;
+  o[0] = float(i); o[1] = float(j); o[2] = (float(i) + 0.5f) * dx; o[3] = (float(j) + 0.5f) * dx; o[4] = z1; o[5] = uh; o[6] = w;
+}
+void launch_tor_candidates(const Grid& g, float dx, const float4* maps, float zmin, float* out, int cap, unsigned* count, cudaStream_t s) {
+  const int ni = (g.nx - 12 + 1) / 2, nj = (g.ny - 12 + 1) / 2;
+  if (ni <= 0 || nj <= 0) return;
+  k_tor_candidates<<<dim3((ni + 31) / 32, (nj + 7) / 8), dim3(32, 8), 0, s>>>(maps, g.nx, g.ny, dx, zmin, out, cap, count);
+}
 void launch_pack(const Grid& g, const Ptr8& src, int nch, int X, int Y, int Z, float* dst, cudaStream_t s) {
   k_pack<<<grid3(X, Y, Z, kB3), kB3, 0, s>>>(g, src, nch, X, Y, Z, dst);
 }

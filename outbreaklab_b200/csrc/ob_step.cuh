@@ -24,6 +24,7 @@ void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStrea
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
 void launch_maps(const Grid& g, const Uni& U, const Fields& F, int par, float4* out, cudaStream_t s);
+void launch_tor_candidates(const Grid& g, float dx, const float4* maps, float zmin, float* out, int cap, unsigned* count, cudaStream_t s);
 void launch_pack(const Grid& g, const Ptr8& src, int nch, int X, int Y, int Z, float* dst, cudaStream_t s);
 void launch_unpack(const Grid& g, const Ptr8& dst, int nch, int X, int Y, int Z, const float* src, cudaStream_t s);
 

@@ -2,8 +2,9 @@
 
 RunLoop mirrors loop() (app.js:1678-1732): steps in batches sized to about 60 ms of GPU work each
 (stepsPerBatch, 1..40), storm-initiation scheduling every 60 s of model time, the radars' due cuts after every step
-(RadarSim.enc_due), a map readback for each replay frame (every `replay_every` s of model time) and for the
-scheduler's echo test, finished volumes written as Archive II files (RadarSim.collect_level2, the server's write,
+(RadarSim.enc_due), the sub-grid tornadoes advanced after every step and updated from each batch's last map readback
+(tornadoTick / tornadoUpdate, tornado.py), a map readback for each replay frame (every `replay_every` s of model time)
+and for the scheduler's echo test, finished volumes written as Archive II files (RadarSim.collect_level2, the server's write,
 server.py:249-284), optional pacing to a multiple of real time, and the simulation rate. The browser parts (status
 bar, map painting, upload retries, the replay UI) have no counterpart here.
 
@@ -128,11 +129,18 @@ class CIScheduler:
 
 class RunLoop:
     def __init__(self, model, dt, t_end, radar=None, ci=None, motion=(0.0, 0.0), replay_every=180.0, out_dir=None,
-                 run="run", epoch0_ms=None, pace=0.0, batch_ms=60.0):
+                 run="run", epoch0_ms=None, pace=0.0, batch_ms=60.0, tornadoes=None):
         self.m, self.dt, self.t_end = model, float(dt), float(t_end)
         self.radar = radar
         self.log = []
         self.ci = CIScheduler(model, ci, motion, self.log) if ci is not None else None
+        # tornadoes: None, or the keyword arguments of TornadoScheme (stp, rate, on, hurricane, ...)
+        self.tor = None
+        if tornadoes is not None:
+            from .tornado import TornadoScheme
+            seed = (ci or {}).get("seed", CI_DEFAULTS["seed"])
+            self.tor = TornadoScheme(model, radar, ci_seed=seed, events=(lambda: self.ci.events if self.ci else []),
+                                     log=self.log, **tornadoes)
         self.replay_every, self.replay_next = float(replay_every), 0.0
         self.out_dir, self.run_name = out_dir, run
         self.epoch0 = int(time.time() * 1000) if epoch0_ms is None else int(epoch0_ms)
@@ -171,6 +179,8 @@ class RunLoop:
                     self.ci_next = m.time + 60.0
                 m.enc_step(self.dt)
                 ran += 1
+                if self.tor is not None:
+                    self.tor.tick(m.time, self.dt)
                 due = self.radar.enc_due(m.time) if self.radar is not None else []
                 if m.time >= self.replay_next:
                     self.frames.append(m.request_maps())
@@ -183,8 +193,10 @@ class RunLoop:
             self.batches.append((ran, el))
             # aim for ~batch_ms of GPU work per batch (app.js:1711)
             self.steps_per_batch = int(min(max(round(max(ran, 1) * (self.batch_ms / max(el, 5.0))), 1), 40))
-            if self.ci is not None and self.ci.ci["auto"]:
+            if (self.ci is not None and self.ci.ci["auto"]) or self.tor is not None:
                 self.maps = m.request_maps()   # the scheduler's echo test reads the latest composite reflectivity
+            if self.tor is not None:
+                self.tor.update(self.maps, self.maps["t"])   # candidates from the device copy of these maps
             if self.pace > 0:
                 want = wall0 + (m.time - sim0) / self.pace
                 wait = want - time.perf_counter()
@@ -194,4 +206,5 @@ class RunLoop:
         self.sim_rate = (m.time - sim0) / max(el, 1e-9)
         return {"time": m.time, "steps": m.steps, "sim_rate": self.sim_rate, "frames": len(self.frames),
                 "volumes": self.volumes, "events": len(self.ci.events) if self.ci else 0, "log": self.log,
-                "steps_per_batch": self.steps_per_batch}
+                "steps_per_batch": self.steps_per_batch,
+                "tornadoes": self.tor.counts() if self.tor else (0, 0)}
