@@ -129,11 +129,14 @@ def peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def ncu_traffic(pass_name):
-    """Per-launch DRAM bytes of a pass from the committed ncu summary (profiles/ncu_traffic.json), if present."""
+def ncu_traffic(pass_name, cells):
+    """DRAM bytes of one pass from the committed ncu summary (profiles/ncu_traffic.json), scaled from the captured
+    workload to this one by the cell count; None when the pass has no entry."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            return json.load(f).get(pass_name)
+            j = json.load(f)
+        v = j.get(pass_name)
+        return None if v is None else v * cells / j["cells"]
     except Exception:
         return None
 
@@ -264,7 +267,7 @@ def run_ours(args, rank, world):
     dom = max(pass_ms, key=lambda k: pass_ms[k])
     achieved = pb[dom] / (pass_ms[dom] / 1000.0) / 1e9
     roof = {"pass": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)", "traffic": ncu_traffic(dom),
+            "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)", "traffic": ncu_traffic(dom, case.cells),
             "algorithmic_bytes": pb[dom], "ms": pass_ms[dom]}
     if dom == "SOLVE":
         fl = solve_flops(case.nx, case.ny, case.nz, m.pad)
@@ -275,9 +278,10 @@ def run_ours(args, rank, world):
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (Weisman-Klemp sounding, seeded bubbles)",
             "cell_steps_per_s": cell_steps,
-            "config": {"workload": "640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)",
+            "config": {"workload": ("640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)" if not args.nx
+                                    else "%dx%dx40 dx 1 km dz 500 m dt 6 s, Lin, 4 warm bubbles (Weisman-Klemp)" % (args.nx, args.nx)),
                        "cells": case.cells, "parallelism": "replicas" if world > 1 else "single domain",
-                       "l2": "state 2.8 GB > 126 MB L2 (no flush needed)",
+                       "l2": "state %.1f GB > 126 MB L2 (no flush needed)" % (2.8 * case.cells / 16384000),
                        "solver": {0: "fp32 SIMT DST", 1: "bf16x3 tensor-core DST",
                                   2: "bf16x3 tensor-core DST + 1 refinement sweep"}[m.solver]},
             "pass_ms": {k: round(v, 4) for k, v in pass_ms.items()},
