@@ -100,6 +100,33 @@ int ob_model_sync(ObModel* m);
 unsigned ob_model_nan_count(ObModel* m);
 /* replaces requestMaps (model.js:1478-1494): 16 floats per column, 4 maps of nx*ny float4 */
 int ob_model_maps(ObModel* m, float* out16xN2);
+/* ---- ensembles (no counterpart in the reference, which runs one domain per tab) ----
+ * An ensemble steps its members together: each pass of the step (LSF, CI, NUT, ADVV1/2, ADVQ1/2, PHYS, DIV, the
+ * solve's transforms, tridiagonals and residual, PROJ, rain) is one launch over every member, the members' sizes,
+ * spacings, soundings and dt free to differ (they must share nz and the solver precision, use the tensor-core solve,
+ * the plain microphysics, and sit at the same step parity). The step is captured as a CUDA graph and replayed.
+ * Members keep their handles: fields, maps, budgets and radars work on them as usual, queued on the ensemble's stream
+ * while they belong to it (so they are ordered with its steps); stepping a member alone in between is allowed (an
+ * even number of steps, to keep the parity). At most 48 members; one ensemble at a time (the members sit in one
+ * constant-memory table); destroy the ensemble before its members. */
+typedef struct ObEnsemble ObEnsemble;
+#define OB_ENS_NTILES 6   /* tunable tiles: block width of NUT, ADVV1, ADVV2, DIV, PROJ; widest solve transform tile */
+int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsemble** out);
+int ob_ensemble_step(ObEnsemble* e, int nsteps);                     /* queued on the ensemble's stream */
+int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms);  /* device time of nsteps steps */
+int ob_ensemble_sync(ObEnsemble* e);
+int ob_ensemble_set_graphs(ObEnsemble* e, int on);
+int ob_ensemble_set_tiles(ObEnsemble* e, const int* tiles);        /* OB_ENS_NTILES values */
+int ob_ensemble_get_tiles(ObEnsemble* e, int* tiles);
+int ob_ensemble_time_pass(ObEnsemble* e, int tile_slot, int reps, float* ms);
+/* the autotuner: times every candidate of every tile slot on the current state, keeps the fastest (tiles, ms:
+ * OB_ENS_NTILES each) */
+int ob_ensemble_tune(ObEnsemble* e, int reps, int* tiles, float* ms);
+/* model time of each member's last LSF pass as the device keeps it (the grouped LSF launch decides on the device) */
+int ob_ensemble_lsf_times(ObEnsemble* e, double* out);
+void* ob_ensemble_stream(ObEnsemble* e);
+void ob_ensemble_destroy(ObEnsemble* e);
+
 /* the sub-grid tornado scheme's candidates (tornadoCandidates, app.js:1457-1472), found on the GPU in the maps of the
  * last ob_model_maps call: 7 floats each (i, j, x, y, 1-km vorticity, 2-5 km updraft helicity, max updraft), in no
  * particular order; *count = all candidates found (only the first cap are written) */

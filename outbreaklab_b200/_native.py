@@ -17,6 +17,7 @@ FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI, FIELD_RAIN = 0, 1, 2, 3, 4, 5
 BOUNDARY_FLOATS, MAX_BOUNDS, CI_FLOATS, MAX_CI = 148, 8, 12, 256
 OB_STATIC_POISSON_MAX_SIDE, OB_STATIC_POISSON_MAX_NZ, OB_STATIC_POISSON_MAX_CELLS = 256, 512, 1 << 20
 RADAR_MAX_RADIALS, RADAR_MAX_TORNADOES, RADAR_TORNADO_FLOATS = 720, 64, 8
+ENS_NTILES, ENS_MAX_MEMBERS = 6, 48
 
 
 class ObError(RuntimeError):
@@ -97,6 +98,18 @@ SYMBOLS = {
     "ob_model_record_micro": (_i, [_vp, _vp, _f]),
     "ob_model_set_graphs": (_i, [_vp, _i]),
     "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),
+    "ob_ensemble_create": (_i, [C.POINTER(_vp), _fp, _i, C.POINTER(_vp)]),
+    "ob_ensemble_step": (_i, [_vp, _i]),
+    "ob_ensemble_timed_steps": (_i, [_vp, _i, _fp]),
+    "ob_ensemble_sync": (_i, [_vp]),
+    "ob_ensemble_set_graphs": (_i, [_vp, _i]),
+    "ob_ensemble_set_tiles": (_i, [_vp, C.POINTER(_i)]),
+    "ob_ensemble_get_tiles": (_i, [_vp, C.POINTER(_i)]),
+    "ob_ensemble_time_pass": (_i, [_vp, _i, _i, _fp]),
+    "ob_ensemble_tune": (_i, [_vp, _i, C.POINTER(_i), _fp]),
+    "ob_ensemble_lsf_times": (_i, [_vp, C.POINTER(_d)]),
+    "ob_ensemble_stream": (_vp, [_vp]),
+    "ob_ensemble_destroy": (None, [_vp]),
     "ob_model_set_surrogate": (_i, [_vp, _vp]),
     "ob_model_surrogate_stats": (_i, [_vp, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]),
 }

@@ -3,7 +3,8 @@
   python -m outbreaklab_b200.benchmarks solve --nx 1024 --ny 1024 --nz 80 --precision 2 --reps 20
   python -m outbreaklab_b200.benchmarks step --case c4 --steps 50
   python -m outbreaklab_b200.benchmarks surrogate [--nx 512] [--minutes 60] [--pairs 100000000]
-  python -m outbreaklab_b200.benchmarks ensemble [--members 24] [--steps 50]     (torchrun: members shard over ranks)
+  python -m outbreaklab_b200.benchmarks ensemble [--members 24] [--steps 50] [--mode grouped|streams]
+                                                                               (torchrun: members shard over ranks)
 
 The solve benchmark's right-hand side is the 5 km-correlated Gaussian random field of the 1024 x 1024 x 80 case
 (zero horizontal mean per level), with the Weisman-Klemp densities; errors and residuals are computed in FP64 on the
@@ -160,13 +161,19 @@ def ensemble(args):
         dist = (torch, td)
     cases = E.draw_members(args.members, args.seed, steps=args.steps)
     mine = [cases[i] for i in E.plan_shards(cases, world)[rank]]
-    local = E.run(mine, args.steps, args.warmup)
+    if args.mode == "grouped":
+        local = E.run_grouped(mine, args.steps, args.warmup, tune=not args.no_tune)
+    else:
+        local = E.run(mine, args.steps, args.warmup)
     res = E.gather(local, dist)
     if rank == 0:
         res.update({"bench": "ensemble", "members": len(cases), "cells": sum(c.cells for c in cases), "steps": args.steps,
                     "n_gpus": world, "host_launch_ms_rank0": local["host_launch_ms"],
                     "device_ms_rank0": local["device_ms"], "nan_guard_count_rank0": local["nan_guard_count"],
-                    "grids": [[c.nx, c.ny, c.nz, c.dx] for c in cases]})
+                    "grids": [[c.nx, c.ny, c.nz, c.dx] for c in cases], "mode": args.mode})
+        for k in ("tiles", "tiles_source", "tune_ms", "launches_per_step"):
+            if k in local:
+                res[k + "_rank0"] = local[k]
         print(json.dumps(res), flush=True)
     if dist:
         dist[1].destroy_process_group()
@@ -203,6 +210,9 @@ def main(argv=None):
     e.add_argument("--steps", type=int, default=50)
     e.add_argument("--warmup", type=int, default=3)
     e.add_argument("--seed", type=int, default=5)
+    e.add_argument("--mode", choices=["grouped", "streams"], default="grouped",
+                   help="grouped: one launch per pass over all members (ObEnsemble); streams: one stream per member")
+    e.add_argument("--no-tune", action="store_true", help="grouped mode: default tiles, no autotuner")
     args = ap.parse_args(argv)
     {"solve": solve, "step": step, "surrogate": surrogate, "ensemble": ensemble}[args.cmd](args)
 

@@ -120,6 +120,9 @@ struct ObModel {
   int nb = 0, nci = 0;
   double time = 0, lsfT = 0;
   int steps = 0, parity = 0;
+  // member of an ensemble: its work goes to the ensemble's stream meanwhile (own_stream is the model's own)
+  void* ens = nullptr;
+  cudaStream_t own_stream = nullptr;
 };
 
 // where the divergence pass writes the solve's right-hand side for the current solver precision
@@ -155,12 +158,13 @@ static void model_free(ObModel* m) {
     if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
   }
   if (m->ev_fork) cudaEventDestroy(m->ev_fork);
+  if (m->ens) m->stream = m->own_stream;  // the ensemble's stream is not the model's to destroy
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
 }
 
 // RegionalModel.writeUniforms (model.js:1391-1425), outbreak mode
-static void write_uniforms(ObModel* m, double dt) {
+static void write_uniforms(ObModel* m, double dt, cudaStream_t ts = nullptr) {
   const ObParams& P = m->P;
   const double DEG = M_PI / 180.0;
   auto v4 = [](double a, double b, double c, double d) { return make_float4(float(a), float(b), float(c), float(d)); };
@@ -191,7 +195,7 @@ static void write_uniforms(ObModel* m, double dt) {
   // sponge tables, remade when a uniform they read or the base state changed
   const float key[8] = {U.sponge.x, U.sponge.y, U.sponge.z, U.sponge.w, U.step.z, fdx, fdz, 0.f};
   if (m->tab_gen != m->base_gen || std::memcmp(key, m->tab_key, sizeof(key)) != 0) {
-    launch_tables(m->g, U, m->F, m->stream);
+    launch_tables(m->g, U, m->F, ts ? ts : m->stream);
     std::memcpy(m->tab_key, key, sizeof(key));
     m->tab_gen = m->base_gen;
   }
@@ -778,6 +782,374 @@ unsigned ob_model_nan_count(ObModel* m) {
 }
 
 void* ob_model_stream(ObModel* m) { return m ? (void*)m->stream : nullptr; }
+
+// ---- ensembles: every member's pass in one launch ----
+struct ObEnsemble {
+  std::vector<ObModel*> mem;
+  std::vector<float> dt;
+  cudaStream_t stream = nullptr;
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+  MemberC* d_members = nullptr;  // device copy of the member table (the constant-memory upload's source)
+  std::vector<MemberC> h_members;
+  bool members_valid = false;
+  double* d_lsfT = nullptr;
+  GroupTable* d_tables = nullptr;  // one per pass
+  int blocks[kGroupPasses] = {};
+  dim3 shape[kGroupPasses];
+  TcGroup* solve = nullptr;
+  unsigned gen = 0;  // bumped when the tables or the member table change: captured steps are then stale
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    unsigned gen = ~0u;
+    int seen = 0;
+  } graphs[2];
+  bool use_graphs = true;
+  int parity = 0;
+  std::vector<double> lsfT;  // what the device copy holds (the device updates it as the host does)
+};
+
+// the grouped kernels read their members from one constant-memory table per device: one ensemble at a time
+static ObEnsemble* g_ensemble = nullptr;
+
+static void ens_drop_graphs(ObEnsemble* e) {
+  for (auto& G : e->graphs) {
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G = ObEnsemble::StepGraph{};
+  }
+}
+
+static void ens_free(ObEnsemble* e) {
+  if (!e) return;
+  ens_drop_graphs(e);
+  for (ObModel* m : e->mem)
+    if (m && m->ens == e) {
+      m->stream = m->own_stream;
+      m->ens = nullptr;
+    }
+  if (e->solve) tc_group_destroy(e->solve);
+  for (void* p : {(void*)e->d_members, (void*)e->d_lsfT, (void*)e->d_tables})
+    if (p) cudaFree(p);
+  for (int i = 0; i < 2; i++) {
+    if (e->side[i]) cudaStreamDestroy(e->side[i]);
+    if (e->ev_join[i]) cudaEventDestroy(e->ev_join[i]);
+  }
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  if (g_ensemble == e) g_ensemble = nullptr;
+  delete e;
+}
+
+static int ens_build_tables(ObEnsemble* e) {
+  const int n = int(e->mem.size());
+  std::vector<Grid> grids(n);
+  for (int i = 0; i < n; i++) grids[i] = e->mem[i]->g;
+  std::vector<GroupTable> T(kGroupPasses);
+  for (int p = 0; p < kGroupPasses; p++) e->blocks[p] = group_fill(grids.data(), n, p, e->shape[p], &T[p]);
+  OB_TRY(cuda_status(cudaMemcpy(e->d_tables, T.data(), sizeof(GroupTable) * kGroupPasses, cudaMemcpyHostToDevice), "ensemble tables"));
+  e->gen++;
+  return OB_OK;
+}
+
+// member table for this step (uniforms for each member's dt); re-uploaded when it changed
+static int ens_prepare(ObEnsemble* e) {
+  const int n = int(e->mem.size());
+  bool changed = !e->members_valid, lsf_changed = false;
+  for (int i = 0; i < n; i++) {
+    ObModel* m = e->mem[i];
+    if (m->parity != e->parity) {
+      set_error("ensemble: member %d was stepped alone an odd number of times (its step parity differs)", i);
+      return OB_ERR_INVALID;
+    }
+    if (m->lsfT != e->lsfT[i]) {  // stepped alone since the last ensemble step
+      e->lsfT[i] = m->lsfT;
+      lsf_changed = true;
+    }
+    write_uniforms(m, e->dt[i], e->stream);
+    if (micro_mode(m) != kMicroPlain) { set_error("ensemble: member %d uses a learned or recording microphysics mode", i); return OB_ERR_INVALID; }
+    OB_TRY(prepare_micro(m));
+    MemberC c;
+    std::memset(&c, 0, sizeof(c));
+    c.g = m->g;
+    c.U = m->U;
+    c.F = m->F;
+    c.lsfT = e->d_lsfT + i;
+    if (std::memcmp(&c, &e->h_members[i], sizeof(MemberC)) != 0) {
+      e->h_members[i] = c;
+      changed = true;
+    }
+  }
+  if (lsf_changed) {
+    OB_TRY(cuda_status(cudaMemcpyAsync(e->d_lsfT, e->lsfT.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->stream), "ensemble members"));
+    OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble members"));
+  }
+  if (changed) {
+    OB_TRY(cuda_status(cudaMemcpyAsync(e->d_members, e->h_members.data(), sizeof(MemberC) * n, cudaMemcpyHostToDevice, e->stream), "ensemble members"));
+    OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble members"));
+    e->members_valid = true;
+    e->gen++;
+  }
+  return OB_OK;
+}
+
+static int ens_enqueue(ObEnsemble* e, cudaStream_t s) {
+  const int n = int(e->mem.size()), par = e->parity;
+  if (group_upload_members(e->d_members, n, e->d_tables, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
+  auto L = [&](int p, cudaStream_t st) { launch_group(p, e->blocks[p], e->shape[p], par, st, kMicroPlain); };
+  L(kGroupLSF, s);
+  L(kGroupCI, s);
+  cudaEventRecord(e->ev_fork, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(e->side[i], e->ev_fork, 0);
+  L(kGroupNUT, e->side[0]);
+  cudaEventRecord(e->ev_join[0], e->side[0]);
+  L(kGroupADVQ1, e->side[1]);
+  L(kGroupADVQ2, e->side[1]);
+  cudaEventRecord(e->ev_join[1], e->side[1]);
+  L(kGroupADVV1, s);
+  L(kGroupADVV2, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(s, e->ev_join[i], 0);
+  L(kGroupPHYS, s);
+  L(kGroupDIV, s);
+  OB_TRY(tc_group_solve(e->solve, s));
+  L(kGroupPROJ, s);
+  L(kGroupRAIN, s);
+  return cuda_status(cudaGetLastError(), "ensemble step launch");
+}
+
+// one step of every member; captured per parity on its second occurrence and replayed while nothing changed
+static int ens_step_once(ObEnsemble* e) {
+  OB_TRY(ens_prepare(e));
+  cudaStream_t s = e->stream;
+  if (!e->use_graphs) {
+    OB_TRY(ens_enqueue(e, s));
+  } else {
+    ObEnsemble::StepGraph& G = e->graphs[e->parity];
+    if (G.exec && G.gen == e->gen) {
+      OB_TRY(cuda_status(cudaGraphLaunch(G.exec, s), "ensemble graph launch"));
+    } else if (G.seen == 0) {
+      G.seen = 1;
+      OB_TRY(ens_enqueue(e, s));
+    } else {
+      if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+      OB_TRY(cuda_status(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "ensemble capture"));
+      const int rc = ens_enqueue(e, s);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      if (rc != OB_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+      OB_TRY(cuda_status(ec, "ensemble capture"));
+      const cudaError_t ei = cudaGraphInstantiate(&G.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      OB_TRY(cuda_status(ei, "ensemble graph instantiate"));
+      G.gen = e->gen;
+      OB_TRY(cuda_status(cudaGraphLaunch(G.exec, s), "ensemble graph launch"));
+    }
+  }
+  // the members' host bookkeeping, as model_step_once keeps it
+  for (size_t i = 0; i < e->mem.size(); i++) {
+    ObModel* m = e->mem[i];
+    if (m->time - m->lsfT >= 60 || m->time == 0) m->lsfT = m->time;
+    e->lsfT[i] = m->lsfT;
+    m->parity = 1 - m->parity;
+    m->time += e->dt[i];
+    m->steps++;
+  }
+  e->parity = 1 - e->parity;
+  return OB_OK;
+}
+
+int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsemble** out) {
+  if (!members || !dts || !out || n < 1) { set_error("ob_ensemble_create: bad arguments"); return OB_ERR_INVALID; }
+  *out = nullptr;
+  if (n > kMaxMembers) { set_error("ob_ensemble_create: at most %d members", kMaxMembers); return OB_ERR_INVALID; }
+  for (int i = 0; i < n; i++) {
+    if (!members[i] || !(dts[i] > 0.f)) { set_error("ob_ensemble_create: member %d is null or has dt <= 0", i); return OB_ERR_INVALID; }
+    if (members[i]->parity != members[0]->parity) { set_error("ob_ensemble_create: members must be at the same step parity"); return OB_ERR_INVALID; }
+    for (int j = 0; j < i; j++)
+      if (members[j] == members[i]) { set_error("ob_ensemble_create: member %d appears twice", i); return OB_ERR_INVALID; }
+    if (members[i]->ens) { set_error("ob_ensemble_create: member %d already belongs to an ensemble", i); return OB_ERR_INVALID; }
+  }
+  if (g_ensemble) { set_error("ob_ensemble_create: another ensemble exists (one at a time: its members sit in one constant-memory table)"); return OB_ERR_INVALID; }
+  ObEnsemble* e = new ObEnsemble();
+  g_ensemble = e;
+  e->mem.assign(members, members + n);
+  e->dt.assign(dts, dts + n);
+  e->h_members.assign(n, MemberC{});
+  for (auto& c : e->h_members) std::memset(&c, 0, sizeof(c));
+  e->parity = members[0]->parity;
+  for (int p = 0; p < kGroupPasses; p++) e->shape[p] = group_default_block(p);
+  int rc = cuda_status(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "ensemble stream");
+  for (int i = 0; i < 2 && rc == OB_OK; i++) rc = cuda_status(cudaStreamCreateWithFlags(&e->side[i], cudaStreamNonBlocking), "ensemble stream");
+  if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming), "ensemble event");
+  for (int i = 0; i < 2 && rc == OB_OK; i++) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_join[i], cudaEventDisableTiming), "ensemble event");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_members, sizeof(MemberC) * n), "ensemble members");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_lsfT, sizeof(double) * n), "ensemble members");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_tables, sizeof(GroupTable) * kGroupPasses), "ensemble tables");
+  // every member's queued work (reset, uploads) completes before the ensemble's stream takes over
+  for (int i = 0; i < n && rc == OB_OK; i++) rc = cuda_status(cudaStreamSynchronize(members[i]->stream), "ensemble members");
+  if (rc == OB_OK) {
+    e->lsfT.resize(n);
+    for (int i = 0; i < n; i++) e->lsfT[i] = members[i]->lsfT;
+    rc = cuda_status(cudaMemcpy(e->d_lsfT, e->lsfT.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "ensemble members");
+  }
+  if (rc == OB_OK) {
+    std::vector<PoissonPlan*> plans(n);
+    std::vector<float*> phi(n);
+    std::vector<const float*> rhs(n);
+    for (int i = 0; i < n; i++) {
+      plans[i] = &members[i]->solver;
+      phi[i] = members[i]->F.phi;
+      rhs[i] = members[i]->F.rhs;
+    }
+    rc = tc_group_create(plans.data(), phi.data(), rhs.data(), n, &e->solve);
+  }
+  if (rc == OB_OK) rc = ens_build_tables(e);
+  if (rc != OB_OK) { ens_free(e); return rc; }
+  // while in the ensemble, each member's own work (field access, maps, radar cuts, a step alone) queues behind and
+  // ahead of the ensemble's steps on one stream
+  for (ObModel* m : e->mem) {
+    m->own_stream = m->stream;
+    m->stream = e->stream;
+    m->ens = e;
+  }
+  *out = e;
+  return OB_OK;
+}
+
+int ob_ensemble_step(ObEnsemble* e, int nsteps) {
+  if (!e || nsteps < 0) { set_error("ob_ensemble_step: bad arguments"); return OB_ERR_INVALID; }
+  for (int s = 0; s < nsteps; s++) OB_TRY(ens_step_once(e));
+  return OB_OK;
+}
+
+int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms) {
+  if (!e || !ms || nsteps < 0) { set_error("ob_ensemble_timed_steps: bad arguments"); return OB_ERR_INVALID; }
+  cudaEvent_t a, b;
+  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
+  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
+  cudaEventRecord(a, e->stream);
+  int rc = OB_OK;
+  for (int s = 0; s < nsteps && rc == OB_OK; s++) rc = ens_step_once(e);
+  cudaEventRecord(b, e->stream);
+  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "ensemble timed steps");
+  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(ms, a, b), "ensemble timed steps");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int ob_ensemble_sync(ObEnsemble* e) {
+  if (!e) { set_error("ob_ensemble_sync: null ensemble"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble step"));
+  return tc_group_check(e->solve);
+}
+
+int ob_ensemble_set_graphs(ObEnsemble* e, int on) {
+  if (!e) { set_error("ob_ensemble_set_graphs: null ensemble"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble set graphs"));
+  ens_drop_graphs(e);
+  e->use_graphs = on != 0;
+  return OB_OK;
+}
+
+// tiles[0 .. OB_NTILES-1]: block width in x (threads; 128 / width rows) of NUT, ADVV1, ADVV2, DIV, PROJ, then the
+// widest transform tile of the solve
+static const int kTunedPasses[OB_ENS_NTILES - 1] = {kGroupNUT, kGroupADVV1, kGroupADVV2, kGroupDIV, kGroupPROJ};
+
+int ob_ensemble_set_tiles(ObEnsemble* e, const int* tiles) {
+  if (!e || !tiles) { set_error("ob_ensemble_set_tiles: bad arguments"); return OB_ERR_INVALID; }
+  for (int t = 0; t < OB_ENS_NTILES - 1; t++)
+    if (tiles[t] != 16 && tiles[t] != 32 && tiles[t] != 64 && tiles[t] != 128) {
+      set_error("ob_ensemble_set_tiles: block width %d not in {16, 32, 64, 128}", tiles[t]);
+      return OB_ERR_INVALID;
+    }
+  OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble set tiles"));
+  for (int t = 0; t < OB_ENS_NTILES - 1; t++) e->shape[kTunedPasses[t]] = dim3(tiles[t], 128 / tiles[t], 1);
+  OB_TRY(tc_group_set_cap(e->solve, tiles[OB_ENS_NTILES - 1]));
+  return ens_build_tables(e);
+}
+
+int ob_ensemble_get_tiles(ObEnsemble* e, int* tiles) {
+  if (!e || !tiles) { set_error("ob_ensemble_get_tiles: bad arguments"); return OB_ERR_INVALID; }
+  for (int t = 0; t < OB_ENS_NTILES - 1; t++) tiles[t] = int(e->shape[kTunedPasses[t]].x);
+  tiles[OB_ENS_NTILES - 1] = tc_group_cap(e->solve);
+  return OB_OK;
+}
+
+// device time of one grouped pass (tile slot t) with the ensemble's current state, averaged over reps launches. Each
+// timed pass only rewrites what the step recomputes from the state (viscosities, advection scratch and next-state
+// slot, the right-hand side, the solve from it, the projected next state), so timing leaves the model state as it
+// was.
+int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
+  if (!e || !ms || t < 0 || t >= OB_ENS_NTILES || reps < 1) { set_error("ob_ensemble_time_pass: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(ens_prepare(e));
+  cudaStream_t s = e->stream;
+  if (group_upload_members(e->d_members, int(e->mem.size()), e->d_tables, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
+  cudaEvent_t a, b;
+  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
+  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
+  auto run = [&]() -> int {
+    if (t < OB_ENS_NTILES - 1) {
+      const int p = kTunedPasses[t];
+      launch_group(p, e->blocks[p], e->shape[p], e->parity, s, kMicroPlain);
+      return OB_OK;
+    }
+    return tc_group_solve(e->solve, s);
+  };
+  int rc = run();  // warm
+  cudaEventRecord(a, s);
+  for (int r = 0; r < reps && rc == OB_OK; r++) rc = run();
+  cudaEventRecord(b, s);
+  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "ensemble pass timing");
+  float el = 0.f;
+  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(&el, a, b), "ensemble pass timing");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = el / float(reps);
+  return rc == OB_OK ? tc_group_check(e->solve) : rc;
+}
+
+// the project's tile autotuner: each tunable slot is set to each of its candidates in turn and its pass timed (the
+// passes are independent, so one slot at a time); the fastest candidate of every slot is kept
+int ob_ensemble_tune(ObEnsemble* e, int reps, int* tiles, float* ms) {
+  if (!e || !tiles || !ms || reps < 1) { set_error("ob_ensemble_tune: bad arguments"); return OB_ERR_INVALID; }
+  int cur[OB_ENS_NTILES];
+  OB_TRY(ob_ensemble_get_tiles(e, cur));
+  static const int kBlockWidths[] = {32, 64, 128, 16};
+  static const int kCaps[] = {256, 128, 64};
+  for (int t = 0; t < OB_ENS_NTILES; t++) {
+    const bool solve = t == OB_ENS_NTILES - 1;
+    const int* cand = solve ? kCaps : kBlockWidths;
+    const int nc = solve ? 3 : 4;
+    int best = cur[t];
+    float best_ms = 1e30f;
+    for (int c = 0; c < nc; c++) {
+      cur[t] = cand[c];
+      OB_TRY(ob_ensemble_set_tiles(e, cur));
+      float v = 0.f;
+      OB_TRY(ob_ensemble_time_pass(e, t, reps, &v));
+      if (v < best_ms) { best_ms = v; best = cand[c]; }
+    }
+    cur[t] = best;
+    ms[t] = best_ms;
+  }
+  OB_TRY(ob_ensemble_set_tiles(e, cur));
+  for (int t = 0; t < OB_ENS_NTILES; t++) tiles[t] = cur[t];
+  return OB_OK;
+}
+
+int ob_ensemble_lsf_times(ObEnsemble* e, double* out) {
+  if (!e || !out) { set_error("ob_ensemble_lsf_times: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaMemcpyAsync(out, e->d_lsfT, sizeof(double) * e->mem.size(), cudaMemcpyDeviceToHost, e->stream), "ensemble LSF times"));
+  return cuda_status(cudaStreamSynchronize(e->stream), "ensemble LSF times");
+}
+
+void* ob_ensemble_stream(ObEnsemble* e) { return e ? (void*)e->stream : nullptr; }
+
+void ob_ensemble_destroy(ObEnsemble* e) {
+  if (!e) return;
+  cudaStreamSynchronize(e->stream);
+  ens_free(e);
+}
 
 // ---- PoissonDirect ----
 struct ObPoisson {

@@ -58,14 +58,66 @@ struct TcOut {
 };
 }  // namespace
 
+// one tile of a transform: its operands, sizes and output, and its corner
+struct TileInfo {
+  const CUtensorMap* f_hi;
+  const CUtensorMap* f_lo;
+  const CUtensorMap* q_hi;
+  const CUtensorMap* q_lo;
+  int K, BN, m0, n0;
+  TcOut out;
+};
+
+// the tiles of one transform given by kernel parameters
+struct OneProblem {
+  const CUtensorMap *f_hi, *f_lo, *q_hi, *q_lo;
+  int K, BN, ntn, ntiles;
+  TcOut out;
+  __device__ __forceinline__ int total() const { return ntiles; }
+  __device__ __forceinline__ void tile(int t, TileInfo& ti) const {
+    ti.f_hi = f_hi; ti.f_lo = f_lo; ti.q_hi = q_hi; ti.q_lo = q_lo;
+    ti.K = K; ti.BN = BN; ti.out = out;
+    ti.m0 = (t / ntn) * BM;
+    ti.n0 = (t % ntn) * BN;
+  }
+};
+
+// one transform of every member of an ensemble (grouped launch): problem p owns tiles [start[p], start[p+1]); its
+// tensor maps live in global memory, written by the host before any launch that reads them
+struct alignas(64) GemmProb {
+  CUtensorMap f[2];
+  CUtensorMap q[2];
+  TcOut out;
+  int K, BN, ntn, pad;
+};
+struct GroupProblems {
+  const GemmProb* probs;
+  const int* start;
+  int n;
+  __device__ __forceinline__ int total() const { return __ldg(start + n); }
+  __device__ __forceinline__ void tile(int t, TileInfo& ti) const {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GemmProb& P = probs[lo];
+    const int r = t - __ldg(start + lo);
+    ti.f_hi = &P.f[0]; ti.f_lo = &P.f[1]; ti.q_hi = &P.q[0]; ti.q_lo = &P.q[1];
+    ti.K = P.K; ti.BN = P.BN; ti.out = P.out;
+    const int ntn = P.ntn;
+    ti.m0 = (r / ntn) * BM;
+    ti.n0 = (r % ntn) * ti.BN;
+  }
+};
+
 // Persistent batched transform C[m][n] = sum_k F[m][k] Q[n][k] in bf16x3: F (the field, M x K, K-major) and Q (the
 // DST matrix, N x K, K-major) are each given as bf16 hi/lo planes by TMA maps; tiles of BM x BN are taken round-robin
-// (n fastest, so that CTAs working at the same time share the field tile through L2).
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
-    k_dst_tc(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
-             const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
-             unsigned int* err) {
+// (n fastest, so that CTAs working at the same time share the field tile through L2). The tiles come from one problem
+// (one model's transform) or from a list of problems (the same transform of every member of an ensemble).
+template <int MODE, class Src>
+__device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -76,8 +128,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nk = (K + BK - 1) / BK;
-  const int mt = (out.M + BM - 1) / BM, ntn = (out.N + BN - 1) / BN, ntiles = mt * ntn;
+  const int ntiles = src.total();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -91,11 +142,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc::mbar_init(done, 1);
     tc::fence_mbar_init();
   }
-  if (warp == 0 && lane == 0) {
-    tc::prefetch_tmap(&tF_hi);
-    tc::prefetch_tmap(&tF_lo);
-    tc::prefetch_tmap(&tQ_hi);
-    tc::prefetch_tmap(&tQ_lo);
+  if (warp == 0 && lane == 0 && ntiles > 0) {
+    TileInfo ti;
+    src.tile(blockIdx.x < unsigned(ntiles) ? int(blockIdx.x) : 0, ti);
+    tc::prefetch_tmap(ti.f_hi);
+    tc::prefetch_tmap(ti.f_lo);
+    tc::prefetch_tmap(ti.q_hi);
+    tc::prefetch_tmap(ti.q_lo);
   }
   if (warp == 1) {
     tc::tmem_alloc(tmem_slot, kTmemCols);
@@ -108,30 +161,35 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
-      const uint32_t bytes = uint32_t(2 * A_TILE + 2 * BN * BK * 2);
       int g = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+        TileInfo ti;
+        src.tile(t, ti);
+        const uint32_t bytes = uint32_t(2 * A_TILE + 2 * ti.BN * BK * 2);
+        const int nk = (ti.K + BK - 1) / BK;
         for (int kt = 0; kt < nk; kt++, g++) {
           const int s = g % STAGES;
           const uint32_t ph = (g / STAGES) & 1;
           if (!(ok = tc::mbar_wait(&empty[s], ph ^ 1, err, 1u))) break;
           uint8_t* st = smem + s * STAGE_BYTES;
           tc::mbar_expect_tx(&full[s], bytes);
-          tc::tma_load_2d(st, &tF_hi, &full[s], kt * BK, m0);
-          tc::tma_load_2d(st + A_TILE, &tF_lo, &full[s], kt * BK, m0);
-          tc::tma_load_2d(st + 2 * A_TILE, &tQ_hi, &full[s], kt * BK, n0);
-          tc::tma_load_2d(st + 2 * A_TILE + B_TILE, &tQ_lo, &full[s], kt * BK, n0);
+          tc::tma_load_2d(st, ti.f_hi, &full[s], kt * BK, ti.m0);
+          tc::tma_load_2d(st + A_TILE, ti.f_lo, &full[s], kt * BK, ti.m0);
+          tc::tma_load_2d(st + 2 * A_TILE, ti.q_hi, &full[s], kt * BK, ti.n0);
+          tc::tma_load_2d(st + 2 * A_TILE + B_TILE, ti.q_lo, &full[s], kt * BK, ti.n0);
         }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      const uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
       int g = 0, it = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, it++) {
+        TileInfo ti;
+        src.tile(t, ti);
+        const uint32_t idesc = tc::idesc_bf16_f32(BM, ti.BN);
+        const int nk = (ti.K + BK - 1) / BK;
         const int b = it & 1;
         if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
         tc::tc_fence_after();
@@ -146,7 +204,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
           const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
           const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + B_TILE));
-          const int ksub = min(BK, K - kt * BK + 15) / 16;  // 16-wide steps holding data (the rest is zero fill)
+          const int ksub = min(BK, ti.K - kt * BK + 15) / 16;  // 16-wide steps holding data (the rest is zero fill)
           for (int kk = 0; kk < ksub; kk++) {
             const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
             tc::mma_bf16(acc, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
@@ -164,8 +222,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;
     int it = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+      TileInfo ti;
+      src.tile(t, ti);
+      const TcOut& out = ti.out;
+      const int BN = ti.BN, m0 = ti.m0, n0 = ti.n0;
       const int b = it & 1;
-      const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
       if (!tc::mbar_wait(&tfull[b], (it >> 1) & 1, err, 8u)) break;
       tc::tc_fence_after();
       const int m = m0 + q * 32 + lane;  // this thread's row of the tile
@@ -234,6 +295,23 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_dst_tc(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
+             const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
+             unsigned int* err) {
+  const int ntn = (out.N + BN - 1) / BN;
+  const OneProblem src{&tF_hi, &tF_lo, &tQ_hi, &tQ_lo, K, BN, ntn, ((out.M + BM - 1) / BM) * ntn, out};
+  dst_tc_run<MODE>(src, err);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) k_dst_tc_grp(const GemmProb* __restrict__ probs, const int* __restrict__ start, int n,
+                                                            unsigned int* err) {
+  const GroupProblems src{probs, start, n};
+  dst_tc_run<MODE>(src, err);
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // fp32 field -> bf16 hi/lo planes with a padded row pitch (rows of `cols` values, pitch ld), zero in the padding
 // ---------------------------------------------------------------------------------------------------------------
@@ -253,9 +331,10 @@ __global__ void k_split_rows(const float* __restrict__ src, long rows, int cols,
 // with phi = 0 on the faces beyond the grid (antisymmetric ghosts, the operator the sine transforms diagonalise) and
 // Neumann in z (lo = 0 at the ground, up = 0 at the lid); written split for the correction solve
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __restrict__ zop, const float* __restrict__ rhs,
-                        const float* __restrict__ phi, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+__device__ __forceinline__ void resid_body(int nx, int ny, int nz, double idx2, const float4* __restrict__ zop, const float* __restrict__ rhs,
+                                           const float* __restrict__ phi, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                           int ld, const int BX, const int BY, const int BZ) {
+  const int i = BX * blockDim.x + threadIdx.x, j = BY, k = BZ;
   if (i >= nx) return;
   const long pl = long(nx) * ny;
   const long o = long(k) * pl + long(j) * nx + i;
@@ -268,6 +347,31 @@ __global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __res
   const float r = float(double(rhs[o]) - Lp);
   const long t = (long(k) * ny + j) * ld + i;
   tc::split_bf16(r, hi[t], lo[t]);
+}
+__global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __restrict__ zop, const float* __restrict__ rhs,
+                        const float* __restrict__ phi, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld) {
+  resid_body(nx, ny, nz, idx2, zop, rhs, phi, hi, lo, ld, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+struct ResidProb {
+  int nx, ny, nz, ld, gx;
+  double idx2;
+  const float4* zop;
+  const float* rhs;
+  const float* phi;
+  __nv_bfloat16* hi;
+  __nv_bfloat16* lo;
+};
+__global__ void k_resid_grp(const ResidProb* __restrict__ probs, const int* __restrict__ start, int n) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const ResidProb& P = probs[lo];
+  const int r = b - __ldg(start + lo);
+  resid_body(P.nx, P.ny, P.nz, P.idx2, P.zop, P.rhs, P.phi, P.hi, P.lo, P.ld, r % P.gx, (r / P.gx) % P.ny, r / (P.gx * P.ny));
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -282,14 +386,14 @@ __global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __res
 template <int NZ>
 constexpr int tri_tm() { return NZ > 40 ? 8 : 16; }
 template <int NZ>
-__global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
-                                                const double* __restrict__ low, const float* __restrict__ T2,
-                                                __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo) {
+__device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
+                                         const double* __restrict__ low, const float* __restrict__ T2,
+                                         __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo, const int BX, const int BY) {
   constexpr int KC = 16;  // levels per transpose chunk
   constexpr int TRI_TM = tri_tm<NZ>();
   __shared__ float tile[KC][TRI_TM][33];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
-  const int l = blockIdx.x * 32 + tx, m = blockIdx.y * TRI_TM + ty;
+  const int l = BX * 32 + tx, m = BY * TRI_TM + ty;
   const bool act = l < nxp && m < nyp;
   const bool lowm = l < 2 && m < 2;
   const long sxy = long(nxp) * nyp;
@@ -343,17 +447,17 @@ __global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, 
     const int nkc = NZ - kc < KC ? NZ - kc : KC;
     for (int t = tid; t < nkc * 32; t += 32 * TRI_TM) {
       const int kk = t >> 5, lx = t & 31;
-      const int ll = blockIdx.x * 32 + lx;
+      const int ll = BX * 32 + lx;
       if (ll < nxp) {
         __align__(16) __nv_bfloat16 h16[TRI_TM], l16[TRI_TM];
 #pragma unroll
         for (int u = 0; u < TRI_TM; u++) tc::split_bf16(tile[kk][u][lx], h16[u], l16[u]);
         // rows hold ldy (a multiple of 8) values: 16-byte aligned; columns past nyp land in the row's zero padding
         // when the pitch has room for them, else they are skipped
-        const long o = (long(kc + kk) * nxp + ll) * ldy + blockIdx.y * TRI_TM;
+        const long o = (long(kc + kk) * nxp + ll) * ldy + BY * TRI_TM;
 #pragma unroll
         for (int h = 0; h < TRI_TM / 8; h++)
-          if (blockIdx.y * TRI_TM + h * 8 + 8 <= ldy) {
+          if (BY * TRI_TM + h * 8 + 8 <= ldy) {
             *reinterpret_cast<uint4*>(ohi + o + h * 8) = *reinterpret_cast<const uint4*>(h16 + h * 8);
             *reinterpret_cast<uint4*>(olo + o + h * 8) = *reinterpret_cast<const uint4*>(l16 + h * 8);
           }
@@ -361,6 +465,42 @@ __global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, 
     }
     __syncthreads();
   }
+}
+template <int NZ>
+__global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
+                                                const double* __restrict__ low, const float* __restrict__ T2,
+                                                __nv_bfloat16* __restrict__ ohi, __nv_bfloat16* __restrict__ olo) {
+  tri_body<NZ>(nxp, nyp, ldy, lam, zop, low, T2, ohi, olo, blockIdx.x, blockIdx.y);
+}
+// the tridiagonals of every member of an ensemble: member p owns the linear blocks [start[p], start[p+1])
+struct TriProb {
+  int nxp, nyp, ldy, gx;
+  const float* lam;
+  const float4* zop;
+  const double* low;
+  const float* T2;
+  __nv_bfloat16* ohi;
+  __nv_bfloat16* olo;
+};
+template <int NZ>
+__global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc_grp(const TriProb* __restrict__ probs, const int* __restrict__ start, int n) {
+  // one thread finds the block's member; the problem is read from shared memory, so that no register holds it
+  // through the sweeps
+  __shared__ TriProb P;
+  __shared__ int r;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    P = probs[lo];
+    r = b - __ldg(start + lo);
+  }
+  __syncthreads();
+  tri_body<NZ>(P.nxp, P.nyp, P.ldy, P.lam, P.zop, P.low, P.T2, P.ohi, P.olo, r % P.gx, r / P.gx);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -395,8 +535,8 @@ static bool make_map_2d(CUtensorMap* m, void* base, long rows, long cols, long l
 }
 
 // tile width for N transform outputs: the fewest tiles of at most 256, then the smallest multiple of 16 covering N
-static int pick_bn(int N) {
-  const int nt = (N + BNMAX - 1) / BNMAX;
+static int pick_bn(int N, int cap = BNMAX) {
+  const int nt = (N + cap - 1) / cap;
   return ((N + nt - 1) / nt + 15) / 16 * 16;
 }
 
@@ -417,6 +557,10 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc<OUT_R_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     attr = true;
   }
 }
@@ -429,12 +573,18 @@ struct TcPlan {
   __nv_bfloat16* mat = nullptr;  // 8 matrices hi/lo: qix, qiy, qy, qx
   __nv_bfloat16 *sx_hi = nullptr, *sx_lo = nullptr, *sy_hi = nullptr, *sy_lo = nullptr;
   __nv_bfloat16 *rx_hi = nullptr, *rx_lo = nullptr;  // the right-hand side, split (zero outside what is written)
+  // the residual of the refined solve, split: a buffer of its own, because the residual fills the padding that the
+  // right-hand side leaves zero (the next step's first pass must see zeros there)
+  __nv_bfloat16 *rr_hi = nullptr, *rr_lo = nullptr;
   float* t2 = nullptr;
   double* low = nullptr;  // FP64 factors of the 4 lowest modes
   unsigned int* err = nullptr;
   int bnx = 0, bny = 0;   // tile widths of the x and y transforms
   CUtensorMap Q[4][2];    // DST matrices, the B operand: [transform][hi/lo]
-  CUtensorMap Fx[2], Fy[2], Fr[2];  // fields, the A operand: S_x, S_y and the split right-hand side
+  __nv_bfloat16* qmat[4][2] = {};  // their bf16 planes: x-fwd, y-fwd, y-inv, x-inv
+  long qld[4] = {};
+  int qdim[4] = {};
+  CUtensorMap Fx[2], Fy[2], Fr[2], Frr[2];  // fields, the A operand: S_x, S_y, the split right-hand side and residual
 };
 
 static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
@@ -466,6 +616,7 @@ int PoissonPlan::tc_create() {
             al((void**)&T->rx_hi, nsx * 2) && al((void**)&T->rx_lo, nsx * 2) &&
             al((void**)&T->sy_hi, nsy * 2) && al((void**)&T->sy_lo, nsy * 2) && al((void**)&T->t2, size_t(nz) * nx * ny * 4) &&
             al((void**)&T->low, size_t(8) * nz * 8) && al((void**)&T->err, 16);
+  if (ok && precision == 2) ok = al((void**)&T->rr_hi, nsx * 2) && al((void**)&T->rr_lo, nsx * 2);
   if (!ok) {
     set_error("poisson: out of device memory for the tensor-core path");
     return OB_ERR_OOM;
@@ -488,6 +639,10 @@ int PoissonPlan::tc_create() {
     cudaMemcpy(mp[t][0], hi.data(), n * 2, cudaMemcpyHostToDevice);
     cudaMemcpy(mp[t][1], lo.data(), n * 2, cudaMemcpyHostToDevice);
     off += 2 * n;
+    T->qmat[t][0] = mp[t][0];
+    T->qmat[t][1] = mp[t][1];
+    T->qld[t] = ld[t];
+    T->qdim[t] = dim[t];
   }
   T->bnx = pick_bn(nx);
   T->bny = pick_bn(ny);
@@ -498,6 +653,8 @@ int PoissonPlan::tc_create() {
   // A operands, planes stacked: S_x and the split rhs [nz * ny][nx] pitch ldx; S_y [nz * nx][ny] pitch ldy
   ok = ok && make_map_2d(&T->Fx[0], T->sx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fx[1], T->sx_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fr[0], T->rx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fr[1], T->rx_lo, long(nz) * ny, nx, T->ldx, BM);
+  if (precision == 2)
+    ok = ok && make_map_2d(&T->Frr[0], T->rr_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Frr[1], T->rr_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fy[0], T->sy_hi, long(nz) * nx, ny, T->ldy, BM) && make_map_2d(&T->Fy[1], T->sy_lo, long(nz) * nx, ny, T->ldy, BM);
   if (!ok) {
     set_error("poisson: tensor map encoding failed");
@@ -539,8 +696,8 @@ int PoissonPlan::tc_factor_low() {
 void PoissonPlan::tc_destroy() {
   TcPlan* T = static_cast<TcPlan*>(tc);
   if (!T) return;
-  for (void* p : {(void*)T->mat, (void*)T->sx_hi, (void*)T->sx_lo, (void*)T->rx_hi, (void*)T->rx_lo, (void*)T->sy_hi, (void*)T->sy_lo,
-                  (void*)T->t2, (void*)T->low, (void*)T->err})
+  for (void* p : {(void*)T->mat, (void*)T->sx_hi, (void*)T->sx_lo, (void*)T->rx_hi, (void*)T->rx_lo, (void*)T->rr_hi, (void*)T->rr_lo,
+                  (void*)T->sy_hi, (void*)T->sy_lo, (void*)T->t2, (void*)T->low, (void*)T->err})
     if (p) cudaFree(p);
   delete T;
   tc = nullptr;
@@ -552,11 +709,12 @@ static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn,
   k_dst_tc<MODE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
 }
 
-// the four transforms and the tridiagonals from the split right-hand side in rx to phi (stored, or added when add)
+// the four transforms and the tridiagonals from a split right-hand side (rx, or the residual rr when add) to phi
+// (stored, or added when add)
 static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s) {
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   // X-fwd: field rows (k, j), K = i, outputs l  -> S_y[k][l][j]
-  launch_tc<OUT_T_BF16X2>(T->Fr, T->Q[0], nx, T->bnx, TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, T->err, s);
+  launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, T->err, s);
   // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
   launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, T->err, s);
   // tridiagonals -> S_y[k][l][m]
@@ -586,7 +744,7 @@ int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
   if (!presplit) k_split_rows<<<1184, 256, 0, s>>>(rhs, long(nz) * ny, nx, T->rx_hi, T->rx_lo, int(T->ldx));
   tc_pass(*this, T, lam, zop, phi, false, s);
   if (precision == 2) {
-    k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rx_hi, T->rx_lo, int(T->ldx));
+    k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rr_hi, T->rr_lo, int(T->ldx));
     tc_pass(*this, T, lam, zop, phi, true, s);
   }
   const cudaError_t e = cudaGetLastError();
@@ -612,6 +770,198 @@ int PoissonPlan::tc_check() {
   if (h) {
     cudaMemset(T->err, 0, sizeof(unsigned int));
     set_error("poisson: a tensor-core pipeline wait timed out (code %u)", h);
+    return OB_ERR_TIMEOUT;
+  }
+  return OB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// grouped solve: the same pass of every member of an ensemble in one launch (persistent transforms over the members'
+// concatenated tile lists, the tridiagonals and residuals over their concatenated blocks)
+// ---------------------------------------------------------------------------------------------------------------
+struct TcGroup {
+  int n = 0, nz = 0, precision = 1, bn_cap = BNMAX;
+  std::vector<PoissonPlan*> plans;
+  std::vector<float*> phi;
+  std::vector<const float*> rhs;
+  GemmProb* d_probs = nullptr;  // [5][n]: x-fwd, y-fwd, y-inv, x-inv, x-fwd of the residual
+  int* d_start = nullptr;       // [5][n + 1] tile starts, [n + 1] tridiagonal block starts, [n + 1] residual block starts
+  TriProb* d_tri = nullptr;
+  ResidProb* d_res = nullptr;
+  unsigned int* err = nullptr;
+  int tiles[5] = {}, tri_blocks = 0, res_blocks = 0;
+};
+
+// problem tables for the tile-width cap (the B operand's box height is the tile width, so its maps are re-encoded)
+static int tc_group_build(TcGroup* G) {
+  const int n = G->n;
+  constexpr int NT = 5;  // transform lists
+  std::vector<GemmProb> probs(size_t(NT) * n);
+  std::vector<int> start(size_t(NT + 2) * (n + 1), 0);
+  std::vector<TriProb> tri(n);
+  std::vector<ResidProb> res(n);
+  const int tm = G->nz == 16 ? tri_tm<16>() : G->nz == 40 ? tri_tm<40>() : tri_tm<80>();
+  for (int i = 0; i < n; i++) {
+    const PoissonPlan* P = G->plans[i];
+    TcPlan* T = static_cast<TcPlan*>(P->tc);
+    const int nx = P->nx, ny = P->ny, nz = P->nz;
+    const int bnx = pick_bn(nx, G->bn_cap), bny = pick_bn(ny, G->bn_cap);
+    // the fifth list is the x-fwd transform again, reading the residual (refined solve only)
+    const int bn[NT] = {bnx, bny, bny, bnx, bnx}, K[NT] = {nx, ny, ny, nx, nx}, qi[NT] = {0, 1, 2, 3, 0};
+    const CUtensorMap* F[NT] = {T->Fr, T->Fy, T->Fy, T->Fx, G->precision == 2 ? T->Frr : T->Fr};
+    const TcOut xfwd{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx};
+    const TcOut out[NT] = {xfwd, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny},
+                           TcOut{nullptr, nullptr, G->phi[i], nx, ny, nz * ny, nx}, xfwd};
+    for (int t = 0; t < NT; t++) {
+      GemmProb& g = probs[size_t(t) * n + i];
+      std::memset(&g, 0, sizeof(g));
+      g.f[0] = F[t][0];
+      g.f[1] = F[t][1];
+      for (int h = 0; h < 2; h++)
+        if (!make_map_2d(&g.q[h], T->qmat[qi[t]][h], T->qdim[qi[t]], T->qdim[qi[t]], T->qld[qi[t]], bn[t])) {
+          set_error("ensemble solve: tensor map encoding failed");
+          return OB_ERR_DEVICE;
+        }
+      g.out = out[t];
+      g.K = K[t];
+      g.BN = bn[t];
+      g.ntn = (out[t].N + bn[t] - 1) / bn[t];
+      const int nt = ((out[t].M + BM - 1) / BM) * g.ntn;
+      start[size_t(t) * (n + 1) + i + 1] = start[size_t(t) * (n + 1) + i] + nt;
+    }
+    const int gx = (nx + 31) / 32, gy = (ny + tm - 1) / tm;
+    tri[i] = TriProb{nx, ny, int(T->ldy), gx, P->lam, P->zop, T->low, T->t2, T->sy_hi, T->sy_lo};
+    start[size_t(NT) * (n + 1) + i + 1] = start[size_t(NT) * (n + 1) + i] + gx * gy;
+    const int rgx = (nx + 127) / 128;
+    res[i] = ResidProb{nx, ny, nz, int(T->ldx), rgx, 1.0 / (P->dx * P->dx), P->zop, G->rhs[i], G->phi[i], T->rr_hi, T->rr_lo};
+    start[size_t(NT + 1) * (n + 1) + i + 1] = start[size_t(NT + 1) * (n + 1) + i] + rgx * ny * nz;
+  }
+  for (int t = 0; t < NT; t++) G->tiles[t] = start[size_t(t) * (n + 1) + n];
+  G->tri_blocks = start[size_t(NT) * (n + 1) + n];
+  G->res_blocks = start[size_t(NT + 1) * (n + 1) + n];
+  const bool ok = cudaMemcpy(G->d_probs, probs.data(), probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(G->d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(G->d_tri, tri.data(), tri.size() * sizeof(TriProb), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(G->d_res, res.data(), res.size() * sizeof(ResidProb), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    set_error("ensemble solve: problem table upload failed");
+    return OB_ERR_DEVICE;
+  }
+  return OB_OK;
+}
+
+void tc_group_destroy(TcGroup* G) {
+  if (!G) return;
+  for (void* p : {(void*)G->d_probs, (void*)G->d_start, (void*)G->d_tri, (void*)G->d_res, (void*)G->err})
+    if (p) cudaFree(p);
+  delete G;
+}
+
+int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* const* rhs, int n, TcGroup** out) {
+  *out = nullptr;
+  if (n < 1) { set_error("ensemble solve: no members"); return OB_ERR_INVALID; }
+  TcGroup* G = new TcGroup();
+  G->n = n;
+  G->nz = plans[0]->nz;
+  G->precision = plans[0]->precision;
+  for (int i = 0; i < n; i++) {
+    const PoissonPlan* P = plans[i];
+    if (!P->tc || P->precision < 1 || !P->presplit) {
+      set_error("ensemble solve: member %d does not use the tensor-core solve with the split right-hand side", i);
+      tc_group_destroy(G);
+      return OB_ERR_INVALID;
+    }
+    if (P->nz != G->nz || P->precision != G->precision) {
+      set_error("ensemble solve: members must share nz and the solver precision (member %d)", i);
+      tc_group_destroy(G);
+      return OB_ERR_INVALID;
+    }
+    if (G->precision == 2 && !rhs[i]) {
+      set_error("ensemble solve: member %d has no fp32 right-hand side for the refinement", i);
+      tc_group_destroy(G);
+      return OB_ERR_INVALID;
+    }
+    G->plans.push_back(plans[i]);
+    G->phi.push_back(phi[i]);
+    G->rhs.push_back(rhs[i]);
+  }
+  if (G->nz != 16 && G->nz != 40 && G->nz != 80) {
+    set_error("ensemble solve: the tensor-core path supports nz in {16, 40, 80}");
+    tc_group_destroy(G);
+    return OB_ERR_INVALID;
+  }
+  const bool ok = cudaMalloc(&G->d_probs, size_t(5) * n * sizeof(GemmProb)) == cudaSuccess &&
+                  cudaMalloc(&G->d_start, size_t(7) * (n + 1) * sizeof(int)) == cudaSuccess &&
+                  cudaMalloc(&G->d_tri, size_t(n) * sizeof(TriProb)) == cudaSuccess &&
+                  cudaMalloc(&G->d_res, size_t(n) * sizeof(ResidProb)) == cudaSuccess && cudaMalloc(&G->err, 16) == cudaSuccess &&
+                  cudaMemset(G->err, 0, 16) == cudaSuccess;
+  if (!ok) {
+    set_error("ensemble solve: out of device memory");
+    tc_group_destroy(G);
+    return OB_ERR_OOM;
+  }
+  set_smem_attrs();
+  const int rc = tc_group_build(G);
+  if (rc != OB_OK) {
+    tc_group_destroy(G);
+    return rc;
+  }
+  *out = G;
+  return OB_OK;
+}
+
+int tc_group_set_cap(TcGroup* G, int bn_cap) {
+  if (bn_cap < 16 || bn_cap > BNMAX || bn_cap % 16) { set_error("ensemble solve: tile width cap %d not in 16..256 (multiple of 16)", bn_cap); return OB_ERR_INVALID; }
+  if (bn_cap == G->bn_cap) return OB_OK;
+  // the tables are read by launches already queued: wait for them before rewriting
+  if (cudaDeviceSynchronize() != cudaSuccess) { set_error("ensemble solve: device error before retiling"); return OB_ERR_DEVICE; }
+  G->bn_cap = bn_cap;
+  return tc_group_build(G);
+}
+int tc_group_cap(const TcGroup* G) { return G->bn_cap; }
+
+template <int MODE>
+static void launch_tc_grp(const TcGroup* G, int t, cudaStream_t s) {
+  if (G->tiles[t] < 1) return;
+  k_dst_tc_grp<MODE><<<std::min(G->tiles[t], num_sms()), kThreads, SMEM_BYTES, s>>>(G->d_probs + size_t(t) * G->n,
+                                                                                     G->d_start + size_t(t) * (G->n + 1), G->n, G->err);
+}
+
+static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s) {
+  const int n = G->n;
+  launch_tc_grp<OUT_T_BF16X2>(G, add ? 4 : 0, s);
+  launch_tc_grp<OUT_T_F32>(G, 1, s);
+  const int* ts = G->d_start + size_t(5) * (n + 1);
+  switch (G->nz) {
+    case 16: k_tri_tc_grp<16><<<G->tri_blocks, dim3(32, tri_tm<16>()), 0, s>>>(G->d_tri, ts, n); break;
+    case 40: k_tri_tc_grp<40><<<G->tri_blocks, dim3(32, tri_tm<40>()), 0, s>>>(G->d_tri, ts, n); break;
+    default: k_tri_tc_grp<80><<<G->tri_blocks, dim3(32, tri_tm<80>()), 0, s>>>(G->d_tri, ts, n); break;
+  }
+  launch_tc_grp<OUT_T_BF16X2>(G, 2, s);
+  if (add) launch_tc_grp<OUT_R_F32_ADD>(G, 3, s);
+  else launch_tc_grp<OUT_R_F32>(G, 3, s);
+}
+
+int tc_group_solve(TcGroup* G, cudaStream_t s) {
+  tc_group_pass(G, false, s);
+  if (G->precision == 2) {
+    k_resid_grp<<<G->res_blocks, 128, 0, s>>>(G->d_res, G->d_start + size_t(6) * (G->n + 1), G->n);
+    tc_group_pass(G, true, s);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("ensemble solve launch: %s", cudaGetErrorString(e));
+    return OB_ERR_DEVICE;
+  }
+  return OB_OK;
+}
+
+int tc_group_check(TcGroup* G) {
+  unsigned int h = 0;
+  cudaMemcpy(&h, G->err, sizeof(h), cudaMemcpyDeviceToHost);
+  if (h) {
+    cudaMemset(G->err, 0, sizeof(unsigned int));
+    set_error("ensemble solve: a tensor-core pipeline wait timed out (code %u)", h);
     return OB_ERR_TIMEOUT;
   }
   return OB_OK;

@@ -42,4 +42,15 @@ struct PoissonPlan {
   void tc_destroy();
 };
 
+// grouped solve of an ensemble: every member's solve in the same few launches (ob_dst_tc.cu). The plans use the
+// tensor-core path with the split right-hand side written by their divergence pass, share nz and precision;
+// phi[i] is member i's output, rhs[i] its fp32 right-hand side (precision 2).
+struct TcGroup;
+int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* const* rhs, int n, TcGroup** out);
+int tc_group_set_cap(TcGroup* G, int bn_cap);  // widest transform tile (16..256, multiple of 16)
+int tc_group_cap(const TcGroup* G);
+int tc_group_solve(TcGroup* G, cudaStream_t s);
+int tc_group_check(TcGroup* G);
+void tc_group_destroy(TcGroup* G);
+
 }  // namespace ob

@@ -12,10 +12,35 @@
 
 namespace ob {
 
+// members of the grouped launches (ensemble steps) and each pass's block table, uploaded by group_upload_members.
+// Both sit in constant memory and the block's member is found from blockIdx and constant loads alone, so the member
+// index is warp-uniform to the compiler and the member's uniforms are read through the uniform datapath.
+__constant__ MemberC c_members[kMaxMembers];
+__constant__ GroupTable c_tables[kGroupPasses];
+__device__ __forceinline__ void group_block_c(const GroupTable& T, int& mem, int& bx, int& by, int& bz) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = T.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (T.start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  mem = lo;
+  const int r = b - T.start[lo], gx = T.gx[lo], gy = T.gy[lo];
+  bx = r % gx;
+  by = (r / gx) % gy;
+  bz = r / (gx * gy);
+}
+#define OB_GROUP_RESOLVE(PASS) \
+  int mem, gbx, gby, gbz;      \
+  group_block_c(c_tables[PASS], mem, gbx, gby, gbz);
+
+// block coordinates: blockIdx for a launch over one model, or the (member, block) a grouped launch resolved
+#define OB_BLOCKS_DIRECT const int BX = blockIdx.x, BY = blockIdx.y, BZ = blockIdx.z;
 #define OB_TEXEL_LOOP_BEGIN(XMAX, YMAX, ZMAX)             \
-  const int ci = blockIdx.x * blockDim.x + threadIdx.x;   \
-  const int cj = blockIdx.y * blockDim.y + threadIdx.y;   \
-  const int ck = blockIdx.z;                              \
+  const int ci = BX * blockDim.x + threadIdx.x;           \
+  const int cj = BY * blockDim.y + threadIdx.y;           \
+  const int ck = BZ;                                      \
   if (ci > (XMAX) || cj > (YMAX) || ck > (ZMAX)) return;
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -68,8 +93,8 @@ __device__ void bpt(const float* bd, int i, float t, float& x, float& y) {
   x = q[0] + q[2] * t;
   y = q[1] + q[3] * t;
 }
-__global__ void k_lsf(Grid g, Uni U, Fields F) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void lsf_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int i = BX * blockDim.x + threadIdx.x, j = BY * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
   const float dx = U.dims.w, t = float(__ldg(F.clock));
   const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
@@ -157,12 +182,21 @@ __global__ void k_lsf(Grid g, Uni U, Fields F) {
     F.phT[g.at(i, j, k)] = ph;
   }
 }
+__global__ void k_lsf(Grid g, Uni U, Fields F) { lsf_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_lsf_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupLSF)
+  {
+    const double t = *c_members[mem].F.clock, t0 = *c_members[mem].lsfT;
+    if (!(t - t0 >= 60.0 || t == 0.0)) return;
+  }
+  lsf_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_CI (model.js:249-281): strongest active updraft-nudging event per column
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_ci(Grid g, Uni U, Fields F) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void ci_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int i = BX * blockDim.x + threadIdx.x, j = BY * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
   const float dx = U.dims.w, t = float(__ldg(F.clock));
   const float x = (float(i) + 0.5f) * dx, y = (float(j) + 0.5f) * dx;
@@ -185,11 +219,22 @@ __global__ void k_ci(Grid g, Uni U, Fields F) {
   }
   F.ciMap[j * g.nx + i] = best;
 }
+__global__ void k_ci(Grid g, Uni U, Fields F) { ci_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_ci_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupCI)
+  if (gbx == 0 && gby == 0 && gbz == 0 && threadIdx.x == 0 && threadIdx.y == 0) {  // after the LSF pass of this step
+    const double t = *c_members[mem].F.clock;
+    double* t0 = c_members[mem].lsfT;
+    if (t - *t0 >= 60.0 || t == 0.0) *t0 = t;
+  }
+  ci_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_INIT (model.js:284-339), outbreak mode (no vortex)
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void k_init(Grid g, Uni U, Fields F) {
+  OB_BLOCKS_DIRECT
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const int k = min(ck, g.nz - 1);
   const float dz = U.dzv.x;
@@ -219,7 +264,7 @@ __global__ void k_init(Grid g, Uni U, Fields F) {
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_NUT (model.js:342-389): Smagorinsky-Lilly viscosities with the Richardson correction
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) {
+__device__ __forceinline__ void nut_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
   // a cell's +1 neighbours on the staggered box always exist; the -1 ones clamp to the edge (offset 0)
   const int o = g.at(ci, cj, ck);
@@ -255,6 +300,11 @@ __global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int pa
   const float dtc = fmaxf(U.step.x, 0.1f);
   F.aux[0][o] = fminf(lh * lh * sS * fst, 0.08f * dx * dx / dtc);
   F.aux[1][o] = fminf(lv * lv * sS * fst, 0.15f * dz * dz / dtc);
+}
+__global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) { nut_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128, 16) k_nut_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupNUT)
+  nut_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -302,7 +352,7 @@ __device__ __forceinline__ float sampleVch(const float* f, const Grid& g, int ch
   return trilerpB(f, g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz);
 }
 
-__global__ void k_advv1(Grid g, Uni U, Fields F, int par) {
+__device__ __forceinline__ void advv1_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
   const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
@@ -317,6 +367,11 @@ __global__ void k_advv1(Grid g, Uni U, Fields F, int par) {
   F.Vt[2][o] = sampleVch(F.V[par][2], g, 2, x, y, z);
   traceV(g, kk, fi + 0.5f, fj + 0.5f, fk + 0.5f, L.vc, 1.f, x, y, z);
   F.Vt[3][o] = sampleVch(F.V[par][3], g, 3, x, y, z);
+}
+__global__ void k_advv1(Grid g, Uni U, Fields F, int par) { advv1_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_advv1_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupADVV1)
+  advv1_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 __device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Grid& g, float x, float y, float z, float ox, float oy, float oz) {
@@ -333,7 +388,7 @@ __device__ __forceinline__ float2 minmax8V(const float* __restrict__ f, const Gr
   return make_float2(lo, hi);
 }
 
-__global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) {
+__device__ __forceinline__ void advv2_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
   const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
@@ -356,6 +411,11 @@ __global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int 
     const float2 m = minmax8V(F.V[par][c], g, x, y, z, ox, oy, oz);
     F.V[1 - par][c][o] = clampf(r, m.x, m.y);
   }
+}
+__global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) { advv2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128, 12) k_advv2_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupADVV2)
+  advv2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -458,8 +518,8 @@ __device__ __forceinline__ bool region_active(const Grid& g, const Fields& F, Re
 
 // ---- ADVQ1 (model.js:500-529): semi-Lagrangian step of the 8 scalars, channels grouped by the fall speed of
 // their trace (qv, qc, qi, spare [and Nr for Lin] at the air's speed; qr, qs, qg, Nr (Thompson) each their own) ----
-__global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int par) {
-  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+__device__ __forceinline__ void advq1_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
   const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
@@ -478,7 +538,7 @@ __global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int 
     r.z1 = max(r.z1, int(floorf(fminf(z + kk[2] * F.fallmax, float(g.nz) - 0.5f) - 0.5f)) + 1);
   }
   const bool active = region_active(g, F, r, F.actQ0, nullptr);
-  const int brick = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+  const int brick = BX + F.nbx * (BY + F.nby * BZ);
   if (in) {
     const Tap t0 = tapQ(g, x, y, z);
     F.Qt[0][o] = gatherQ(F.Q[0][0], t0);
@@ -513,6 +573,11 @@ __global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int 
     F.zeroQt[brick] = active ? 0u : 1u;
   }
 }
+__global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int par) { advq1_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128, 10) k_advq1_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupADVQ1)
+  advq1_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
+}
 
 // ---- ADVQ2 (model.js:530-576): MacCormack correction, limiter on the departure cell's 8 texels, clip >= 0 ----
 __device__ __forceinline__ float advq2_channel(const Fields& F, const Grid& g, const float kk[3], const float p[3], const float v[3],
@@ -526,8 +591,8 @@ __device__ __forceinline__ float advq2_channel(const Fields& F, const Grid& g, c
   return fmaxf(clampf(r, m.x, m.y), 0.f);
 }
 
-__global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int par) {
-  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+__device__ __forceinline__ void advq2_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
   const bool in = ci < g.nx && cj < g.ny && ck < g.nz;
   const int o = in ? g.at(ci, cj, ck) : 0;
   const float kk[3] = {U.der.x, U.der.x, U.der.y};  // dt/dx, dt/dx, dt/dz
@@ -548,7 +613,7 @@ __global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int 
     r.z1 = max(r.z1, int(floorf(fminf(fmaxf(zb, zf) + dzf, float(g.nz) - 0.5f) - 0.5f)) + 1);
   }
   const bool active = region_active(g, F, r, F.actQ0, F.actQt);
-  const int brick = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+  const int brick = BX + F.nbx * (BY + F.nby * BZ);
   if (in) {
     const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
     const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
@@ -594,6 +659,11 @@ __global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int 
     }
   }
   if (threadIdx.x == 0 && threadIdx.y == 0) F.zeroQ1[brick] = active ? 0u : 1u;
+}
+__global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int par) { advq2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128, 8) k_advq2_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupADVQ2)
+  advq2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 // hydrometeor flags of Q slot 0 per brick, from scratch (after a reset or a host upload of Q); the scratch-known-zero
@@ -891,21 +961,28 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
 }
 
 template <int MM>
-__global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) {
-  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+__device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
     hyd = U.cor.z > 0.5f ? phys_texel<true, MM>(g, U, F, par, ci, cj, ck) : phys_texel<false, MM>(g, U, F, par, ci, cj, ck);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
-  if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && ck < g.nz)
-    F.actQ0[blockIdx.x + F.nbx * (blockIdx.y + F.nby * ck)] = any ? 1u : 0u;
+  if (threadIdx.x == 0 && threadIdx.y == 0 && int(BX) < F.nbx && int(BY) < F.nby && ck < g.nz)
+    F.actQ0[BX + F.nbx * (BY + F.nby * ck)] = any ? 1u : 0u;
+}
+template <int MM>
+__global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+template <int MM>
+__global__ void __launch_bounds__(128, 8) k_phys_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupPHYS)
+  phys_body<MM>(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_DIV (model.js:909-925): density-weighted divergence / dt on the padded solve grid
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_div(Grid g, Uni U, Fields F, int par) {
+__device__ __forceinline__ void div_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
   const int o = g.at(ci, cj, ck);
   const float* __restrict__ u = F.V[par][0];
@@ -925,11 +1002,16 @@ __global__ void k_div(Grid g, Uni U, Fields F, int par) {
   }
   if (F.rhs) F.rhs[g.pidx(ci, cj, ck)] = r;  // fp32 solve, or the residual of the refined solve
 }
+__global__ void k_div(Grid g, Uni U, Fields F, int par) { div_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_div_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupDIV)
+  div_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_PROJ (model.js:927-946): u -= dt grad(phi), phi from the padded solve
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_proj(Grid g, Uni U, Fields F, int par) {
+__device__ __forceinline__ void proj_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   auto P = [&](int a, int b, int c) {
     return __ldg(F.phi + g.pidx(clampi(a, -g.pad, g.nx + g.pad - 1), clampi(b, -g.pad, g.ny + g.pad - 1), clampi(c, 0, g.nz - 1)));
@@ -947,10 +1029,15 @@ __global__ void k_proj(Grid g, Uni U, Fields F, int par) {
   F.V[1 - par][2][o] = w;
   F.V[1 - par][3][o] = __ldg(F.V[par][3] + o);
 }
+__global__ void k_proj(Grid g, Uni U, Fields F, int par) { proj_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_proj_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupPROJ)
+  proj_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
+}
 
 // accumulated surface precipitation (no counterpart in the reference): rho(0) sum_x q_x vt_x at the lowest level
-__global__ void k_rain(Grid g, Uni U, Fields F) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void rain_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
+  const int i = BX * blockDim.x + threadIdx.x, j = BY * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
   const int o = g.at(i, j, 0);
   const Fall fl{U.step.z, U.micro2.z > 0.5f};
@@ -960,6 +1047,11 @@ __global__ void k_rain(Grid g, Uni U, Fields F) {
   const double flux = double(rho) * (double(qr) * double(fv.x) + double(qs) * double(fl.vtS(qs, rho)) + double(qg) * double(fl.vtGrau(qg, rho)));
   F.rain[j * g.nx + i] += flux * double(U.step.x);
   if (i == 0 && j == 0) *F.clock += double(U.step.x);  // the step's last pass advances the model time
+}
+__global__ void k_rain(Grid g, Uni U, Fields F) { rain_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_rain_grp(int par) {
+  OB_GROUP_RESOLVE(kGroupRAIN)
+  rain_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1036,6 +1128,7 @@ __global__ void k_maps(Grid g, Uni U, Fields F, int par, float4* out) {
 // layout conversion between the texel float4 layout of the C ABI and the device SoA layout
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void k_pack(Grid g, Ptr8 src, int nch, int X, int Y, int Z, float* dst) {
+  OB_BLOCKS_DIRECT
   OB_TEXEL_LOOP_BEGIN(X - 1, Y - 1, Z - 1)
   const int o = g.at(ci, cj, ck);
   const size_t t = (size_t(ck) * Y + cj) * X + ci;
@@ -1044,6 +1137,7 @@ __global__ void k_pack(Grid g, Ptr8 src, int nch, int X, int Y, int Z, float* ds
     if (c < nch) dst[t * nch + c] = src.p[c][o];
 }
 __global__ void k_unpack(Grid g, Ptr8 dst, int nch, int X, int Y, int Z, const float* src) {
+  OB_BLOCKS_DIRECT
   OB_TEXEL_LOOP_BEGIN(X - 1, Y - 1, Z - 1)
   const int o = g.at(ci, cj, ck);
   const size_t t = (size_t(ck) * Y + cj) * X + ci;
@@ -1136,6 +1230,71 @@ __global__ void k_tor_candidates(const float4* __restrict__ maps, int nx, int ny
   float* o = out + size_t(slot) * 7;
   o[0] = float(i); o[1] = float(j); o[2] = (float(i) + 0.5f) * dx; o[3] = (float(j) + 0.5f) * dx; o[4] = z1; o[5] = uh; o[6] = w;
 }
+// ---------------------------------------------------------------------------------------------------------------
+// grouped launches (ensemble steps)
+// ---------------------------------------------------------------------------------------------------------------
+int group_kind(int pass) {
+  switch (pass) {
+    case kGroupLSF: case kGroupCI: case kGroupRAIN: return kGroup2D;
+    case kGroupNUT: case kGroupADVQ1: case kGroupADVQ2: case kGroupDIV: return kGroupCell;
+    default: return kGroupStag;
+  }
+}
+
+dim3 group_default_block(int pass) { return group_kind(pass) == kGroup2D ? kB2 : kB3; }
+
+bool group_block_fixed(int pass) {
+  // the scalar advection and the physics pass share the 32 x 4 bricks of the clear-air flags; the 2-D passes are
+  // not worth tuning
+  return pass == kGroupADVQ1 || pass == kGroupADVQ2 || pass == kGroupPHYS || group_kind(pass) == kGroup2D;
+}
+
+int group_fill(const Grid* grids, int n, int pass, dim3 block, GroupTable* T) {
+  if (n < 1 || n > kMaxMembers) return -1;
+  const int kind = group_kind(pass);
+  T->n = n;
+  T->start[0] = 0;
+  for (int i = 0; i < n; i++) {
+    const Grid& g = grids[i];
+    int X = g.nx, Y = g.ny, Z = g.nz;
+    if (kind == kGroupStag) { X++; Y++; Z++; }
+    if (kind == kGroup2D) Z = 1;
+    const int gx = (X + block.x - 1) / block.x, gy = (Y + block.y - 1) / block.y;
+    T->gx[i] = gx;
+    T->gy[i] = gy;
+    T->start[i + 1] = T->start[i] + gx * gy * Z;
+  }
+  return T->start[n];
+}
+
+int group_upload_members(const MemberC* d_src, int n, const GroupTable* d_tables, cudaStream_t s) {
+  if (n < 1 || n > kMaxMembers) return -1;
+  if (cudaMemcpyToSymbolAsync(c_members, d_src, sizeof(MemberC) * n, 0, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return -1;
+  return cudaMemcpyToSymbolAsync(c_tables, d_tables, sizeof(GroupTable) * kGroupPasses, 0, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -1;
+}
+
+void launch_group(int pass, int blocks, dim3 block, int par, cudaStream_t s, int micro_mode) {
+  if (blocks < 1) return;
+  switch (pass) {
+    case kGroupLSF: k_lsf_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupCI: k_ci_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupNUT: k_nut_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupADVV1: k_advv1_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupADVV2: k_advv2_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupADVQ1: k_advq1_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupADVQ2: k_advq2_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupPHYS:
+      if (micro_mode == kMicroRecord) k_phys_grp<kMicroRecord><<<blocks, block, 0, s>>>(par);
+      else if (micro_mode == kMicroSurrogate) k_phys_grp<kMicroSurrogate><<<blocks, block, 0, s>>>(par);
+      else k_phys_grp<kMicroPlain><<<blocks, block, 0, s>>>(par);
+      break;
+    case kGroupDIV: k_div_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupPROJ: k_proj_grp<<<blocks, block, 0, s>>>(par); break;
+    case kGroupRAIN: k_rain_grp<<<blocks, block, 0, s>>>(par); break;
+    default: break;
+  }
+}
+
 void launch_tor_candidates(const Grid& g, float dx, const float4* maps, float zmin, float* out, int cap, unsigned* count, cudaStream_t s) {
   const int ni = (g.nx - 12 + 1) / 2, nj = (g.ny - 12 + 1) / 2;
   if (ni <= 0 || nj <= 0) return;

@@ -24,6 +24,18 @@ void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStrea
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);
 void launch_maps(const Grid& g, const Uni& U, const Fields& F, int par, float4* out, cudaStream_t s);
+// grouped launches: one launch of a pass over every member of an ensemble (members and each pass's GroupTable, built
+// for the pass's block shape, in constant memory, uploaded from device copies)
+enum { kGroupLSF = 0, kGroupCI, kGroupNUT, kGroupADVV1, kGroupADVV2, kGroupADVQ1, kGroupADVQ2, kGroupPHYS, kGroupDIV, kGroupPROJ,
+       kGroupRAIN, kGroupPasses };
+enum { kGroupStag = 0, kGroupCell = 1, kGroup2D = 2 };
+int group_kind(int pass);
+dim3 group_default_block(int pass);
+bool group_block_fixed(int pass);
+int group_fill(const Grid* grids, int n, int pass, dim3 block, GroupTable* T);  // host: returns the launch's blocks
+// copies the member table and the per-pass block tables (kGroupPasses of them) into constant memory on stream s
+int group_upload_members(const MemberC* d_src, int n, const GroupTable* d_tables, cudaStream_t s);
+void launch_group(int pass, int blocks, dim3 block, int par, cudaStream_t s, int micro_mode = 0);
 void launch_tor_candidates(const Grid& g, float dx, const float4* maps, float zmin, float* out, int cap, unsigned* count, cudaStream_t s);
 void launch_pack(const Grid& g, const Ptr8& src, int nch, int X, int Y, int Z, float* dst, cudaStream_t s);
 void launch_unpack(const Grid& g, const Ptr8& dst, int nch, int X, int Y, int Z, const float* src, cudaStream_t s);

@@ -5,16 +5,22 @@ Members differ in grid size, spacing and sounding: nx x ny drawn in [128, 384] x
 surface theta and moisture are drawn until its mixed-layer CAPE (sounding.analyze, sounding.js:86-137) lies in
 1500-4000 J/kg, and a 0-6 km shear drawn in 10-35 m/s; Thompson-style microphysics; one or two warm bubbles.
 
-Each member is an independent model with its own CUDA stream; an ensemble step queues every member's step without
-waiting, so small members run side by side and fill the GPU. The per-step uniforms (model time among them) are
-kernel parameters, so the steps are launched, not replayed from captured graphs; with 21 launches per member step
-the host stays ahead of the GPU (its launch time is reported next to the device time). Across GPUs the members are
+Two ways to step them. `run` gives each member its own CUDA stream and replays each member's captured step there, so
+small members run side by side (24 graph launches per ensemble step, 21 kernels each). `run_grouped` makes the
+members one ObEnsemble: every pass of the step is ONE launch over all members (the members' grids, uniforms and
+field pointers sit in a table the kernels index by block; the solve's transforms take their tiles from every
+member's problem list), 22 launches per ensemble step whatever the member count (16 with a one-pass solve), captured as one CUDA graph. Its
+tile shapes (block widths of the stencil passes, the widest transform tile of the solve) are picked by the
+project's autotuner (ob_ensemble_tune) and cached per member set (TileCache). Across GPUs the members are
 independent units: plan_shards balances them over ranks by cell count, and the only collective is the final gather
 of the metrics.
 """
 from __future__ import annotations
 
+import ctypes as C
+import json
 import math
+import os
 import time
 
 import numpy as np
@@ -138,3 +144,156 @@ def gather(local: dict, dist=None):
     return {"cell_steps_per_s": cell_steps / (span / 1000.0), "device_ms_max": span,
             "latency_ms_p50": float(np.percentile(allat, 50)), "latency_ms_p99": float(np.percentile(allat, 99)),
             "ranks": len(parts)}
+
+
+class TileCache:
+    """Autotuned tiles per member set, in a JSON file: {signature: {"tiles": [...], "ms": [...]}}. The signature
+    names the device and every member's grid, spacing and dt, so a cached choice is reused only for the same work."""
+
+    def __init__(self, path=None):
+        self.path = path or os.path.join(os.path.expanduser("~"), ".cache", "outbreaklab_b200", "ensemble_tiles.json")
+
+    @staticmethod
+    def signature(cases, device=""):
+        parts = ["%dx%dx%d@%g/%g" % (c.nx, c.ny, c.nz, c.dx, c.dt) for c in cases]
+        return device + "|" + ";".join(parts)
+
+    def load(self):
+        try:
+            with open(self.path) as f:
+                return json.load(f)
+        except (OSError, ValueError):
+            return {}
+
+    def get(self, sig):
+        e = self.load().get(sig)
+        if e and isinstance(e.get("tiles"), list):
+            return [int(x) for x in e["tiles"]]
+        return None
+
+    def put(self, sig, tiles, ms):
+        d = self.load()
+        d[sig] = {"tiles": [int(x) for x in tiles], "ms": [float(x) for x in ms]}
+        os.makedirs(os.path.dirname(self.path) or ".", exist_ok=True)
+        tmp = self.path + ".part"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, self.path)
+
+
+class Ensemble:
+    """An ObEnsemble over RegionalModels (members keep their handles)."""
+
+    def __init__(self, models, dts):
+        from . import _native as N
+        self.N = N
+        self.models = list(models)
+        arr = (C.c_void_p * len(self.models))(*[m.h for m in self.models])
+        d = np.asarray(dts, np.float32)
+        h = C.c_void_p()
+        N.check(N.lib().ob_ensemble_create(arr, N.fptr(d), len(self.models), C.byref(h)))
+        self.h = h
+        self.dts = d
+
+    def step(self, n=1):
+        self.N.check(self.N.lib().ob_ensemble_step(self.h, int(n)))
+
+    def sync(self):
+        self.N.check(self.N.lib().ob_ensemble_sync(self.h))
+
+    def timed_steps(self, n):
+        ms = C.c_float()
+        self.N.check(self.N.lib().ob_ensemble_timed_steps(self.h, int(n), C.byref(ms)))
+        return ms.value
+
+    def set_graphs(self, on):
+        self.N.check(self.N.lib().ob_ensemble_set_graphs(self.h, int(bool(on))))
+
+    def tiles(self):
+        t = (C.c_int * self.N.ENS_NTILES)()
+        self.N.check(self.N.lib().ob_ensemble_get_tiles(self.h, t))
+        return list(t)
+
+    def set_tiles(self, tiles):
+        t = (C.c_int * self.N.ENS_NTILES)(*[int(x) for x in tiles])
+        self.N.check(self.N.lib().ob_ensemble_set_tiles(self.h, t))
+
+    def tune(self, reps=5):
+        t = (C.c_int * self.N.ENS_NTILES)()
+        ms = np.zeros(self.N.ENS_NTILES, np.float32)
+        self.N.check(self.N.lib().ob_ensemble_tune(self.h, int(reps), t, self.N.fptr(ms)))
+        return list(t), ms.tolist()
+
+    def lsf_times(self):
+        t = (C.c_double * len(self.models))()
+        self.N.check(self.N.lib().ob_ensemble_lsf_times(self.h, t))
+        return list(t)
+
+    @property
+    def stream(self):
+        return self.N.lib().ob_ensemble_stream(self.h)
+
+    def destroy(self):
+        if self.h:
+            self.N.lib().ob_ensemble_destroy(self.h)
+            self.h = None
+
+
+def run_grouped(cases, steps: int = 50, warmup: int = 3, tune: bool = True, cache: TileCache = None, reps: int = 5):
+    """Steps every member `steps` times as one ObEnsemble. Tiles come from the cache for this member set, else from
+    the autotuner (then cached). Returns the metrics of this process: cell-steps per second over the device time of
+    the timed steps, the ensemble step's latency percentiles (per-step CUDA events) and the tiles used."""
+    import torch
+    from . import _native as N, model as M
+    models = []
+    for c in cases:
+        m, _ = M.setup_case(c)
+        if m.solver < 1:
+            m.set_solver(2)
+        models.append(m)
+    ens = Ensemble(models, [c.dt for c in cases])
+    try:
+        return _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps)
+    finally:
+        ens.destroy()
+        for m in models:
+            m.destroy()
+
+
+def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps):
+    import torch
+    tiles_src, tune_ms = "default", None
+    if tune:
+        cache = cache or TileCache()
+        sig = TileCache.signature(cases, torch.cuda.get_device_name(0) if torch.cuda.is_available() else "")
+        t = cache.get(sig)
+        if t is not None:
+            ens.set_tiles(t)
+            tiles_src = "cache"
+        else:
+            ens.step(1)           # a state with motion in it for the timing
+            ens.sync()
+            t, tune_ms = ens.tune(reps)
+            cache.put(sig, t, tune_ms)
+            tiles_src = "autotuned"
+    ens.step(warmup)
+    ens.sync()
+    stream = torch.cuda.ExternalStream(int(ens.stream or 0))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    t0 = time.perf_counter()
+    for s in range(steps):
+        ev[s][0].record(stream)
+        ens.step(1)
+        ev[s][1].record(stream)
+    host_s = time.perf_counter() - t0
+    ens.sync()
+    lat = np.array([a.elapsed_time(b) for a, b in ev])
+    span_ms = ev[0][0].elapsed_time(ev[-1][1])
+    cells = sum(c.cells for c in cases)
+    out = {"members": len(cases), "cells": cells, "steps": steps, "device_ms": span_ms, "host_launch_ms": host_s * 1e3,
+           "cell_steps_per_s": cells * steps / (span_ms / 1000.0),
+           "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+           "latency_ms_all": lat.tolist(), "nan_guard_count": int(sum(m.nan_count for m in models)),
+           "tiles": ens.tiles(), "tiles_source": tiles_src, "tune_ms": tune_ms,
+           "launches_per_step": 11 + (11 if models[0].solver == 2 else 5)}
+    return out

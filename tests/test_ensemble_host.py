@@ -69,3 +69,22 @@ def test_gather_over_two_gloo_ranks():
         lat = np.array([1, 2, 3] + [2, 3, 4] * 2, float)
         assert np.isclose(g["latency_ms_p50"], np.percentile(lat, 50))
         assert np.isclose(g["latency_ms_p99"], np.percentile(lat, 99))
+
+
+def test_tile_cache_roundtrip(tmp_path):
+    from outbreaklab_b200 import ensemble as E
+    cs = E.draw_members(3, seed=2)
+    c = E.TileCache(str(tmp_path / "sub" / "tiles.json"))
+    sig = E.TileCache.signature(cs, "B200")
+    assert c.get(sig) is None
+    c.put(sig, [64, 32, 32, 128, 16, 128], [0.1, 0.2, 0.3, 0.05, 0.07, 1.5])
+    assert c.get(sig) == [64, 32, 32, 128, 16, 128]
+    # another member set or device has its own entry
+    assert c.get(E.TileCache.signature(cs[:2], "B200")) is None
+    assert c.get(E.TileCache.signature(cs, "H100")) is None
+    c.put(E.TileCache.signature(cs[:2], "B200"), [32] * 5 + [256], [1.0] * 6)
+    assert c.get(sig) == [64, 32, 32, 128, 16, 128]
+    # an unreadable file is an empty cache
+    with open(c.path, "w") as f:
+        f.write("{not json")
+    assert c.get(sig) is None

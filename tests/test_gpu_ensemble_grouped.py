@@ -1,0 +1,220 @@
+"""Grouped ensemble steps (ObEnsemble: one launch per pass over every member) against the same members stepped one by
+one through ob_model_step, for members of different sizes, spacings, time steps and microphysics, across the members'
+LSF passes (every 60 s of each member's own model time); with graphs on and off; with tiles set by hand and by the
+autotuner; and the error paths.
+
+The grouped kernels are separate instantiations of the same per-texel code (their uniforms come from a constant-memory
+table instead of kernel parameters), and the compiler may fuse multiply-adds differently in them: one step agrees
+with the one-by-one step to a few float32 ulps of each field's scale, and 25 steps (a storm growing from a bubble)
+stay within 1e-4 of it. Where both sides run the same instantiation (graphs on / off, tiles) they agree bit for bit."""
+import numpy as np
+import pytest
+
+from outbreaklab_b200 import _native as N, ensemble as E, model as M, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = (N.FIELD_V, N.FIELD_Q1, N.FIELD_Q2, N.FIELD_AUX, N.FIELD_PHI, N.FIELD_RAIN)
+
+
+def cases():
+    out = []
+    for i, (nx, ny, dx, scheme) in enumerate([(48, 40, 1000.0, 1), (64, 56, 1500.0, 0), (40, 64, 2000.0, 1), (72, 48, 1000.0, 0)]):
+        Lx, Ly = nx * dx, ny * dx
+        out.append(W.StormCase("g%d" % i, nx, ny, 40, dx, 6.0 * dx / 1000.0, 1, scheme=scheme,
+                               bubbles=[(0.5 * Lx, 0.5 * Ly)], bubble_rh=min(10000.0, 0.2 * min(Lx, Ly)), seed=10 + i))
+    return out
+
+
+def setup(cs):
+    return [M.setup_case(c)[0] for c in cs]
+
+
+def fields(m):
+    return [m.get_field(f).copy() for f in FIELDS]
+
+
+def assert_same(a, b, exact=True, rtol=1e-5, rtol_phi=None):
+    for ma, mb in zip(a, b):
+        for f, x, y in zip(FIELDS, fields(ma), fields(mb)):
+            if exact:
+                assert np.array_equal(x, y, equal_nan=True), (f, float(np.max(np.abs(x.astype(np.float64) - y))))
+            else:
+                scale = max(float(np.max(np.abs(x))), 1e-30)
+                err = float(np.max(np.abs(x.astype(np.float64) - y)))
+                tol = rtol_phi if (f == N.FIELD_PHI and rtol_phi is not None) else rtol
+                assert err <= tol * scale, (f, err, scale)
+
+
+class Ens:
+    """An Ensemble that is destroyed however the test ends (one ensemble may exist at a time)."""
+
+    def __init__(self, ms, cs):
+        self.e = E.Ensemble(ms, [c.dt for c in cs])
+
+    def __enter__(self):
+        return self.e
+
+    def __exit__(self, *exc):
+        self.e.destroy()
+        return False
+
+
+def one_by_one(cs, steps):
+    ms = setup(cs)
+    for m, c in zip(ms, cs):
+        m.enc_step(c.dt, steps)
+    for m in ms:
+        m.sync()
+    return ms
+
+
+@pytest.fixture(scope="module")
+def reference(native):
+    cs = cases()
+    ms = one_by_one(cs, 25)
+    yield cs, ms
+    for m in ms:
+        m.destroy()
+
+
+@pytest.fixture(scope="module")
+def grouped(native):
+    """The members stepped 25 times as an ensemble (graphs on)."""
+    cs = cases()
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        ens.step(25)
+        ens.sync()
+        lsf = ens.lsf_times()
+    yield cs, ms, lsf
+    for m in ms:
+        m.destroy()
+
+
+def test_one_grouped_step_matches(native):
+    cs = cases()
+    ref = one_by_one(cs, 1)
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        ens.step(1)
+        ens.sync()
+    # the pressure is the solve of the divergence, whose last-bit differences the solve carries over the domain
+    assert_same(ref, ms, exact=False, rtol=2e-6, rtol_phi=2e-5)
+    for m in ref + ms:
+        m.destroy()
+
+
+def test_grouped_matches_one_by_one(reference, grouped):
+    cs, ref = reference
+    _, ms, lsf = grouped
+    assert_same(ref, ms, exact=False, rtol=1e-4)
+    for m, c, t in zip(ms, cs, lsf):
+        assert m.steps == 25 and abs(m.time - 25 * c.dt) < 1e-9
+        assert m.nan_count == 0
+        # LSF every 60 s of the member's own time: the last one at the largest multiple of dt reached after 60 s
+        n = int(np.ceil(60.0 / c.dt - 1e-9))
+        assert t == pytest.approx((25 - 1) // n * n * c.dt)
+
+
+def test_graphs_off_equals_on(grouped):
+    cs, ms_on, _ = grouped
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        ens.set_graphs(False)
+        ens.step(25)
+        ens.sync()
+    assert_same(ms_on, ms)
+    for m in ms:
+        m.destroy()
+
+
+def test_hand_set_tiles(grouped):
+    cs, ref, _ = grouped
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        assert ens.tiles() == [32, 32, 32, 32, 32, 256]
+        ens.set_tiles([64, 16, 128, 64, 128, 64])
+        assert ens.tiles() == [64, 16, 128, 64, 128, 64]
+        ens.step(25)
+        ens.sync()
+        # the stencil passes compute each texel alone; the transforms' accumulation order per element does not
+        # depend on the tile width
+        assert_same(ref, ms, exact=True)
+        with pytest.raises(N.ObError):
+            ens.set_tiles([48, 32, 32, 32, 32, 256])
+        with pytest.raises(N.ObError):
+            ens.set_tiles([32, 32, 32, 32, 32, 40])
+    for m in ms:
+        m.destroy()
+
+
+def test_autotuner_keeps_results(grouped, tmp_path):
+    cs, ref, _ = grouped
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        ens.step(5)
+        ens.sync()
+        tiles, tms = ens.tune(reps=2)
+        assert all(t in (16, 32, 64, 128) for t in tiles[:5]) and tiles[5] in (64, 128, 256)
+        assert all(x > 0 for x in tms)
+        assert ens.tiles() == tiles
+        ens.step(20)   # tuning rewrote only what each step recomputes: the run goes on as if it had not happened
+        ens.sync()
+    for m, r in zip(ms, ref):
+        for f in (N.FIELD_V, N.FIELD_Q1, N.FIELD_Q2, N.FIELD_RAIN):
+            assert np.array_equal(m.get_field(f), r.get_field(f)), f
+    cache = E.TileCache(str(tmp_path / "tiles.json"))
+    sig = E.TileCache.signature(cs, "B200")
+    cache.put(sig, tiles, tms)
+    assert cache.get(sig) == tiles
+    for m in ms:
+        m.destroy()
+
+
+def test_bad_ensembles(native):
+    cs = cases()[:2]
+    ms = setup(cs)
+    with pytest.raises(N.ObError):
+        E.Ensemble([ms[0], ms[0]], [6.0, 6.0])
+    with pytest.raises(N.ObError):
+        E.Ensemble(ms, [6.0, 0.0])
+    odd = M.setup_case(W.StormCase("nz16", 40, 40, 16, 2000.0, 12.0, 1, bubbles=[(40000.0, 40000.0)]))[0]
+    with pytest.raises(N.ObError):
+        E.Ensemble([ms[0], odd], [6.0, 12.0])
+    ms[1].enc_step(cs[1].dt, 1)   # parity differs now
+    with pytest.raises(N.ObError):
+        E.Ensemble(ms, [c.dt for c in cs])
+    for m in ms + [odd]:
+        m.destroy()
+
+
+def test_run_grouped_metrics(native, tmp_path):
+    cs = cases()
+    cache = E.TileCache(str(tmp_path / "t.json"))
+    r = E.run_grouped(cs, steps=6, warmup=3, tune=True, cache=cache, reps=2)
+    assert r["tiles_source"] == "autotuned" and r["cell_steps_per_s"] > 0 and r["nan_guard_count"] == 0
+    assert r["latency_ms_p50"] > 0 and len(r["latency_ms_all"]) == 6
+    r2 = E.run_grouped(cs, steps=4, warmup=3, tune=True, cache=cache)
+    assert r2["tiles_source"] == "cache" and r2["tiles"] == r["tiles"]
+
+
+def test_members_work_inside_and_after(native):
+    cs = cases()[:2]
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        ens.step(3)
+        mp = ms[0].request_maps()          # queued on the ensemble's stream, after its steps
+        assert np.isfinite(mp["m0"]).all() and ms[0].steps == 3
+        ms[1].enc_step(cs[1].dt, 2)        # two steps alone keep the parity
+        ens.step(1)
+        ens.sync()
+        assert ms[1].steps == 6 and ms[0].steps == 4
+        ms[1].enc_step(cs[1].dt, 1)        # one step alone breaks it
+        with pytest.raises(N.ObError):
+            ens.step(1)
+    for m, c in zip(ms, cs):           # on their own streams again
+        m.enc_step(c.dt, 1)
+        m.sync()
+        assert m.nan_count == 0
+        m.destroy()
