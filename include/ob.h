@@ -110,8 +110,13 @@ int ob_model_maps(ObModel* m, float* out16xN2);
  * even number of steps, to keep the parity). At most 48 members; one ensemble at a time (the members sit in one
  * constant-memory table); destroy the ensemble before its members. */
 typedef struct ObEnsemble ObEnsemble;
+#define OB_ENS_MAX_LANES 2
 #define OB_ENS_NTILES 6   /* tunable tiles: block width of NUT, ADVV1, ADVV2, DIV, PROJ; widest solve transform tile */
 int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsemble** out);
+/* members split into 1 or 2 lanes balanced by cells (default 1): each lane runs the passes as grouped launches on
+ * its own streams, so that one lane's solve overlaps the other's stencils (2 x the launches) */
+int ob_ensemble_set_lanes(ObEnsemble* e, int lanes);
+int ob_ensemble_lanes(ObEnsemble* e);
 int ob_ensemble_step(ObEnsemble* e, int nsteps);                     /* queued on the ensemble's stream */
 int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms);  /* device time of nsteps steps */
 int ob_ensemble_sync(ObEnsemble* e);

@@ -99,6 +99,8 @@ SYMBOLS = {
     "ob_model_set_graphs": (_i, [_vp, _i]),
     "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),
     "ob_ensemble_create": (_i, [C.POINTER(_vp), _fp, _i, C.POINTER(_vp)]),
+    "ob_ensemble_set_lanes": (_i, [_vp, _i]),
+    "ob_ensemble_lanes": (_i, [_vp]),
     "ob_ensemble_step": (_i, [_vp, _i]),
     "ob_ensemble_timed_steps": (_i, [_vp, _i, _fp]),
     "ob_ensemble_sync": (_i, [_vp]),

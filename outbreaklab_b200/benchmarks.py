@@ -171,7 +171,7 @@ def ensemble(args):
                     "n_gpus": world, "host_launch_ms_rank0": local["host_launch_ms"],
                     "device_ms_rank0": local["device_ms"], "nan_guard_count_rank0": local["nan_guard_count"],
                     "grids": [[c.nx, c.ny, c.nz, c.dx] for c in cases], "mode": args.mode})
-        for k in ("tiles", "tiles_source", "tune_ms", "launches_per_step"):
+        for k in ("tiles", "tiles_source", "tune_ms", "lanes", "lane_step_ms", "launches_per_step"):
             if k in local:
                 res[k + "_rank0"] = local[k]
         print(json.dumps(res), flush=True)

@@ -783,21 +783,31 @@ unsigned ob_model_nan_count(ObModel* m) {
 
 void* ob_model_stream(ObModel* m) { return m ? (void*)m->stream : nullptr; }
 
-// ---- ensembles: every member's pass in one launch ----
+// ---- ensembles: every member's pass in one launch per lane ----
+// Members are split into lanes (1 or 2) balanced by cell count; each lane runs the step's passes as grouped launches
+// on its own streams, so that with two lanes one lane's solve (tensor cores) runs beside the other's stencils.
 struct ObEnsemble {
   std::vector<ObModel*> mem;
   std::vector<float> dt;
-  cudaStream_t stream = nullptr;
-  cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
-  MemberC* d_members = nullptr;  // device copy of the member table (the constant-memory upload's source)
+  cudaStream_t stream = nullptr;  // lane 0's main stream; the ensemble's work is ordered on it
+  cudaEvent_t ev_start = nullptr, ev_done = nullptr;
+  struct Lane {
+    std::vector<int> idx;  // members (indices into mem) at table positions base .. base + idx.size() - 1
+    int base = 0;
+    cudaStream_t s = nullptr;  // lane 0: the ensemble's stream
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    TcGroup* solve = nullptr;
+    int blocks[kGroupPasses] = {};
+  } lane[kMaxLanes];
+  int nlanes = 1;
+  MemberC* d_members = nullptr;  // device copy of the member table, in lane order (the constant upload's source)
   std::vector<MemberC> h_members;
   bool members_valid = false;
-  double* d_lsfT = nullptr;
-  GroupTable* d_tables = nullptr;  // one per pass
-  int blocks[kGroupPasses] = {};
+  double* d_lsfT = nullptr;      // per member (mem order)
+  GroupTable* d_tables = nullptr;  // [kMaxLanes][kGroupPasses]
   dim3 shape[kGroupPasses];
-  TcGroup* solve = nullptr;
+  int bn_cap = 256;
   unsigned gen = 0;  // bumped when the tables or the member table change: captured steps are then stale
   struct StepGraph {
     cudaGraphExec_t exec = nullptr;
@@ -819,6 +829,17 @@ static void ens_drop_graphs(ObEnsemble* e) {
   }
 }
 
+static void lane_free(ObEnsemble::Lane& L, bool own_stream) {
+  if (L.solve) tc_group_destroy(L.solve);
+  for (int i = 0; i < 2; i++) {
+    if (L.side[i]) cudaStreamDestroy(L.side[i]);
+    if (L.ev_join[i]) cudaEventDestroy(L.ev_join[i]);
+  }
+  if (L.ev_fork) cudaEventDestroy(L.ev_fork);
+  if (own_stream && L.s) cudaStreamDestroy(L.s);
+  L = ObEnsemble::Lane{};
+}
+
 static void ens_free(ObEnsemble* e) {
   if (!e) return;
   ens_drop_graphs(e);
@@ -827,56 +848,124 @@ static void ens_free(ObEnsemble* e) {
       m->stream = m->own_stream;
       m->ens = nullptr;
     }
-  if (e->solve) tc_group_destroy(e->solve);
+  for (int l = 0; l < kMaxLanes; l++) lane_free(e->lane[l], l > 0);
   for (void* p : {(void*)e->d_members, (void*)e->d_lsfT, (void*)e->d_tables})
     if (p) cudaFree(p);
-  for (int i = 0; i < 2; i++) {
-    if (e->side[i]) cudaStreamDestroy(e->side[i]);
-    if (e->ev_join[i]) cudaEventDestroy(e->ev_join[i]);
-  }
-  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_start) cudaEventDestroy(e->ev_start);
+  if (e->ev_done) cudaEventDestroy(e->ev_done);
   if (e->stream) cudaStreamDestroy(e->stream);
   if (g_ensemble == e) g_ensemble = nullptr;
   delete e;
 }
 
 static int ens_build_tables(ObEnsemble* e) {
-  const int n = int(e->mem.size());
-  std::vector<Grid> grids(n);
-  for (int i = 0; i < n; i++) grids[i] = e->mem[i]->g;
-  std::vector<GroupTable> T(kGroupPasses);
-  for (int p = 0; p < kGroupPasses; p++) e->blocks[p] = group_fill(grids.data(), n, p, e->shape[p], &T[p]);
-  OB_TRY(cuda_status(cudaMemcpy(e->d_tables, T.data(), sizeof(GroupTable) * kGroupPasses, cudaMemcpyHostToDevice), "ensemble tables"));
+  std::vector<GroupTable> T(size_t(kMaxLanes) * kGroupPasses);
+  std::memset(T.data(), 0, T.size() * sizeof(GroupTable));
+  for (int l = 0; l < e->nlanes; l++) {
+    ObEnsemble::Lane& L = e->lane[l];
+    std::vector<Grid> grids;
+    for (int i : L.idx) grids.push_back(e->mem[i]->g);
+    for (int p = 0; p < kGroupPasses; p++)
+      L.blocks[p] = group_fill(grids.data(), int(grids.size()), L.base, p, e->shape[p], &T[size_t(l) * kGroupPasses + p]);
+  }
+  OB_TRY(cuda_status(cudaMemcpy(e->d_tables, T.data(), sizeof(GroupTable) * T.size(), cudaMemcpyHostToDevice), "ensemble tables"));
   e->gen++;
   return OB_OK;
 }
 
-// member table for this step (uniforms for each member's dt); re-uploaded when it changed
+// splits the members into k lanes (largest first onto the lane with fewer cells), with a grouped solve per lane
+static int ens_set_lanes(ObEnsemble* e, int k) {
+  const int n = int(e->mem.size());
+  if (k < 1 || k > kMaxLanes || k > n) { set_error("ensemble: %d lanes for %d members (1..%d)", k, n, kMaxLanes); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble lanes"));
+  for (int l = 1; l < kMaxLanes; l++)
+    if (e->lane[l].s) OB_TRY(cuda_status(cudaStreamSynchronize(e->lane[l].s), "ensemble lanes"));
+  ens_drop_graphs(e);
+  for (int l = 0; l < kMaxLanes; l++) {
+    ObEnsemble::Lane& L = e->lane[l];
+    if (L.solve) { tc_group_destroy(L.solve); L.solve = nullptr; }
+    L.idx.clear();
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const Grid &ga = e->mem[a]->g, &gb = e->mem[b]->g;
+    return long(ga.nx) * ga.ny * ga.nz > long(gb.nx) * gb.ny * gb.nz;
+  });
+  std::vector<long> load(k, 0);
+  for (int i : order) {
+    int best = 0;
+    for (int l = 1; l < k; l++)
+      if (load[l] < load[best]) best = l;
+    e->lane[best].idx.push_back(i);
+    const Grid& g = e->mem[i]->g;
+    load[best] += long(g.nx) * g.ny * g.nz;
+  }
+  int base = 0;
+  for (int l = 0; l < k; l++) {
+    ObEnsemble::Lane& L = e->lane[l];
+    std::sort(L.idx.begin(), L.idx.end());
+    L.base = base;
+    base += int(L.idx.size());
+    if (!L.s) {
+      if (l == 0) L.s = e->stream;
+      else OB_TRY(cuda_status(cudaStreamCreateWithFlags(&L.s, cudaStreamNonBlocking), "ensemble stream"));
+    }
+    for (int i = 0; i < 2; i++) {
+      if (!L.side[i]) OB_TRY(cuda_status(cudaStreamCreateWithFlags(&L.side[i], cudaStreamNonBlocking), "ensemble stream"));
+      if (!L.ev_join[i]) OB_TRY(cuda_status(cudaEventCreateWithFlags(&L.ev_join[i], cudaEventDisableTiming), "ensemble event"));
+    }
+    if (!L.ev_fork) OB_TRY(cuda_status(cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming), "ensemble event"));
+    std::vector<PoissonPlan*> plans;
+    std::vector<float*> phi;
+    std::vector<const float*> rhs;
+    for (int i : L.idx) {
+      plans.push_back(&e->mem[i]->solver);
+      phi.push_back(e->mem[i]->F.phi);
+      rhs.push_back(e->mem[i]->F.rhs);
+    }
+    OB_TRY(tc_group_create(plans.data(), phi.data(), rhs.data(), int(plans.size()), &L.solve));
+    OB_TRY(tc_group_set_cap(L.solve, e->bn_cap));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    tc_group_set_ctas(L.solve, k > 1 ? (nsm + k - 1) / k : 0);
+  }
+  e->nlanes = k;
+  e->members_valid = false;  // table order follows the lanes
+  return ens_build_tables(e);
+}
+
+// member table for this step (uniforms for each member's dt), in lane order; re-uploaded when it changed
 static int ens_prepare(ObEnsemble* e) {
   const int n = int(e->mem.size());
   bool changed = !e->members_valid, lsf_changed = false;
-  for (int i = 0; i < n; i++) {
-    ObModel* m = e->mem[i];
-    if (m->parity != e->parity) {
-      set_error("ensemble: member %d was stepped alone an odd number of times (its step parity differs)", i);
-      return OB_ERR_INVALID;
-    }
-    if (m->lsfT != e->lsfT[i]) {  // stepped alone since the last ensemble step
-      e->lsfT[i] = m->lsfT;
-      lsf_changed = true;
-    }
-    write_uniforms(m, e->dt[i], e->stream);
-    if (micro_mode(m) != kMicroPlain) { set_error("ensemble: member %d uses a learned or recording microphysics mode", i); return OB_ERR_INVALID; }
-    OB_TRY(prepare_micro(m));
-    MemberC c;
-    std::memset(&c, 0, sizeof(c));
-    c.g = m->g;
-    c.U = m->U;
-    c.F = m->F;
-    c.lsfT = e->d_lsfT + i;
-    if (std::memcmp(&c, &e->h_members[i], sizeof(MemberC)) != 0) {
-      e->h_members[i] = c;
-      changed = true;
+  for (int l = 0; l < e->nlanes; l++) {
+    const ObEnsemble::Lane& L = e->lane[l];
+    for (size_t q = 0; q < L.idx.size(); q++) {
+      const int i = L.idx[q];
+      ObModel* m = e->mem[i];
+      if (m->parity != e->parity) {
+        set_error("ensemble: member %d was stepped alone an odd number of times (its step parity differs)", i);
+        return OB_ERR_INVALID;
+      }
+      if (m->lsfT != e->lsfT[i]) {  // stepped alone since the last ensemble step
+        e->lsfT[i] = m->lsfT;
+        lsf_changed = true;
+      }
+      write_uniforms(m, e->dt[i], e->stream);
+      if (micro_mode(m) != kMicroPlain) { set_error("ensemble: member %d uses a learned or recording microphysics mode", i); return OB_ERR_INVALID; }
+      OB_TRY(prepare_micro(m));
+      MemberC c;
+      std::memset(&c, 0, sizeof(c));
+      c.g = m->g;
+      c.U = m->U;
+      c.F = m->F;
+      c.lsfT = e->d_lsfT + i;
+      MemberC& slot = e->h_members[L.base + q];
+      if (std::memcmp(&c, &slot, sizeof(MemberC)) != 0) {
+        slot = c;
+        changed = true;
+      }
     }
   }
   if (lsf_changed) {
@@ -892,27 +981,43 @@ static int ens_prepare(ObEnsemble* e) {
   return OB_OK;
 }
 
+static int lane_enqueue(ObEnsemble* e, int l) {
+  ObEnsemble::Lane& L = e->lane[l];
+  const int par = e->parity;
+  cudaStream_t s = L.s;
+  auto G = [&](int p, cudaStream_t st) { launch_group(l, p, L.blocks[p], e->shape[p], par, st, kMicroPlain); };
+  G(kGroupLSF, s);
+  G(kGroupCI, s);
+  cudaEventRecord(L.ev_fork, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(L.side[i], L.ev_fork, 0);
+  G(kGroupNUT, L.side[0]);
+  cudaEventRecord(L.ev_join[0], L.side[0]);
+  G(kGroupADVQ1, L.side[1]);
+  G(kGroupADVQ2, L.side[1]);
+  cudaEventRecord(L.ev_join[1], L.side[1]);
+  G(kGroupADVV1, s);
+  G(kGroupADVV2, s);
+  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(s, L.ev_join[i], 0);
+  G(kGroupPHYS, s);
+  G(kGroupDIV, s);
+  OB_TRY(tc_group_solve(L.solve, s));
+  G(kGroupPROJ, s);
+  G(kGroupRAIN, s);
+  return OB_OK;
+}
+
 static int ens_enqueue(ObEnsemble* e, cudaStream_t s) {
-  const int n = int(e->mem.size()), par = e->parity;
+  const int n = int(e->mem.size());
   if (group_upload_members(e->d_members, n, e->d_tables, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
-  auto L = [&](int p, cudaStream_t st) { launch_group(p, e->blocks[p], e->shape[p], par, st, kMicroPlain); };
-  L(kGroupLSF, s);
-  L(kGroupCI, s);
-  cudaEventRecord(e->ev_fork, s);
-  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(e->side[i], e->ev_fork, 0);
-  L(kGroupNUT, e->side[0]);
-  cudaEventRecord(e->ev_join[0], e->side[0]);
-  L(kGroupADVQ1, e->side[1]);
-  L(kGroupADVQ2, e->side[1]);
-  cudaEventRecord(e->ev_join[1], e->side[1]);
-  L(kGroupADVV1, s);
-  L(kGroupADVV2, s);
-  for (int i = 0; i < 2; i++) cudaStreamWaitEvent(s, e->ev_join[i], 0);
-  L(kGroupPHYS, s);
-  L(kGroupDIV, s);
-  OB_TRY(tc_group_solve(e->solve, s));
-  L(kGroupPROJ, s);
-  L(kGroupRAIN, s);
+  if (e->nlanes > 1) {
+    cudaEventRecord(e->ev_start, s);
+    for (int l = 1; l < e->nlanes; l++) cudaStreamWaitEvent(e->lane[l].s, e->ev_start, 0);
+  }
+  for (int l = 0; l < e->nlanes; l++) OB_TRY(lane_enqueue(e, l));
+  for (int l = 1; l < e->nlanes; l++) {
+    cudaEventRecord(e->ev_done, e->lane[l].s);
+    cudaStreamWaitEvent(s, e->ev_done, 0);
+  }
   return cuda_status(cudaGetLastError(), "ensemble step launch");
 }
 
@@ -978,31 +1083,19 @@ int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsem
   e->parity = members[0]->parity;
   for (int p = 0; p < kGroupPasses; p++) e->shape[p] = group_default_block(p);
   int rc = cuda_status(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "ensemble stream");
-  for (int i = 0; i < 2 && rc == OB_OK; i++) rc = cuda_status(cudaStreamCreateWithFlags(&e->side[i], cudaStreamNonBlocking), "ensemble stream");
-  if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming), "ensemble event");
-  for (int i = 0; i < 2 && rc == OB_OK; i++) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_join[i], cudaEventDisableTiming), "ensemble event");
+  if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_start, cudaEventDisableTiming), "ensemble event");
+  if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_done, cudaEventDisableTiming), "ensemble event");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_members, sizeof(MemberC) * n), "ensemble members");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_lsfT, sizeof(double) * n), "ensemble members");
-  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_tables, sizeof(GroupTable) * kGroupPasses), "ensemble tables");
-  // every member's queued work (reset, uploads) completes before the ensemble's stream takes over
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_tables, sizeof(GroupTable) * kMaxLanes * kGroupPasses), "ensemble tables");
+  // every member's queued work (reset, uploads) completes before the ensemble's streams take over
   for (int i = 0; i < n && rc == OB_OK; i++) rc = cuda_status(cudaStreamSynchronize(members[i]->stream), "ensemble members");
   if (rc == OB_OK) {
     e->lsfT.resize(n);
     for (int i = 0; i < n; i++) e->lsfT[i] = members[i]->lsfT;
     rc = cuda_status(cudaMemcpy(e->d_lsfT, e->lsfT.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "ensemble members");
   }
-  if (rc == OB_OK) {
-    std::vector<PoissonPlan*> plans(n);
-    std::vector<float*> phi(n);
-    std::vector<const float*> rhs(n);
-    for (int i = 0; i < n; i++) {
-      plans[i] = &members[i]->solver;
-      phi[i] = members[i]->F.phi;
-      rhs[i] = members[i]->F.rhs;
-    }
-    rc = tc_group_create(plans.data(), phi.data(), rhs.data(), n, &e->solve);
-  }
-  if (rc == OB_OK) rc = ens_build_tables(e);
+  if (rc == OB_OK) rc = ens_set_lanes(e, 1);
   if (rc != OB_OK) { ens_free(e); return rc; }
   // while in the ensemble, each member's own work (field access, maps, radar cuts, a step alone) queues behind and
   // ahead of the ensemble's steps on one stream
@@ -1014,6 +1107,13 @@ int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsem
   *out = e;
   return OB_OK;
 }
+
+int ob_ensemble_set_lanes(ObEnsemble* e, int lanes) {
+  if (!e) { set_error("ob_ensemble_set_lanes: null ensemble"); return OB_ERR_INVALID; }
+  return ens_set_lanes(e, lanes);
+}
+
+int ob_ensemble_lanes(ObEnsemble* e) { return e ? e->nlanes : 0; }
 
 int ob_ensemble_step(ObEnsemble* e, int nsteps) {
   if (!e || nsteps < 0) { set_error("ob_ensemble_step: bad arguments"); return OB_ERR_INVALID; }
@@ -1037,10 +1137,15 @@ int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms) {
   return rc;
 }
 
+static int ens_check(ObEnsemble* e) {
+  for (int l = 0; l < e->nlanes; l++) OB_TRY(tc_group_check(e->lane[l].solve));
+  return OB_OK;
+}
+
 int ob_ensemble_sync(ObEnsemble* e) {
   if (!e) { set_error("ob_ensemble_sync: null ensemble"); return OB_ERR_INVALID; }
   OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble step"));
-  return tc_group_check(e->solve);
+  return ens_check(e);
 }
 
 int ob_ensemble_set_graphs(ObEnsemble* e, int on) {
@@ -1051,7 +1156,7 @@ int ob_ensemble_set_graphs(ObEnsemble* e, int on) {
   return OB_OK;
 }
 
-// tiles[0 .. OB_NTILES-1]: block width in x (threads; 128 / width rows) of NUT, ADVV1, ADVV2, DIV, PROJ, then the
+// tiles[0 .. OB_ENS_NTILES-1]: block width in x (threads; 128 / width rows) of NUT, ADVV1, ADVV2, DIV, PROJ, then the
 // widest transform tile of the solve
 static const int kTunedPasses[OB_ENS_NTILES - 1] = {kGroupNUT, kGroupADVV1, kGroupADVV2, kGroupDIV, kGroupPROJ};
 
@@ -1062,23 +1167,26 @@ int ob_ensemble_set_tiles(ObEnsemble* e, const int* tiles) {
       set_error("ob_ensemble_set_tiles: block width %d not in {16, 32, 64, 128}", tiles[t]);
       return OB_ERR_INVALID;
     }
-  OB_TRY(cuda_status(cudaStreamSynchronize(e->stream), "ensemble set tiles"));
+  const int cap = tiles[OB_ENS_NTILES - 1];
+  if (cap < 16 || cap > 256 || cap % 16) { set_error("ob_ensemble_set_tiles: solve tile width %d not in 16..256 (multiple of 16)", cap); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaDeviceSynchronize(), "ensemble set tiles"));
   for (int t = 0; t < OB_ENS_NTILES - 1; t++) e->shape[kTunedPasses[t]] = dim3(tiles[t], 128 / tiles[t], 1);
-  OB_TRY(tc_group_set_cap(e->solve, tiles[OB_ENS_NTILES - 1]));
+  e->bn_cap = cap;
+  for (int l = 0; l < e->nlanes; l++) OB_TRY(tc_group_set_cap(e->lane[l].solve, cap));
   return ens_build_tables(e);
 }
 
 int ob_ensemble_get_tiles(ObEnsemble* e, int* tiles) {
   if (!e || !tiles) { set_error("ob_ensemble_get_tiles: bad arguments"); return OB_ERR_INVALID; }
   for (int t = 0; t < OB_ENS_NTILES - 1; t++) tiles[t] = int(e->shape[kTunedPasses[t]].x);
-  tiles[OB_ENS_NTILES - 1] = tc_group_cap(e->solve);
+  tiles[OB_ENS_NTILES - 1] = e->bn_cap;
   return OB_OK;
 }
 
-// device time of one grouped pass (tile slot t) with the ensemble's current state, averaged over reps launches. Each
-// timed pass only rewrites what the step recomputes from the state (viscosities, advection scratch and next-state
-// slot, the right-hand side, the solve from it, the projected next state), so timing leaves the model state as it
-// was.
+// device time of one grouped pass (tile slot t) with the ensemble's current state, averaged over reps launches (every
+// lane's launch of it, one after another). Each timed pass only rewrites what the step recomputes from the state
+// (viscosities, advection scratch and next-state slot, the right-hand side, the solve from it, the projected next
+// state), so timing leaves the model state as it was.
 int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
   if (!e || !ms || t < 0 || t >= OB_ENS_NTILES || reps < 1) { set_error("ob_ensemble_time_pass: bad arguments"); return OB_ERR_INVALID; }
   OB_TRY(ens_prepare(e));
@@ -1088,12 +1196,15 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
   OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
   OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
   auto run = [&]() -> int {
-    if (t < OB_ENS_NTILES - 1) {
-      const int p = kTunedPasses[t];
-      launch_group(p, e->blocks[p], e->shape[p], e->parity, s, kMicroPlain);
-      return OB_OK;
+    for (int l = 0; l < e->nlanes; l++) {
+      if (t < OB_ENS_NTILES - 1) {
+        const int p = kTunedPasses[t];
+        launch_group(l, p, e->lane[l].blocks[p], e->shape[p], e->parity, s, kMicroPlain);
+      } else {
+        OB_TRY(tc_group_solve(e->lane[l].solve, s));
+      }
     }
-    return tc_group_solve(e->solve, s);
+    return OB_OK;
   };
   int rc = run();  // warm
   cudaEventRecord(a, s);
@@ -1105,7 +1216,7 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *ms = el / float(reps);
-  return rc == OB_OK ? tc_group_check(e->solve) : rc;
+  return rc == OB_OK ? ens_check(e) : rc;
 }
 
 // the project's tile autotuner: each tunable slot is set to each of its candidates in turn and its pass timed (the
@@ -1147,7 +1258,7 @@ void* ob_ensemble_stream(ObEnsemble* e) { return e ? (void*)e->stream : nullptr;
 
 void ob_ensemble_destroy(ObEnsemble* e) {
   if (!e) return;
-  cudaStreamSynchronize(e->stream);
+  cudaDeviceSynchronize();
   ens_free(e);
 }
 

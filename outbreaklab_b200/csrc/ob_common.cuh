@@ -82,6 +82,7 @@ struct Fields {
 
 // ---- grouped launches: one launch of a pass over every member of an ensemble ----
 constexpr int kMaxMembers = 48;
+constexpr int kMaxLanes = 2;  // concurrent groups of members within one ensemble step
 // one member of a grouped launch (held in constant memory by the step kernels)
 struct MemberC {
   Grid g;
@@ -89,9 +90,10 @@ struct MemberC {
   Fields F;
   double* lsfT;  // model time of the member's last LSF pass (device copy of the host's bookkeeping)
 };
-// blocks of a grouped launch: member m owns the linear blocks [start[m], start[m+1]), gx x gy x (rest) of them
+// blocks of a grouped launch over the members base .. base+n-1: member base+m owns the linear blocks
+// [start[m], start[m+1]), gx x gy x (rest) of them
 struct GroupTable {
-  int n;
+  int n, base;
   int start[kMaxMembers + 1];
   int gx[kMaxMembers], gy[kMaxMembers];
 };

@@ -790,6 +790,7 @@ struct TcGroup {
   ResidProb* d_res = nullptr;
   unsigned int* err = nullptr;
   int tiles[5] = {}, tri_blocks = 0, res_blocks = 0;
+  int ctas = 0;  // CTAs of a transform launch (0: one per SM)
 };
 
 // problem tables for the tile-width cap (the B operand's box height is the tile width, so its maps are re-encoded)
@@ -919,11 +920,12 @@ int tc_group_set_cap(TcGroup* G, int bn_cap) {
   return tc_group_build(G);
 }
 int tc_group_cap(const TcGroup* G) { return G->bn_cap; }
+void tc_group_set_ctas(TcGroup* G, int ctas) { G->ctas = ctas > 0 ? ctas : 0; }
 
 template <int MODE>
 static void launch_tc_grp(const TcGroup* G, int t, cudaStream_t s) {
   if (G->tiles[t] < 1) return;
-  k_dst_tc_grp<MODE><<<std::min(G->tiles[t], num_sms()), kThreads, SMEM_BYTES, s>>>(G->d_probs + size_t(t) * G->n,
+  k_dst_tc_grp<MODE><<<std::min(G->tiles[t], G->ctas ? G->ctas : num_sms()), kThreads, SMEM_BYTES, s>>>(G->d_probs + size_t(t) * G->n,
                                                                                      G->d_start + size_t(t) * (G->n + 1), G->n, G->err);
 }
 

@@ -49,6 +49,7 @@ struct TcGroup;
 int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* const* rhs, int n, TcGroup** out);
 int tc_group_set_cap(TcGroup* G, int bn_cap);  // widest transform tile (16..256, multiple of 16)
 int tc_group_cap(const TcGroup* G);
+void tc_group_set_ctas(TcGroup* G, int ctas);  // CTAs per transform launch (0: one per SM)
 int tc_group_solve(TcGroup* G, cudaStream_t s);
 int tc_group_check(TcGroup* G);
 void tc_group_destroy(TcGroup* G);

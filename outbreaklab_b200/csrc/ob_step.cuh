@@ -32,10 +32,11 @@ enum { kGroupStag = 0, kGroupCell = 1, kGroup2D = 2 };
 int group_kind(int pass);
 dim3 group_default_block(int pass);
 bool group_block_fixed(int pass);
-int group_fill(const Grid* grids, int n, int pass, dim3 block, GroupTable* T);  // host: returns the launch's blocks
-// copies the member table and the per-pass block tables (kGroupPasses of them) into constant memory on stream s
+// host: the table of one lane's launch of a pass over members base .. base+n-1 (grids of those); returns its blocks
+int group_fill(const Grid* grids, int n, int base, int pass, dim3 block, GroupTable* T);
+// copies the member table and the block tables (kMaxLanes x kGroupPasses of them) into constant memory on stream s
 int group_upload_members(const MemberC* d_src, int n, const GroupTable* d_tables, cudaStream_t s);
-void launch_group(int pass, int blocks, dim3 block, int par, cudaStream_t s, int micro_mode = 0);
+void launch_group(int lane, int pass, int blocks, dim3 block, int par, cudaStream_t s, int micro_mode = 0);
 void launch_tor_candidates(const Grid& g, float dx, const float4* maps, float zmin, float* out, int cap, unsigned* count, cudaStream_t s);
 void launch_pack(const Grid& g, const Ptr8& src, int nch, int X, int Y, int Z, float* dst, cudaStream_t s);
 void launch_unpack(const Grid& g, const Ptr8& dst, int nch, int X, int Y, int Z, const float* src, cudaStream_t s);

@@ -171,9 +171,15 @@ class TileCache:
             return [int(x) for x in e["tiles"]]
         return None
 
-    def put(self, sig, tiles, ms):
+    def get_lanes(self, sig):
+        e = self.load().get(sig)
+        return int(e["lanes"]) if e and "lanes" in e else None
+
+    def put(self, sig, tiles, ms, lanes=None):
         d = self.load()
         d[sig] = {"tiles": [int(x) for x in tiles], "ms": [float(x) for x in ms]}
+        if lanes is not None:
+            d[sig]["lanes"] = int(lanes)
         os.makedirs(os.path.dirname(self.path) or ".", exist_ok=True)
         tmp = self.path + ".part"
         with open(tmp, "w") as f:
@@ -209,6 +215,13 @@ class Ensemble:
     def set_graphs(self, on):
         self.N.check(self.N.lib().ob_ensemble_set_graphs(self.h, int(bool(on))))
 
+    def set_lanes(self, k):
+        self.N.check(self.N.lib().ob_ensemble_set_lanes(self.h, int(k)))
+
+    @property
+    def lanes(self):
+        return int(self.N.lib().ob_ensemble_lanes(self.h))
+
     def tiles(self):
         t = (C.c_int * self.N.ENS_NTILES)()
         self.N.check(self.N.lib().ob_ensemble_get_tiles(self.h, t))
@@ -239,10 +252,13 @@ class Ensemble:
             self.h = None
 
 
-def run_grouped(cases, steps: int = 50, warmup: int = 3, tune: bool = True, cache: TileCache = None, reps: int = 5):
-    """Steps every member `steps` times as one ObEnsemble. Tiles come from the cache for this member set, else from
-    the autotuner (then cached). Returns the metrics of this process: cell-steps per second over the device time of
-    the timed steps, the ensemble step's latency percentiles (per-step CUDA events) and the tiles used."""
+def run_grouped(cases, steps: int = 50, warmup: int = 3, tune: bool = True, cache: TileCache = None, reps: int = 5,
+                lanes=None):
+    """Steps every member `steps` times as one ObEnsemble. Tiles and the lane count come from the cache for this
+    member set, else from the autotuner (tiles) and from timing a few warm-up steps with one and with two lanes (the
+    lane count changes no result, only which launches overlap); both are then cached. Returns the metrics of this
+    process: cell-steps per second over the device time of the timed steps, the ensemble step's latency percentiles
+    (per-step CUDA events), the tiles and lanes used."""
     import torch
     from . import _native as N, model as M
     models = []
@@ -253,16 +269,18 @@ def run_grouped(cases, steps: int = 50, warmup: int = 3, tune: bool = True, cach
         models.append(m)
     ens = Ensemble(models, [c.dt for c in cases])
     try:
-        return _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps)
+        return _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes)
     finally:
         ens.destroy()
         for m in models:
             m.destroy()
 
 
-def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps):
+def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes):
     import torch
-    tiles_src, tune_ms = "default", None
+    tiles_src, tune_ms, lane_ms = "default", None, None
+    if lanes is not None:
+        ens.set_lanes(lanes)
     if tune:
         cache = cache or TileCache()
         sig = TileCache.signature(cases, torch.cuda.get_device_name(0) if torch.cuda.is_available() else "")
@@ -270,11 +288,20 @@ def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps):
         if t is not None:
             ens.set_tiles(t)
             tiles_src = "cache"
+            if lanes is None and cache.get_lanes(sig):
+                ens.set_lanes(min(cache.get_lanes(sig), len(models)))
         else:
             ens.step(1)           # a state with motion in it for the timing
             ens.sync()
             t, tune_ms = ens.tune(reps)
-            cache.put(sig, t, tune_ms)
+            if lanes is None and len(models) > 1:
+                lane_ms = {}
+                for k in (1, 2):
+                    ens.set_lanes(k)
+                    ens.step(2)   # capture
+                    lane_ms[k] = ens.timed_steps(4) / 4
+                ens.set_lanes(min(lane_ms, key=lane_ms.get))
+            cache.put(sig, t, tune_ms, ens.lanes)
             tiles_src = "autotuned"
     ens.step(warmup)
     ens.sync()
@@ -294,6 +321,6 @@ def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps):
            "cell_steps_per_s": cells * steps / (span_ms / 1000.0),
            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
            "latency_ms_all": lat.tolist(), "nan_guard_count": int(sum(m.nan_count for m in models)),
-           "tiles": ens.tiles(), "tiles_source": tiles_src, "tune_ms": tune_ms,
-           "launches_per_step": 11 + (11 if models[0].solver == 2 else 5)}
+           "tiles": ens.tiles(), "tiles_source": tiles_src, "tune_ms": tune_ms, "lanes": ens.lanes, "lane_step_ms": lane_ms,
+           "launches_per_step": ens.lanes * (11 + (11 if models[0].solver == 2 else 5))}
     return out

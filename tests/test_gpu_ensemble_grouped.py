@@ -129,6 +129,25 @@ def test_graphs_off_equals_on(grouped):
         m.destroy()
 
 
+def test_two_lanes_equal_one(grouped):
+    """Two lanes (members split by cells, each lane's passes on its own streams) run the same kernels per member."""
+    cs, ref, _ = grouped
+    ms = setup(cs)
+    with Ens(ms, cs) as ens:
+        assert ens.lanes == 1
+        ens.set_lanes(2)
+        assert ens.lanes == 2
+        ens.step(12)
+        ens.set_lanes(1)   # and back, mid-run
+        ens.step(13)
+        ens.sync()
+        with pytest.raises(N.ObError):
+            ens.set_lanes(3)
+    assert_same(ref, ms)
+    for m in ms:
+        m.destroy()
+
+
 def test_hand_set_tiles(grouped):
     cs, ref, _ = grouped
     ms = setup(cs)
