@@ -798,14 +798,14 @@ struct ObEnsemble {
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     TcGroup* solve = nullptr;
-    int blocks[kGroupPasses] = {};
+    uint2* d_map[kGroupPasses] = {};  // block maps of the lane's grouped launches
+    int nxy[kGroupPasses] = {}, Z[kGroupPasses] = {};
   } lane[kMaxLanes];
   int nlanes = 1;
   MemberC* d_members = nullptr;  // device copy of the member table, in lane order (the constant upload's source)
   std::vector<MemberC> h_members;
   bool members_valid = false;
   double* d_lsfT = nullptr;      // per member (mem order)
-  GroupTable* d_tables = nullptr;  // [kMaxLanes][kGroupPasses]
   dim3 shape[kGroupPasses];
   int bn_cap = 256;
   unsigned gen = 0;  // bumped when the tables or the member table change: captured steps are then stale
@@ -831,6 +831,8 @@ static void ens_drop_graphs(ObEnsemble* e) {
 
 static void lane_free(ObEnsemble::Lane& L, bool own_stream) {
   if (L.solve) tc_group_destroy(L.solve);
+  for (uint2* p : L.d_map)
+    if (p) cudaFree(p);
   for (int i = 0; i < 2; i++) {
     if (L.side[i]) cudaStreamDestroy(L.side[i]);
     if (L.ev_join[i]) cudaEventDestroy(L.ev_join[i]);
@@ -849,7 +851,7 @@ static void ens_free(ObEnsemble* e) {
       m->ens = nullptr;
     }
   for (int l = 0; l < kMaxLanes; l++) lane_free(e->lane[l], l > 0);
-  for (void* p : {(void*)e->d_members, (void*)e->d_lsfT, (void*)e->d_tables})
+  for (void* p : {(void*)e->d_members, (void*)e->d_lsfT})
     if (p) cudaFree(p);
   if (e->ev_start) cudaEventDestroy(e->ev_start);
   if (e->ev_done) cudaEventDestroy(e->ev_done);
@@ -859,16 +861,25 @@ static void ens_free(ObEnsemble* e) {
 }
 
 static int ens_build_tables(ObEnsemble* e) {
-  std::vector<GroupTable> T(size_t(kMaxLanes) * kGroupPasses);
-  std::memset(T.data(), 0, T.size() * sizeof(GroupTable));
   for (int l = 0; l < e->nlanes; l++) {
     ObEnsemble::Lane& L = e->lane[l];
     std::vector<Grid> grids;
-    for (int i : L.idx) grids.push_back(e->mem[i]->g);
-    for (int p = 0; p < kGroupPasses; p++)
-      L.blocks[p] = group_fill(grids.data(), int(grids.size()), L.base, p, e->shape[p], &T[size_t(l) * kGroupPasses + p]);
+    std::vector<int> pos;
+    for (size_t q = 0; q < L.idx.size(); q++) {
+      grids.push_back(e->mem[L.idx[q]]->g);
+      pos.push_back(L.base + int(q));
+    }
+    std::vector<uint2> map;
+    for (int p = 0; p < kGroupPasses; p++) {
+      const int Z = group_map(grids.data(), pos.data(), int(grids.size()), p, e->shape[p], map);
+      if (Z < 1) { set_error("ensemble: members must share nz"); return OB_ERR_INVALID; }
+      if (L.d_map[p]) { cudaFree(L.d_map[p]); L.d_map[p] = nullptr; }
+      OB_TRY(cuda_status(cudaMalloc(&L.d_map[p], map.size() * sizeof(uint2)), "ensemble block maps"));
+      OB_TRY(cuda_status(cudaMemcpy(L.d_map[p], map.data(), map.size() * sizeof(uint2), cudaMemcpyHostToDevice), "ensemble block maps"));
+      L.nxy[p] = int(map.size());
+      L.Z[p] = Z;
+    }
   }
-  OB_TRY(cuda_status(cudaMemcpy(e->d_tables, T.data(), sizeof(GroupTable) * T.size(), cudaMemcpyHostToDevice), "ensemble tables"));
   e->gen++;
   return OB_OK;
 }
@@ -985,7 +996,7 @@ static int lane_enqueue(ObEnsemble* e, int l) {
   ObEnsemble::Lane& L = e->lane[l];
   const int par = e->parity;
   cudaStream_t s = L.s;
-  auto G = [&](int p, cudaStream_t st) { launch_group(l, p, L.blocks[p], e->shape[p], par, st, kMicroPlain); };
+  auto G = [&](int p, cudaStream_t st) { launch_group(p, L.d_map[p], L.nxy[p], L.Z[p], e->shape[p], par, st, kMicroPlain); };
   G(kGroupLSF, s);
   G(kGroupCI, s);
   cudaEventRecord(L.ev_fork, s);
@@ -1008,7 +1019,7 @@ static int lane_enqueue(ObEnsemble* e, int l) {
 
 static int ens_enqueue(ObEnsemble* e, cudaStream_t s) {
   const int n = int(e->mem.size());
-  if (group_upload_members(e->d_members, n, e->d_tables, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
+  if (group_upload_members(e->d_members, n, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
   if (e->nlanes > 1) {
     cudaEventRecord(e->ev_start, s);
     for (int l = 1; l < e->nlanes; l++) cudaStreamWaitEvent(e->lane[l].s, e->ev_start, 0);
@@ -1087,7 +1098,6 @@ int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsem
   if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_done, cudaEventDisableTiming), "ensemble event");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_members, sizeof(MemberC) * n), "ensemble members");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_lsfT, sizeof(double) * n), "ensemble members");
-  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_tables, sizeof(GroupTable) * kMaxLanes * kGroupPasses), "ensemble tables");
   // every member's queued work (reset, uploads) completes before the ensemble's streams take over
   for (int i = 0; i < n && rc == OB_OK; i++) rc = cuda_status(cudaStreamSynchronize(members[i]->stream), "ensemble members");
   if (rc == OB_OK) {
@@ -1191,7 +1201,7 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
   if (!e || !ms || t < 0 || t >= OB_ENS_NTILES || reps < 1) { set_error("ob_ensemble_time_pass: bad arguments"); return OB_ERR_INVALID; }
   OB_TRY(ens_prepare(e));
   cudaStream_t s = e->stream;
-  if (group_upload_members(e->d_members, int(e->mem.size()), e->d_tables, s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
+  if (group_upload_members(e->d_members, int(e->mem.size()), s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
   cudaEvent_t a, b;
   OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
   OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
@@ -1199,7 +1209,8 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
     for (int l = 0; l < e->nlanes; l++) {
       if (t < OB_ENS_NTILES - 1) {
         const int p = kTunedPasses[t];
-        launch_group(l, p, e->lane[l].blocks[p], e->shape[p], e->parity, s, kMicroPlain);
+        const ObEnsemble::Lane& L = e->lane[l];
+        launch_group(p, L.d_map[p], L.nxy[p], L.Z[p], e->shape[p], e->parity, s, kMicroPlain);
       } else {
         OB_TRY(tc_group_solve(e->lane[l].solve, s));
       }

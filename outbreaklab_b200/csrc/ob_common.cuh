@@ -90,13 +90,6 @@ struct MemberC {
   Fields F;
   double* lsfT;  // model time of the member's last LSF pass (device copy of the host's bookkeeping)
 };
-// blocks of a grouped launch over the members base .. base+n-1: member base+m owns the linear blocks
-// [start[m], start[m+1]), gx x gy x (rest) of them
-struct GroupTable {
-  int n, base;
-  int start[kMaxMembers + 1];
-  int gx[kMaxMembers], gy[kMaxMembers];
-};
 constexpr float T0K = 273.15f;
 constexpr double CPDd = 1005.7, RVCd = 461.5, LVCd = 2.501e6, LFCd = 3.337e5, LSCd = 2.834e6;
 

@@ -353,7 +353,7 @@ __global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __res
   resid_body(nx, ny, nz, idx2, zop, rhs, phi, hi, lo, ld, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 struct ResidProb {
-  int nx, ny, nz, ld, gx;
+  int nx, ny, nz, ld;
   double idx2;
   const float4* zop;
   const float* rhs;
@@ -361,17 +361,11 @@ struct ResidProb {
   __nv_bfloat16* hi;
   __nv_bfloat16* lo;
 };
-__global__ void k_resid_grp(const ResidProb* __restrict__ probs, const int* __restrict__ start, int n) {
-  const int b = blockIdx.x;
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(start + mid) <= b) lo = mid;
-    else hi = mid - 1;
-  }
-  const ResidProb& P = probs[lo];
-  const int r = b - __ldg(start + lo);
-  resid_body(P.nx, P.ny, P.nz, P.idx2, P.zop, P.rhs, P.phi, P.hi, P.lo, P.ld, r % P.gx, (r / P.gx) % P.ny, r / (P.gx * P.ny));
+// grid (x-y blocks of all members, 1, levels): map[blockIdx.x] = (member, bx | by << 16)
+__global__ void k_resid_grp(const ResidProb* __restrict__ probs, const uint2* __restrict__ map) {
+  const uint2 e = __ldg(map + blockIdx.x);
+  const ResidProb& P = probs[e.x];
+  resid_body(P.nx, P.ny, P.nz, P.idx2, P.zop, P.rhs, P.phi, P.hi, P.lo, P.ld, int(e.y & 0xffffu), int(e.y >> 16u), int(blockIdx.z));
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -788,6 +782,7 @@ struct TcGroup {
   int* d_start = nullptr;       // [5][n + 1] tile starts, [n + 1] tridiagonal block starts, [n + 1] residual block starts
   TriProb* d_tri = nullptr;
   ResidProb* d_res = nullptr;
+  uint2* d_res_map = nullptr;  // block map of the residual launch
   unsigned int* err = nullptr;
   int tiles[5] = {}, tri_blocks = 0, res_blocks = 0;
   int ctas = 0;  // CTAs of a transform launch (0: one per SM)
@@ -801,6 +796,7 @@ static int tc_group_build(TcGroup* G) {
   std::vector<int> start(size_t(NT + 2) * (n + 1), 0);
   std::vector<TriProb> tri(n);
   std::vector<ResidProb> res(n);
+  std::vector<uint2> res_map;
   const int tm = G->nz == 16 ? tri_tm<16>() : G->nz == 40 ? tri_tm<40>() : tri_tm<80>();
   for (int i = 0; i < n; i++) {
     const PoissonPlan* P = G->plans[i];
@@ -834,8 +830,10 @@ static int tc_group_build(TcGroup* G) {
     tri[i] = TriProb{nx, ny, int(T->ldy), gx, P->lam, P->zop, T->low, T->t2, T->sy_hi, T->sy_lo};
     start[size_t(NT) * (n + 1) + i + 1] = start[size_t(NT) * (n + 1) + i] + gx * gy;
     const int rgx = (nx + 127) / 128;
-    res[i] = ResidProb{nx, ny, nz, int(T->ldx), rgx, 1.0 / (P->dx * P->dx), P->zop, G->rhs[i], G->phi[i], T->rr_hi, T->rr_lo};
-    start[size_t(NT + 1) * (n + 1) + i + 1] = start[size_t(NT + 1) * (n + 1) + i] + rgx * ny * nz;
+    res[i] = ResidProb{nx, ny, nz, int(T->ldx), 1.0 / (P->dx * P->dx), P->zop, G->rhs[i], G->phi[i], T->rr_hi, T->rr_lo};
+    for (int by = 0; by < ny; by++)
+      for (int bx = 0; bx < rgx; bx++) res_map.push_back(make_uint2(unsigned(i), unsigned(bx) | (unsigned(by) << 16)));
+    start[size_t(NT + 1) * (n + 1) + i + 1] = start[size_t(NT + 1) * (n + 1) + i] + rgx * ny;
   }
   for (int t = 0; t < NT; t++) G->tiles[t] = start[size_t(t) * (n + 1) + n];
   G->tri_blocks = start[size_t(NT) * (n + 1) + n];
@@ -843,7 +841,8 @@ static int tc_group_build(TcGroup* G) {
   const bool ok = cudaMemcpy(G->d_probs, probs.data(), probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_tri, tri.data(), tri.size() * sizeof(TriProb), cudaMemcpyHostToDevice) == cudaSuccess &&
-                  cudaMemcpy(G->d_res, res.data(), res.size() * sizeof(ResidProb), cudaMemcpyHostToDevice) == cudaSuccess;
+                  cudaMemcpy(G->d_res, res.data(), res.size() * sizeof(ResidProb), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(G->d_res_map, res_map.data(), res_map.size() * sizeof(uint2), cudaMemcpyHostToDevice) == cudaSuccess;
   if (!ok) {
     set_error("ensemble solve: problem table upload failed");
     return OB_ERR_DEVICE;
@@ -853,9 +852,15 @@ static int tc_group_build(TcGroup* G) {
 
 void tc_group_destroy(TcGroup* G) {
   if (!G) return;
-  for (void* p : {(void*)G->d_probs, (void*)G->d_start, (void*)G->d_tri, (void*)G->d_res, (void*)G->err})
+  for (void* p : {(void*)G->d_probs, (void*)G->d_start, (void*)G->d_tri, (void*)G->d_res, (void*)G->d_res_map, (void*)G->err})
     if (p) cudaFree(p);
   delete G;
+}
+
+static size_t res_map_blocks(PoissonPlan* const* plans, int n) {
+  size_t b = 0;
+  for (int i = 0; i < n; i++) b += size_t((plans[i]->nx + 127) / 128) * plans[i]->ny;
+  return b;
 }
 
 int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* const* rhs, int n, TcGroup** out) {
@@ -895,6 +900,7 @@ int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* c
                   cudaMalloc(&G->d_start, size_t(7) * (n + 1) * sizeof(int)) == cudaSuccess &&
                   cudaMalloc(&G->d_tri, size_t(n) * sizeof(TriProb)) == cudaSuccess &&
                   cudaMalloc(&G->d_res, size_t(n) * sizeof(ResidProb)) == cudaSuccess && cudaMalloc(&G->err, 16) == cudaSuccess &&
+                  cudaMalloc(&G->d_res_map, res_map_blocks(plans, n) * sizeof(uint2)) == cudaSuccess &&
                   cudaMemset(G->err, 0, 16) == cudaSuccess;
   if (!ok) {
     set_error("ensemble solve: out of device memory");
@@ -947,7 +953,7 @@ static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s) {
 int tc_group_solve(TcGroup* G, cudaStream_t s) {
   tc_group_pass(G, false, s);
   if (G->precision == 2) {
-    k_resid_grp<<<G->res_blocks, 128, 0, s>>>(G->d_res, G->d_start + size_t(6) * (G->n + 1), G->n);
+    k_resid_grp<<<dim3(G->res_blocks, 1, G->nz), 128, 0, s>>>(G->d_res, G->d_res_map);
     tc_group_pass(G, true, s);
   }
   const cudaError_t e = cudaGetLastError();

@@ -5,6 +5,7 @@
 // read, neighbours served from L1/L2. Semi-Lagrangian sampling is a software trilinear filter in fp32 (exact
 // weights; WebGPU's hardware filter uses low-precision fixed-point weights, which are not reproduced).
 #include <algorithm>
+#include <vector>
 
 #include "ob_common.cuh"
 #include "ob_micro.cuh"
@@ -12,28 +13,14 @@
 
 namespace ob {
 
-// members of the grouped launches (ensemble steps) and each pass's block table, uploaded by group_upload_members.
-// Both sit in constant memory and the block's member is found from blockIdx and constant loads alone, so the member
-// index is warp-uniform to the compiler and the member's uniforms are read through the uniform datapath.
+// members of the grouped launches (ensemble steps), uploaded by group_upload_members. A grouped launch's grid is
+// (x-y blocks of all members, 1, levels): the members share nz, and blockIdx.x indexes a map that gives each x-y
+// block its member and its block coordinates (one 8-byte load per thread, the same for the whole block).
 __constant__ MemberC c_members[kMaxMembers];
-__constant__ GroupTable c_tables[kMaxLanes][kGroupPasses];
-__device__ __forceinline__ void group_block_c(const GroupTable& T, int& mem, int& bx, int& by, int& bz) {
-  const int b = blockIdx.x;
-  int lo = 0, hi = T.n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (T.start[mid] <= b) lo = mid;
-    else hi = mid - 1;
-  }
-  mem = T.base + lo;
-  const int r = b - T.start[lo], gx = T.gx[lo], gy = T.gy[lo];
-  bx = r % gx;
-  by = (r / gx) % gy;
-  bz = r / (gx * gy);
-}
-#define OB_GROUP_RESOLVE(PASS) \
-  int mem, gbx, gby, gbz;      \
-  group_block_c(c_tables[lane][PASS], mem, gbx, gby, gbz);
+#define OB_GROUP_RESOLVE                                                               \
+  const uint2 gm__ = __ldg(map + blockIdx.x);                                         \
+  const int mem = int(gm__.x), gbx = int(gm__.y & 0xffffu), gby = int(gm__.y >> 16u), \
+            gbz = int(blockIdx.z);
 
 // block coordinates: blockIdx for a launch over one model, or the (member, block) a grouped launch resolved
 #define OB_BLOCKS_DIRECT const int BX = blockIdx.x, BY = blockIdx.y, BZ = blockIdx.z;
@@ -183,8 +170,8 @@ __device__ __forceinline__ void lsf_body(const Grid& g, const Uni& U, const Fiel
   }
 }
 __global__ void k_lsf(Grid g, Uni U, Fields F) { lsf_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_lsf_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupLSF)
+__global__ void k_lsf_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   {
     const double t = *c_members[mem].F.clock, t0 = *c_members[mem].lsfT;
     if (!(t - t0 >= 60.0 || t == 0.0)) return;
@@ -220,8 +207,8 @@ __device__ __forceinline__ void ci_body(const Grid& g, const Uni& U, const Field
   F.ciMap[j * g.nx + i] = best;
 }
 __global__ void k_ci(Grid g, Uni U, Fields F) { ci_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_ci_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupCI)
+__global__ void k_ci_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   if (gbx == 0 && gby == 0 && gbz == 0 && threadIdx.x == 0 && threadIdx.y == 0) {  // after the LSF pass of this step
     const double t = *c_members[mem].F.clock;
     double* t0 = c_members[mem].lsfT;
@@ -302,8 +289,8 @@ __device__ __forceinline__ void nut_body(const Grid& g, const Uni& U, const Fiel
   F.aux[1][o] = fminf(lv * lv * sS * fst, 0.15f * dz * dz / dtc);
 }
 __global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) { nut_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 16) k_nut_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupNUT)
+__global__ void __launch_bounds__(128, 16) k_nut_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   nut_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -369,8 +356,8 @@ __device__ __forceinline__ void advv1_body(const Grid& g, const Uni& U, const Fi
   F.Vt[3][o] = sampleVch(F.V[par][3], g, 3, x, y, z);
 }
 __global__ void k_advv1(Grid g, Uni U, Fields F, int par) { advv1_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_advv1_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupADVV1)
+__global__ void k_advv1_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   advv1_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -413,8 +400,8 @@ __device__ __forceinline__ void advv2_body(const Grid& g, const Uni& U, const Fi
   }
 }
 __global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) { advv2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 12) k_advv2_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupADVV2)
+__global__ void __launch_bounds__(128, 12) k_advv2_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   advv2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -574,8 +561,8 @@ __device__ __forceinline__ void advq1_body(const Grid& g, const Uni& U, const Fi
   }
 }
 __global__ void __launch_bounds__(128, 12) k_advq1(Grid g, Uni U, Fields F, int par) { advq1_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 10) k_advq1_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupADVQ1)
+__global__ void __launch_bounds__(128, 12) k_advq1_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   advq1_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -661,8 +648,8 @@ __device__ __forceinline__ void advq2_body(const Grid& g, const Uni& U, const Fi
   if (threadIdx.x == 0 && threadIdx.y == 0) F.zeroQ1[brick] = active ? 0u : 1u;
 }
 __global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int par) { advq2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 8) k_advq2_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupADVQ2)
+__global__ void __launch_bounds__(128, 10) k_advq2_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   advq2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -974,8 +961,8 @@ __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fie
 template <int MM>
 __global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
 template <int MM>
-__global__ void __launch_bounds__(128, 8) k_phys_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupPHYS)
+__global__ void __launch_bounds__(128, 10) k_phys_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   phys_body<MM>(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -1003,8 +990,8 @@ __device__ __forceinline__ void div_body(const Grid& g, const Uni& U, const Fiel
   if (F.rhs) F.rhs[g.pidx(ci, cj, ck)] = r;  // fp32 solve, or the residual of the refined solve
 }
 __global__ void k_div(Grid g, Uni U, Fields F, int par) { div_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_div_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupDIV)
+__global__ void k_div_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   div_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -1030,8 +1017,8 @@ __device__ __forceinline__ void proj_body(const Grid& g, const Uni& U, const Fie
   F.V[1 - par][3][o] = __ldg(F.V[par][3] + o);
 }
 __global__ void k_proj(Grid g, Uni U, Fields F, int par) { proj_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_proj_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupPROJ)
+__global__ void k_proj_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   proj_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -1049,8 +1036,8 @@ __device__ __forceinline__ void rain_body(const Grid& g, const Uni& U, const Fie
   if (i == 0 && j == 0) *F.clock += double(U.step.x);  // the step's last pass advances the model time
 }
 __global__ void k_rain(Grid g, Uni U, Fields F) { rain_body(g, U, F, 0, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void k_rain_grp(int lane, int par) {
-  OB_GROUP_RESOLVE(kGroupRAIN)
+__global__ void k_rain_grp(const uint2* __restrict__ map, int par) {
+  OB_GROUP_RESOLVE
   rain_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
 
@@ -1249,49 +1236,50 @@ bool group_block_fixed(int pass) {
   return pass == kGroupADVQ1 || pass == kGroupADVQ2 || pass == kGroupPHYS || group_kind(pass) == kGroup2D;
 }
 
-int group_fill(const Grid* grids, int n, int base, int pass, dim3 block, GroupTable* T) {
+int group_map(const Grid* grids, const int* pos, int n, int pass, dim3 block, std::vector<uint2>& map) {
   if (n < 1 || n > kMaxMembers) return -1;
   const int kind = group_kind(pass);
-  T->n = n;
-  T->base = base;
-  T->start[0] = 0;
+  map.clear();
+  int Z = -1;
   for (int i = 0; i < n; i++) {
     const Grid& g = grids[i];
-    int X = g.nx, Y = g.ny, Z = g.nz;
-    if (kind == kGroupStag) { X++; Y++; Z++; }
-    if (kind == kGroup2D) Z = 1;
+    int X = g.nx, Y = g.ny, z = g.nz;
+    if (kind == kGroupStag) { X++; Y++; z++; }
+    if (kind == kGroup2D) z = 1;
+    if (Z >= 0 && z != Z) return -1;  // the members share nz
+    Z = z;
     const int gx = (X + block.x - 1) / block.x, gy = (Y + block.y - 1) / block.y;
-    T->gx[i] = gx;
-    T->gy[i] = gy;
-    T->start[i + 1] = T->start[i] + gx * gy * Z;
+    if (gx > 65535 || gy > 65535) return -1;
+    for (int by = 0; by < gy; by++)
+      for (int bx = 0; bx < gx; bx++) map.push_back(make_uint2(unsigned(pos[i]), unsigned(bx) | (unsigned(by) << 16)));
   }
-  return T->start[n];
+  return Z;
 }
 
-int group_upload_members(const MemberC* d_src, int n, const GroupTable* d_tables, cudaStream_t s) {
+int group_upload_members(const MemberC* d_src, int n, cudaStream_t s) {
   if (n < 1 || n > kMaxMembers) return -1;
-  if (cudaMemcpyToSymbolAsync(c_members, d_src, sizeof(MemberC) * n, 0, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return -1;
-  return cudaMemcpyToSymbolAsync(c_tables, d_tables, sizeof(GroupTable) * kMaxLanes * kGroupPasses, 0, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -1;
+  return cudaMemcpyToSymbolAsync(c_members, d_src, sizeof(MemberC) * n, 0, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -1;
 }
 
-void launch_group(int lane, int pass, int blocks, dim3 block, int par, cudaStream_t s, int micro_mode) {
-  if (blocks < 1) return;
+void launch_group(int pass, const uint2* map, int nxy, int Z, dim3 block, int par, cudaStream_t s, int micro_mode) {
+  if (nxy < 1 || Z < 1) return;
+  const dim3 grid(nxy, 1, Z);
   switch (pass) {
-    case kGroupLSF: k_lsf_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupCI: k_ci_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupNUT: k_nut_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupADVV1: k_advv1_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupADVV2: k_advv2_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupADVQ1: k_advq1_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupADVQ2: k_advq2_grp<<<blocks, block, 0, s>>>(lane, par); break;
+    case kGroupLSF: k_lsf_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupCI: k_ci_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupNUT: k_nut_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupADVV1: k_advv1_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupADVV2: k_advv2_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupADVQ1: k_advq1_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupADVQ2: k_advq2_grp<<<grid, block, 0, s>>>(map, par); break;
     case kGroupPHYS:
-      if (micro_mode == kMicroRecord) k_phys_grp<kMicroRecord><<<blocks, block, 0, s>>>(lane, par);
-      else if (micro_mode == kMicroSurrogate) k_phys_grp<kMicroSurrogate><<<blocks, block, 0, s>>>(lane, par);
-      else k_phys_grp<kMicroPlain><<<blocks, block, 0, s>>>(lane, par);
+      if (micro_mode == kMicroRecord) k_phys_grp<kMicroRecord><<<grid, block, 0, s>>>(map, par);
+      else if (micro_mode == kMicroSurrogate) k_phys_grp<kMicroSurrogate><<<grid, block, 0, s>>>(map, par);
+      else k_phys_grp<kMicroPlain><<<grid, block, 0, s>>>(map, par);
       break;
-    case kGroupDIV: k_div_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupPROJ: k_proj_grp<<<blocks, block, 0, s>>>(lane, par); break;
-    case kGroupRAIN: k_rain_grp<<<blocks, block, 0, s>>>(lane, par); break;
+    case kGroupDIV: k_div_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupPROJ: k_proj_grp<<<grid, block, 0, s>>>(map, par); break;
+    case kGroupRAIN: k_rain_grp<<<grid, block, 0, s>>>(map, par); break;
     default: break;
   }
 }
