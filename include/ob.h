@@ -51,6 +51,31 @@ typedef struct ObParams {
   float mcFloor, scheme, evapT, dtScale; /* scheme: 0 Lin-type, 1 Thompson-style; dtScale (app.js:1666) */
 } ObParams;
 
+/* Hurricane mode (RegionalModel.setSurface's hur argument, model.js:1296-1303, with the values app.js:1631 passes
+ * and the defaults writeUniforms applies, model.js:1402-1420): a warm sea under the domain. */
+typedef struct ObHurricane {
+  float ck;            /* bulk exchange coefficient of heat and moisture at 10 m */
+  float landMoist;     /* moisture availability of land (0..1) */
+  float sfcP;          /* base surface pressure (Pa) */
+  float tauRad;        /* radiative relaxation time (s) */
+  float radCap;        /* cap of the radiative relaxation (K/s) */
+  float blDepth;       /* boundary-layer depth (m) */
+  float u10f;          /* U10 / lowest-level wind */
+  float gust;          /* gustiness (m/s) */
+  float thermals;      /* boundary-layer thermal forcing (K/s, 0 = none) */
+  float thermalScale;  /* its scale factor */
+  float maritime;      /* 1: maritime graupel in the Lin scheme */
+  float filter4;       /* 2-dx filter strength per pass (every 4th step, 4x); 0 = off */
+  float cdCap;         /* sea drag cap at 10 m */
+  float dissHeat;      /* 1: dissipative heating */
+  float centreX, centreY;  /* storm centre (model m) for the environment hold and the thermals */
+  float thermalR;      /* radius of the thermal forcing (m) */
+  float envR;          /* environment-hold radius (m) */
+  float cnOld;         /* share of the last step's pressure force applied before advection (0 = none) */
+  float traj2;         /* 1: midpoint trajectories */
+} ObHurricane;
+void ob_hurricane_default(ObHurricane* h);  /* app.js:1631 and model.js:1402-1420 defaults, centre at the origin */
+
 /* Grid: dx (m), nx, ny, nz. dz = 20000/nz and the solver padding gridPad(dx) follow model.js:1122, 1203. */
 typedef struct ObGrid {
   int nx, ny, nz;
@@ -131,6 +156,18 @@ int ob_ensemble_tune(ObEnsemble* e, int reps, int* tiles, float* ms);
 int ob_ensemble_lsf_times(ObEnsemble* e, double* out);
 void* ob_ensemble_stream(ObEnsemble* e);
 void ob_ensemble_destroy(ObEnsemble* e);
+
+/* hurricane mode (RegionalModel.setSurface / setVortex, model.js:1290-1365): surf nx*ny*4 floats (land fraction, SST K,
+ * 0, 0) per column or NULL (no sea); hur NULL = outbreak mode. The kernels then run the hurricane branches: sea
+ * fluxes, drag and dissipative heating, radiative relaxation, the far-field hold, boundary-layer thermals and the
+ * K-profile boundary layer, warm-bubble storm starts, settling cloud ice, maritime graupel, midpoint trajectories,
+ * 40 % of the last pressure force carried along the trajectories (WGSL_M_PREP) and the 2-dx filter every 4th step
+ * (WGSL_M_FILT). The plain microphysics only; not inside an ensemble. */
+int ob_model_set_surface(ObModel* m, const float* surf, const ObHurricane* hur);
+int ob_model_set_hurricane(ObModel* m, const ObHurricane* hur);  /* parameters only (e.g. the tracked centre) */
+/* setVortex's table, built on the host: nz x nr x 4 floats (tangential wind m/s, theta' K, 0, 0) at radii i*dr; the
+ * centre (model m), the moist core's radius (m) and relative humidity; nr = 0 clears it. Read by ob_model_reset. */
+int ob_model_set_vortex(ObModel* m, const float* tab, int nr, float x, float y, float dr, float moist_r, float moist_rh);
 
 /* the sub-grid tornado scheme's candidates (tornadoCandidates, app.js:1457-1472), found on the GPU in the maps of the
  * last ob_model_maps call: 7 floats each (i, j, x, y, 1-km vorticity, 2-5 km updraft helicity, max updraft), in no

@@ -14,7 +14,8 @@
 // (i + 1/2)/N in normalised coordinates. This restatement works in texel units directly and uses exact linear
 // weights; the hardware's low-precision fixed-point filter weights are not reproduced.
 //
-// Outbreak mode only (hur = 0, model.js:1412): the hurricane branches (model.js:107-119, 377-386, 713-774, 948-1026)
+// Outbreak mode and hurricane mode (setSurface with a hurricane, model.js:1290-1365, 1402-1420): the hurricane branches
+// (model.js:107-119, 308-336, 377-386, 424-433, 494-499, 640-690, 713-774, 893-896, 948-1026) are restated too
 // are not restated.
 #include <algorithm>
 #include <cmath>
@@ -220,6 +221,17 @@ template <class R> struct Model {
   int steps = 0, parity = 0;
   double rhoSfc = 1.15;
   std::vector<double> rain;
+  // hurricane mode (model.js:1290-1365, 1402-1420)
+  bool hur_on = false;
+  ObHurricane H{};
+  std::vector<R> Vp;   // the winds the advection carries (WGSL_M_PREP)
+  std::vector<R> vx;   // vortex table, nz x nr x (tangential wind, theta')
+  int vx_nr = 0;
+  double vx_x = 0, vx_y = 0, vx_dr = 1, vx_moistR = 1, vx_moistRH = 0;
+  bool vortex = false;
+  double phiScale = 1;
+  bool cnNow = false, filtNow = false;
+  const std::vector<R>* trajV = nullptr;  // the winds the midpoint trajectories sample
 
   int VX() const { return nx + 1; }
   int VY() const { return ny + 1; }
@@ -286,14 +298,32 @@ template <class R> struct Model {
     S.cor = v4(2 * 7.292e-5 * std::sin(P.lat * DEG), P.nudgeTau, nb, P.moistMix);
     S.ci = v4(nci, 0, 0, 0);
     S.micro2 = v4(0, P.sortQ, P.scheme > 0.5f ? 1 : 0, P.evapT);
-    S.hur = v4(0, 0, 0, 0);
-    S.hur2 = v4(1, 0, 1, 0.8);
-    S.hur3 = v4(0, 1, 0, 0);
-    S.hur4 = v4(0, 0, 1, 1e9);
-    S.hur5 = v4(2.4e-3, 0, 0, 0);
-    S.cn = v4(0, 1, 1, 0);
-    S.vtx = v4(0, 0, 1, 0);
-    S.vtx2 = v4(1, 0, 0, 0);
+    if (hur_on) {
+      S.hur = v4(1, H.ck, H.landMoist, H.sfcP);
+      S.hur2 = v4(H.tauRad, H.radCap, H.blDepth, H.u10f);
+      S.hur3 = v4(std::pow(0.41 / std::log(0.5 * dz / 0.3 + 1), 2), H.gust, double(H.thermals) * double(H.thermalScale), H.maritime > 0.5f ? 1 : 0);
+      filtNow = steps % 4 == 3 && H.filter4 > 0;
+      S.hur5 = v4(H.cdCap, H.dissHeat > 0.5f ? 1 : 0, 4 * double(H.filter4), 0);
+      S.hur4 = v4(H.centreX, H.centreY, H.thermalR, H.envR);
+    } else {
+      S.hur = v4(0, 0, 0, 0);
+      S.hur2 = v4(1, 0, 1, 0.8);
+      S.hur3 = v4(0, 1, 0, 0);
+      S.hur4 = v4(0, 0, 1, 1e9);
+      S.hur5 = v4(2.4e-3, 0, 0, 0);
+      filtNow = false;
+    }
+    // off-centred trajectory-averaged pressure force, not on the first step after a reset (model.js:1413-1417)
+    const bool cn = hur_on && steps > 0 && H.cnOld > 0;
+    cnNow = cn;
+    S.cn = v4(cn ? H.cnOld : 0, phiScale, cn ? 1 / (1 - double(H.cnOld)) : 1, hur_on && H.traj2 > 0.5f ? 1 : 0);
+    if (vortex) {
+      S.vtx = v4(vx_x, vx_y, vx_dr, vx_nr);
+      S.vtx2 = v4(vx_moistR, vx_moistRH, 1, 0);
+    } else {
+      S.vtx = v4(0, 0, 1, 0);
+      S.vtx2 = v4(1, 0, 0, 0);
+    }
     S.pad = v4(pad, nxp, nyp, 0);
     S.dzv = v4(dz, 1 / dx, 1 / dz, P.mcFloor);
     // the uniforms are f32 on the GPU; in the FP64 instantiation they are those same f32 values widened, except
@@ -343,7 +373,23 @@ template <class R> struct Model {
     if (thompson()) { vtRT(qr, nr, rho, vm, vn); return; }
     vm = vn = vtR(qr, rho);
   }
-  R vtGrau(R qg, R rho) const { return thompson() ? vtGT(qg, rho) : vtG(qg, rho); }
+  bool hurOn() const { return S.hur.x > R(0.5); }
+  bool maritime() const { return S.hur3.w > R(0.5) && !thompson(); }  // model.js:90
+  R vtGM(R q, R rho) const {  // model.js:91
+    return clampv(R(5) * std::pow(std::max(R(1000) * rho * q, R(1e-6)), R(0.25)), R(1), R(9)) * std::sqrt(S.step.z / rho);
+  }
+  R vtGrau(R qg, R rho) const {
+    if (maritime()) return vtGM(qg, rho);
+    return thompson() ? vtGT(qg, rho) : vtG(qg, rho);
+  }
+  R vtI(R q, R rho) const {  // model.js:112: cloud ice settles in hurricane mode
+    return (hurOn() && q > R(1e-9)) ? std::min(R(3.29) * std::pow(std::max(rho * q, R(1e-12)), R(0.16)), R(1.5)) : R(0);
+  }
+  R cdSfc(R u1, R land) const {  // model.js:115-119
+    R f = S.hur2.w;
+    R cs = std::min((R(0.75) + R(0.067) * f * u1) * R(1e-3), S.hur5.x) * f * f;
+    return mixv(cs, S.hur3.x, clampv(land, R(0), R(1)));
+  }
   R zRain(R qr, R nr, R rho) const {
     if (!thompson()) return R(3.63e9) * std::pow(std::max(rho * qr, R(0)), R(1.75));
     if (qr < R(1e-9)) return R(0);
@@ -352,6 +398,7 @@ template <class R> struct Model {
     return R(720e18) * rho * nb_ / (l * l * l * l * l * l);
   }
   R zGrau(R qg, R rho, R T) const {
+    if (maritime()) return (T < R(T0K) ? R(1.3e9) : R(1.0e10)) * std::pow(std::max(rho * qg, R(0)), R(1.75));
     if (!thompson()) return (T < R(T0K) ? R(1.2e10) : R(4.33e10)) * std::pow(std::max(rho * qg, R(0)), R(1.75));
     if (qg < R(1e-9)) return R(0);
     R l = lamG(qg, rho), l2 = l * l;
@@ -551,7 +598,18 @@ template <class R> struct Model {
       }
   }
 
-  // ---- WGSL_M_INIT (model.js:284-339), no vortex ----
+  // ---- WGSL_M_INIT (model.js:284-339) ----
+  // the vortex table at radius r, level k (model.js:292-297)
+  void vxAt(R r, int k, R& vt, R& th) const {
+    int nr = int(S.vtx.w);
+    R fr = r / S.vtx.z;
+    int i0 = int(std::floor(fr));
+    if (i0 >= nr - 1) { vt = R(0); th = R(0); return; }
+    size_t o = (size_t(clampi(k, 0, nz - 1)) * nr + i0) * 4;
+    R a = fr - R(i0);
+    vt = mixv(vx[o], vx[o + 4], a);
+    th = mixv(vx[o + 1], vx[o + 5], a);
+  }
   void k_init() {
 #pragma omp parallel for schedule(static)
     for (int ck = 0; ck <= nz; ck++)
@@ -561,12 +619,42 @@ template <class R> struct Model {
           const R* A = l2(lsfA, ci, cj);
           R z = (R(k) + R(0.5)) * DZS();
           R nz0 = sstep(R(800), R(1500), z);
+          const R dxv = DXS();
+          if (S.vtx2.z > R(0.5)) {
+            R px = (R(ci) + R(0.5)) * dxv - S.vtx.x, py = (R(cj) + R(0.5)) * dxv - S.vtx.y;
+            nz0 = std::sqrt(px * px + py * py) < S.vtx2.x ? sstep(R(6000), R(8000), z) : R(1);
+          }
           R noise = S.misc.z * (rnd3<R>(ci + 17, cj + 3, ck + 5) - R(0.5)) * R(2) * (R(1) - nz0);
           R th = tgtTh(A, k) + noise;
           R u = (cj < ny && ck < nz) ? tgtU(ci, cj, k) : R(0);
           R v = (ci < nx && ck < nz) ? tgtV(ci, cj, k) : R(0);
+          const bool vort = S.vtx2.z > R(0.5);
+          if (vort) {  // a warm-core vortex in gradient-wind and hydrostatic balance (setVortex's table)
+            R pux = R(ci) * dxv - S.vtx.x, puy = (R(cj) + R(0.5)) * dxv - S.vtx.y;
+            R ru = std::max(std::sqrt(pux * pux + puy * puy), R(1));
+            R pvx = (R(ci) + R(0.5)) * dxv - S.vtx.x, pvy = R(cj) * dxv - S.vtx.y;
+            R rv = std::max(std::sqrt(pvx * pvx + pvy * pvy), R(1));
+            R pcx = (R(ci) + R(0.5)) * dxv - S.vtx.x, pcy = (R(cj) + R(0.5)) * dxv - S.vtx.y;
+            R rc = std::sqrt(pcx * pcx + pcy * pcy);
+            R vt, tp;
+            vxAt(ru, k, vt, tp);
+            u -= vt * puy / ru;
+            vxAt(rv, k, vt, tp);
+            v += vt * pvx / rv;
+            vxAt(rc, k, vt, tp);
+            th += tp;
+          }
           R T = th * bsB(k)[0];
           R qv = std::min(tgtQv(A, k), R(0.95) * qvsat(T, bsB(k)[1], fIce(T)));
+          if (vort) {  // a nearly saturated core; the same density
+            R pcx = (R(ci) + R(0.5)) * dxv - S.vtx.x, pcy = (R(cj) + R(0.5)) * dxv - S.vtx.y;
+            R f = (R(1) - sstep(R(0.6), R(1), std::sqrt(pcx * pcx + pcy * pcy) / S.vtx2.x)) * sstep(R(500), R(1500), z) *
+                  (R(1) - sstep(R(7000), R(10000), z));
+            R q2 = std::max(qv, f * S.vtx2.y * qvsat(T, bsB(k)[1], fIce(T)));
+            R dqv = q2 - qv;
+            qv = q2;
+            th -= R(0.608) * dqv * bsA(k)[0];
+          }
           R* o = &V[0][vidx(ci, cj, ck) * 4];
           o[0] = u; o[1] = v; o[2] = R(0); o[3] = th;
           if (ci < nx && cj < ny && ck < nz) {
@@ -606,6 +694,15 @@ template <class R> struct Model {
           R lh = S.turb.x * dxv, lv = R(0.18) * dzv;
           R nuh = std::min(lh * lh * sS * fst, R(0.08) * dxv * dxv / std::max(DTS(), R(0.1)));
           R nuv = std::min(lv * lv * sS * fst, R(0.15) * dzv * dzv / std::max(DTS(), R(0.1)));
+          R zc = (R(k) + R(0.5)) * dzv, h = S.hur2.z;
+          if (hurOn() && zc < h) {  // K-profile boundary layer (model.js:377-386)
+            const R* s0 = L(i, j, 0);
+            R ua = R(0.5) * (s0[0] + L(i + 1, j, 0)[0]), va = R(0.5) * (s0[1] + L(i, j + 1, 0)[1]);
+            R u1 = std::sqrt(ua * ua + va * va);
+            R ust = std::sqrt(cdSfc(u1, sfc[(size_t(j) * nx + i) * 4])) * std::max(u1, S.hur3.y);
+            R q = R(1) - zc / h;
+            nuv = std::max(nuv, std::min(R(0.4) * ust * zc * q * q, R(0.15) * dzv * dzv / std::max(DTS(), R(0.1))));
+          }
           size_t o = qidx(i, j, k) * 2;
           aux[o] = nuh;
           aux[o + 1] = nuv;
@@ -630,12 +727,26 @@ template <class R> struct Model {
     return o;
   }
   void kvec(R k[3]) const { k[0] = DTS() / DXS(); k[1] = DTS() / DXS(); k[2] = DTS() / DZS(); }
-  // trace (model.js:428-432), first order: clampX(p - s k v0)
+  // the wind at a point in grid units (model.js:420-423)
+  void velAt(const R x[3], R v[3]) const {
+    const std::vector<R>& W = *trajV;
+    v[0] = sampleV(W, x[0], x[1] - R(0.5), x[2] - R(0.5), 0);
+    v[1] = sampleV(W, x[0] - R(0.5), x[1], x[2] - R(0.5), 1);
+    v[2] = sampleV(W, x[0] - R(0.5), x[1] - R(0.5), x[2], 2);
+  }
+  // trace (model.js:424-433): first order clampX(p - s k v0); midpoint with the wind at p - s k v0 / 2 (cn.w)
   void trace(const R p[3], const R v0[3], R s, R out[3]) const {
     R k[3];
     kvec(k);
     R N[3] = {R(nx), R(ny), R(nz)};
-    for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * v0[a], R(0), N[a]);
+    if (S.cn.w < R(0.5)) {
+      for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * v0[a], R(0), N[a]);
+      return;
+    }
+    R m[3], vm[3];
+    for (int a = 0; a < 3; a++) m[a] = clampv(p[a] - R(0.5) * s * k[a] * v0[a], R(0), N[a]);
+    velAt(m, vm);
+    for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * vm[a], R(0), N[a]);
   }
   // 8-texel min/max at the departure cell (model.js:455-459)
   void mmV(const std::vector<R>& Vv, const R x[3], const R off[3], int ch, R& lo, R& hi) const {
@@ -647,8 +758,8 @@ template <class R> struct Model {
     }
   }
 
-  // ---- WGSL_M_ADVV1 (model.js:434-450) ----
-  void k_advv1(const std::vector<R>& Vin) {
+  // ---- WGSL_M_ADVV1 (model.js:434-450): trajectories from Vin, values carried from Vval (Vp in hurricane mode) ----
+  void k_advv1(const std::vector<R>& Vin, const std::vector<R>& Vval) {
 #pragma omp parallel for schedule(static)
     for (int k = 0; k <= nz; k++)
       for (int j = 0; j <= ny; j++)
@@ -659,17 +770,17 @@ template <class R> struct Model {
           R x[3];
           R* o = &Vt[vidx(i, j, k) * 4];
           trace(pu, L.vu, R(1), x);
-          o[0] = sampleV(Vin, x[0], x[1] - R(0.5), x[2] - R(0.5), 0);
+          o[0] = sampleV(Vval, x[0], x[1] - R(0.5), x[2] - R(0.5), 0);
           trace(pv, L.vv, R(1), x);
-          o[1] = sampleV(Vin, x[0] - R(0.5), x[1], x[2] - R(0.5), 1);
+          o[1] = sampleV(Vval, x[0] - R(0.5), x[1], x[2] - R(0.5), 1);
           trace(pw, L.vw, R(1), x);
-          o[2] = sampleV(Vin, x[0] - R(0.5), x[1] - R(0.5), x[2], 2);
+          o[2] = sampleV(Vval, x[0] - R(0.5), x[1] - R(0.5), x[2], 2);
           trace(pc, L.vc, R(1), x);
-          o[3] = sampleV(Vin, x[0] - R(0.5), x[1] - R(0.5), x[2] - R(0.5), 3);
+          o[3] = sampleV(Vval, x[0] - R(0.5), x[1] - R(0.5), x[2] - R(0.5), 3);
         }
   }
   // ---- WGSL_M_ADVV2 (model.js:451-481) ----
-  void k_advv2(const std::vector<R>& Vin, std::vector<R>& Vout) {
+  void k_advv2(const std::vector<R>& Vin, const std::vector<R>& Vval, std::vector<R>& Vout) {
 #pragma omp parallel for schedule(static)
     for (int k = 0; k <= nz; k++)
       for (int j = 0; j <= ny; j++)
@@ -680,7 +791,7 @@ template <class R> struct Model {
           R pu[3] = {R(i), R(j) + R(0.5), R(k) + R(0.5)}, pv[3] = {R(i) + R(0.5), R(j), R(k) + R(0.5)};
           R pw[3] = {R(i) + R(0.5), R(j) + R(0.5), R(k)}, pc[3] = {R(i) + R(0.5), R(j) + R(0.5), R(k) + R(0.5)};
           const R* hat = &Vt[vidx(i, j, k) * 4];
-          const R* old = ldV(Vin, i, j, k);
+          const R* old = ldV(Vval, i, j, k);
           R x[3], b[4];
           trace(pu, L.vu, R(-1), x);
           b[0] = sampleV(Vt, x[0], x[1] - R(0.5), x[2] - R(0.5), 0);
@@ -702,7 +813,7 @@ template <class R> struct Model {
           for (int c = 0; c < 4; c++) {
             trace(pts[c], vels[c], R(1), x);
             R lo, hi;
-            mmV(Vin, x, offs[c], c, lo, hi);
+            mmV(Vval, x, offs[c], c, lo, hi);
             o[c] = clampv(r[c], lo, hi);
           }
         }
@@ -715,12 +826,19 @@ template <class R> struct Model {
     v[1] = R(0.5) * (p[1] + ldV(Vin, i, j + 1, k)[1]);
     v[2] = R(0.5) * (p[2] + ldV(Vin, i, j, k + 1)[2]);
   }
-  void traceQ(const R p[3], const R v0[3], R fall, R s, R out[3]) const {
+  void traceQ(const R p[3], const R v0[3], R fall, R s, R out[3]) const {  // model.js:494-499
     R k[3];
     kvec(k);
     R N[3] = {R(nx), R(ny), R(nz)};
     R f[3] = {R(0), R(0), fall};
-    for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * (v0[a] - f[a]), R(0.5), N[a] - R(0.5));
+    if (S.cn.w < R(0.5)) {
+      for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * (v0[a] - f[a]), R(0.5), N[a] - R(0.5));
+      return;
+    }
+    R m[3], vm[3];
+    for (int a = 0; a < 3; a++) m[a] = clampv(p[a] - R(0.5) * s * k[a] * (v0[a] - f[a]), R(0), N[a]);
+    velAt(m, vm);
+    for (int a = 0; a < 3; a++) out[a] = clampv(p[a] - s * k[a] * (vm[a] - f[a]), R(0.5), N[a] - R(0.5));
   }
   R sQ(const std::vector<R>& t, const R x[3], int ch) const { return sampleQ(t, x[0] - R(0.5), x[1] - R(0.5), x[2] - R(0.5), ch); }
   void mmQ(const std::vector<R>& t, const R x[3], R lo[4], R hi[4]) const {
@@ -743,10 +861,16 @@ template <class R> struct Model {
           R rho = bsA(k)[2];
           R fr, fn;
           vtRain(q1[3], q2[2], rho, fr, fn);
-          R fs = vtS(q2[0], rho), fg = vtGrau(q2[1], rho);
+          R fs = vtS(q2[0], rho), fg = vtGrau(q2[1], rho), fi = vtI(q1[2], rho);
           R a[4];
           traceQ(p, v, R(0), R(1), x);
           for (int c = 0; c < 4; c++) a[c] = sQ(Q1[0], x, c);
+          R bq0[3] = {x[0], x[1], x[2]};
+          if (fi > R(0)) {
+            traceQ(p, v, fi, R(1), x);
+            a[2] = sQ(Q1[0], x, 2);
+          }
+          x[0] = bq0[0]; x[1] = bq0[1]; x[2] = bq0[2];
           R bq[4];
           for (int c = 0; c < 4; c++) bq[c] = sQ(Q2[0], x, c);
           traceQ(p, v, fr, R(1), x);
@@ -776,7 +900,7 @@ template <class R> struct Model {
           R rho = bsA(k)[2];
           R fr, fnv;
           vtRain(q1[3], q2[2], rho, fr, fnv);
-          R fs = vtS(q2[0], rho), fg = vtGrau(q2[1], rho);
+          R fs = vtS(q2[0], rho), fg = vtGrau(q2[1], rho), fi = vtI(q1[2], rho);
           const R* h1 = &Q1t[qidx(i, j, k) * 4];
           const R* h2 = &Q2t[qidx(i, j, k) * 4];
           R cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
@@ -795,6 +919,10 @@ template <class R> struct Model {
           traceQ(p, v, fn_, R(-1), x);
           R bn = sQ(Q2t, x, 2);
           R bi = b1[2];
+          if (fi > R(0)) {
+            traceQ(p, v, fi, R(-1), x);
+            bi = sQ(Q1t, x, 2);
+          }
           R r1[4] = {h1[0] + sm * (q1[0] - b1[0]), h1[1] + sm * (q1[1] - b1[1]), h1[2] + sm * (q1[2] - bi), h1[3] + sm * (q1[3] - br)};
           R r2[4] = {h2[0] + sm * (q2[0] - bs), h2[1] + sm * (q2[1] - bg), h2[2] + sm * (q2[2] - bn), h2[3] + sm * (q2[3] - b2[3])};
           R lo[4], hi[4], lo2[4], hi2[4];
@@ -803,8 +931,13 @@ template <class R> struct Model {
           mmQ(Q2[0], x, lo2, hi2);
           r1[0] = clampv(r1[0], lo[0], hi[0]);
           r1[1] = clampv(r1[1], lo[1], hi[1]);
-          r1[2] = clampv(r1[2], lo[2], hi[2]);  // cloud ice does not fall outside hurricane mode: mi = m1
           r2[3] = clampv(r2[3], lo2[3], hi2[3]);
+          {  // cloud ice at its own fall speed (the air's trace when it does not fall: mi = m1)
+            R xi[3], loi[4], hii[4];
+            traceQ(p, v, fi, R(1), xi);
+            mmQ(Q1[0], xi, loi, hii);
+            r1[2] = clampv(r1[2], loi[2], hii[2]);
+          }
           traceQ(p, v, fr, R(1), x);
           mmQ(Q1[0], x, lo, hi);
           r1[3] = clampv(r1[3], lo[3], hi[3]);
@@ -893,6 +1026,10 @@ template <class R> struct Model {
             if (ck == 0 && S.turb.w > R(0.5)) {
               R g0 = V[0], g1 = vbar, h0 = ut, h1 = vtb;
               R cd = S.micro.w;
+              if (hurOn()) {
+                R land = R(0.5) * (sfc[(size_t(cj) * nx + std::max(ci - 1, 0)) * 4] + sfc[(size_t(std::min(cj, ny - 1)) * nx + std::min(ci, nx - 1)) * 4]);
+                cd = cdSfc(std::sqrt(g0 * g0 + g1 * g1), land);
+              }
               du += cd * (-std::sqrt(g0 * g0 + g1 * g1) * g0 + std::sqrt(h0 * h0 + h1 * h1) * h0) / dzv;
             }
             o[0] = V[0] + dt * du;
@@ -913,6 +1050,10 @@ template <class R> struct Model {
             if (ck == 0 && S.turb.w > R(0.5)) {
               R g0 = ubar, g1 = V[1], h0 = utb, h1 = vt;
               R cd = S.micro.w;
+              if (hurOn()) {
+                R land = R(0.5) * (sfc[(size_t(std::max(cj - 1, 0)) * nx + ci) * 4] + sfc[(size_t(std::min(cj, ny - 1)) * nx + std::min(ci, nx - 1)) * 4]);
+                cd = cdSfc(std::sqrt(g0 * g0 + g1 * g1), land);
+              }
               dv += cd * (-std::sqrt(g0 * g0 + g1 * g1) * g1 + std::sqrt(h0 * h0 + h1 * h1) * h1) / dzv;
             }
             o[1] = V[1] + dt * dv;
@@ -926,7 +1067,7 @@ template <class R> struct Model {
             dw += R(0.5) * (buoy(ci, cj, ck - 1) + buoy(ci, cj, ck)) - (ldP(ci, cj, ck) - ldP(ci, cj, ck - 1)) / dzv;
             dw += (spongeLat(xmx, xmy) + spongeTop(z)) * (R(0) - V[2]);
             const R* civ = &ciMap[(size_t(cj) * nx + ci) * 4];
-            if (civ[0] > R(0)) {
+            if (civ[0] > R(0) && !hurOn()) {
               R zz = std::abs(z - civ[2]) / civ[3];
               if (zz < R(1)) {
                 R cv = std::cos(R(1.5707963) * zz);
@@ -958,6 +1099,51 @@ template <class R> struct Model {
             l1z[0] -= qvb;
             for (int c = 0; c < 3; c++) q1[c] = q1[c] + dt * (nux * l1[c] * ix2 + nuy * l1z[c] * iz2);
             q1[0] += dt * relax * (tqv - q1[0]);
+            if (hurOn()) {  // model.js:713-774
+              th += dt * clampv((tth - V[3]) / S.hur2.x, -S.hur2.y, S.hur2.y);
+              const R* cs = &ciMap[(size_t(cj) * nx + ci) * 4];
+              if (cs[0] > R(0)) {
+                R zz = std::abs(z - cs[2]) / cs[3];
+                if (zz < R(1)) {
+                  R f = cs[0] * std::cos(R(1.5707963) * zz) * cs[1] / R(8);
+                  th += dt * R(1.2e-3) * f;
+                  q1[0] += dt * f / R(600) * std::max(R(0.97) * qvsat(V[3] * Bb[0], Bb[1], R(0)) - q1[0], R(0));
+                }
+              }
+              R dxh = xmx - S.hur4.x, dyh = xmy - S.hur4.y;
+              R rS = std::sqrt(dxh * dxh + dyh * dyh);
+              R wEnv = sstep(S.hur4.w, R(1.5) * S.hur4.w, rS) / R(3600);
+              th += dt * wEnv * (tth - V[3]);
+              q1[0] += dt * wEnv * (tqv - q1[0]);
+              if (z < S.hur2.z) {
+                const R* s0 = L(ci, cj, 0);
+                R ua = R(0.5) * (s0[0] + L(ci + 1, cj, 0)[0]), va = R(0.5) * (s0[1] + L(ci, cj + 1, 0)[1]);
+                R u1 = std::sqrt(ua * ua + va * va);
+                R e = S.step.y / R(900), e0 = std::floor(e);
+                R qx = xmx / R(6000), qy = xmy / R(6000);
+                R r = R(0.5) * mixv(gnoise2<R>(qx + R(37.1) * e0, qy + R(11.3) * e0), gnoise2<R>(qx + R(37.1) * (e0 + R(1)), qy + R(11.3) * (e0 + R(1))),
+                                    sstep(R(0), R(1), fractv(e)));
+                R fu = std::min(u1 * u1 / R(225), R(1)) * (R(1) - sstep(R(20), R(32), u1)) * (R(1) - sstep(S.hur4.z, R(1.5) * S.hur4.z, rS));
+                th += dt * S.hur3.z * R(2) * r * fu * (R(1) - z / S.hur2.z);
+              }
+              if (ck == 0) {  // the sea's sensible and latent heat, dissipative heating
+                const R* sf = &sfc[(size_t(cj) * nx + ci) * 4];
+                R land = clampv(sf[0], R(0), R(1));
+                R ua = R(0.5) * (V[0] + L(ci + 1, cj, ck)[0]), va = R(0.5) * (V[1] + L(ci, cj + 1, ck)[1]);
+                R u1 = std::sqrt(ua * ua + va * va);
+                R ch = S.hur.y * S.hur2.w * std::max(u1, S.hur3.y) / dzv;
+                R ps = std::max(S.hur.w + A[2] * S.cn.y * phi[pidx(ci, cj, ck)], R(50000));
+                R ths = sf[1] * std::pow(R(1e5) / ps, R(0.2854));
+                th += dt * ch * (R(1) - land) * (ths - V[3]);
+                if (S.hur5.y > R(0.5)) {
+                  R cdh = cdSfc(u1, land);
+                  th += dt * cdh * u1 * u1 * u1 / (R(CPD) * dzv) / Bb[0];
+                }
+                R qsS = qvsat(sf[1], ps, R(0));
+                R qsL = qvsat(V[3] * Bb[0], ps, R(0));
+                q1[0] += dt * ch * ((R(1) - land) * (qsS - q1[0]) + land * S.hur.z * std::max(qsL - q1[0], R(0)));
+              }
+            }
             for (int c = 0; c < 4; c++) { q1[c] = std::max(q1[c], R(0)); q2[c] = std::max(q2[c], R(0)); }
             R pi0 = Bb[0], p0 = Bb[1], rho = A[2];
             R T = th * pi0;
@@ -1068,7 +1254,12 @@ template <class R> struct Model {
             qi = f * qcl; qc = qcl - qi;
             T += R(LFC / CPD) * (qi - qi0 - f * dsum);
             th = T / pi0;
-            R keep = R(1) / (R(1) + R(2) * dt * spongeLat(xmx, xmy));
+            R envDecay = R(0);
+            if (hurOn()) {
+              R dxh = xmx - S.hur4.x, dyh = xmy - S.hur4.y;
+              envDecay = sstep(S.hur4.w, R(1.5) * S.hur4.w, std::sqrt(dxh * dxh + dyh * dyh)) / R(1800);
+            }
+            R keep = R(1) / (R(1) + R(2) * dt * spongeLat(xmx, xmy) + dt * envDecay);
             qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
             R* o1 = &Q1[0][qidx(ci, cj, ck) * 4];
             R* o2 = &Q2[0][qidx(ci, cj, ck) * 4];
@@ -1137,9 +1328,60 @@ template <class R> struct Model {
       }
   }
 
+  // ---- WGSL_M_FILT (model.js:948-994): the 2-dx filter of hurricane mode, into V[1-parity], Q1[1], Q2[1] ----
+  void k_filt(const std::vector<R>& Vin, std::vector<R>& Vout) {
+    const R a = S.hur5.z;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k <= nz; k++)
+      for (int j = 0; j <= ny; j++)
+        for (int i = 0; i <= nx; i++) {
+          auto bih = [&](auto ld, int c) {
+            return R(20) * ld(i, j, c) - R(8) * (ld(i + 1, j, c) + ld(i - 1, j, c) + ld(i, j + 1, c) + ld(i, j - 1, c)) +
+                   R(2) * (ld(i + 1, j + 1, c) + ld(i + 1, j - 1, c) + ld(i - 1, j + 1, c) + ld(i - 1, j - 1, c)) + ld(i + 2, j, c) +
+                   ld(i - 2, j, c) + ld(i, j + 2, c) + ld(i, j - 2, c);
+          };
+          R* o = &Vout[vidx(i, j, k) * 4];
+          for (int c = 0; c < 4; c++) {
+            auto ldv = [&](int a_, int b_, int c_) { return ldV(Vin, a_, b_, k)[c_]; };
+            o[c] = ldV(Vin, i, j, k)[c] - a * bih(ldv, c);
+          }
+          if (k == 0 || k >= nz) o[2] = R(0);
+          if (i < nx && j < ny && k < nz) {
+            R* o1 = &Q1[1][qidx(i, j, k) * 4];
+            R* o2 = &Q2[1][qidx(i, j, k) * 4];
+            for (int c = 0; c < 4; c++) {
+              auto ld1 = [&](int a_, int b_, int c_) { return ldQ(Q1[0], a_, b_, k)[c_]; };
+              auto ld2 = [&](int a_, int b_, int c_) { return ldQ(Q2[0], a_, b_, k)[c_]; };
+              o1[c] = std::max(ldQ(Q1[0], i, j, k)[c] - a * bih(ld1, c), R(0));
+              o2[c] = std::max(ldQ(Q2[0], i, j, k)[c] - a * bih(ld2, c), R(0));
+            }
+          }
+        }
+  }
+  // ---- WGSL_M_PREP (model.js:996-1026): the winds the advection carries, with cn.x of the last pressure force ----
+  void k_prep(const std::vector<R>& Vin) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k <= nz; k++)
+      for (int j = 0; j <= ny; j++)
+        for (int i = 0; i <= nx; i++) {
+          auto Pf = [&](int a, int b, int c) {
+            return phi[pidx(clampi(a, -pad, nx + pad - 1), clampi(b, -pad, ny + pad - 1), clampi(c, 0, nz - 1))];
+          };
+          const R* V = ldV(Vin, i, j, k);
+          R o[4] = {V[0], V[1], V[2], V[3]};
+          R f = S.cn.x * S.cn.y;
+          R kx = f * DTS() / DXS(), kz = f * DTS() / DZS();
+          if (j < ny && k < nz) o[0] = V[0] - kx * (Pf(i, j, k) - Pf(i - 1, j, k));
+          if (i < nx && k < nz) o[1] = V[1] - kx * (Pf(i, j, k) - Pf(i, j - 1, k));
+          if (i < nx && j < ny && k > 0 && k < nz) o[2] = V[2] - kz * (Pf(i, j, k) - Pf(i, j, k - 1));
+          R* out = &Vp[vidx(i, j, k) * 4];
+          for (int c = 0; c < 4; c++) out[c] = o[c];
+        }
+  }
+
   // ---- RegionalModel.reset / encStep (model.js:1427-1476) ----
   void reset() {
-    time = 0; steps = 0; parity = 0;
+    time = 0; steps = 0; parity = 0; phiScale = 1;
     write_uniforms(1);
     k_lsf();
     k_init();
@@ -1153,11 +1395,20 @@ template <class R> struct Model {
     write_uniforms(dt);
     std::vector<R>& Vc = V[parity];
     std::vector<R>& Vn = V[1 - parity];
+    if (hur_on && filtNow) {  // every 4th step: state -> scratch -> back (model.js:1448-1455)
+      k_filt(Vc, Vn);
+      Vc = Vn;
+      Q1[0] = Q1[1];
+      Q2[0] = Q2[1];
+    }
+    if (hur_on) k_prep(Vc);
+    const std::vector<R>& Vval = hur_on ? Vp : Vc;
+    trajV = &Vc;
     if (time - lsfT >= 60 || time == 0) { k_lsf(); lsfT = time; }
     k_ci();
     k_nut(Vc, Q1[0]);
-    k_advv1(Vc);
-    k_advv2(Vc, Vn);
+    k_advv1(Vc, Vval);
+    k_advv2(Vc, Vval, Vn);
     k_advq1(Vc);
     k_advq2(Vc);
     k_phys(Vn, Vc);
@@ -1168,11 +1419,29 @@ template <class R> struct Model {
     parity = 1 - parity;
     time += dt;
     steps++;
+    phiScale = cnNow ? 1 / (1 - double(H.cnOld)) : 1;
+  }
+  // setSurface (model.js:1296-1303): surf nx*ny*4 (land fraction, SST K, 0, 0) or null; hur null = outbreak mode
+  void set_surface(const float* surf, const ObHurricane* h) {
+    for (size_t i = 0; i < sfc.size(); i++) sfc[i] = surf ? R(surf[i]) : R(0);
+    hur_on = h != nullptr;
+    if (h) H = *h;
+    if (hur_on) Vp.assign(V[0].size(), R(0));
+    else Vp.clear();
+  }
+  // setVortex's table (model.js:1318-1365, built on the host): nz x nr x 4; nr = 0 clears it
+  void set_vortex(const float* tab, int nr, double x, double y, double dr, double moistR, double moistRH) {
+    vortex = nr > 0 && tab;
+    vx_nr = nr; vx_x = x; vx_y = y; vx_dr = dr; vx_moistR = moistR; vx_moistRH = moistRH;
+    vx.assign(vortex ? size_t(nz) * nr * 4 : 0, R(0));
+    for (size_t i = 0; i < vx.size(); i++) vx[i] = R(tab[i]);
   }
 
   // ---- WGSL_M_MAP (model.js:1028-1100) ----
   void maps(float* out) {
-    write_uniforms(S.step.x);
+    // the uniforms of the last step; in hurricane mode they carry that step's pressure factors (cn), which a rewrite
+    // after the step would change
+    if (!hur_on) write_uniforms(S.step.x);
     const std::vector<R>& Vin = V[parity];
     const size_t n2 = size_t(nx) * ny;
     auto cvel = [&](int i, int j, int k, R v[3]) { cellVel(Vin, i, j, k, v); };
@@ -1511,6 +1780,13 @@ void ob_params_default(ObParams* p) {
   p->ciRate = 0.5f; p->nudgeTau = 5400.f; p->lat = 35.f; p->moistMix = 0.f;
   p->mcFloor = 0.25f; p->scheme = 0.f; p->evapT = 0.3f; p->dtScale = 1.0f;
 }
+void ob_hurricane_default(ObHurricane* h) {
+  // app.js:1631 and the writeUniforms defaults (model.js:1402-1420); centre at the origin, sfcP for 1000 hPa
+  h->ck = 1.3e-3f; h->landMoist = 0.3f; h->sfcP = 100000.f; h->tauRad = 43200.f; h->radCap = 2.f / 86400.f;
+  h->blDepth = 1000.f; h->u10f = 0.8f; h->gust = 1.5f; h->thermals = 0.4f / 300.f; h->thermalScale = 1.f;
+  h->maritime = 1.f; h->filter4 = 0.003f; h->cdCap = 2.0e-3f; h->dissHeat = 1.f; h->centreX = 0.f; h->centreY = 0.f;
+  h->thermalR = 200000.f; h->envR = 300000.f; h->cnOld = 0.4f; h->traj2 = 1.f;
+}
 int ob_grid_pad(float dx) {  // model.js:1122
   double v = std::round(10000.0 / dx / 8.0) * 8.0;
   return int(std::min(std::max(v, 8.0), 64.0));
@@ -1551,6 +1827,10 @@ void oro_set_ci(OroModel* m, const float* ev, int n) {
   });
 }
 void oro_reset(OroModel* m) { ORO_BOTH(M.reset()); }
+void oro_set_surface(OroModel* m, const float* surf, const ObHurricane* h) { ORO_BOTH(M.set_surface(surf, h)); }
+void oro_set_vortex(OroModel* m, const float* tab, int nr, double x, double y, double dr, double moistR, double moistRH) {
+  ORO_BOTH(M.set_vortex(tab, nr, x, y, dr, moistR, moistRH));
+}
 void oro_step(OroModel* m, double dt, int nsteps) { ORO_BOTH(for (int s = 0; s < nsteps; s++) M.step(dt)); }
 double oro_time(OroModel* m) { double t = 0; ORO_BOTH(t = M.time); return t; }
 int oro_parity(OroModel* m) { int p = 0; ORO_BOTH(p = M.parity); return p; }

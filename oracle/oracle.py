@@ -44,6 +44,13 @@ class ObParams(C.Structure):
         "dtScale")]
 
 
+class ObHurricane(C.Structure):
+    """include/ob.h ObHurricane (hurricane mode)."""
+    _fields_ = [(n, C.c_float) for n in (
+        "ck", "landMoist", "sfcP", "tauRad", "radCap", "blDepth", "u10f", "gust", "thermals", "thermalScale", "maritime",
+        "filter4", "cdCap", "dissHeat", "centreX", "centreY", "thermalR", "envR", "cnOld", "traj2")]
+
+
 def _declare(L):
     vp, i, d, f = C.c_void_p, C.c_int, C.c_double, C.c_float
     fp = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -56,6 +63,9 @@ def _declare(L):
     L.oro_set_boundaries.argtypes = [vp, fp, i]
     L.oro_set_ci.argtypes = [vp, fp, i]
     L.oro_reset.argtypes = [vp]
+    L.oro_set_surface.argtypes = [vp, vp, C.POINTER(ObHurricane)]
+    L.oro_set_vortex.argtypes = [vp, vp, i, d, d, d, d, d]
+    L.ob_hurricane_default.argtypes = [C.POINTER(ObHurricane)]
     L.oro_step.argtypes = [vp, d, i]
     L.oro_time.restype = d
     L.oro_time.argtypes = [vp]
@@ -100,6 +110,12 @@ def default_params() -> ObParams:
     return p
 
 
+def default_hurricane() -> ObHurricane:
+    h = ObHurricane()
+    lib().ob_hurricane_default(C.byref(h))
+    return h
+
+
 class OracleModel:
     """The reference's RegionalModel step on the CPU (precision 4 = float, 8 = double)."""
 
@@ -134,6 +150,17 @@ class OracleModel:
 
     def reset(self):
         lib().oro_reset(self.h)
+
+    def set_surface(self, surf, hur):
+        """setSurface (model.js:1296-1303): surf (ny, nx, 4) float32 or None, hur an ObHurricane or None."""
+        a = None if surf is None else np.ascontiguousarray(surf, np.float32).reshape(-1)
+        lib().oro_set_surface(self.h, a.ctypes.data if a is not None else None, C.byref(hur) if hur is not None else None)
+
+    def set_vortex(self, tab, nr, x, y, dr, moist_r, moist_rh):
+        """setVortex's table (nz, nr, 4) float32, or nr = 0 to clear it."""
+        a = None if tab is None else np.ascontiguousarray(tab, np.float32).reshape(-1)
+        lib().oro_set_vortex(self.h, a.ctypes.data if a is not None else None, int(nr), float(x), float(y), float(dr),
+                             float(moist_r), float(moist_rh))
 
     def step(self, dt, n=1):
         lib().oro_step(self.h, float(dt), int(n))

@@ -33,6 +33,13 @@ class ObParams(C.Structure):
         "dtScale")]
 
 
+class ObHurricane(C.Structure):
+    """include/ob.h ObHurricane (hurricane mode)."""
+    _fields_ = [(n, C.c_float) for n in (
+        "ck", "landMoist", "sfcP", "tauRad", "radCap", "blDepth", "u10f", "gust", "thermals", "thermalScale", "maritime",
+        "filter4", "cdCap", "dissHeat", "centreX", "centreY", "thermalR", "envR", "cnOld", "traj2")]
+
+
 class ObGrid(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_float)]
 
@@ -98,6 +105,10 @@ SYMBOLS = {
     "ob_model_record_micro": (_i, [_vp, _vp, _f]),
     "ob_model_set_graphs": (_i, [_vp, _i]),
     "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),
+    "ob_hurricane_default": (None, [C.POINTER(ObHurricane)]),
+    "ob_model_set_surface": (_i, [_vp, _fp, C.POINTER(ObHurricane)]),
+    "ob_model_set_hurricane": (_i, [_vp, C.POINTER(ObHurricane)]),
+    "ob_model_set_vortex": (_i, [_vp, _fp, _i, _f, _f, _f, _f, _f]),
     "ob_ensemble_create": (_i, [C.POINTER(_vp), _fp, _i, C.POINTER(_vp)]),
     "ob_ensemble_set_lanes": (_i, [_vp, _i]),
     "ob_ensemble_lanes": (_i, [_vp]),

@@ -112,7 +112,7 @@ struct ObModel {
     Uni U{};
     Fields F{};
     int seen = 0;
-  } graphs[2][2][3];
+  } graphs[2][2][3][2];  // [parity][LSF][microphysics mode][2-dx filter this step]
   bool use_graphs = true;
   PoissonPlan solver;
   std::vector<float> Bh;
@@ -120,6 +120,17 @@ struct ObModel {
   int nb = 0, nci = 0;
   double time = 0, lsfT = 0;
   int steps = 0, parity = 0;
+  // hurricane mode (setSurface / setVortex, model.js:1290-1365; uniforms model.js:1402-1420)
+  bool hur_on = false;
+  ObHurricane H{};
+  size_t fs = 0;             // floats per field array
+  float* d_vp = nullptr;     // the winds the advection carries (4 arrays), hurricane mode only
+  float4* d_vx = nullptr;    // vortex table
+  int vx_nr = 0;
+  double vx_x = 0, vx_y = 0, vx_dr = 1, vx_moistR = 1, vx_moistRH = 0;
+  bool vortex = false;
+  double phiScale = 1;       // stored phi -> p'/rho factor of the next step (cn.y)
+  bool cnNow = false, filtNow = false;
   // member of an ensemble: its work goes to the ensemble's stream meanwhile (own_stream is the model's own)
   void* ens = nullptr;
   cudaStream_t own_stream = nullptr;
@@ -140,17 +151,18 @@ static void model_bind_solver(ObModel* m) {
 static void drop_graphs(ObModel* m) {
   for (auto& a : m->graphs)
     for (auto& b : a)
-      for (auto& G : b) {
-        if (G.exec) cudaGraphExecDestroy(G.exec);
-        G = ObModel::StepGraph{};
-      }
+      for (auto& c : b)
+        for (auto& G : c) {
+          if (G.exec) cudaGraphExecDestroy(G.exec);
+          G = ObModel::StepGraph{};
+        }
 }
 
 static void model_free(ObModel* m) {
   if (!m) return;
   drop_graphs(m);
   m->solver.destroy();
-  for (void* p : {(void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_queue, (void*)m->d_mlpc, m->d_surr, (void*)m->d_clock, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
+  for (void* p : {(void*)m->d_vp, (void*)m->d_vx, (void*)m->pool, (void*)m->stage, (void*)m->rhs32, (void*)m->d_act, (void*)m->d_tab, (void*)m->d_queue, (void*)m->d_mlpc, m->d_surr, (void*)m->d_clock, (void*)m->d_B, (void*)m->d_bnd, (void*)m->d_ci, (void*)m->d_rain,
                   (void*)m->d_flags, (void*)m->d_maps, (void*)m->d_2d, (void*)m->d_red, (void*)m->d_qptr})
     if (p) cudaFree(p);
   for (int i = 0; i < 2; i++) {
@@ -179,14 +191,33 @@ static void write_uniforms(ObModel* m, double dt, cudaStream_t ts = nullptr) {
   U.cor = v4(2 * 7.292e-5 * std::sin(P.lat * DEG), P.nudgeTau, m->nb, P.moistMix);
   U.ci = v4(m->nci, 0, 0, 0);
   U.micro2 = v4(0, P.sortQ, P.scheme > 0.5f ? 1 : 0, P.evapT);
-  U.hur = v4(0, 0, 0, 0);
-  U.hur2 = v4(1, 0, 1, 0.8);
-  U.hur3 = v4(0, 1, 0, 0);
-  U.hur4 = v4(0, 0, 1, 1e9);
-  U.hur5 = v4(2.4e-3, 0, 0, 0);
-  U.cn = v4(0, 1, 1, 0);
-  U.vtx = v4(0, 0, 1, 0);
-  U.vtx2 = v4(1, 0, 0, 0);
+  if (m->hur_on) {
+    const ObHurricane& H = m->H;
+    U.hur = v4(1, H.ck, H.landMoist, H.sfcP);
+    U.hur2 = v4(H.tauRad, H.radCap, H.blDepth, H.u10f);
+    U.hur3 = v4(std::pow(0.41 / std::log(0.5 * m->dz / 0.3 + 1), 2), H.gust, double(H.thermals) * double(H.thermalScale), H.maritime > 0.5f ? 1 : 0);
+    m->filtNow = m->steps % 4 == 3 && H.filter4 > 0;  // the 2-dx filter: every 4th step at 4x strength
+    U.hur5 = v4(H.cdCap, H.dissHeat > 0.5f ? 1 : 0, 4 * double(H.filter4), 0);
+    U.hur4 = v4(H.centreX, H.centreY, H.thermalR, H.envR);
+  } else {
+    U.hur = v4(0, 0, 0, 0);
+    U.hur2 = v4(1, 0, 1, 0.8);
+    U.hur3 = v4(0, 1, 0, 0);
+    U.hur4 = v4(0, 0, 1, 1e9);
+    U.hur5 = v4(2.4e-3, 0, 0, 0);
+    m->filtNow = false;
+  }
+  // the trajectory-averaged pressure force: off-centred, not on the first step after a reset (model.js:1413-1417)
+  const bool cn = m->hur_on && m->steps > 0 && m->H.cnOld > 0;
+  m->cnNow = cn;
+  U.cn = v4(cn ? m->H.cnOld : 0, m->phiScale, cn ? 1 / (1 - double(m->H.cnOld)) : 1, m->hur_on && m->H.traj2 > 0.5f ? 1 : 0);
+  if (m->vortex) {
+    U.vtx = v4(m->vx_x, m->vx_y, m->vx_dr, m->vx_nr);
+    U.vtx2 = v4(m->vx_moistR, m->vx_moistRH, 1, 0);
+  } else {
+    U.vtx = v4(0, 0, 1, 0);
+    U.vtx2 = v4(1, 0, 0, 0);
+  }
   U.pad = v4(m->g.pad, m->g.nxp, m->g.nyp, 0);
   U.dzv = v4(m->dz, 1 / m->dx, 1 / m->dz, P.mcFloor);
   // the same float expressions the kernels would evaluate per thread, once on the host (IEEE float arithmetic)
@@ -249,6 +280,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   const double fieldsz = double(g.plane) * (nz + 1);
   if (fieldsz * 39 * 4 > 170e9) { delete m; set_error("ob_model_create: grid too large for one GPU"); return OB_ERR_INVALID; }
   const size_t fs = (size_t(g.plane) * (nz + 1) + 63) / 64 * 64;
+  m->fs = fs;
   const size_t n2 = size_t(nx) * ny, np = size_t(g.nxp) * g.nyp * nz;
   int rc = OB_OK;
   auto alloc = [&](void** p, size_t bytes, const char* what) {
@@ -395,7 +427,7 @@ int ob_model_set_ci(ObModel* m, const float* ev, int n) {
 
 int ob_model_reset(ObModel* m) {
   if (!m) { set_error("ob_model_reset: null model"); return OB_ERR_INVALID; }
-  m->time = 0; m->steps = 0; m->parity = 0;
+  m->time = 0; m->steps = 0; m->parity = 0; m->phiScale = 1;
   cudaMemsetAsync(m->d_clock, 0, sizeof(double), m->stream);
   write_uniforms(m, 1.0);
   const Grid& g = m->g;
@@ -428,6 +460,7 @@ static int micro_mode(const ObModel* m) { return m->surrogate ? kMicroSurrogate 
 // the microphysics fields of the kernel parameters for the model's mode (before a step is launched or captured)
 static int prepare_micro(ObModel* m) {
   const int mode = micro_mode(m);
+  if (m->hur_on && mode != kMicroPlain) { set_error("hurricane mode runs the plain microphysics (no surrogate, no pair recording)"); return OB_ERR_INVALID; }
   if (mode == kMicroSurrogate) {
     if (m->P.scheme < 0.5f) { set_error("the microphysics surrogate emulates the Thompson-style scheme (params.scheme = 1)"); return OB_ERR_INVALID; }
     m->F.mlp_buf = reinterpret_cast<float*>(m->d_queue);
@@ -465,6 +498,13 @@ static int physics_pass(ObModel* m, int par, cudaStream_t s) {
 static int enqueue_step(ObModel* m, bool lsf, cudaStream_t s) {
   const Grid& g = m->g;
   const int par = m->parity;
+  if (m->hur_on && m->filtNow) {  // state -> scratch -> back (model.js:1448-1455)
+    launch_filt(g, m->U, m->F, par, s);
+    const size_t bytes = m->fs * sizeof(float);
+    for (int c = 0; c < 4; c++) OB_TRY(cuda_status(cudaMemcpyAsync(m->F.V[par][c], m->F.V[1 - par][c], bytes, cudaMemcpyDeviceToDevice, s), "filter"));
+    for (int c = 0; c < 8; c++) OB_TRY(cuda_status(cudaMemcpyAsync(m->F.Q[0][c], m->F.Q[1][c], bytes, cudaMemcpyDeviceToDevice, s), "filter"));
+  }
+  if (m->hur_on) launch_prep(g, m->U, m->F, par, s);
   if (lsf) launch_lsf(g, m->U, m->F, s);
   launch_ci(g, m->U, m->F, s);
   cudaEventRecord(m->ev_fork, s);
@@ -496,7 +536,7 @@ static int model_step_once(ObModel* m, double dt) {
   if (!m->use_graphs) {
     OB_TRY(enqueue_step(m, lsf, s));
   } else {
-    ObModel::StepGraph& G = m->graphs[m->parity][lsf ? 1 : 0][micro_mode(m)];
+    ObModel::StepGraph& G = m->graphs[m->parity][lsf ? 1 : 0][micro_mode(m)][m->filtNow ? 1 : 0];
     const bool match = G.exec && std::memcmp(&G.U, &m->U, sizeof(Uni)) == 0 && std::memcmp(&G.F, &m->F, sizeof(Fields)) == 0;
     if (match) {
       OB_TRY(cuda_status(cudaGraphLaunch(G.exec, s), "step graph launch"));
@@ -522,6 +562,7 @@ static int model_step_once(ObModel* m, double dt) {
   m->parity = 1 - m->parity;
   m->time += dt;
   m->steps++;
+  m->phiScale = m->cnNow ? 1 / (1 - double(m->H.cnOld)) : 1;
   return cuda_status(cudaGetLastError(), "step launch");
 }
 
@@ -783,6 +824,62 @@ unsigned ob_model_nan_count(ObModel* m) {
 
 void* ob_model_stream(ObModel* m) { return m ? (void*)m->stream : nullptr; }
 
+void ob_hurricane_default(ObHurricane* h) {
+  // app.js:1631 and the writeUniforms defaults (model.js:1402-1420); centre at the origin, sfcP for 1000 hPa
+  h->ck = 1.3e-3f; h->landMoist = 0.3f; h->sfcP = 100000.f; h->tauRad = 43200.f; h->radCap = 2.f / 86400.f;
+  h->blDepth = 1000.f; h->u10f = 0.8f; h->gust = 1.5f; h->thermals = 0.4f / 300.f; h->thermalScale = 1.f;
+  h->maritime = 1.f; h->filter4 = 0.003f; h->cdCap = 2.0e-3f; h->dissHeat = 1.f; h->centreX = 0.f; h->centreY = 0.f;
+  h->thermalR = 200000.f; h->envR = 300000.f; h->cnOld = 0.4f; h->traj2 = 1.f;
+}
+
+// setSurface (model.js:1296-1303): surf nx*ny*4 (land fraction, SST K, 0, 0) or null (no sea); hur null = outbreak
+int ob_model_set_surface(ObModel* m, const float* surf, const ObHurricane* hur) {
+  if (!m) { set_error("ob_model_set_surface: null model"); return OB_ERR_INVALID; }
+  if (m->ens) { set_error("ob_model_set_surface: the model belongs to an ensemble (hurricane mode runs alone)"); return OB_ERR_INVALID; }
+  const size_t n2 = size_t(m->g.nx) * m->g.ny;
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set surface"));
+  if (surf) OB_TRY(cuda_status(cudaMemcpy(const_cast<float4*>(m->F.sfc), surf, n2 * sizeof(float4), cudaMemcpyHostToDevice), "surface"));
+  else OB_TRY(cuda_status(cudaMemset(const_cast<float4*>(m->F.sfc), 0, n2 * sizeof(float4)), "surface"));
+  m->hur_on = hur != nullptr;
+  if (hur) m->H = *hur;
+  if (m->hur_on && !m->d_vp) {  // the prep field (model.js:1290-1295)
+    OB_TRY(cuda_status(cudaMalloc(&m->d_vp, 4 * m->fs * sizeof(float)), "prep field"));
+    OB_TRY(cuda_status(cudaMemset(m->d_vp, 0, 4 * m->fs * sizeof(float)), "prep field"));
+  } else if (!m->hur_on && m->d_vp) {
+    cudaFree(m->d_vp);
+    m->d_vp = nullptr;
+  }
+  for (int c = 0; c < 4; c++) m->F.Vp[c] = m->d_vp ? m->d_vp + c * m->fs : nullptr;
+  drop_graphs(m);
+  return OB_OK;
+}
+
+// the hurricane's parameters alone (its centre follows the storm, app.js hurricaneUpdate)
+int ob_model_set_hurricane(ObModel* m, const ObHurricane* hur) {
+  if (!m || !hur) { set_error("ob_model_set_hurricane: bad arguments"); return OB_ERR_INVALID; }
+  if (!m->hur_on) { set_error("ob_model_set_hurricane: not in hurricane mode (ob_model_set_surface first)"); return OB_ERR_INVALID; }
+  m->H = *hur;
+  return OB_OK;
+}
+
+// setVortex's table (built on the host, model.js:1318-1365): nz x nr of (tangential wind, theta', 0, 0), the centre,
+// the table spacing, the moist core's radius and relative humidity; nr = 0 clears it
+int ob_model_set_vortex(ObModel* m, const float* tab, int nr, float x, float y, float dr, float moistR, float moistRH) {
+  if (!m || nr < 0 || (nr > 0 && (!tab || !(dr > 0.f)))) { set_error("ob_model_set_vortex: bad arguments"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set vortex"));
+  if (m->d_vx) { cudaFree(m->d_vx); m->d_vx = nullptr; }
+  m->vortex = nr > 0;
+  m->F.vx = nullptr;
+  if (m->vortex) {
+    const size_t n = size_t(m->g.nz) * nr;
+    OB_TRY(cuda_status(cudaMalloc(&m->d_vx, n * sizeof(float4)), "vortex table"));
+    OB_TRY(cuda_status(cudaMemcpy(m->d_vx, tab, n * sizeof(float4), cudaMemcpyHostToDevice), "vortex table"));
+    m->F.vx = m->d_vx;
+    m->vx_nr = nr; m->vx_x = x; m->vx_y = y; m->vx_dr = dr; m->vx_moistR = moistR; m->vx_moistRH = moistRH;
+  }
+  return OB_OK;
+}
+
 // ---- ensembles: every member's pass in one launch per lane ----
 // Members are split into lanes (1 or 2) balanced by cell count; each lane runs the step's passes as grouped launches
 // on its own streams, so that with two lanes one lane's solve (tensor cores) runs beside the other's stencils.
@@ -963,6 +1060,7 @@ static int ens_prepare(ObEnsemble* e) {
         e->lsfT[i] = m->lsfT;
         lsf_changed = true;
       }
+      if (m->hur_on) { set_error("ensemble: member %d is in hurricane mode (it runs alone)", i); return OB_ERR_INVALID; }
       write_uniforms(m, e->dt[i], e->stream);
       if (micro_mode(m) != kMicroPlain) { set_error("ensemble: member %d uses a learned or recording microphysics mode", i); return OB_ERR_INVALID; }
       OB_TRY(prepare_micro(m));

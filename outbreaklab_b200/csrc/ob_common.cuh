@@ -78,7 +78,25 @@ struct Fields {
   // model time (s) on the device: read by the passes that move with time (LSF, CI, the record-mode draw) and
   // advanced by the last pass of each step, so a captured step replays unchanged
   double* clock;
+  // hurricane mode: the winds the advection carries (WGSL_M_PREP; null outside hurricane mode) and the initial
+  // vortex table (nz x nr of (tangential wind, theta', 0, 0); null when there is none)
+  float* Vp[4];
+  const float4* vx;
 };
+
+// ---- hurricane mode (model.js:107-119) ----
+__device__ __forceinline__ bool hurOn(const Uni& U) { return U.hur.x > 0.5f; }
+// cloud ice settles in hurricane mode (model.js:112)
+__device__ __forceinline__ float vtI(const Uni& U, float q, float rho) {
+  return (U.hur.x > 0.5f && q > 1e-9f) ? fminf(3.29f * powf(fmaxf(rho * q, 1e-12f), 0.16f), 1.5f) : 0.f;
+}
+// drag coefficient for the lowest-level wind u1 over sea and land (model.js:115-119)
+__device__ __forceinline__ float cdSfc(const Uni& U, float u1, float land) {
+  const float f = U.hur2.w;
+  const float cs = fminf((0.75f + 0.067f * f * u1) * 1e-3f, U.hur5.x) * f * f;
+  const float t = fminf(fmaxf(land, 0.f), 1.f);
+  return cs * (1.f - t) + U.hur3.x * t;
+}
 
 // ---- grouped launches: one launch of a pass over every member of an ensemble ----
 constexpr int kMaxMembers = 48;
@@ -167,6 +185,7 @@ __device__ __forceinline__ float qvsat1(float T, float p, float f) {
 struct Fall {
   float rsfc;   // surface density (step.z)
   bool thm;     // Thompson-style scheme
+  bool mar = false;  // maritime graupel (hurricane mode, Lin scheme: model.js:87-92)
   __device__ __forceinline__ float vtR(float q, float rho) const {
     float f = sqrtf(rsfc / rho);
     return fminf(36.34f * powf(fmaxf(0.001f * rho * q, 0.f), 0.1364f) * f, 10.f * f);
@@ -198,7 +217,13 @@ struct Fall {
     float v = vtR(qr, rho);
     return make_float2(v, v);
   }
-  __device__ __forceinline__ float vtGrau(float qg, float rho) const { return thm ? vtGT(qg, rho) : vtG(qg, rho); }
+  __device__ __forceinline__ float vtGM(float q, float rho) const {
+    return clampf(5.f * powf(fmaxf(1000.f * rho * q, 1e-6f), 0.25f), 1.f, 9.f) * sqrtf(rsfc / rho);
+  }
+  __device__ __forceinline__ float vtGrau(float qg, float rho) const {
+    if (mar) return vtGM(qg, rho);
+    return thm ? vtGT(qg, rho) : vtG(qg, rho);
+  }
   // equivalent reflectivity (mm^6/m^3), model.js:103-116
   __device__ __forceinline__ float zRain(float qr, float nr, float rho) const {
     if (!thm) return 3.63e9f * powf(fmaxf(rho * qr, 0.f), 1.75f);
@@ -208,6 +233,7 @@ struct Fall {
     return 720e18f * rho * nb / (l * l * l * l * l * l);
   }
   __device__ __forceinline__ float zGrau(float qg, float rho, float T) const {
+    if (mar) return (T < T0K ? 1.3e9f : 1.0e10f) * powf(fmaxf(rho * qg, 0.f), 1.75f);
     if (!thm) return (T < T0K ? 1.2e10f : 4.33e10f) * powf(fmaxf(rho * qg, 0.f), 1.75f);
     if (qg < 1e-9f) return 0.f;
     float l = lamG(qg, rho), l2 = l * l;

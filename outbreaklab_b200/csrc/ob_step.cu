@@ -227,13 +227,51 @@ __global__ void k_init(Grid g, Uni U, Fields F) {
   const float dz = U.dzv.x;
   const float4 A = l2d(F.lsfA, g, ci, cj);
   const float z = (float(k) + 0.5f) * dz;
-  const float nz0 = sstep(800.f, 1500.f, z);
+  const float dx = U.dims.w;
+  const bool vortex = U.vtx2.z > 0.5f && F.vx;
+  float nz0 = sstep(800.f, 1500.f, z);
+  // hurricane mode: the noise reaches up through the moist core (model.js:306-309)
+  if (U.vtx2.z > 0.5f) {
+    const float px = (float(ci) + 0.5f) * dx - U.vtx.x, py = (float(cj) + 0.5f) * dx - U.vtx.y;
+    nz0 = sqrtf(px * px + py * py) < U.vtx2.x ? sstep(6000.f, 8000.f, z) : 1.f;
+  }
   const float noise = U.misc.z * (rnd3(ci + 17, cj + 3, ck + 5) - 0.5f) * 2.f * (1.f - nz0);
-  const float th = tgtTh(F.B, g, dz, A, k) + noise;
-  const float u = (cj < g.ny && ck < g.nz) ? tgtU(F, g, dz, ci, cj, k) : 0.f;
-  const float v = (ci < g.nx && ck < g.nz) ? tgtV(F, g, dz, ci, cj, k) : 0.f;
+  float th = tgtTh(F.B, g, dz, A, k) + noise;
+  float u = (cj < g.ny && ck < g.nz) ? tgtU(F, g, dz, ci, cj, k) : 0.f;
+  float v = (ci < g.nx && ck < g.nz) ? tgtV(F, g, dz, ci, cj, k) : 0.f;
+  // the vortex table at radius r (model.js:292-297): (tangential wind, theta')
+  auto vxAt = [&](float r) {
+    const int nr = int(U.vtx.w);
+    const float fr = r / U.vtx.z;
+    const int i0 = int(floorf(fr));
+    if (i0 >= nr - 1) return make_float2(0.f, 0.f);
+    const int q = clampi(k, 0, g.nz - 1) * nr + i0;
+    const float4 a = __ldg(F.vx + q), b = __ldg(F.vx + q + 1);
+    const float t = fr - float(i0);
+    return make_float2(a.x * (1.f - t) + b.x * t, a.y * (1.f - t) + b.y * t);
+  };
+  if (vortex) {  // a warm-core vortex in gradient-wind and hydrostatic balance (model.js:314-325)
+    const float pux = float(ci) * dx - U.vtx.x, puy = (float(cj) + 0.5f) * dx - U.vtx.y;
+    const float ru = fmaxf(sqrtf(pux * pux + puy * puy), 1.f);
+    const float pvx = (float(ci) + 0.5f) * dx - U.vtx.x, pvy = float(cj) * dx - U.vtx.y;
+    const float rv = fmaxf(sqrtf(pvx * pvx + pvy * pvy), 1.f);
+    const float pcx = (float(ci) + 0.5f) * dx - U.vtx.x, pcy = (float(cj) + 0.5f) * dx - U.vtx.y;
+    const float rc = sqrtf(pcx * pcx + pcy * pcy);
+    u -= vxAt(ru).x * puy / ru;
+    v += vxAt(rv).x * pvx / rv;
+    th += vxAt(rc).y;
+  }
   const float T = th * bsB(F.B, g.nz, k).x;
-  const float qv = fminf(tgtQv(F.B, g, dz, A, k), 0.95f * qvsat(T, bsB(F.B, g.nz, k).y, fIce(T)));
+  float qv = fminf(tgtQv(F.B, g, dz, A, k), 0.95f * qvsat(T, bsB(F.B, g.nz, k).y, fIce(T)));
+  if (vortex) {  // a nearly saturated core at the same density (model.js:328-335)
+    const float pcx = (float(ci) + 0.5f) * dx - U.vtx.x, pcy = (float(cj) + 0.5f) * dx - U.vtx.y;
+    const float f = (1.f - sstep(0.6f, 1.f, sqrtf(pcx * pcx + pcy * pcy) / U.vtx2.x)) * sstep(500.f, 1500.f, z) *
+                    (1.f - sstep(7000.f, 10000.f, z));
+    const float q2 = fmaxf(qv, f * U.vtx2.y * qvsat(T, bsB(F.B, g.nz, k).y, fIce(T)));
+    const float dqv = q2 - qv;
+    qv = q2;
+    th -= 0.608f * dqv * bsA(F.B, g.nz, k).x;
+  }
   const int o = g.at(ci, cj, ck);
   for (int p = 0; p < 2; p++) {  // both ping-pong slots (reset copies V0 to V1, model.js:1437)
     F.V[p][0][o] = u;
@@ -251,6 +289,7 @@ __global__ void k_init(Grid g, Uni U, Fields F) {
 // ---------------------------------------------------------------------------------------------------------------
 // WGSL_M_NUT (model.js:342-389): Smagorinsky-Lilly viscosities with the Richardson correction
 // ---------------------------------------------------------------------------------------------------------------
+template <bool HUR = false>
 __device__ __forceinline__ void nut_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx - 1, g.ny - 1, g.nz - 1)
   // a cell's +1 neighbours on the staggered box always exist; the -1 ones clamp to the edge (offset 0)
@@ -286,9 +325,23 @@ __device__ __forceinline__ void nut_body(const Grid& g, const Uni& U, const Fiel
   const float lh = U.turb.x * dx, lv = 0.18f * dz;
   const float dtc = fmaxf(U.step.x, 0.1f);
   F.aux[0][o] = fminf(lh * lh * sS * fst, 0.08f * dx * dx / dtc);
-  F.aux[1][o] = fminf(lv * lv * sS * fst, 0.15f * dz * dz / dtc);
+  float nuv = fminf(lv * lv * sS * fst, 0.15f * dz * dz / dtc);
+  if (HUR) {  // hurricane mode: a K-profile boundary layer (model.js:377-386)
+    const float zc = (float(ck) + 0.5f) * dz, h = U.hur2.z;
+    if (zc < h) {
+      const int o0 = g.at(ci, cj, 0);
+      const float ua = 0.5f * (__ldg(F.V[par][0] + o0) + __ldg(F.V[par][0] + o0 + 1));
+      const float va = 0.5f * (__ldg(F.V[par][1] + o0) + __ldg(F.V[par][1] + o0 + g.px));
+      const float u1 = sqrtf(ua * ua + va * va);
+      const float ust = sqrtf(cdSfc(U, u1, __ldg(F.sfc + cj * g.nx + ci).x)) * fmaxf(u1, U.hur3.y);
+      const float q = 1.f - zc / h;
+      nuv = fmaxf(nuv, fminf(0.4f * ust * zc * q * q, 0.15f * dz * dz / dtc));
+    }
+  }
+  F.aux[1][o] = nuv;
 }
 __global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) { nut_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void k_nut_hur(Grid g, Uni U, Fields F, int par) { nut_body<true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
 __global__ void __launch_bounds__(128, 16) k_nut_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
   nut_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
@@ -734,7 +787,7 @@ __device__ __forceinline__ unsigned warp_append(unsigned* ctr) {
 // offsets below are the clamped index minus the texel's own, for the staggered box [0, n] (V) and the cell box
 // [0, n-1] (Q, aux, phi_t), computed once per texel. BND: boundary air masses present (else the target state is the
 // base state, see tgtUb).
-template <bool BND, int MM>
+template <bool BND, int MM, bool HUR = false>
 __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
   bool hyd = false;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -790,7 +843,11 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     du += fc * (vbar - vtb);
     if (BND && ci > 0 && ci < nx) du -= (LP(0) - LP(-1)) / dx;
     if (ck == 0 && U.turb.w > 0.5f) {
-      const float cd = U.micro.w;
+      float cd = U.micro.w;
+      if (HUR) {  // sea / land drag (model.js:649-652)
+        const float land = 0.5f * (__ldg(F.sfc + cj * nx + max(ci - 1, 0)).x + __ldg(F.sfc + min(cj, ny - 1) * nx + min(ci, nx - 1)).x);
+        cd = cdSfc(U, sqrtf(V[0] * V[0] + vbar * vbar), land);
+      }
       du += cd * (-sqrtf(V[0] * V[0] + vbar * vbar) * V[0] + sqrtf(ut * ut + vtb * vtb) * ut) / dz;
     }
     out[0] = V[0] + dt * du;
@@ -813,7 +870,11 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     dv -= fc * (ubar - utb);
     if (BND && cj > 0 && cj < ny) dv -= (LP(0) - LP(-g.px)) / dx;
     if (ck == 0 && U.turb.w > 0.5f) {
-      const float cd = U.micro.w;
+      float cd = U.micro.w;
+      if (HUR) {
+        const float land = 0.5f * (__ldg(F.sfc + max(cj - 1, 0) * nx + ci).x + __ldg(F.sfc + min(cj, ny - 1) * nx + min(ci, nx - 1)).x);
+        cd = cdSfc(U, sqrtf(ubar * ubar + V[1] * V[1]), land);
+      }
       dv += cd * (-sqrtf(ubar * ubar + V[1] * V[1]) * V[1] + sqrtf(utb * utb + vt * vt) * vt) / dz;
     }
     out[1] = V[1] + dt * dv;
@@ -833,7 +894,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     if (BND) dw -= (LP(0) - LP(-g.plane)) / dz;
     dw += (fmaxf(slx.y, sly.y) + spk.y) * (0.f - V[2]);
     const float4 civ = __ldg(F.ciMap + cj * nx + ci);
-    if (civ.x > 0.f) {
+    if (!HUR && civ.x > 0.f) {  // hurricane mode starts storms as warm bubbles instead (model.js:686-687)
       const float z = float(ck) * dz;
       const float zz = fabsf(z - civ.z) / civ.w;
       if (zz < 1.f) {
@@ -870,6 +931,56 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
 #pragma unroll
     for (int c = 0; c < 3; c++) q1[c] = q1[c] + dt * (nux * l1[c] * ix2 + nuy * l1z[c] * iz2);
     q1[0] += dt * relax * (tqv - q1[0]);
+    const float xmx = (float(ci) + 0.5f) * dx, xmy = (float(cj) + 0.5f) * dx;
+    float envDecay = 0.f;
+    if (HUR) {  // the warm sea and the tropical environment (model.js:713-774)
+      const float z = (float(ck) + 0.5f) * dz;
+      th += dt * clampf((tth - V[3]) / U.hur2.x, -U.hur2.y, U.hur2.y);
+      const float4 cs = __ldg(F.ciMap + cj * nx + ci);
+      if (cs.x > 0.f) {  // storm starts: a warm, moist bubble through the push's depth
+        const float zz = fabsf(z - cs.z) / cs.w;
+        if (zz < 1.f) {
+          const float f = cs.x * cosf(1.5707963f * zz) * cs.y / 8.f;
+          th += dt * 1.2e-3f * f;
+          q1[0] += dt * f / 600.f * fmaxf(0.97f * qvsat(V[3] * Bb.x, Bb.y, 0.f) - q1[0], 0.f);
+        }
+      }
+      const float dxh = xmx - U.hur4.x, dyh = xmy - U.hur4.y;
+      const float rS = sqrtf(dxh * dxh + dyh * dyh);
+      const float wEnv = sstep(U.hur4.w, 1.5f * U.hur4.w, rS) / 3600.f;  // the far field held to the sounding
+      th += dt * wEnv * (tth - V[3]);
+      q1[0] += dt * wEnv * (tqv - q1[0]);
+      envDecay = sstep(U.hur4.w, 1.5f * U.hur4.w, rS) / 1800.f;
+      if (z < U.hur2.z) {  // boundary-layer thermals: coherent ~6 km cells living ~15 min
+        const int o0 = g.at(ci, cj, 0);
+        const float ua = 0.5f * (__ldg(F.V[1 - par][0] + o0) + __ldg(F.V[1 - par][0] + o0 + 1));
+        const float va = 0.5f * (__ldg(F.V[1 - par][1] + o0) + __ldg(F.V[1 - par][1] + o0 + g.px));
+        const float u1 = sqrtf(ua * ua + va * va);
+        const float e = float(__ldg(F.clock)) / 900.f, e0 = floorf(e);
+        const float qx = xmx / 6000.f, qy = xmy / 6000.f;
+        const float r = 0.5f * mixf(gnoise2(qx + 37.1f * e0, qy + 11.3f * e0), gnoise2(qx + 37.1f * (e0 + 1.f), qy + 11.3f * (e0 + 1.f)),
+                                    sstep(0.f, 1.f, e - floorf(e)));
+        const float fu = fminf(u1 * u1 / 225.f, 1.f) * (1.f - sstep(20.f, 32.f, u1)) * (1.f - sstep(U.hur4.z, 1.5f * U.hur4.z, rS));
+        th += dt * U.hur3.z * 2.f * r * fu * (1.f - z / U.hur2.z);
+      }
+      if (ck == 0) {  // the sea's sensible and latent heat; dissipative heating
+        const float4 sf = __ldg(F.sfc + cj * nx + ci);
+        const float land = clampf(sf.x, 0.f, 1.f);
+        const float ua = 0.5f * (V[0] + __ldg(Vu + 1)), va = 0.5f * (V[1] + __ldg(Vv + g.px));
+        const float u1 = sqrtf(ua * ua + va * va);
+        const float ch = U.hur.y * U.hur2.w * fmaxf(u1, U.hur3.y) / dz;
+        const float ps = fmaxf(U.hur.w + A.z * U.cn.y * __ldg(F.phi + g.pidx(ci, cj, ck)), 50000.f);
+        const float ths = sf.y * powf(1.0e5f / ps, 0.2854f);
+        th += dt * ch * (1.f - land) * (ths - V[3]);
+        if (U.hur5.y > 0.5f) {
+          const float cdh = cdSfc(U, u1, land);
+          th += dt * cdh * u1 * u1 * u1 / (1005.7f * dz) / Bb.x;
+        }
+        const float qsS = qvsat(sf.y, ps, 0.f);
+        const float qsL = qvsat(V[3] * Bb.x, ps, 0.f);
+        q1[0] += dt * ch * ((1.f - land) * (qsS - q1[0]) + land * U.hur.z * fmaxf(qsL - q1[0], 0.f));
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       q1[c] = fmaxf(q1[c], 0.f);
@@ -919,7 +1030,8 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       T = mc.T; qv = mc.qv; qc = mc.qc; qi = mc.qi; qr = mc.qr; qs = mc.qs; qg = mc.qg;
       float nr = mc.nr;
       th = T / pi0;
-      const float keep = sl > 0.f ? 1.f / (1.f + 2.f * dt * sl) : 1.f;  // 1 / (1 + 0) == 1 exactly: no division
+      // 1 / (1 + 0) == 1 exactly: no division outside the sponge (and, in hurricane mode, the far-field decay)
+      const float keep = HUR ? 1.f / (1.f + 2.f * dt * sl + dt * envDecay) : (sl > 0.f ? 1.f / (1.f + 2.f * dt * sl) : 1.f);
       qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
       F.Q[0][0][o] = fmaxf(qv, 0.f);
       F.Q[0][1][o] = fmaxf(qc, 0.f);
@@ -947,12 +1059,12 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   return hyd;
 }
 
-template <int MM>
+template <int MM, bool HUR = false>
 __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
-    hyd = U.cor.z > 0.5f ? phys_texel<true, MM>(g, U, F, par, ci, cj, ck) : phys_texel<false, MM>(g, U, F, par, ci, cj, ck);
+    hyd = U.cor.z > 0.5f ? phys_texel<true, MM, HUR>(g, U, F, par, ci, cj, ck) : phys_texel<false, MM, HUR>(g, U, F, par, ci, cj, ck);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(BX) < F.nbx && int(BY) < F.nby && ck < g.nz)
@@ -960,6 +1072,9 @@ __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fie
 }
 template <int MM>
 __global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128) k_phys_hur(Grid g, Uni U, Fields F, int par) {
+  phys_body<kMicroPlain, true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 template <int MM>
 __global__ void __launch_bounds__(128, 10) k_phys_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
@@ -1027,7 +1142,7 @@ __device__ __forceinline__ void rain_body(const Grid& g, const Uni& U, const Fie
   const int i = BX * blockDim.x + threadIdx.x, j = BY * blockDim.y + threadIdx.y;
   if (i >= g.nx || j >= g.ny) return;
   const int o = g.at(i, j, 0);
-  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  const Fall fl{U.step.z, U.micro2.z > 0.5f, U.hur3.w > 0.5f && U.micro2.z <= 0.5f};
   const float rho = bsA(F.B, g.nz, 0).z;
   const float qr = F.Q[0][3][o], qs = F.Q[0][4][o], qg = F.Q[0][5][o];
   const float2 fv = fl.vtRain(qr, F.Q[0][6][o], rho);
@@ -1055,7 +1170,7 @@ __global__ void k_maps(Grid g, Uni U, Fields F, int par, float4* out) {
     v[1] = 0.5f * (L(1, a, b, c) + L(1, a, b + 1, c));
     v[2] = 0.5f * (L(2, a, b, c) + L(2, a, b, c + 1));
   };
-  const Fall fl{U.step.z, U.micro2.z > 0.5f};
+  const Fall fl{U.step.z, U.micro2.z > 0.5f, U.hur3.w > 0.5f && U.micro2.z <= 0.5f};
   auto dbz = [&](int k) {
     const int o = g.at(i, j, k);
     const float rho = bsA(F.B, nz, k).z;
@@ -1134,6 +1249,206 @@ __global__ void k_unpack(Grid g, Ptr8 dst, int nch, int X, int Y, int Z, const f
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// hurricane mode: the advection with midpoint trajectories and settling ice, the pressure force carried along the
+// trajectories (WGSL_M_PREP) and the 2-dx filter (WGSL_M_FILT). Straight restatements, one thread per texel, no
+// clear-air skip (these runs are the few, not the bench's).
+// ---------------------------------------------------------------------------------------------------------------
+// the winds at a point in grid units, from the true winds (model.js:420-423)
+__device__ __forceinline__ void velAt(const Fields& F, const Grid& g, int par, float x, float y, float z, float v[3]) {
+  v[0] = sampleVch(F.V[par][0], g, 0, x, y, z);
+  v[1] = sampleVch(F.V[par][1], g, 1, x, y, z);
+  v[2] = sampleVch(F.V[par][2], g, 2, x, y, z);
+}
+// departure (s = 1) or forward (s = -1) point: first order, or with the wind at the midpoint when cn.w (model.js:424-433)
+__device__ __forceinline__ void traceH(const Uni& U, const Fields& F, const Grid& g, int par, const float k[3], float px, float py,
+                                       float pz, const float v[3], float s, float& x, float& y, float& z) {
+  if (U.cn.w < 0.5f) {
+    traceV(g, k, px, py, pz, v, s, x, y, z);
+    return;
+  }
+  float mx, my, mz, vm[3];
+  traceV(g, k, px, py, pz, v, 0.5f * s, mx, my, mz);
+  velAt(F, g, par, mx, my, mz, vm);
+  traceV(g, k, px, py, pz, vm, s, x, y, z);
+}
+// the same for a cell centre and something falling at `fall` (model.js:494-499)
+__device__ __forceinline__ void traceQH(const Uni& U, const Fields& F, const Grid& g, int par, const float k[3], const float p[3],
+                                        const float v[3], float fall, float s, float& x, float& y, float& z) {
+  if (U.cn.w < 0.5f) {
+    traceQ(g, k, p, v, fall, s, x, y, z);
+    return;
+  }
+  const float mx = clampf(p[0] - 0.5f * s * k[0] * v[0], 0.f, float(g.nx));
+  const float my = clampf(p[1] - 0.5f * s * k[1] * v[1], 0.f, float(g.ny));
+  const float mz = clampf(p[2] - 0.5f * s * k[2] * (v[2] - fall), 0.f, float(g.nz));
+  float vm[3];
+  velAt(F, g, par, mx, my, mz, vm);
+  traceQ(g, k, p, vm, fall, s, x, y, z);
+}
+
+__global__ void k_prep(Grid g, Uni U, Fields F, int par) {
+  OB_BLOCKS_DIRECT
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  auto P = [&](int a, int b, int c) {
+    return __ldg(F.phi + g.pidx(clampi(a, -g.pad, g.nx + g.pad - 1), clampi(b, -g.pad, g.ny + g.pad - 1), clampi(c, 0, g.nz - 1)));
+  };
+  const int o = g.at(ci, cj, ck);
+  const float f = U.cn.x * U.cn.y;
+  const float kx = f * U.step.x / U.dims.w, kz = f * U.step.x / U.dzv.x;
+  const float pc = P(ci, cj, ck);
+  float u = __ldg(F.V[par][0] + o), v = __ldg(F.V[par][1] + o), w = __ldg(F.V[par][2] + o);
+  if (cj < g.ny && ck < g.nz) u = u - kx * (pc - P(ci - 1, cj, ck));
+  if (ci < g.nx && ck < g.nz) v = v - kx * (pc - P(ci, cj - 1, ck));
+  if (ci < g.nx && cj < g.ny && ck > 0 && ck < g.nz) w = w - kz * (pc - P(ci, cj, ck - 1));
+  F.Vp[0][o] = u;
+  F.Vp[1][o] = v;
+  F.Vp[2][o] = w;
+  F.Vp[3][o] = __ldg(F.V[par][3] + o);
+}
+
+// 4th-order horizontal hyperdiffusion of V and Q into V[1-par], Q slot 1 (model.js:948-994)
+__global__ void k_filt(Grid g, Uni U, Fields F, int par) {
+  OB_BLOCKS_DIRECT
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const float a = U.hur5.z;
+  auto bih = [&](const float* __restrict__ f, int X, int Y) {
+    auto L = [&](int i, int j) { return __ldg(f + g.at(clampi(i, 0, X), clampi(j, 0, Y), ck)); };
+    return 20.f * L(ci, cj) - 8.f * (L(ci + 1, cj) + L(ci - 1, cj) + L(ci, cj + 1) + L(ci, cj - 1)) +
+           2.f * (L(ci + 1, cj + 1) + L(ci + 1, cj - 1) + L(ci - 1, cj + 1) + L(ci - 1, cj - 1)) + L(ci + 2, cj) + L(ci - 2, cj) +
+           L(ci, cj + 2) + L(ci, cj - 2);
+  };
+  const int o = g.at(ci, cj, ck);
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    float val = __ldg(F.V[par][c] + o) - a * bih(F.V[par][c], g.nx, g.ny);
+    if (c == 2 && (ck == 0 || ck >= g.nz)) val = 0.f;  // the lid / ground faces of w stay zero
+    F.V[1 - par][c][o] = val;
+  }
+  if (ci < g.nx && cj < g.ny && ck < g.nz) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) F.Q[1][c][o] = fmaxf(__ldg(F.Q[0][c] + o) - a * bih(F.Q[0][c], g.nx - 1, g.ny - 1), 0.f);
+  }
+}
+
+// ADVV1/2 of hurricane mode (model.js:434-481): trajectories from the true winds, values carried from Vp
+__global__ void k_advv1_hur(Grid g, Uni U, Fields F, int par) {
+  OB_BLOCKS_DIRECT
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const Loc L = localVel(F, g, par, ci, cj, ck);
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};
+  const float fi = float(ci), fj = float(cj), fk = float(ck);
+  const int o = g.at(ci, cj, ck);
+  const float P[4][3] = {{fi, fj + 0.5f, fk + 0.5f}, {fi + 0.5f, fj, fk + 0.5f}, {fi + 0.5f, fj + 0.5f, fk}, {fi + 0.5f, fj + 0.5f, fk + 0.5f}};
+  const float* vel[4] = {L.vu, L.vv, L.vw, L.vc};
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    float x, y, z;
+    traceH(U, F, g, par, kk, P[c][0], P[c][1], P[c][2], vel[c], 1.f, x, y, z);
+    F.Vt[c][o] = sampleVch(F.Vp[c], g, c, x, y, z);
+  }
+}
+__global__ void k_advv2_hur(Grid g, Uni U, Fields F, int par) {
+  OB_BLOCKS_DIRECT
+  OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
+  const Loc L = localVel(F, g, par, ci, cj, ck);
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};
+  const float fi = float(ci), fj = float(cj), fk = float(ck);
+  const float P[4][3] = {{fi, fj + 0.5f, fk + 0.5f}, {fi + 0.5f, fj, fk + 0.5f}, {fi + 0.5f, fj + 0.5f, fk}, {fi + 0.5f, fj + 0.5f, fk + 0.5f}};
+  const float* vel[4] = {L.vu, L.vv, L.vw, L.vc};
+  const float cx = L.vc[0] * kk[0], cy = L.vc[1] * kk[1], cz = L.vc[2] * kk[2];
+  const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
+  const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
+  const int o = g.at(ci, cj, ck);
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float ox = c == 0 ? 0.f : 0.5f, oy = c == 1 ? 0.f : 0.5f, oz = c == 2 ? 0.f : 0.5f;
+    float x, y, z;
+    traceH(U, F, g, par, kk, P[c][0], P[c][1], P[c][2], vel[c], -1.f, x, y, z);
+    const float b = sampleVch(F.Vt[c], g, c, x, y, z);
+    const float hat = __ldg(F.Vt[c] + o), old = __ldg(F.Vp[c] + o);
+    const float r = hat + sm * (old - b);
+    traceH(U, F, g, par, kk, P[c][0], P[c][1], P[c][2], vel[c], 1.f, x, y, z);
+    const float2 m = minmax8V(F.Vp[c], g, x, y, z, ox, oy, oz);
+    F.V[1 - par][c][o] = clampf(r, m.x, m.y);
+  }
+}
+
+// ADVQ1/2 of hurricane mode (model.js:500-576): every channel, maritime graupel, settling ice. The brick flags of the
+// clear-air skip are left saying "may hold hydrometeors", so that a later run without the hurricane stays exact.
+__device__ __forceinline__ void brick_flags_all(const Grid& g, const Fields& F, unsigned* a, unsigned* zq, unsigned* z1) {
+  if (threadIdx.x == 0 && threadIdx.y == 0 && int(blockIdx.x) < F.nbx && int(blockIdx.y) < F.nby && int(blockIdx.z) < g.nz) {
+    const int b = blockIdx.x + F.nbx * (blockIdx.y + F.nby * blockIdx.z);
+    if (a) a[b] = 1u;
+    if (zq) zq[b] = 0u;
+    if (z1) z1[b] = 0u;
+  }
+}
+__global__ void k_advq1_hur(Grid g, Uni U, Fields F, int par) {
+  brick_flags_all(g, F, F.actQt, F.zeroQt, nullptr);
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  if (ci >= g.nx || cj >= g.ny || ck >= g.nz) return;
+  const int o = g.at(ci, cj, ck);
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};
+  const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
+  float v[3];
+  cellVel(F, g, par, ci, cj, ck, v);
+  const float rho = bsA(F.B, g.nz, ck).z;
+  const bool thm = U.micro2.z > 0.5f;
+  const Fall fl{U.step.z, thm, U.hur3.w > 0.5f && !thm};
+  const float2 fv = fl.vtRain(__ldg(F.Q[0][3] + o), __ldg(F.Q[0][6] + o), rho);
+  const float fs = fl.vtS(__ldg(F.Q[0][4] + o), rho), fg = fl.vtGrau(__ldg(F.Q[0][5] + o), rho), fi = vtI(U, __ldg(F.Q[0][2] + o), rho);
+  float x, y, z;
+  auto at = [&](float fall, int c) {
+    traceQH(U, F, g, par, kk, p, v, fall, 1.f, x, y, z);
+    return gatherQ(F.Q[0][c], tapQ(g, x, y, z));
+  };
+  traceQH(U, F, g, par, kk, p, v, 0.f, 1.f, x, y, z);
+  const Tap t0 = tapQ(g, x, y, z);
+  F.Qt[0][o] = gatherQ(F.Q[0][0], t0);
+  F.Qt[1][o] = gatherQ(F.Q[0][1], t0);
+  F.Qt[2][o] = fi > 0.f ? at(fi, 2) : gatherQ(F.Q[0][2], t0);
+  F.Qt[3][o] = at(fv.x, 3);
+  F.Qt[4][o] = at(fs, 4);
+  F.Qt[5][o] = at(fg, 5);
+  F.Qt[6][o] = thm ? at(fv.y, 6) : gatherQ(F.Q[0][6], t0);
+  F.Qt[7][o] = gatherQ(F.Q[0][7], t0);
+}
+__global__ void k_advq2_hur(Grid g, Uni U, Fields F, int par) {
+  brick_flags_all(g, F, nullptr, nullptr, F.zeroQ1);
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x, cj = blockIdx.y * blockDim.y + threadIdx.y, ck = blockIdx.z;
+  if (ci >= g.nx || cj >= g.ny || ck >= g.nz) return;
+  const int o = g.at(ci, cj, ck);
+  const float kk[3] = {U.der.x, U.der.x, U.der.y};
+  const float p[3] = {float(ci) + 0.5f, float(cj) + 0.5f, float(ck) + 0.5f};
+  float v[3];
+  cellVel(F, g, par, ci, cj, ck, v);
+  const float rho = bsA(F.B, g.nz, ck).z;
+  const bool thm = U.micro2.z > 0.5f;
+  const Fall fl{U.step.z, thm, U.hur3.w > 0.5f && !thm};
+  float q[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) q[c] = __ldg(F.Q[0][c] + o);
+  const float2 fv = fl.vtRain(q[3], q[6], rho);
+  const float fs = fl.vtS(q[4], rho), fg = fl.vtGrau(q[5], rho), fi = vtI(U, q[2], rho);
+  const float fn = thm ? fv.y : 0.f;
+  const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
+  const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
+  const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
+  // each channel's fall speed (0: the air's)
+  const float fall[8] = {0.f, 0.f, fi, fv.x, fs, fg, fn, 0.f};
+  float x, y, z;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    traceQH(U, F, g, par, kk, p, v, fall[c], -1.f, x, y, z);
+    const float b = gatherQ(F.Qt[c], tapQ(g, x, y, z));
+    const float r = __ldg(F.Qt[c] + o) + sm * (q[c] - b);
+    traceQH(U, F, g, par, kk, p, v, fall[c], 1.f, x, y, z);
+    const float2 m = minmaxQ(F.Q[0][c], tapQ(g, x, y, z));
+    F.Q[1][c][o] = fmaxf(clampf(r, m.x, m.y), 0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------------------------------
 static inline dim3 grid3(int X, int Y, int Z, dim3 b) { return dim3((X + b.x - 1) / b.x, (Y + b.y - 1) / b.y, Z); }
@@ -1150,15 +1465,32 @@ void launch_init(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s) {
   k_init<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F);
 }
 void launch_nut(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
-  k_nut<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+  if (U.hur.x > 0.5f) k_nut_hur<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+  else k_nut<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
 }
 void launch_advv(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  if (U.hur.x > 0.5f && F.Vp[0]) {
+    k_advv1_hur<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+    k_advv2_hur<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+    return;
+  }
   k_advv1<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
   k_advv2<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
 }
 void launch_advq(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  if (U.hur.x > 0.5f) {
+    k_advq1_hur<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+    k_advq2_hur<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+    return;
+  }
   k_advq1<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
   k_advq2<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_prep(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_prep<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+}
+void launch_filt(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
+  k_filt<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
 }
 void launch_activity(const Grid& g, const Fields& F, cudaStream_t s) {
   k_activity<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, F);
@@ -1168,6 +1500,10 @@ void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s)
   k_tables<<<(n + 127) / 128, 128, 0, s>>>(g, U, F.B, const_cast<float*>(F.spz), const_cast<float*>(F.slx), const_cast<float*>(F.sly));
 }
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s, int micro_mode) {
+  if (U.hur.x > 0.5f) {  // hurricane mode runs the scheme (model.js:578-907 with its hurricane branches)
+    k_phys_hur<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+    return;
+  }
   if (micro_mode == kMicroRecord) k_phys<kMicroRecord><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
   else if (micro_mode == kMicroSurrogate) k_phys<kMicroSurrogate><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
   else k_phys<kMicroPlain><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);

@@ -22,6 +22,9 @@ void launch_tables(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s)
 // microphysics modes of the physics pass
 enum { kMicroPlain = 0, kMicroRecord = 1, kMicroSurrogate = 2 };
 void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s, int micro_mode = kMicroPlain);
+// hurricane mode: the winds the advection carries (WGSL_M_PREP), the 2-dx filter into V[1-par] and Q slot 1
+void launch_prep(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
+void launch_filt(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_proj(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s);
 void launch_rain(const Grid& g, const Uni& U, const Fields& F, cudaStream_t s);

@@ -132,19 +132,37 @@ class RegionalModel:
         self.ci_events = act
         N.check(N.lib().ob_model_set_ci(self.h, N.fptr(f), len(act)))
 
-    def set_surface(self, surf=None, hur=None):
-        """model.js:1273-1278. Outbreak mode only: the hurricane surface is not built in this library."""
-        if surf is not None or hur is not None:
-            raise N.ObError(N.OB_ERR_INVALID, "hurricane mode is not supported by this library")
-
-    def set_vortex(self, v=None):
-        if v is not None:
-            raise N.ObError(N.OB_ERR_INVALID, "the hurricane vortex is not supported by this library")
-
     # ---- stepping (model.js:1427-1476) ----
     def reset(self):
         self._sync_params()
         N.check(N.lib().ob_model_reset(self.h))
+
+    # ---- hurricane mode (model.js:1290-1365) ----
+    def set_surface(self, surf=None, hur=None):
+        """setSurface: surf (ny, nx, 4) float32 (land fraction, SST K, 0, 0) or None; hur an ObHurricane or None."""
+        a = None if surf is None else np.ascontiguousarray(surf, np.float32).reshape(-1)
+        if a is not None and a.size != self.nx * self.ny * 4:
+            raise N.ObError(N.OB_ERR_INVALID, "set_surface: %d floats, want nx * ny * 4 = %d" % (a.size, self.nx * self.ny * 4))
+        if hur is not None and not isinstance(hur, N.ObHurricane):
+            raise N.ObError(N.OB_ERR_INVALID, "set_surface: the hurricane is an ObHurricane (hurricane.default_hurricane())")
+        N.check(N.lib().ob_model_set_surface(self.h, N.fptr(a) if a is not None else None,
+                                             C.byref(hur) if hur is not None else None))
+        self.hurricane = hur
+
+    def set_hurricane(self, hur):
+        N.check(N.lib().ob_model_set_hurricane(self.h, C.byref(hur)))
+        self.hurricane = hur
+
+    def set_vortex(self, tab=None, info=None):
+        """setVortex's table (hurricane.vortex_table) or None to clear it; read by reset."""
+        if tab is None:
+            N.check(N.lib().ob_model_set_vortex(self.h, None, 0, 0.0, 0.0, 1.0, 1.0, 0.0))
+            return
+        t = np.ascontiguousarray(tab, np.float32)
+        if t.ndim != 3 or t.shape[0] != self.nz or t.shape[2] != 4:
+            raise N.ObError(N.OB_ERR_INVALID, "set_vortex: the table is (nz, nr, 4)")
+        N.check(N.lib().ob_model_set_vortex(self.h, N.fptr(t.reshape(-1)), int(t.shape[1]), float(info["x"]), float(info["y"]),
+                                            float(info["dr"]), float(info["moistR"]), float(info["moistRH"])))
 
     def enc_step(self, dt, nsteps=1):
         self._sync_params()

@@ -2,16 +2,13 @@
 tornadoCandidates (app.js:1453-1466), on the maps of a growing Thompson supercell, at the scheme's threshold and at
 lower ones that let many more lattice points through to the maximum and helicity / updraft tests; then the scheme and
 the run loop on the GPU candidates."""
-import os
-import sys
 
 import numpy as np
 import pytest
 
 from outbreaklab_b200 import model as M, runloop as RL, tornado as TS, workloads as W
 
-sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
-import tornado_oracle as TO  # noqa: E402
+from oracle import tornado_oracle as TO
 
 pytestmark = pytest.mark.gpu
 

@@ -2,16 +2,13 @@
 and the host logic (mesocyclone tracking, spawning, following, roping out, the per-step tick) with the oracle's
 candidate search standing in for the GPU one."""
 import math
-import sys
-import os
 
 import numpy as np
 import pytest
 
 from outbreaklab_b200 import runloop as RL, tornado as TS, workloads as W
 
-sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
-import tornado_oracle as TO  # noqa: E402
+from oracle import tornado_oracle as TO
 
 
 def blank_maps(nx, ny):
