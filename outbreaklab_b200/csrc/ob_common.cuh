@@ -7,7 +7,8 @@
 // means a semi-Lagrangian gather of u touches only u bytes (a float4 texel would drag v, w, theta through L1/L2).
 //
 // The physics formulas restate the reference's WGSL (model.js:41-134, 578-907) in fp32 with IEEE division and
-// square root; the hurricane-mode branches are not built (outbreak mode only, model.js:1412).
+// square root; the hurricane-mode branches (model.js:107-119 and the kernels' hurricane parts) are template flags or
+// separate kernels, so the outbreak-mode kernels carry none of their code.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
