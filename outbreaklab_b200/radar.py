@@ -219,7 +219,8 @@ class RadarSim:
         U.mdl2[:] = [m.dz, g.groundMSL, -m.Lx / 2, -m.Ly / 2]
         U.phys[:] = [m.rho_sfc or 1.15, R["opts"].get("minDbz", 0) or 0,
                      1 if m.params.get("scheme") == "thompson" else 0, self.nTor]
-        U.phys2[:] = [0, 0, 0, 0]
+        hur = getattr(m, "hurricane", None)   # hurricane mode's maritime graupel (radar.js:384)
+        U.phys2[:] = [1 if hur is not None and hur.maritime > 0.5 else 0, 0, 0, 0]
         return U
 
     def enc_cut(self, R, c, sim_t):
