@@ -129,7 +129,8 @@ int ob_model_maps(ObModel* m, float* out16xN2);
  * An ensemble steps its members together: each pass of the step (LSF, CI, NUT, ADVV1/2, ADVQ1/2, PHYS, DIV, the
  * solve's transforms, tridiagonals and residual, PROJ, rain) is one launch over every member, the members' sizes,
  * spacings, soundings and dt free to differ (they must share nz and the solver precision, use the tensor-core solve,
- * the plain microphysics, and sit at the same step parity). The step is captured as a CUDA graph and replayed.
+ * all the scheme or all one surrogate network (ob_model_set_surrogate on each member first: one grouped inference
+ * launch serves every member's queue), and sit at the same step parity). The step is captured as a CUDA graph and replayed.
  * Members keep their handles: fields, maps, budgets and radars work on them as usual, queued on the ensemble's stream
  * while they belong to it (so they are ordered with its steps); stepping a member alone in between is allowed (an
  * even number of steps, to keep the parity). At most 48 members; one ensemble at a time (the members sit in one

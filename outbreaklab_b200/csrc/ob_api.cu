@@ -100,6 +100,7 @@ struct ObModel {
   unsigned* d_mlpc = nullptr;
   unsigned queue_cap = 0;
   void* d_surr = nullptr;
+  const ObMlp* surr_net = nullptr;  // the network the inference copy was made from
   mlp::Norm surr_norm{};
   bool surrogate = false;
   ObMlp* rec = nullptr;  // recording (state, tendency) pairs into this network's buffer, at rate rec_rate
@@ -448,6 +449,8 @@ namespace ob {
 int surrogate_prepare(const ObMlp* net, void** d_image, mlp::Norm* norm);
 void launch_surrogate(const Grid& g, const Uni& U, const Fields& F, int par, const void* d_image, const mlp::Norm& nm,
                       unsigned int* err, cudaStream_t s);
+void launch_surrogate_grp(const MemberC* d_members, int n, int par, const void* d_image, const mlp::Norm& nm, unsigned int* err,
+                          cudaStream_t s);
 void mlp_record_target(ObMlp* n, float** buf, unsigned** count, unsigned* cap);
 void launch_level2(const uint8_t* vol, size_t vol_bytes, const ObL2Sweep* d_sweeps, int nsweeps, int max_nrad, const uint8_t* d_tpl,
                    uint8_t* d_out, cudaStream_t s);
@@ -774,6 +777,7 @@ int ob_model_set_surrogate(ObModel* m, const ObMlp* net) {
   }
   OB_TRY(surrogate_prepare(net, &m->d_surr, &m->surr_norm));
   m->surrogate = true;
+  m->surr_net = net;
   return OB_OK;
 }
 
@@ -914,6 +918,8 @@ struct ObEnsemble {
   bool use_graphs = true;
   int parity = 0;
   std::vector<double> lsfT;  // what the device copy holds (the device updates it as the host does)
+  int micro = kMicroPlain;   // every member's microphysics mode (the scheme, or one shared surrogate)
+  unsigned* d_err = nullptr; // the grouped surrogate's timeout word
 };
 
 // the grouped kernels read their members from one constant-memory table per device: one ensemble at a time
@@ -948,7 +954,7 @@ static void ens_free(ObEnsemble* e) {
       m->ens = nullptr;
     }
   for (int l = 0; l < kMaxLanes; l++) lane_free(e->lane[l], l > 0);
-  for (void* p : {(void*)e->d_members, (void*)e->d_lsfT})
+  for (void* p : {(void*)e->d_members, (void*)e->d_lsfT, (void*)e->d_err})
     if (p) cudaFree(p);
   if (e->ev_start) cudaEventDestroy(e->ev_start);
   if (e->ev_done) cudaEventDestroy(e->ev_done);
@@ -1062,7 +1068,14 @@ static int ens_prepare(ObEnsemble* e) {
       }
       if (m->hur_on) { set_error("ensemble: member %d is in hurricane mode (it runs alone)", i); return OB_ERR_INVALID; }
       write_uniforms(m, e->dt[i], e->stream);
-      if (micro_mode(m) != kMicroPlain) { set_error("ensemble: member %d uses a learned or recording microphysics mode", i); return OB_ERR_INVALID; }
+      const int mode = micro_mode(m);
+      if (mode == kMicroRecord) { set_error("ensemble: member %d records microphysics pairs (record on the model alone)", i); return OB_ERR_INVALID; }
+      if (l == 0 && q == 0) e->micro = mode;
+      if (mode != e->micro) { set_error("ensemble: the members must all use the scheme or all the surrogate (member %d differs)", i); return OB_ERR_INVALID; }
+      if (mode == kMicroSurrogate && m->surr_net != e->mem[e->lane[0].idx[0]]->surr_net) {
+        set_error("ensemble: the members' surrogates must be one network (member %d differs)", i);
+        return OB_ERR_INVALID;
+      }
       OB_TRY(prepare_micro(m));
       MemberC c;
       std::memset(&c, 0, sizeof(c));
@@ -1070,6 +1083,7 @@ static int ens_prepare(ObEnsemble* e) {
       c.U = m->U;
       c.F = m->F;
       c.lsfT = e->d_lsfT + i;
+      c.micro = mode;
       MemberC& slot = e->h_members[L.base + q];
       if (std::memcmp(&c, &slot, sizeof(MemberC)) != 0) {
         slot = c;
@@ -1094,7 +1108,7 @@ static int lane_enqueue(ObEnsemble* e, int l) {
   ObEnsemble::Lane& L = e->lane[l];
   const int par = e->parity;
   cudaStream_t s = L.s;
-  auto G = [&](int p, cudaStream_t st) { launch_group(p, L.d_map[p], L.nxy[p], L.Z[p], e->shape[p], par, st, kMicroPlain); };
+  auto G = [&](int p, cudaStream_t st) { launch_group(p, L.d_map[p], L.nxy[p], L.Z[p], e->shape[p], par, st, e->micro); };
   G(kGroupLSF, s);
   G(kGroupCI, s);
   cudaEventRecord(L.ev_fork, s);
@@ -1108,6 +1122,10 @@ static int lane_enqueue(ObEnsemble* e, int l) {
   G(kGroupADVV2, s);
   for (int i = 0; i < 2; i++) cudaStreamWaitEvent(s, L.ev_join[i], 0);
   G(kGroupPHYS, s);
+  if (e->micro == kMicroSurrogate) {
+    const ObModel* m0 = e->mem[L.idx[0]];
+    launch_surrogate_grp(e->d_members + L.base, int(L.idx.size()), par, m0->d_surr, m0->surr_norm, e->d_err, s);
+  }
   G(kGroupDIV, s);
   OB_TRY(tc_group_solve(L.solve, s));
   G(kGroupPROJ, s);
@@ -1196,6 +1214,8 @@ int ob_ensemble_create(ObModel* const* members, const float* dts, int n, ObEnsem
   if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&e->ev_done, cudaEventDisableTiming), "ensemble event");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_members, sizeof(MemberC) * n), "ensemble members");
   if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_lsfT, sizeof(double) * n), "ensemble members");
+  if (rc == OB_OK) rc = cuda_status(cudaMalloc(&e->d_err, sizeof(unsigned)), "ensemble error word");
+  if (rc == OB_OK) rc = cuda_status(cudaMemset(e->d_err, 0, sizeof(unsigned)), "ensemble error word");
   // every member's queued work (reset, uploads) completes before the ensemble's streams take over
   for (int i = 0; i < n && rc == OB_OK; i++) rc = cuda_status(cudaStreamSynchronize(members[i]->stream), "ensemble members");
   if (rc == OB_OK) {
@@ -1247,6 +1267,13 @@ int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms) {
 
 static int ens_check(ObEnsemble* e) {
   for (int l = 0; l < e->nlanes; l++) OB_TRY(tc_group_check(e->lane[l].solve));
+  unsigned h = 0;
+  cudaMemcpy(&h, e->d_err, sizeof(h), cudaMemcpyDeviceToHost);
+  if (h) {
+    cudaMemset(e->d_err, 0, sizeof(unsigned));
+    set_error("ensemble surrogate: a tensor-core pipeline wait timed out (code %u)", h);
+    return OB_ERR_TIMEOUT;
+  }
   return OB_OK;
 }
 

@@ -108,6 +108,7 @@ struct MemberC {
   Uni U;
   Fields F;
   double* lsfT;  // model time of the member's last LSF pass (device copy of the host's bookkeeping)
+  int micro;     // microphysics mode of the step (0 the scheme, 2 the surrogate)
 };
 constexpr float T0K = 273.15f;
 constexpr double CPDd = 1005.7, RVCd = 461.5, LVCd = 2.501e6, LFCd = 3.337e5, LSCd = 2.834e6;

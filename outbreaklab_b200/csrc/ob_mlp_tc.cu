@@ -104,7 +104,11 @@ __device__ __forceinline__ void issue_layer(uint32_t tacc, uint32_t a_base, uint
   tc::mma_commit(bar);
 }
 
-__global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, int par, Infer net, Norm nm, unsigned int* err) {
+// The inference of the queued cells of one model, or of several (an ensemble's grouped step: the members' queues are
+// taken one after another, their tiles dealt round-robin to the CTAs' two groups as one sequence).
+template <bool GROUP>
+__device__ __forceinline__ void surrogate_run(const MemberC* __restrict__ members, int nmem, const Grid& g0, const Uni& U0,
+                                              const Fields& F0, int par, const Infer& net, const Norm& nm, unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* wimg = smem;
@@ -132,110 +136,122 @@ __global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, i
   const uint32_t thid = *tmem_slot + uint32_t(grp * 256), tout = thid + 128;
   const uint32_t tbase = thid + (uint32_t((warp & 3) * 32) << 16);
   const uint32_t a_s = tc::smem_u32(act), w_s = tc::smem_u32(wimg);
-  const unsigned count = min(*F.mlp_count, F.mlp_cap);
-  const unsigned* list = reinterpret_cast<const unsigned*>(F.mlp_buf);
-  const float dt = U.step.x, tscale = nm.dt > 0.f ? dt / nm.dt : 1.f;
   uint32_t phase = 0;
   // a timed-out wait marks this thread failed: it stops waiting and writing but keeps every group barrier, so the
   // kernel still ends (the host reads the error word)
   bool failed = false;
-  const int ntiles = int((count + 127) / 128);
-  for (int t = blockIdx.x * 2 + grp; t < ntiles; t += gridDim.x * 2) {
-    const unsigned ci = unsigned(t) * 128u + unsigned(row);
-    const bool valid = ci < count;
-    const int o = valid ? int(list[ci]) : 0;
-    const int k = o / g.plane, rem = o - k * g.plane, j = rem / g.px, i = rem - j * g.px;
-    const float4 A = bsA(F.B, g.nz, k), Bb = bsB(F.B, g.nz, k);
-    const float pi0 = Bb.x, p0 = Bb.y, rho = A.z;
-    MCell m{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float ni = 0.f, w = 0.f;
-    if (valid) {
-      m.T = F.V[par][3][o] * pi0;
-      m.qv = F.Q[0][0][o]; m.qc = F.Q[0][1][o]; m.qi = F.Q[0][2][o]; m.qr = F.Q[0][3][o];
-      m.qs = F.Q[0][4][o]; m.qg = F.Q[0][5][o]; m.nr = F.Q[0][6][o];
-      ni = F.Q[0][7][o];
-      w = F.V[1 - par][2][o];
-    }
-    const float raw[NIN] = {m.T, p0, rho, m.qv, m.qc, m.qr, m.qi, m.qs, m.qg, m.nr, ni, w};
-    bool inrange = true;
-    __align__(16) __nv_bfloat16 xb[16];
-#pragma unroll
-    for (int e = 0; e < NIN; e++) {
-      inrange = inrange && raw[e] >= nm.in_lo[e] && raw[e] <= nm.in_hi[e];
-      xb[e] = __float2bfloat16_rn((feature(e, raw[e]) - nm.in_mean[e]) * nm.in_scale[e]);
-    }
-#pragma unroll
-    for (int e = NIN; e < 16; e++) xb[e] = __float2bfloat16_rn(0.f);
-    *reinterpret_cast<uint4*>(act + swz(row, 0, 128)) = *reinterpret_cast<const uint4*>(xb);
-    *reinterpret_cast<uint4*>(act + swz(row, 8, 128)) = *reinterpret_cast<const uint4*>(xb + 8);
-    // layers 1-3 into the hidden accumulator, layer 4 into the output accumulator
-#pragma unroll 1
-    for (int layer = 0; layer < 4; layer++) {
-      fence_async_smem();
-      tc::tc_fence_before();
-      group_sync(1 + grp);
-      if (row == 0 && !failed) {
+  const int start = blockIdx.x * 2 + grp, stride = gridDim.x * 2;
+  int base = 0;
+  for (int mi = 0; mi < (GROUP ? nmem : 1); mi++) {
+    const Grid& g = GROUP ? members[mi].g : g0;
+    const Uni& U = GROUP ? members[mi].U : U0;
+    const Fields& F = GROUP ? members[mi].F : F0;
+    const unsigned count = min(*F.mlp_count, F.mlp_cap);
+    const unsigned* list = reinterpret_cast<const unsigned*>(F.mlp_buf);
+    const float dt = U.step.x, tscale = nm.dt > 0.f ? dt / nm.dt : 1.f;
+    const int ntiles = int((count + 127) / 128);
+    int t0 = start;
+    if (t0 < base) t0 += (base - t0 + stride - 1) / stride * stride;
+    for (int tt = t0; tt < base + ntiles; tt += stride) {
+      const int t = tt - base;
+      const unsigned ci = unsigned(t) * 128u + unsigned(row);
+      const bool valid = ci < count;
+      const int o = valid ? int(list[ci]) : 0;
+      const int k = o / g.plane, rem = o - k * g.plane, j = rem / g.px, i = rem - j * g.px;
+      const float4 A = bsA(F.B, g.nz, k), Bb = bsB(F.B, g.nz, k);
+      const float pi0 = Bb.x, p0 = Bb.y, rho = A.z;
+      MCell m{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float ni = 0.f, w = 0.f;
+      if (valid) {
+        m.T = F.V[par][3][o] * pi0;
+        m.qv = F.Q[0][0][o]; m.qc = F.Q[0][1][o]; m.qi = F.Q[0][2][o]; m.qr = F.Q[0][3][o];
+        m.qs = F.Q[0][4][o]; m.qg = F.Q[0][5][o]; m.nr = F.Q[0][6][o];
+        ni = F.Q[0][7][o];
+        w = F.V[1 - par][2][o];
+      }
+      const float raw[NIN] = {m.T, p0, rho, m.qv, m.qc, m.qr, m.qi, m.qs, m.qg, m.nr, ni, w};
+      bool inrange = true;
+      __align__(16) __nv_bfloat16 xb[16];
+  #pragma unroll
+      for (int e = 0; e < NIN; e++) {
+        inrange = inrange && raw[e] >= nm.in_lo[e] && raw[e] <= nm.in_hi[e];
+        xb[e] = __float2bfloat16_rn((feature(e, raw[e]) - nm.in_mean[e]) * nm.in_scale[e]);
+      }
+  #pragma unroll
+      for (int e = NIN; e < 16; e++) xb[e] = __float2bfloat16_rn(0.f);
+      *reinterpret_cast<uint4*>(act + swz(row, 0, 128)) = *reinterpret_cast<const uint4*>(xb);
+      *reinterpret_cast<uint4*>(act + swz(row, 8, 128)) = *reinterpret_cast<const uint4*>(xb + 8);
+      // layers 1-3 into the hidden accumulator, layer 4 into the output accumulator
+  #pragma unroll 1
+      for (int layer = 0; layer < 4; layer++) {
+        fence_async_smem();
+        tc::tc_fence_before();
+        group_sync(1 + grp);
+        if (row == 0 && !failed) {
+          tc::tc_fence_after();
+          if (layer == 0) issue_layer(thid, a_s, w_s + OFF_W1, NH, 16, NH, &bars[grp]);
+          else if (layer < 3) issue_layer(thid, a_s, w_s + (layer == 1 ? OFF_W2 : OFF_W3), NH, NH, NH, &bars[grp]);
+          else issue_layer(tout, a_s, w_s + OFF_W4, W4_ROWS, NH, W4_ROWS, &bars[grp]);
+        }
+        if (!failed) failed = !tc::mbar_wait(&bars[grp], phase, err, 16u);
+        phase ^= 1u;
         tc::tc_fence_after();
-        if (layer == 0) issue_layer(thid, a_s, w_s + OFF_W1, NH, 16, NH, &bars[grp]);
-        else if (layer < 3) issue_layer(thid, a_s, w_s + (layer == 1 ? OFF_W2 : OFF_W3), NH, NH, NH, &bars[grp]);
-        else issue_layer(tout, a_s, w_s + OFF_W4, W4_ROWS, NH, W4_ROWS, &bars[grp]);
+        if (layer < 3) hidden_to_smem(tbase, net.bias + layer * NH, act, row);
       }
-      if (!failed) failed = !tc::mbar_wait(&bars[grp], phase, err, 16u);
-      phase ^= 1u;
-      tc::tc_fence_after();
-      if (layer < 3) hidden_to_smem(tbase, net.bias + layer * NH, act, row);
-    }
-    float y[16];
-    tmem_ld16(tbase + 128, y);
-    if (!valid || failed) continue;
-    const float rs = __ldg(F.spz + 4 * k + 2);
-    const float sl = fmaxf(__ldg(F.slx + 2 * i + 1), __ldg(F.sly + 2 * j + 1));
-    bool finite = true;
-#pragma unroll
-    for (int e = 0; e < NLOSS; e++) finite = finite && isfinite(y[e]);
-    if (inrange && finite) {
-      float d[NLOSS];
-#pragma unroll
-      for (int e = 0; e < NLOSS; e++) d[e] = (y[e] + __ldg(net.bias + 3 * NH + e)) * nm.out_scale[e] * tscale;
-      // no species appears from below the network's noise floor; no species loses more than it holds; the six
-      // water tendencies sum to zero (total water), by shrinking whichever side, gains or losses, is larger
-      float q[6] = {m.qv, m.qc, m.qi, m.qr, m.qs, m.qg};
-      float gain = 0.f, loss = 0.f;
-#pragma unroll
-      for (int s = 0; s < 6; s++) {
-        if (q[s] == 0.f && d[1 + s] < kNewSpeciesFloor) d[1 + s] = 0.f;
-        d[1 + s] = fmaxf(d[1 + s], -q[s]);
-        if (d[1 + s] > 0.f) gain += d[1 + s]; else loss -= d[1 + s];
+      float y[16];
+      tmem_ld16(tbase + 128, y);
+      if (!valid || failed) continue;
+      const float rs = __ldg(F.spz + 4 * k + 2);
+      const float sl = fmaxf(__ldg(F.slx + 2 * i + 1), __ldg(F.sly + 2 * j + 1));
+      bool finite = true;
+  #pragma unroll
+      for (int e = 0; e < NLOSS; e++) finite = finite && isfinite(y[e]);
+      if (inrange && finite) {
+        float d[NLOSS];
+  #pragma unroll
+        for (int e = 0; e < NLOSS; e++) d[e] = (y[e] + __ldg(net.bias + 3 * NH + e)) * nm.out_scale[e] * tscale;
+        // no species appears from below the network's noise floor; no species loses more than it holds; the six
+        // water tendencies sum to zero (total water), by shrinking whichever side, gains or losses, is larger
+        float q[6] = {m.qv, m.qc, m.qi, m.qr, m.qs, m.qg};
+        float gain = 0.f, loss = 0.f;
+  #pragma unroll
+        for (int s = 0; s < 6; s++) {
+          if (q[s] == 0.f && d[1 + s] < kNewSpeciesFloor) d[1 + s] = 0.f;
+          d[1 + s] = fmaxf(d[1 + s], -q[s]);
+          if (d[1 + s] > 0.f) gain += d[1 + s]; else loss -= d[1 + s];
+        }
+        const float fg = gain > loss ? loss / gain : 1.f, fl = loss > gain ? gain / loss : 1.f;
+  #pragma unroll
+        for (int s = 0; s < 6; s++) q[s] += d[1 + s] * (d[1 + s] > 0.f ? fg : fl);
+        m.qv = q[0]; m.qc = q[1]; m.qi = q[2]; m.qr = q[3]; m.qs = q[4]; m.qg = q[5];
+        m.T += d[0];
+        // the scheme's own bounds on the rain number (model.js:874-884): none without rain, else within the
+        // mass-weighted limits
+        const float nr = m.nr + d[7];
+        m.nr = m.qr > 1e-9f ? clampf(nr, m.qr * 3.183e5f, m.qr * 3.183e11f) : 0.f;
+        // the saturation adjustment is thermodynamic equilibrium, not a process rate: it runs as in the scheme
+        sat_adjust(p0, m);
+      } else {
+        micro_plain(U, dt, p0, rho, rs, m);
+        atomicAdd(F.mlp_count + 1, 1u);  // fallbacks of this step
       }
-      const float fg = gain > loss ? loss / gain : 1.f, fl = loss > gain ? gain / loss : 1.f;
-#pragma unroll
-      for (int s = 0; s < 6; s++) q[s] += d[1 + s] * (d[1 + s] > 0.f ? fg : fl);
-      m.qv = q[0]; m.qc = q[1]; m.qi = q[2]; m.qr = q[3]; m.qs = q[4]; m.qg = q[5];
-      m.T += d[0];
-      // the scheme's own bounds on the rain number (model.js:874-884): none without rain, else within the
-      // mass-weighted limits
-      const float nr = m.nr + d[7];
-      m.nr = m.qr > 1e-9f ? clampf(nr, m.qr * 3.183e5f, m.qr * 3.183e11f) : 0.f;
-      // the saturation adjustment is thermodynamic equilibrium, not a process rate: it runs as in the scheme
-      sat_adjust(p0, m);
-    } else {
-      micro_plain(U, dt, p0, rho, rs, m);
-      atomicAdd(F.mlp_count + 1, 1u);  // fallbacks of this step
+      const float keep = 1.f / (1.f + 2.f * dt * sl);
+      float th = m.T / pi0;
+      if (!(th == th)) {
+        th = A.x;
+        atomicAdd(F.flags, 1u);
+      }
+      F.V[par][3][o] = th;
+      F.Q[0][0][o] = fmaxf(m.qv, 0.f);
+      F.Q[0][1][o] = fmaxf(m.qc * keep, 0.f);
+      F.Q[0][2][o] = fmaxf(m.qi * keep, 0.f);
+      F.Q[0][3][o] = fmaxf(m.qr * keep, 0.f);
+      F.Q[0][4][o] = fmaxf(m.qs * keep, 0.f);
+      F.Q[0][5][o] = fmaxf(m.qg * keep, 0.f);
+      F.Q[0][6][o] = fmaxf(m.nr * keep, 0.f);
+  
     }
-    const float keep = 1.f / (1.f + 2.f * dt * sl);
-    float th = m.T / pi0;
-    if (!(th == th)) {
-      th = A.x;
-      atomicAdd(F.flags, 1u);
-    }
-    F.V[par][3][o] = th;
-    F.Q[0][0][o] = fmaxf(m.qv, 0.f);
-    F.Q[0][1][o] = fmaxf(m.qc * keep, 0.f);
-    F.Q[0][2][o] = fmaxf(m.qi * keep, 0.f);
-    F.Q[0][3][o] = fmaxf(m.qr * keep, 0.f);
-    F.Q[0][4][o] = fmaxf(m.qs * keep, 0.f);
-    F.Q[0][5][o] = fmaxf(m.qg * keep, 0.f);
-    F.Q[0][6][o] = fmaxf(m.nr * keep, 0.f);
+    base += ntiles;
   }
   tc::tc_fence_before();
   __syncthreads();
@@ -243,6 +259,14 @@ __global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, i
     tc::tc_fence_after();
     tc::tmem_dealloc(*tmem_slot, 512);
   }
+}
+
+__global__ void __launch_bounds__(256, 1) k_surrogate(Grid g, Uni U, Fields F, int par, Infer net, Norm nm, unsigned int* err) {
+  surrogate_run<false>(nullptr, 1, g, U, F, par, net, nm, err);
+}
+__global__ void __launch_bounds__(256, 1) k_surrogate_grp(const MemberC* __restrict__ members, int n, int par, Infer net, Norm nm,
+                                                          unsigned int* err) {
+  surrogate_run<true>(members, n, members[0].g, members[0].U, members[0].F, par, net, nm, err);
 }
 
 }  // namespace mlp
@@ -307,6 +331,21 @@ void launch_surrogate(const Grid& g, const Uni& U, const Fields& F, int par, con
   }
   Infer net{reinterpret_cast<const uint4*>(d_image), reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(d_image) + WIMG_BYTES)};
   k_surrogate<<<nsm, 256, SMEM_INFER, s>>>(g, U, F, par, net, nm, err);
+}
+
+void launch_surrogate_grp(const MemberC* d_members, int n, int par, const void* d_image, const mlp::Norm& nm, unsigned int* err,
+                          cudaStream_t s) {
+  using namespace mlp;
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm <= 0) nsm = 148;
+    cudaFuncSetAttribute(k_surrogate_grp, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_INFER);
+  }
+  Infer net{reinterpret_cast<const uint4*>(d_image), reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(d_image) + WIMG_BYTES)};
+  k_surrogate_grp<<<nsm, 256, SMEM_INFER, s>>>(d_members, n, par, net, nm, err);
 }
 
 }  // namespace ob

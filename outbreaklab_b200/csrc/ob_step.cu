@@ -213,6 +213,10 @@ __global__ void k_ci_grp(const uint2* __restrict__ map, int par) {
     const double t = *c_members[mem].F.clock;
     double* t0 = c_members[mem].lsfT;
     if (t - *t0 >= 60.0 || t == 0.0) *t0 = t;
+    if (c_members[mem].micro == kMicroSurrogate) {  // this step's surrogate queue and fallback count start empty
+      c_members[mem].F.mlp_count[0] = 0u;
+      c_members[mem].F.mlp_count[1] = 0u;
+    }
   }
   ci_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
