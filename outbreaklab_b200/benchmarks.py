@@ -162,7 +162,8 @@ def ensemble(args):
     cases = E.draw_members(args.members, args.seed, steps=args.steps)
     mine = [cases[i] for i in E.plan_shards(cases, world)[rank]]
     if args.mode == "grouped":
-        local = E.run_grouped(mine, args.steps, args.warmup, tune=not args.no_tune)
+        local = E.run_grouped(mine, args.steps, args.warmup, tune=not args.no_tune,
+                              surrogate={} if args.surrogate else None)
     else:
         local = E.run(mine, args.steps, args.warmup)
     res = E.gather(local, dist)
@@ -171,7 +172,7 @@ def ensemble(args):
                     "n_gpus": world, "host_launch_ms_rank0": local["host_launch_ms"],
                     "device_ms_rank0": local["device_ms"], "nan_guard_count_rank0": local["nan_guard_count"],
                     "grids": [[c.nx, c.ny, c.nz, c.dx] for c in cases], "mode": args.mode})
-        for k in ("tiles", "tiles_source", "tune_ms", "lanes", "lane_step_ms", "launches_per_step"):
+        for k in ("tiles", "tiles_source", "tune_ms", "lanes", "lane_step_ms", "launches_per_step", "surrogate"):
             if k in local:
                 res[k + "_rank0"] = local[k]
         print(json.dumps(res), flush=True)
@@ -213,6 +214,7 @@ def main(argv=None):
     e.add_argument("--mode", choices=["grouped", "streams"], default="grouped",
                    help="grouped: one launch per pass over all members (ObEnsemble); streams: one stream per member")
     e.add_argument("--no-tune", action="store_true", help="grouped mode: default tiles, no autotuner")
+    e.add_argument("--surrogate", action="store_true", help="grouped mode: the members run the MLP microphysics surrogate")
     args = ap.parse_args(argv)
     {"solve": solve, "step": step, "surrogate": surrogate, "ensemble": ensemble}[args.cmd](args)
 

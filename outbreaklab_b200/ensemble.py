@@ -252,28 +252,63 @@ class Ensemble:
             self.h = None
 
 
+def train_surrogate(cases, rec_minutes=20.0, rate=0.3, pairs=20_000_000, train_steps=6000, batch=16384, lr=1e-3, seed=7,
+                    margin=0.05):
+    """The members' learned microphysics: pairs recorded from a plain Thompson run of a donor member (a fresh copy of
+    the first 1-km member, or of the first member), normalised with a margin on the trusted input range, trained on
+    the GPU. The network serves every member; its tendencies scale with each member's dt (the surrogate kernel's
+    dt ratio), the saturation adjustment after them does not need to."""
+    from . import model as M, surrogate as S
+    donor = next((c for c in cases if c.dx == 1000.0), cases[0])
+    net = S.MicroSurrogate(seed=seed)
+    net.reserve(pairs)
+    m, _ = M.setup_case(donor)
+    t0 = time.time()
+    S.record(m, net, max(1, int(rec_minutes * 60 / donor.dt)), donor.dt, rate)
+    m.sync()
+    m.destroy()
+    info = {"donor": [donor.nx, donor.ny, donor.nz, donor.dx], "record_s": time.time() - t0, "pairs": net.count()}
+    net.fit_norm(donor.dt, margin=margin)
+    t0 = time.time()
+    losses = [net.train(batch, max(1, int(train_steps * frac)), l) for l, frac in ((lr, 0.6), (lr * 0.3, 0.25), (lr * 0.1, 0.15))]
+    info.update({"train_s": time.time() - t0, "train_loss": losses})
+    return net, info
+
+
 def run_grouped(cases, steps: int = 50, warmup: int = 3, tune: bool = True, cache: TileCache = None, reps: int = 5,
-                lanes=None):
+                lanes=None, surrogate=None):
     """Steps every member `steps` times as one ObEnsemble. Tiles and the lane count come from the cache for this
     member set, else from the autotuner (tiles) and from timing a few warm-up steps with one and with two lanes (the
-    lane count changes no result, only which launches overlap); both are then cached. Returns the metrics of this
-    process: cell-steps per second over the device time of the timed steps, the ensemble step's latency percentiles
-    (per-step CUDA events), the tiles and lanes used."""
+    lane count changes no result, only which launches overlap); both are then cached. surrogate: None (the
+    Thompson-style scheme as it is) or the keyword arguments of train_surrogate (the members then run the learned
+    microphysics). Returns the metrics of this process: cell-steps per second over the device time of the timed
+    steps, the ensemble step's latency percentiles (per-step CUDA events), the tiles and lanes used."""
     import torch
     from . import _native as N, model as M
+    net, sinfo = (None, None)
+    if surrogate is not None:
+        net, sinfo = train_surrogate(cases, **surrogate)
     models = []
     for c in cases:
         m, _ = M.setup_case(c)
         if m.solver < 1:
             m.set_solver(2)
+        if net is not None:
+            m.set_surrogate(net)
         models.append(m)
     ens = Ensemble(models, [c.dt for c in cases])
     try:
-        return _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes)
+        out = _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes)
+        if net is not None:
+            q = [m.surrogate_stats() for m in models]
+            out["surrogate"] = dict(sinfo, queued_last_step=int(sum(a for a, _ in q)), fallbacks_last_step=int(sum(b for _, b in q)))
+        return out
     finally:
         ens.destroy()
         for m in models:
             m.destroy()
+        if net is not None:
+            net.close()
 
 
 def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes):
@@ -322,5 +357,5 @@ def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes):
            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
            "latency_ms_all": lat.tolist(), "nan_guard_count": int(sum(m.nan_count for m in models)),
            "tiles": ens.tiles(), "tiles_source": tiles_src, "tune_ms": tune_ms, "lanes": ens.lanes, "lane_step_ms": lane_ms,
-           "launches_per_step": ens.lanes * (11 + (11 if models[0].solver == 2 else 5))}
+           "launches_per_step": ens.lanes * (11 + (11 if models[0].solver == 2 else 5) + (1 if getattr(models[0], "surrogate", False) else 0))}
     return out

@@ -204,6 +204,7 @@ class RegionalModel:
         """From the next step on, the microphysics of queued cells runs through a copy of net's current weights on
         the tensor cores (None: the plain scheme)."""
         N.check(N.lib().ob_model_set_surrogate(self.h, net.h if net is not None else None))
+        self.surrogate = net is not None
 
     def surrogate_stats(self):
         """(cells the last step queued for the surrogate, how many of them fell back to the scheme)."""
