@@ -283,7 +283,8 @@ def run_ours(args, rank, world):
                        "cells": case.cells, "parallelism": "replicas" if world > 1 else "single domain",
                        "l2": "state %.1f GB > 126 MB L2 (no flush needed)" % (2.8 * case.cells / 16384000),
                        "solver": {0: "fp32 SIMT DST", 1: "bf16x3 tensor-core DST",
-                                  2: "bf16x3 tensor-core DST + 1 refinement sweep"}[m.solver]},
+                                  2: "bf16x3 tensor-core DST + 1 refinement sweep",
+                                  3: "bf16x3 tensor-core DST + 1 plain-bf16 refinement sweep"}[m.solver]},
             "pass_ms": {k: round(v, 4) for k, v in pass_ms.items()},
             "step_hbm": {"algorithmic_bytes": step_bytes, "gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac_of_measured_peak": step_bytes / (step_ms / 1000.0) / 1e9 / hbm},

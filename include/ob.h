@@ -196,7 +196,8 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
  * launches every kernel directly. Results are identical either way. */
 int ob_model_set_graphs(ObModel* m, int on);
 /* pressure-solve precision of the model: 0 = fp32 SIMT transforms (the reference's arithmetic), 1 = bf16x3
- * tensor-core transforms, 2 = bf16x3 + one refinement sweep (the default where nz is 16, 40 or 80).
+ * tensor-core transforms, 2 = bf16x3 + one bf16x3 refinement sweep (the default where nz is 16, 40 or 80),
+ * 3 = bf16x3 + one plain-bf16 refinement sweep.
  * No counterpart in the reference. */
 int ob_model_set_solver(ObModel* m, int precision);
 int ob_model_solver(ObModel* m);
@@ -206,7 +207,7 @@ void* ob_model_stream(ObModel* m);
 /* ---- PoissonDirect (solver.js:105-165) ---- */
 /* replaces new PoissonDirect(nx, ny, nz, dx, dz) (solver.js:106-137); precision 0 = FP32 SIMT transforms,
  * 1 = bf16x3 tensor-core transforms (FP32 accumulate), 2 = the same plus one iterative-refinement sweep on the
- * FP64-accumulated residual (precisions 1 and 2 need nz in {16, 40, 80}) */
+ * FP64-accumulated residual, 3 = that sweep in plain bf16 (precisions 1 to 3 need nz in {16, 40, 80}) */
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out);
 int ob_poisson_destroy(ObPoisson* p);
 /* replaces setDensity (solver.js:139-146): rhoC[nz] at centres, rhoW[nz+1] at bottom faces */

@@ -800,7 +800,7 @@ int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks) 
 }
 
 int ob_model_set_solver(ObModel* m, int precision) {
-  if (!m || precision < 0 || precision > 2) { set_error("ob_model_set_solver: precision must be 0, 1 or 2"); return OB_ERR_INVALID; }
+  if (!m || precision < 0 || precision > 3) { set_error("ob_model_set_solver: precision must be 0, 1, 2 or 3"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
   if (precision >= 1 && g.nz != 16 && g.nz != 40 && g.nz != 80) {
     set_error("ob_model_set_solver: the tensor-core solve supports nz in {16, 40, 80}");
@@ -1407,7 +1407,7 @@ struct ObPoisson {
 };
 
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out) {
-  if (!out || precision < 0 || precision > 2) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
+  if (!out || precision < 0 || precision > 3) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
   *out = nullptr;
   ObPoisson* p = new ObPoisson();
   int rc = p->plan.create(nx, ny, nz, dx, dz, precision);

@@ -116,7 +116,9 @@ struct GroupProblems {
 // DST matrix, N x K, K-major) are each given as bf16 hi/lo planes by TMA maps; tiles of BM x BN are taken round-robin
 // (n fastest, so that CTAs working at the same time share the field tile through L2). The tiles come from one problem
 // (one model's transform) or from a list of problems (the same transform of every member of an ensemble).
-template <int MODE, class Src>
+// ONE: the correction pass of the refined solve, in plain bf16 (the hi planes alone, one MMA per k-step): its input
+// is the residual of a bf16x3 pass, and the correction needs only bf16 accuracy of itself
+template <int MODE, bool ONE, class Src>
 __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -166,7 +168,7 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         TileInfo ti;
         src.tile(t, ti);
-        const uint32_t bytes = uint32_t(2 * A_TILE + 2 * ti.BN * BK * 2);
+        const uint32_t bytes = ONE ? uint32_t(A_TILE + ti.BN * BK * 2) : uint32_t(2 * A_TILE + 2 * ti.BN * BK * 2);
         const int nk = (ti.K + BK - 1) / BK;
         for (int kt = 0; kt < nk; kt++, g++) {
           const int s = g % STAGES;
@@ -175,9 +177,9 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
           uint8_t* st = smem + s * STAGE_BYTES;
           tc::mbar_expect_tx(&full[s], bytes);
           tc::tma_load_2d(st, ti.f_hi, &full[s], kt * BK, ti.m0);
-          tc::tma_load_2d(st + A_TILE, ti.f_lo, &full[s], kt * BK, ti.m0);
+          if (!ONE) tc::tma_load_2d(st + A_TILE, ti.f_lo, &full[s], kt * BK, ti.m0);
           tc::tma_load_2d(st + 2 * A_TILE, ti.q_hi, &full[s], kt * BK, ti.n0);
-          tc::tma_load_2d(st + 2 * A_TILE + B_TILE, ti.q_lo, &full[s], kt * BK, ti.n0);
+          if (!ONE) tc::tma_load_2d(st + 2 * A_TILE + B_TILE, ti.q_lo, &full[s], kt * BK, ti.n0);
         }
       }
     }
@@ -208,8 +210,10 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
           for (int kk = 0; kk < ksub; kk++) {
             const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
             tc::mma_bf16(acc, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
-            tc::mma_bf16(acc, dah + o, dbl + o, idesc, 1u);
-            tc::mma_bf16(acc, dal + o, dbh + o, idesc, 1u);
+            if (!ONE) {
+              tc::mma_bf16(acc, dah + o, dbl + o, idesc, 1u);
+              tc::mma_bf16(acc, dal + o, dbh + o, idesc, 1u);
+            }
           }
           tc::mma_commit(&empty[s]);
         }
@@ -248,6 +252,8 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
                 const long a = base + long(c0 + c) * out.ld;
                 if (MODE == OUT_T_F32) {
                   out.f[a] = v[c];
+                } else if (ONE) {  // the next transform of a plain-bf16 pass reads the hi plane alone
+                  out.hi[a] = __float2bfloat16_rn(v[c]);
                 } else {
                   __nv_bfloat16 h, l;
                   tc::split_bf16(v[c], h, l);
@@ -295,21 +301,21 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   }
 }
 
-template <int MODE>
+template <int MODE, bool ONE = false>
 __global__ void __launch_bounds__(kThreads, 1)
     k_dst_tc(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
              const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
              unsigned int* err) {
   const int ntn = (out.N + BN - 1) / BN;
   const OneProblem src{&tF_hi, &tF_lo, &tQ_hi, &tQ_lo, K, BN, ntn, ((out.M + BM - 1) / BM) * ntn, out};
-  dst_tc_run<MODE>(src, err);
+  dst_tc_run<MODE, ONE>(src, err);
 }
 
-template <int MODE>
+template <int MODE, bool ONE = false>
 __global__ void __launch_bounds__(kThreads, 1) k_dst_tc_grp(const GemmProb* __restrict__ probs, const int* __restrict__ start, int n,
                                                             unsigned int* err) {
   const GroupProblems src{probs, start, n};
-  dst_tc_run<MODE>(src, err);
+  dst_tc_run<MODE, ONE>(src, err);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -555,6 +561,12 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     attr = true;
   }
 }
@@ -610,7 +622,7 @@ int PoissonPlan::tc_create() {
             al((void**)&T->rx_hi, nsx * 2) && al((void**)&T->rx_lo, nsx * 2) &&
             al((void**)&T->sy_hi, nsy * 2) && al((void**)&T->sy_lo, nsy * 2) && al((void**)&T->t2, size_t(nz) * nx * ny * 4) &&
             al((void**)&T->low, size_t(8) * nz * 8) && al((void**)&T->err, 16);
-  if (ok && precision == 2) ok = al((void**)&T->rr_hi, nsx * 2) && al((void**)&T->rr_lo, nsx * 2);
+  if (ok && precision >= 2) ok = al((void**)&T->rr_hi, nsx * 2) && al((void**)&T->rr_lo, nsx * 2);
   if (!ok) {
     set_error("poisson: out of device memory for the tensor-core path");
     return OB_ERR_OOM;
@@ -647,7 +659,7 @@ int PoissonPlan::tc_create() {
   // A operands, planes stacked: S_x and the split rhs [nz * ny][nx] pitch ldx; S_y [nz * nx][ny] pitch ldy
   ok = ok && make_map_2d(&T->Fx[0], T->sx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fx[1], T->sx_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fr[0], T->rx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fr[1], T->rx_lo, long(nz) * ny, nx, T->ldx, BM);
-  if (precision == 2)
+  if (precision >= 2)
     ok = ok && make_map_2d(&T->Frr[0], T->rr_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Frr[1], T->rr_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fy[0], T->sy_hi, long(nz) * nx, ny, T->ldy, BM) && make_map_2d(&T->Fy[1], T->sy_lo, long(nz) * nx, ny, T->ldy, BM);
   if (!ok) {
@@ -697,20 +709,24 @@ void PoissonPlan::tc_destroy() {
   tc = nullptr;
 }
 
-template <int MODE>
+template <int MODE, bool ONE = false>
 static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn, const TcOut& o, unsigned int* err, cudaStream_t s) {
   const int tiles = ((o.M + BM - 1) / BM) * ((o.N + bn - 1) / bn);
-  k_dst_tc<MODE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
+  k_dst_tc<MODE, ONE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
 }
 
 // the four transforms and the tridiagonals from a split right-hand side (rx, or the residual rr when add) to phi
 // (stored, or added when add)
-static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s) {
+static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s,
+                    bool one = false) {
   const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const TcOut sy{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, t2{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny};
   // X-fwd: field rows (k, j), K = i, outputs l  -> S_y[k][l][j]
-  launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, TcOut{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, T->err, s);
+  if (one) launch_tc<OUT_T_BF16X2, true>(T->Frr, T->Q[0], nx, T->bnx, sy, T->err, s);
+  else launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, sy, T->err, s);
   // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
-  launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, T->err, s);
+  if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
+  else launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
   // tridiagonals -> S_y[k][l][m]
   switch (nz) {
     case 16: k_tri_tc<16><<<dim3((nx + 31) / 32, (ny + tri_tm<16>() - 1) / tri_tm<16>()), dim3(32, tri_tm<16>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
@@ -718,28 +734,33 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
     default: k_tri_tc<80><<<dim3((nx + 31) / 32, (ny + tri_tm<80>() - 1) / tri_tm<80>()), dim3(32, tri_tm<80>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
   }
   // Y-inv: field rows (k, l), K = m, outputs j  -> S_x[k][j][l]
-  launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny}, T->err, s);
+  const TcOut sx{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny};
+  if (one) launch_tc<OUT_T_BF16X2, true>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s);
+  else launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s);
   // X-inv: field rows (k, j), K = l, outputs i  -> phi[k][j][i]
   const TcOut o{nullptr, nullptr, phi, nx, ny, nz * ny, nx};
-  if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
+  if (one) launch_tc<OUT_R_F32_ADD, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
+  else if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
   else launch_tc<OUT_R_F32>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
 }
 
-// precision 1: one bf16x3 pass; precision 2: a second pass on the FP64-accumulated residual (iterative refinement).
+// precision 1: one bf16x3 pass; precision 2: a second bf16x3 pass on the FP64-accumulated residual (iterative
+// refinement); precision 3: the second pass in plain bf16 (the correction is ~5e-4 of the solution, so bf16 accuracy
+// of it leaves an error near 5e-4 x 4e-3 of the solution).
 // rhs: the fp32 right-hand side (nx*ny*nz), needed by precision 2 and by either when the split is not pre-made
 // (presplit: the model's divergence pass writes the split into rx itself).
 int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
   TcPlan* T = static_cast<TcPlan*>(tc);
   if (!T) { set_error("poisson: tensor-core plan missing"); return OB_ERR_INVALID; }
   if (nz != 16 && nz != 40 && nz != 80) { set_error("poisson: the tensor-core path supports nz in {16, 40, 80}"); return OB_ERR_INVALID; }
-  if (!presplit || precision == 2) {
+  if (!presplit || precision >= 2) {
     if (!rhs) { set_error("poisson: right-hand side missing"); return OB_ERR_INVALID; }
   }
   if (!presplit) k_split_rows<<<1184, 256, 0, s>>>(rhs, long(nz) * ny, nx, T->rx_hi, T->rx_lo, int(T->ldx));
   tc_pass(*this, T, lam, zop, phi, false, s);
-  if (precision == 2) {
+  if (precision >= 2) {
     k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rr_hi, T->rr_lo, int(T->ldx));
-    tc_pass(*this, T, lam, zop, phi, true, s);
+    tc_pass(*this, T, lam, zop, phi, true, s, precision == 3);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -805,7 +826,7 @@ static int tc_group_build(TcGroup* G) {
     const int bnx = pick_bn(nx, G->bn_cap), bny = pick_bn(ny, G->bn_cap);
     // the fifth list is the x-fwd transform again, reading the residual (refined solve only)
     const int bn[NT] = {bnx, bny, bny, bnx, bnx}, K[NT] = {nx, ny, ny, nx, nx}, qi[NT] = {0, 1, 2, 3, 0};
-    const CUtensorMap* F[NT] = {T->Fr, T->Fy, T->Fy, T->Fx, G->precision == 2 ? T->Frr : T->Fr};
+    const CUtensorMap* F[NT] = {T->Fr, T->Fy, T->Fy, T->Fx, G->precision >= 2 ? T->Frr : T->Fr};
     const TcOut xfwd{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx};
     const TcOut out[NT] = {xfwd, TcOut{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny}, TcOut{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny},
                            TcOut{nullptr, nullptr, G->phi[i], nx, ny, nz * ny, nx}, xfwd};
@@ -882,7 +903,7 @@ int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* c
       tc_group_destroy(G);
       return OB_ERR_INVALID;
     }
-    if (G->precision == 2 && !rhs[i]) {
+    if (G->precision >= 2 && !rhs[i]) {
       set_error("ensemble solve: member %d has no fp32 right-hand side for the refinement", i);
       tc_group_destroy(G);
       return OB_ERR_INVALID;
@@ -928,33 +949,43 @@ int tc_group_set_cap(TcGroup* G, int bn_cap) {
 int tc_group_cap(const TcGroup* G) { return G->bn_cap; }
 void tc_group_set_ctas(TcGroup* G, int ctas) { G->ctas = ctas > 0 ? ctas : 0; }
 
-template <int MODE>
+template <int MODE, bool ONE = false>
 static void launch_tc_grp(const TcGroup* G, int t, cudaStream_t s) {
   if (G->tiles[t] < 1) return;
-  k_dst_tc_grp<MODE><<<std::min(G->tiles[t], G->ctas ? G->ctas : num_sms()), kThreads, SMEM_BYTES, s>>>(G->d_probs + size_t(t) * G->n,
+  k_dst_tc_grp<MODE, ONE><<<std::min(G->tiles[t], G->ctas ? G->ctas : num_sms()), kThreads, SMEM_BYTES, s>>>(G->d_probs + size_t(t) * G->n,
                                                                                      G->d_start + size_t(t) * (G->n + 1), G->n, G->err);
 }
 
-static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s) {
+static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one = false) {
   const int n = G->n;
-  launch_tc_grp<OUT_T_BF16X2>(G, add ? 4 : 0, s);
-  launch_tc_grp<OUT_T_F32>(G, 1, s);
+  if (one) {
+    launch_tc_grp<OUT_T_BF16X2, true>(G, 4, s);
+    launch_tc_grp<OUT_T_F32, true>(G, 1, s);
+  } else {
+    launch_tc_grp<OUT_T_BF16X2>(G, add ? 4 : 0, s);
+    launch_tc_grp<OUT_T_F32>(G, 1, s);
+  }
   const int* ts = G->d_start + size_t(5) * (n + 1);
   switch (G->nz) {
     case 16: k_tri_tc_grp<16><<<G->tri_blocks, dim3(32, tri_tm<16>()), 0, s>>>(G->d_tri, ts, n); break;
     case 40: k_tri_tc_grp<40><<<G->tri_blocks, dim3(32, tri_tm<40>()), 0, s>>>(G->d_tri, ts, n); break;
     default: k_tri_tc_grp<80><<<G->tri_blocks, dim3(32, tri_tm<80>()), 0, s>>>(G->d_tri, ts, n); break;
   }
-  launch_tc_grp<OUT_T_BF16X2>(G, 2, s);
-  if (add) launch_tc_grp<OUT_R_F32_ADD>(G, 3, s);
-  else launch_tc_grp<OUT_R_F32>(G, 3, s);
+  if (one) {
+    launch_tc_grp<OUT_T_BF16X2, true>(G, 2, s);
+    launch_tc_grp<OUT_R_F32_ADD, true>(G, 3, s);
+  } else {
+    launch_tc_grp<OUT_T_BF16X2>(G, 2, s);
+    if (add) launch_tc_grp<OUT_R_F32_ADD>(G, 3, s);
+    else launch_tc_grp<OUT_R_F32>(G, 3, s);
+  }
 }
 
 int tc_group_solve(TcGroup* G, cudaStream_t s) {
   tc_group_pass(G, false, s);
-  if (G->precision == 2) {
+  if (G->precision >= 2) {
     k_resid_grp<<<dim3(G->res_blocks, 1, G->nz), 128, 0, s>>>(G->d_res, G->d_res_map);
-    tc_group_pass(G, true, s);
+    tc_group_pass(G, true, s, G->precision == 3);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -4,7 +4,8 @@
 //
 // Orthonormal DST-II in x and y (four dense transforms), one tridiagonal per horizontal mode (l, m) in z.
 //   precision 0: fp32 SIMT transforms (tiled GEMM, 64 x 64 tiles, fp32 FMA) — the reference's own precision;
-//   precision 1: bf16x3 tensor-core transforms (ob_dst_tc.cu) with fp32 accumulation.
+//   precision 1: bf16x3 tensor-core transforms (ob_dst_tc.cu) with fp32 accumulation; 2: plus a bf16x3
+//   refinement sweep on the FP64-accumulated residual; 3: that sweep in plain bf16.
 // The tridiagonals: fp32 Thomas with the forward-sweep coefficients in registers for every mode except the lowest
 // 2 x 2 modes, which are near-singular (Neumann in z, shift ~ -(pi/L)^2) and run in FP64.
 #include <cstdio>
