@@ -295,7 +295,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
     if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&m->ev_join[i], cudaEventDisableTiming), "event");
   }
   if (rc == OB_OK) rc = cuda_status(cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming), "event");
-  alloc((void**)&m->pool, fs * 39 * sizeof(float), "model fields");
+  alloc((void**)&m->pool, fs * 47 * sizeof(float), "model fields");
   alloc((void**)&m->d_B, size_t(nz + 1) * 8 * sizeof(float), "base state");
   alloc((void**)&m->d_bnd, size_t(OB_MAX_BOUNDS) * OB_BOUNDARY_FLOATS * sizeof(float), "boundaries");
   alloc((void**)&m->d_ci, size_t(OB_MAX_CI) * OB_CI_FLOATS * sizeof(float), "CI events");
@@ -320,7 +320,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, prec);
   if (rc != OB_OK) {
     if (rc == OB_ERR_OOM) {
-      const double gb = (fs * 39.0 * 4 + np * 4.0 * 5 + n2 * 200.0) / 1e9;
+      const double gb = (fs * 47.0 * 4 + np * 4.0 * 5 + n2 * 200.0) / 1e9;
       set_error("not enough GPU memory for this grid (it needs about %.1f GB)", gb);
     }
     model_free(m);
@@ -331,6 +331,8 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   for (int s = 0; s < 2; s++)
     for (int c = 0; c < 4; c++) m->F.V[s][c] = take();
   for (int c = 0; c < 4; c++) m->F.Vt[c] = take();
+  for (int c = 0; c < 4; c++) m->F.Vlo[c] = take();
+  for (int c = 0; c < 4; c++) m->F.Vhi[c] = take();
   for (int s = 0; s < 2; s++)
     for (int c = 0; c < 8; c++) m->F.Q[s][c] = take();
   for (int c = 0; c < 8; c++) m->F.Qt[c] = take();

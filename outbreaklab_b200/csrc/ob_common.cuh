@@ -37,6 +37,8 @@ struct Grid {
 struct Fields {
   float* V[2][4];   // (u, v, w, theta) ping-pong
   float* Vt[4];     // advection scratch (ADVV1 output)
+  float* Vlo[4];    // min and max of the 8 texels around each texel's departure point (ADVV1 output; the limiter
+  float* Vhi[4];    // of ADVV2 reads them instead of tracing and gathering the same 8 texels again)
   float* Q[2][8];   // (qv, qc, qi, qr, qs, qg, Nr, spare): slot 0 = state, slot 1 = after advection
   float* Qt[8];     // advection scratch (ADVQ1 output)
   float* aux[2];    // nu_h, nu_v
@@ -264,6 +266,27 @@ __device__ __forceinline__ float trilerp(const float* __restrict__ f, const Grid
 
 // the same filter where the trace is already clamped to the box, so that the floor index of every axis lies in
 // [-1, extent - 1]: then max(i0, 0) and min(i0 + 1, extent - 1) are the clamped corners (same texels, fewer bounds)
+// the same sample, and the min / max of its 8 texels (the MacCormack limiter's window at that point)
+__device__ __forceinline__ float trilerpB_mm(const float* __restrict__ f, const Grid& g, int X, int Y, int Z, float x, float y, float z,
+                                             float& lo, float& hi) {
+  const int i0 = __float2int_rd(x), j0 = __float2int_rd(y), k0 = __float2int_rd(z);
+  const float ax = x - float(i0), ay = y - float(j0), az = z - float(k0);
+  const int ia = max(i0, 0), ib = min(i0 + 1, X - 1);
+  const int ja = max(j0, 0), jb = min(j0 + 1, Y - 1);
+  const int ka = max(k0, 0), kb = min(k0 + 1, Z - 1);
+  const int r00 = g.px * (ja + g.py * ka), r10 = g.px * (jb + g.py * ka), r01 = g.px * (ja + g.py * kb), r11 = g.px * (jb + g.py * kb);
+  const float a = __ldg(f + r00 + ia), b = __ldg(f + r00 + ib), c = __ldg(f + r10 + ia), d = __ldg(f + r10 + ib);
+  const float e = __ldg(f + r01 + ia), h = __ldg(f + r01 + ib), k = __ldg(f + r11 + ia), l = __ldg(f + r11 + ib);
+  lo = fminf(fminf(fminf(a, b), fminf(c, d)), fminf(fminf(e, h), fminf(k, l)));
+  hi = fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), fmaxf(fmaxf(e, h), fmaxf(k, l)));
+  const float c00 = a * (1.f - ax) + b * ax;
+  const float c10 = c * (1.f - ax) + d * ax;
+  const float c01 = e * (1.f - ax) + h * ax;
+  const float c11 = k * (1.f - ax) + l * ax;
+  const float c0 = c00 * (1.f - ay) + c10 * ay;
+  const float c1 = c01 * (1.f - ay) + c11 * ay;
+  return c0 * (1.f - az) + c1 * az;
+}
 __device__ __forceinline__ float trilerpB(const float* __restrict__ f, const Grid& g, int X, int Y, int Z, float x, float y, float z) {
   const int i0 = __float2int_rd(x), j0 = __float2int_rd(y), k0 = __float2int_rd(z);
   const float ax = x - float(i0), ay = y - float(j0), az = z - float(k0);

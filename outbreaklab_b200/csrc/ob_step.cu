@@ -396,6 +396,15 @@ __device__ __forceinline__ float sampleVch(const float* f, const Grid& g, int ch
   return trilerpB(f, g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz);
 }
 
+// the departure-point sample of a channel, with the min / max of its 8 texels (ADVV2's limiter window: the
+// reference's limiter traces the same point, model.js:455-479)
+__device__ __forceinline__ void sampleVch_mm(const Fields& F, const Grid& g, int par, int ch, int o, float x, float y, float z) {
+  const float ox = ch == 0 ? 0.f : 0.5f, oy = ch == 1 ? 0.f : 0.5f, oz = ch == 2 ? 0.f : 0.5f;
+  float lo, hi;
+  F.Vt[ch][o] = trilerpB_mm(F.V[par][ch], g, g.nx + 1, g.ny + 1, g.nz + 1, x - ox, y - oy, z - oz, lo, hi);
+  F.Vlo[ch][o] = lo;
+  F.Vhi[ch][o] = hi;
+}
 __device__ __forceinline__ void advv1_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   OB_TEXEL_LOOP_BEGIN(g.nx, g.ny, g.nz)
   const Loc L = localVel(F, g, par, ci, cj, ck);
@@ -404,13 +413,13 @@ __device__ __forceinline__ void advv1_body(const Grid& g, const Uni& U, const Fi
   const int o = g.at(ci, cj, ck);
   float x, y, z;
   traceV(g, kk, fi, fj + 0.5f, fk + 0.5f, L.vu, 1.f, x, y, z);
-  F.Vt[0][o] = sampleVch(F.V[par][0], g, 0, x, y, z);
+  sampleVch_mm(F, g, par, 0, o, x, y, z);
   traceV(g, kk, fi + 0.5f, fj, fk + 0.5f, L.vv, 1.f, x, y, z);
-  F.Vt[1][o] = sampleVch(F.V[par][1], g, 1, x, y, z);
+  sampleVch_mm(F, g, par, 1, o, x, y, z);
   traceV(g, kk, fi + 0.5f, fj + 0.5f, fk, L.vw, 1.f, x, y, z);
-  F.Vt[2][o] = sampleVch(F.V[par][2], g, 2, x, y, z);
+  sampleVch_mm(F, g, par, 2, o, x, y, z);
   traceV(g, kk, fi + 0.5f, fj + 0.5f, fk + 0.5f, L.vc, 1.f, x, y, z);
-  F.Vt[3][o] = sampleVch(F.V[par][3], g, 3, x, y, z);
+  sampleVch_mm(F, g, par, 3, o, x, y, z);
 }
 __global__ void k_advv1(Grid g, Uni U, Fields F, int par) { advv1_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
 __global__ void k_advv1_grp(const uint2* __restrict__ map, int par) {
@@ -445,15 +454,12 @@ __device__ __forceinline__ void advv2_body(const Grid& g, const Uni& U, const Fi
   const int o = g.at(ci, cj, ck);
 #pragma unroll
   for (int c = 0; c < 4; c++) {
-    const float ox = c == 0 ? 0.f : 0.5f, oy = c == 1 ? 0.f : 0.5f, oz = c == 2 ? 0.f : 0.5f;
     float x, y, z;
     traceV(g, kk, P[c][0], P[c][1], P[c][2], vel[c], -1.f, x, y, z);
     const float b = sampleVch(F.Vt[c], g, c, x, y, z);
     const float hat = __ldg(F.Vt[c] + o), old = __ldg(F.V[par][c] + o);
     const float r = hat + sm * (old - b);
-    traceV(g, kk, P[c][0], P[c][1], P[c][2], vel[c], 1.f, x, y, z);
-    const float2 m = minmax8V(F.V[par][c], g, x, y, z, ox, oy, oz);
-    F.V[1 - par][c][o] = clampf(r, m.x, m.y);
+    F.V[1 - par][c][o] = clampf(r, __ldg(F.Vlo[c] + o), __ldg(F.Vhi[c] + o));
   }
 }
 __global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) { advv2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
