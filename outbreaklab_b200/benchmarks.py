@@ -38,7 +38,8 @@ def solve(args):
     P.set_density(rc, rw)
     phi = P.solve(rhs)
     ms = P.device_ms(args.reps)
-    flops = 4.0 * nx * ny * nz * (nx + ny) * (3 if args.precision >= 1 else 1) * (2 if args.precision == 2 else 1)
+    # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16)
+    flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4}[args.precision]
     out = {"bench": "pressure solve", "nx": nx, "ny": ny, "nz": nz, "precision": args.precision, "ms": ms,
            "dst_flops": flops, "tflops": flops / (ms * 1e-3) / 1e12}
     if args.check:
