@@ -248,15 +248,26 @@ def run_ours(args, rank, world):
     per_rank_sim = args.steps * case.dt
     value = world * per_rank_sim / (t_ms / 1000.0)
     cell_steps = world * args.steps * case.cells / (t_ms / 1000.0)
-    # end to end through the public API
+    # end to end through the public API: every step uploads the app's storm-start list (setCI, model.js:1383) from
+    # pinned host memory, steps, and reads back the step's FP64 water / mass / rain budgets. The list holds one event
+    # scheduled after the run (its window opens at 1e9 s), so the CI pass reads it every step while the workload
+    # stays the bubbles-only case.
     ke = max(1, min(args.steps, 100))
-    forcing = np.zeros(N.CI_FLOATS, np.float32)
-    pinned = forcing  # numpy host memory; the C ABI copies it (queue.writeBuffer semantics)
+    import torch
+    pinned_t = torch.zeros(N.CI_FLOATS, dtype=torch.float32, pin_memory=True)
+    pinned = pinned_t.numpy()
+    pinned[:] = [0.5 * case.nx * case.dx, 0.5 * case.ny * case.dx, 1500.0, 10000.0, 1500.0, 5.0, 1e9, 1e9 + 1800.0,
+                 0.0, 0.0, 0.0, 600.0]
+    h2d_bytes = int(pinned.nbytes)
+    d2h_bytes = 8 * 8   # ob_model_budgets copies back its block of 8 FP64 sums
+    N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 1))   # untimed: the first step with the list recaptures the graph
+    m.enc_step(case.dt)
+    m.budgets()
     barrier()
     m.sync()
     t0 = time.perf_counter()
     for _ in range(ke):
-        N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 0))
+        N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 1))
         m.enc_step(case.dt)
         b = m.budgets()
     e2e_s = allmax(time.perf_counter() - t0)
@@ -298,8 +309,8 @@ def run_ours(args, rank, world):
             "step_hbm": {"algorithmic_bytes": step_bytes, "gbs": step_bytes / (step_ms / 1000.0) / 1e9,
                          "frac_of_measured_peak": step_bytes / (step_ms / 1000.0) / 1e9 / hbm},
             "roofline": roof, "solve_roofline": solve_roof, "clocks": clk,
-            "e2e": {"value": e2e_val, "unit": "sim-s/wall-s", "h2d_bytes_per_step": int(pinned.nbytes * 0) + 304,
-                    "d2h_bytes_per_step": 24, "steps": ke},
+            "e2e": {"value": e2e_val, "unit": "sim-s/wall-s", "h2d_bytes_per_step": h2d_bytes,
+                    "d2h_bytes_per_step": d2h_bytes, "steps": ke},
             "gpu_launches": None, "nan_guard_count": m.nan_count}
     # CI, NUT, ADVV x2, ADVQ x2, PHYS, DIV, the refined solve (8 transforms, 2 tridiagonals, 1 residual), PROJ, RAIN;
     # LSF every 60 s of model time

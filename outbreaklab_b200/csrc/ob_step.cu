@@ -346,7 +346,7 @@ __device__ __forceinline__ void nut_body(const Grid& g, const Uni& U, const Fiel
 }
 __global__ void __launch_bounds__(128, 16) k_nut(Grid g, Uni U, Fields F, int par) { nut_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
 __global__ void k_nut_hur(Grid g, Uni U, Fields F, int par) { nut_body<true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 16) k_nut_grp(const uint2* __restrict__ map, int par) {
+__global__ void __launch_bounds__(128, 12) k_nut_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
   nut_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
@@ -463,7 +463,7 @@ __device__ __forceinline__ void advv2_body(const Grid& g, const Uni& U, const Fi
   }
 }
 __global__ void __launch_bounds__(128, 12) k_advv2(Grid g, Uni U, Fields F, int par) { advv2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 12) k_advv2_grp(const uint2* __restrict__ map, int par) {
+__global__ void __launch_bounds__(128, 10) k_advv2_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
   advv2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
@@ -711,7 +711,7 @@ __device__ __forceinline__ void advq2_body(const Grid& g, const Uni& U, const Fi
   if (threadIdx.x == 0 && threadIdx.y == 0) F.zeroQ1[brick] = active ? 0u : 1u;
 }
 __global__ void __launch_bounds__(128, 10) k_advq2(Grid g, Uni U, Fields F, int par) { advq2_body(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
-__global__ void __launch_bounds__(128, 10) k_advq2_grp(const uint2* __restrict__ map, int par) {
+__global__ void __launch_bounds__(128, 9) k_advq2_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
   advq2_body(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
@@ -1086,7 +1086,7 @@ __global__ void __launch_bounds__(128) k_phys_hur(Grid g, Uni U, Fields F, int p
   phys_body<kMicroPlain, true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int MM>
-__global__ void __launch_bounds__(128, 10) k_phys_grp(const uint2* __restrict__ map, int par) {
+__global__ void __launch_bounds__(128, 9) k_phys_grp(const uint2* __restrict__ map, int par) {
   OB_GROUP_RESOLVE
   phys_body<MM>(c_members[mem].g, c_members[mem].U, c_members[mem].F, par, gbx, gby, gbz);
 }
