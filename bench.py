@@ -9,9 +9,11 @@ Klemp analytic sounding, 8 seeded +3 K warm bubbles; synthetic inputs (no datase
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 value  = simulated seconds per wall second over the K timed steps (device time, CUDA events, max over ranks);
-e2e    = the same metric through the public Python API (RegionalModel.enc_step) with the per-step forcing upload from
-         pinned host memory and a device-to-host read of the step's FP64 budgets inside the timed region;
-roofline = the dominant pass of the step against the measured HBM copy peak (MEASURED_PEAKS.json);
+e2e    = the same metric through the public Python API (RegionalModel.enc_step) over the same K steps of a second copy
+         of the case, with the per-step forcing upload from pinned host memory and a device-to-host read of the step's
+         FP64 budgets inside the timed region (wall clock, max over ranks);
+roofline = the dominant kernel of the step against the measured HBM copy peak (MEASURED_PEAKS.json), and
+           solve_roofline the pressure solve's MMA work against the measured bf16 peak;
 cpu_baseline = the CPU restatement of the reference step (oracle, fp32, OpenMP) on a bounded sample.
 With --gpus N > 1 each rank runs an independent replica of the domain ("replicas only": a single domain does not
 shard); value sums the simulated seconds of all ranks over the slowest rank's time.
@@ -248,11 +250,12 @@ def run_ours(args, rank, world):
     per_rank_sim = args.steps * case.dt
     value = world * per_rank_sim / (t_ms / 1000.0)
     cell_steps = world * args.steps * case.cells / (t_ms / 1000.0)
-    # end to end through the public API: every step uploads the app's storm-start list (setCI, model.js:1383) from
-    # pinned host memory, steps, and reads back the step's FP64 water / mass / rain budgets. The list holds one event
-    # scheduled after the run (its window opens at 1e9 s), so the CI pass reads it every step while the workload
-    # stays the bubbles-only case.
-    ke = max(1, min(args.steps, 100))
+    # end to end through the public API, on a second copy of the case over the same steps as the timed region (the
+    # storms grow, so later steps cost more): every step uploads the app's storm-start list (setCI, model.js:1383)
+    # from pinned host memory, steps, and reads back the step's FP64 water / mass / rain budgets. The list holds one
+    # event scheduled after the run (its window opens at 1e9 s), so the CI pass reads it every step while the
+    # workload stays the bubbles-only case. The untimed warm-up has as many steps as precede the device-timed region,
+    # which also captures every step graph of the list's uniforms before the timing starts.
     import torch
     pinned_t = torch.zeros(N.CI_FLOATS, dtype=torch.float32, pin_memory=True)
     pinned = pinned_t.numpy()
@@ -260,18 +263,24 @@ def run_ours(args, rank, world):
                  0.0, 0.0, 0.0, 600.0]
     h2d_bytes = int(pinned.nbytes)
     d2h_bytes = 8 * 8   # ob_model_budgets copies back its block of 8 FP64 sums
-    N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 1))   # untimed: the first step with the list recaptures the graph
-    m.enc_step(case.dt)
-    m.budgets()
+    m2, _ = M.setup_case(case)
+
+    def e2e_step():
+        N.check(lib.ob_model_set_ci(m2.h, N.fptr(pinned), 1))
+        m2.enc_step(case.dt)
+        return m2.budgets()
+
+    for _ in range(args.warmup + nprof):
+        e2e_step()
     barrier()
-    m.sync()
+    m2.sync()
+    ke = args.steps
     t0 = time.perf_counter()
     for _ in range(ke):
-        N.check(lib.ob_model_set_ci(m.h, N.fptr(pinned), 1))
-        m.enc_step(case.dt)
-        b = m.budgets()
+        e2e_step()
     e2e_s = allmax(time.perf_counter() - t0)
     e2e_val = world * ke * case.dt / e2e_s
+    m2.destroy()
     # roofline of the dominant kernel: the pass with the longest time per kernel launch (PHYS, NUT and DIV are one
     # kernel each; ADVV, ADVQ, PROJ+RAIN and LSF+CI two; the refined solve eleven)
     hbm, bf16, src = peaks()

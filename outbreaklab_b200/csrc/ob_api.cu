@@ -37,14 +37,48 @@ static int cuda_status(cudaError_t e, const char* what) {
     if (rc__ != OB_OK) return rc__; \
   } while (0)
 
-__global__ void k_budget(Grid g, const float* B, float* const* q, double dV, double* out) {
-  // sum rho q_total dV and sum rho dV over the interior cells; one block per (y, z) row
-  const int j = blockIdx.x, k = blockIdx.y;
-  const double rho = double(B[k * 8 + 2]);
-  double w = 0.0;
-  for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
-    const int o = g.at(i, j, k);
-    w += double(q[0][o]) + double(q[1][o]) + double(q[2][o]) + double(q[3][o]) + double(q[4][o]) + double(q[5][o]);
+// two timing events, destroyed on every return path of the function that holds them
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  int create() {
+    OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
+    return cuda_status(cudaEventCreate(&b), "event");
+  }
+  // device time from a to b (waits for b)
+  int elapsed(float* ms, const char* what) const {
+    OB_TRY(cuda_status(cudaEventSynchronize(b), what));
+    return cuda_status(cudaEventElapsedTime(ms, a, b), what);
+  }
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// sum rho q_total dV and sum rho dV over the interior cells. Each block walks (y, z) rows in a grid-stride loop and
+// adds its two partial sums once: a few FP64 atomics per block rather than two per row, which on the same two
+// addresses serialise in L2 and would dominate the pass.
+constexpr int kBudgetBlocks = 1184;  // 8 blocks of 256 threads per SM of a 148-SM B200
+__global__ void __launch_bounds__(256) k_budget(Grid g, const float* __restrict__ B, float* const* q, double dV, double* out) {
+  const float* __restrict__ q0 = q[0];
+  const float* __restrict__ q1 = q[1];
+  const float* __restrict__ q2 = q[2];
+  const float* __restrict__ q3 = q[3];
+  const float* __restrict__ q4 = q[4];
+  const float* __restrict__ q5 = q[5];
+  double w = 0.0, mass = 0.0;
+  const int nrows = g.ny * g.nz;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int j = r % g.ny, k = r / g.ny;
+    const double rho = double(__ldg(B + k * 8 + 2));
+    double row = 0.0;
+    for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
+      const int o = g.at(i, j, k);
+      row += double(__ldg(q0 + o)) + double(__ldg(q1 + o)) + double(__ldg(q2 + o)) + double(__ldg(q3 + o)) +
+             double(__ldg(q4 + o)) + double(__ldg(q5 + o));
+    }
+    w += row * rho;
+    if (threadIdx.x == 0) mass += rho * g.nx;
   }
   for (int s = 16; s > 0; s >>= 1) w += __shfl_xor_sync(0xffffffffu, w, s);
   __shared__ double part[32];
@@ -53,8 +87,8 @@ __global__ void k_budget(Grid g, const float* B, float* const* q, double dV, dou
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int i = 0; i < int(blockDim.x >> 5); i++) t += part[i];
-    atomicAdd(out, t * rho * dV);
-    atomicAdd(out + 1, rho * dV * g.nx);
+    atomicAdd(out, t * dV);
+    atomicAdd(out + 1, mass * dV);
   }
 }
 __global__ void k_sum_rain(const double* rain, int n, double cell_area, double* out) {
@@ -360,13 +394,17 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   m->F.spz = m->d_tab;                      // 4 floats per level: 16-byte aligned
   m->F.slx = m->d_tab + 4 * (nz + 1);       // 2 floats per column: 8-byte aligned
   m->F.sly = m->F.slx + 2 * (nx + 1);
-  cudaMemcpy(m->d_qptr, m->F.Q[0], 8 * sizeof(float*), cudaMemcpyHostToDevice);
+  rc = cuda_status(cudaMemcpy(m->d_qptr, m->F.Q[0], 8 * sizeof(float*), cudaMemcpyHostToDevice), "pointer table");
   // a neutral base state until one is set
   m->Bh.assign(size_t(nz + 1) * 8, 0.f);
   for (int k = 0; k <= nz; k++) {
     m->Bh[k * 8 + 0] = 300.f; m->Bh[k * 8 + 2] = 1.f; m->Bh[k * 8 + 3] = 1.f; m->Bh[k * 8 + 4] = 1.f; m->Bh[k * 8 + 5] = 1e5f;
   }
-  cudaMemcpy(m->d_B, m->Bh.data(), m->Bh.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (rc == OB_OK) rc = cuda_status(cudaMemcpy(m->d_B, m->Bh.data(), m->Bh.size() * sizeof(float), cudaMemcpyHostToDevice), "base state");
+  if (rc != OB_OK) {
+    model_free(m);
+    return rc;
+  }
   *out = m;
   return OB_OK;
 }
@@ -431,16 +469,16 @@ int ob_model_set_ci(ObModel* m, const float* ev, int n) {
 int ob_model_reset(ObModel* m) {
   if (!m) { set_error("ob_model_reset: null model"); return OB_ERR_INVALID; }
   m->time = 0; m->steps = 0; m->parity = 0; m->phiScale = 1;
-  cudaMemsetAsync(m->d_clock, 0, sizeof(double), m->stream);
+  OB_TRY(cuda_status(cudaMemsetAsync(m->d_clock, 0, sizeof(double), m->stream), "reset"));
   write_uniforms(m, 1.0);
   const Grid& g = m->g;
   launch_lsf(g, m->U, m->F, m->stream);
   launch_init(g, m->U, m->F, m->stream);
   const size_t np = size_t(g.nxp) * g.nyp * g.nz;
-  cudaMemsetAsync(m->F.phi, 0, np * sizeof(float), m->stream);
-  cudaMemsetAsync(m->rhs32, 0, np * sizeof(float), m->stream);
-  cudaMemsetAsync(m->d_rain, 0, size_t(g.nx) * g.ny * sizeof(double), m->stream);
-  cudaMemsetAsync(m->d_flags, 0, 64 * sizeof(unsigned), m->stream);
+  OB_TRY(cuda_status(cudaMemsetAsync(m->F.phi, 0, np * sizeof(float), m->stream), "reset"));
+  OB_TRY(cuda_status(cudaMemsetAsync(m->rhs32, 0, np * sizeof(float), m->stream), "reset"));
+  OB_TRY(cuda_status(cudaMemsetAsync(m->d_rain, 0, size_t(g.nx) * g.ny * sizeof(double), m->stream), "reset"));
+  OB_TRY(cuda_status(cudaMemsetAsync(m->d_flags, 0, 64 * sizeof(unsigned), m->stream), "reset"));
   launch_activity(g, m->F, m->stream);
   m->lsfT = 0;
   return cuda_status(cudaGetLastError(), "reset");
@@ -684,7 +722,7 @@ int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain) {
   if (!m) { set_error("ob_model_budgets: null model"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
   OB_TRY(cuda_status(cudaMemsetAsync(m->d_red, 0, 8 * sizeof(double), m->stream), "budgets"));
-  k_budget<<<dim3(g.ny, g.nz), 128, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->dx * m->dx * m->dz, m->d_red);
+  k_budget<<<std::min(g.ny * g.nz, kBudgetBlocks), 256, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->dx * m->dx * m->dz, m->d_red);
   k_sum_rain<<<64, 256, 0, m->stream>>>(m->d_rain, g.nx * g.ny, m->dx * m->dx, m->d_red);
   double h[8];
   OB_TRY(cuda_status(cudaMemcpyAsync(h, m->d_red, sizeof(h), cudaMemcpyDeviceToHost, m->stream), "budgets"));
@@ -698,25 +736,30 @@ int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain) {
 // K steps bracketed by CUDA events on the model's stream; *ms = device time of the K steps
 int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms) {
   if (!m || !ms || !(dt > 0.f) || nsteps < 0) { set_error("ob_model_timed_steps: bad arguments"); return OB_ERR_INVALID; }
-  cudaEvent_t a, b;
-  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
-  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
-  cudaEventRecord(a, m->stream);
+  EventPair ev;
+  OB_TRY(ev.create());
+  OB_TRY(cuda_status(cudaEventRecord(ev.a, m->stream), "timed steps"));
   int rc = OB_OK;
   for (int s = 0; s < nsteps && rc == OB_OK; s++) rc = model_step_once(m, dt);
-  cudaEventRecord(b, m->stream);
-  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "timed steps");
-  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(ms, a, b), "timed steps");
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.b, m->stream), "timed steps");
+  if (rc == OB_OK) rc = ev.elapsed(ms, "timed steps");
   return rc;
 }
 
 // one step with an event between passes: ms[i] = device time of pass i (OB_PASS_* order), returns the pass count
 int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   if (!m || !ms || max_passes < OB_NPASS) { set_error("ob_model_profile_step: need %d slots", OB_NPASS); return -OB_ERR_INVALID; }
-  cudaEvent_t ev[OB_NPASS + 1];
-  for (int i = 0; i <= OB_NPASS; i++) cudaEventCreate(&ev[i]);
+  // the pass boundaries: OB_NPASS + 1 events, destroyed on every return path
+  struct Events {
+    cudaEvent_t e[OB_NPASS + 1] = {};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } evs;
+  cudaEvent_t* ev = evs.e;
+  for (int i = 0; i <= OB_NPASS; i++)
+    if (cuda_status(cudaEventCreate(&ev[i]), "profile step") != OB_OK) return -OB_ERR_DEVICE;
   write_uniforms(m, dt);
   const Grid& g = m->g;
   const int par = m->parity;
@@ -745,9 +788,9 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes) {
   m->parity = 1 - m->parity;
   m->time += dt;
   m->steps++;
+  if (rc == OB_OK) rc = cuda_status(cudaGetLastError(), "profile step");
   if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(ev[e - 1]), "profile step");
-  for (int i = 0; i + 1 < e && rc == OB_OK; i++) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
-  for (int i = 0; i <= OB_NPASS; i++) cudaEventDestroy(ev[i]);
+  for (int i = 0; i + 1 < e && rc == OB_OK; i++) rc = cuda_status(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]), "profile step");
   return rc == OB_OK ? e - 1 : -rc;
 }
 
@@ -1042,8 +1085,8 @@ static int ens_set_lanes(ObEnsemble* e, int k) {
     }
     OB_TRY(tc_group_create(plans.data(), phi.data(), rhs.data(), int(plans.size()), &L.solve));
     OB_TRY(tc_group_set_cap(L.solve, e->bn_cap));
-    int nsm = 148;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    int nsm = 148, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) nsm = 148;
     tc_group_set_ctas(L.solve, k > 1 ? (nsm + k - 1) / k : 0);
   }
   e->nlanes = k;
@@ -1253,26 +1296,22 @@ int ob_ensemble_step(ObEnsemble* e, int nsteps) {
 
 int ob_ensemble_timed_steps(ObEnsemble* e, int nsteps, float* ms) {
   if (!e || !ms || nsteps < 0) { set_error("ob_ensemble_timed_steps: bad arguments"); return OB_ERR_INVALID; }
-  cudaEvent_t a, b;
-  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
-  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
-  cudaEventRecord(a, e->stream);
+  EventPair ev;
+  OB_TRY(ev.create());
+  OB_TRY(cuda_status(cudaEventRecord(ev.a, e->stream), "ensemble timed steps"));
   int rc = OB_OK;
   for (int s = 0; s < nsteps && rc == OB_OK; s++) rc = ens_step_once(e);
-  cudaEventRecord(b, e->stream);
-  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "ensemble timed steps");
-  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(ms, a, b), "ensemble timed steps");
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.b, e->stream), "ensemble timed steps");
+  if (rc == OB_OK) rc = ev.elapsed(ms, "ensemble timed steps");
   return rc;
 }
 
 static int ens_check(ObEnsemble* e) {
   for (int l = 0; l < e->nlanes; l++) OB_TRY(tc_group_check(e->lane[l].solve));
   unsigned h = 0;
-  cudaMemcpy(&h, e->d_err, sizeof(h), cudaMemcpyDeviceToHost);
+  OB_TRY(cuda_status(cudaMemcpy(&h, e->d_err, sizeof(h), cudaMemcpyDeviceToHost), "ensemble error word"));
   if (h) {
-    cudaMemset(e->d_err, 0, sizeof(unsigned));
+    OB_TRY(cuda_status(cudaMemset(e->d_err, 0, sizeof(unsigned)), "ensemble error word"));
     set_error("ensemble surrogate: a tensor-core pipeline wait timed out (code %u)", h);
     return OB_ERR_TIMEOUT;
   }
@@ -1329,9 +1368,8 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
   OB_TRY(ens_prepare(e));
   cudaStream_t s = e->stream;
   if (group_upload_members(e->d_members, int(e->mem.size()), s) != 0) { set_error("ensemble: member table upload failed"); return OB_ERR_DEVICE; }
-  cudaEvent_t a, b;
-  OB_TRY(cuda_status(cudaEventCreate(&a), "event"));
-  OB_TRY(cuda_status(cudaEventCreate(&b), "event"));
+  EventPair ev;
+  OB_TRY(ev.create());
   auto run = [&]() -> int {
     for (int l = 0; l < e->nlanes; l++) {
       if (t < OB_ENS_NTILES - 1) {
@@ -1345,14 +1383,11 @@ int ob_ensemble_time_pass(ObEnsemble* e, int t, int reps, float* ms) {
     return OB_OK;
   };
   int rc = run();  // warm
-  cudaEventRecord(a, s);
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.a, s), "ensemble pass timing");
   for (int r = 0; r < reps && rc == OB_OK; r++) rc = run();
-  cudaEventRecord(b, s);
-  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "ensemble pass timing");
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.b, s), "ensemble pass timing");
   float el = 0.f;
-  if (rc == OB_OK) rc = cuda_status(cudaEventElapsedTime(&el, a, b), "ensemble pass timing");
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  if (rc == OB_OK) rc = ev.elapsed(&el, "ensemble pass timing");
   *ms = el / float(reps);
   return rc == OB_OK ? ens_check(e) : rc;
 }
@@ -1449,19 +1484,15 @@ int ob_poisson_solve(ObPoisson* p, const float* rhs, float* phi) {
 }
 int ob_poisson_time(ObPoisson* p, int reps, float* ms) {
   if (!p || reps < 1 || !ms) { set_error("ob_poisson_time: bad arguments"); return OB_ERR_INVALID; }
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
+  EventPair ev;
+  OB_TRY(ev.create());
   int rc = p->plan.solve(p->d_rhs, p->d_phi, p->stream);  // warm-up
-  cudaEventRecord(a, p->stream);
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.a, p->stream), "poisson timing");
   for (int r = 0; r < reps && rc == OB_OK; r++) rc = p->plan.solve(p->d_rhs, p->d_phi, p->stream);
-  cudaEventRecord(b, p->stream);
-  if (rc == OB_OK) rc = cuda_status(cudaEventSynchronize(b), "poisson timing");
+  if (rc == OB_OK) rc = cuda_status(cudaEventRecord(ev.b, p->stream), "poisson timing");
   float t = 0.f;
-  if (rc == OB_OK) cudaEventElapsedTime(&t, a, b);
+  if (rc == OB_OK) rc = ev.elapsed(&t, "poisson timing");
   *ms = t / reps;
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   if (rc == OB_OK) rc = p->plan.tc_check();
   return rc;
 }

@@ -70,6 +70,7 @@ class RegionalModel:
         return self
 
     def destroy(self):
+        self._params_sent = None   # a later handle may reuse this one's address
         if self.h:
             N.lib().ob_model_destroy(self.h)
             self.h = None
@@ -81,11 +82,17 @@ class RegionalModel:
             pass
 
     def _sync_params(self):
+        """Sends `params` to the library when they differ from what this handle last received (only
+        ob_model_set_params writes the library's copy, so an unchanged dict needs no call on every step)."""
+        vals = tuple(float(self.params[k]) for k in _PARAM_MAP) + (self.params.get("scheme") == "thompson",)
+        if getattr(self, "_params_sent", None) == (self.h.value, vals):
+            return
         p = N.default_params()
         for k, v in _PARAM_MAP.items():
             setattr(p, v, float(self.params[k]))
         p.scheme = 1.0 if self.params.get("scheme") == "thompson" else 0.0
         N.check(N.lib().ob_model_set_params(self.h, C.byref(p)))
+        self._params_sent = (self.h.value, vals)
 
     # ---- inputs ----
     def set_sounding(self, text: str):
