@@ -1081,7 +1081,7 @@ __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fie
     F.actQ0[BX + F.nbx * (BY + F.nby * ck)] = any ? 1u : 0u;
 }
 template <int MM>
-__global__ void __launch_bounds__(128, 10) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+__global__ void __launch_bounds__(128, 9) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
 __global__ void __launch_bounds__(128) k_phys_hur(Grid g, Uni U, Fields F, int par) {
   phys_body<kMicroPlain, true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z);
 }
