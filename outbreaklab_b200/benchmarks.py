@@ -7,15 +7,14 @@
                                                                                (torchrun: members shard over ranks)
 
 The solve benchmark's right-hand side is the 5 km-correlated Gaussian random field of the 1024 x 1024 x 80 case
-(zero horizontal mean per level), with the Weisman-Klemp densities; errors and residuals are computed in FP64 on the
-host when --check is given (the FP64 solve of the CPU oracle takes minutes at full size).
+(zero horizontal mean per level), with the Weisman-Klemp densities. Its residual at this size and at the 640 x 640 x 40
+step's solve grid is held to the solve tests' bar in tests/test_gpu_full_size.py.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import sys
 import time
 
 import numpy as np
@@ -36,22 +35,12 @@ def solve(args):
     rhs = W.gaussian_rhs(nx, ny, nz, dx, corr_len=5000.0, seed=3).astype(np.float32)
     P = M.PoissonDirect(nx, ny, nz, dx, dz, args.precision)
     P.set_density(rc, rw)
-    phi = P.solve(rhs)
+    P.solve(rhs)   # uploads the right-hand side that device_ms solves again
     ms = P.device_ms(args.reps)
     # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16)
     flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4}[args.precision]
     out = {"bench": "pressure solve", "nx": nx, "ny": ny, "nz": nz, "precision": args.precision, "ms": ms,
            "dst_flops": flops, "tflops": flops / (ms * 1e-3) / 1e12}
-    if args.check:
-        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-        from oracle import oracle as O
-        r64, w64 = rc.astype(np.float64), rw.astype(np.float64)
-        ref = O.poisson_solve(rhs.astype(np.float64), dx, dz, r64, w64, 8)
-        res = O.poisson_apply(phi.astype(np.float64), dx, dz, r64, w64) - rhs
-        out.update(err_inf=float(np.abs(phi - ref).max() / np.abs(ref).max()),
-                   err_l2=float(np.sqrt(((phi - ref) ** 2).sum() / (ref ** 2).sum())),
-                   resid_inf=float(np.abs(res).max() / np.abs(rhs).max()),
-                   resid_l2=float(np.sqrt((res ** 2).sum() / (rhs.astype(np.float64) ** 2).sum())))
     print(json.dumps(out), flush=True)
 
 
@@ -191,7 +180,6 @@ def main(argv=None):
     a.add_argument("--dx", type=float, default=1000.0)
     a.add_argument("--precision", type=int, default=2)
     a.add_argument("--reps", type=int, default=10)
-    a.add_argument("--check", action="store_true")
     b = sub.add_parser("step")
     b.add_argument("--case", default="c4")
     b.add_argument("--steps", type=int, default=50)
