@@ -58,10 +58,10 @@ struct Fields {
   const float* ci;  // events x 12
   unsigned int* flags;  // [0] NaN/Inf counter
   // clear-air skip of the hydrometeor channels, per brick of 32 x 4 x 1 cells (nbx x nby x nz bricks)
-  unsigned int* actQ0;   // Q slot 0 holds a hydrometeor in the brick
+  unsigned int* actQ0;   // Q slot 0 holds a hydrometeor or a nonzero spare channel in the brick
   unsigned int* actQt;   // the advection scratch Qt holds one (its block computed them)
-  unsigned int* zeroQt;  // the scratch's hydrometeor channels are known to be zero there
-  unsigned int* zeroQ1;  // Q slot 1's hydrometeor channels are known to be zero there
+  unsigned int* zeroQt;  // the scratch's hydrometeor and spare channels are known to be zero there
+  unsigned int* zeroQ1;  // Q slot 1's hydrometeor and spare channels are known to be zero there
   int nbx, nby;
   float fallmax;         // bound on every hydrometeor fall speed of the base state (m/s)
   // sponge coefficients tabulated once per parameter set (k_tables): spz[2k] = top sponge at the cell centre height

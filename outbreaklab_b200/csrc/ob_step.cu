@@ -523,10 +523,11 @@ __device__ __forceinline__ float2 minmaxQ(const float* __restrict__ f, const Tap
                      fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), fmaxf(fmaxf(e, h), fmaxf(k, l))));
 }
 
-// Clear-air skip of the hydrometeor channels (qc, qi, qr, qs, qg, Nr). A block (one brick of 32 x 4 x 1 cells) reads
-// those channels only inside the footprints of its departure points; if every brick touching that region holds no
-// hydrometeor, the semi-Lagrangian samples, the MacCormack correction, the limiter and the clip all give exactly +0,
-// so the block writes zeros (once) instead of gathering. Falling hydrometeors shift a departure point vertically by
+// Clear-air skip of the hydrometeor channels (qc, qi, qr, qs, qg, Nr) and of the spare fourth Q2 channel, which no
+// scheme sets and physics only carries. A block (one brick of 32 x 4 x 1 cells) reads those channels only inside the
+// footprints of its departure points; if every brick touching that region holds none of them (a hydrometeor or a
+// nonzero spare), the semi-Lagrangian samples, the MacCormack correction, the limiter and the clip all give exactly
+// +0, so the block writes zeros (once) instead of gathering. Falling hydrometeors shift a departure point vertically by
 // at most dt/dz * fallmax, which widens the region in z.
 struct Region {
   int x0, x1, y0, y1, z0, z1;
@@ -592,10 +593,10 @@ __device__ __forceinline__ void advq1_body(const Grid& g, const Uni& U, const Fi
   if (in) {
     const Tap t0 = tapQ(g, x, y, z);
     F.Qt[0][o] = gatherQ(F.Q[0][0], t0);
-    F.Qt[7][o] = gatherQ(F.Q[0][7], t0);
     if (active) {
       F.Qt[1][o] = gatherQ(F.Q[0][1], t0);
       F.Qt[2][o] = gatherQ(F.Q[0][2], t0);
+      F.Qt[7][o] = gatherQ(F.Q[0][7], t0);
       const float nr0 = gatherQ(F.Q[0][6], t0);
       const Fall fl{U.step.z, U.micro2.z > 0.5f};
       const float rho = bsA(F.B, g.nz, ck).z;
@@ -615,7 +616,7 @@ __device__ __forceinline__ void advq1_body(const Grid& g, const Uni& U, const Fi
       }
     } else if (!F.zeroQt[brick]) {
 #pragma unroll
-      for (int c = 1; c < 7; c++) F.Qt[c][o] = 0.f;
+      for (int c = 1; c < 8; c++) F.Qt[c][o] = 0.f;
     }
   }
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -668,19 +669,20 @@ __device__ __forceinline__ void advq2_body(const Grid& g, const Uni& U, const Fi
     const float cx = v[0] * kk[0], cy = v[1] * kk[1], cz = v[2] * kk[2];
     const float cour = sqrtf(cx * cx + cy * cy + cz * cz);
     const float sm = 0.5f * U.misc.y * clampf(cour / 0.35f, U.dzv.w, 1.f);
-    {  // the air-speed group: qv and the spare channel always
+    {  // the air-speed group: qv always; qc, qi and the spare channel where active
       const Tap tb = tapQ(g, xb, yb, zb), tf = tapQ(g, xf, yf, zf);
-#pragma unroll
-      for (int c = 0; c < 8; c += 7) {
-        const float b = gatherQ(F.Qt[c], tb);
-        const float rr = __ldg(F.Qt[c] + o) + sm * (__ldg(F.Q[0][c] + o) - b);
-        const float2 m = minmaxQ(F.Q[0][c], tf);
-        F.Q[1][c][o] = fmaxf(clampf(rr, m.x, m.y), 0.f);
+      {
+        const float b = gatherQ(F.Qt[0], tb);
+        const float rr = __ldg(F.Qt[0] + o) + sm * (__ldg(F.Q[0][0] + o) - b);
+        const float2 m = minmaxQ(F.Q[0][0], tf);
+        F.Q[1][0][o] = fmaxf(clampf(rr, m.x, m.y), 0.f);
       }
       if (active) {
         const Fall fl{U.step.z, U.micro2.z > 0.5f};
+        constexpr int kAir[3] = {1, 2, 7};  // qc, qi, spare
 #pragma unroll
-        for (int c = 1; c < 3; c++) {
+        for (int i = 0; i < 3; i++) {
+          const int c = kAir[i];
           const float b = gatherQ(F.Qt[c], tb);
           const float rr = __ldg(F.Qt[c] + o) + sm * (__ldg(F.Q[0][c] + o) - b);
           const float2 m = minmaxQ(F.Q[0][c], tf);
@@ -705,7 +707,7 @@ __device__ __forceinline__ void advq2_body(const Grid& g, const Uni& U, const Fi
       if (fl.thm) F.Q[1][6][o] = advq2_channel(F, g, kk, p, v, fv.y, sm, q6, 6, o);
     } else if (!F.zeroQ1[brick]) {
 #pragma unroll
-      for (int c = 1; c < 7; c++) F.Q[1][c][o] = 0.f;
+      for (int c = 1; c < 8; c++) F.Q[1][c][o] = 0.f;
     }
   }
   if (threadIdx.x == 0 && threadIdx.y == 0) F.zeroQ1[brick] = active ? 0u : 1u;
@@ -724,7 +726,7 @@ __global__ void __launch_bounds__(128) k_activity(Grid g, Fields F) {
   if (ci < g.nx && cj < g.ny && ck < g.nz) {
     const int o = g.at(ci, cj, ck);
 #pragma unroll
-    for (int c = 1; c < 7; c++) act |= F.Q[0][c][o] != 0.f;
+    for (int c = 1; c < 8; c++) act |= F.Q[0][c][o] != 0.f;
   }
   const bool any = __syncthreads_or(act) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -1052,7 +1054,7 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
       F.Q[0][7][o] = q2[3];
       out[3] = th;
-      hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f;
+      hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f || q2[3] > 0.f;
     }
   }
   const float sp = sqrtf(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
