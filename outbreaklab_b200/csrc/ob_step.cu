@@ -800,7 +800,8 @@ __device__ __forceinline__ unsigned warp_append(unsigned* ctr) {
 // [0, n-1] (Q, aux, phi_t), computed once per texel. BND: boundary air masses present (else the target state is the
 // base state, see tgtUb).
 template <bool BND, int MM, bool HUR = false>
-__device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck) {
+__device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fields& F, int par, int ci, int cj, int ck, bool dry,
+                                           bool was0) {
   bool hyd = false;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int o = g.at(ci, cj, ck);
@@ -898,9 +899,13 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     float dw = nux * lapH(2, V[2]) * ix2 + nuy * (__ldg(Vw - g.plane) + __ldg(Vw + g.plane) - 2.f * V[2]) * iz2;
     auto buoy = [&](int kk, int off) {
       const float4 A = bsA(F.B, nz, kk);
+      float h[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+      if (!dry) {
+#pragma unroll
+        for (int c = 0; c < 5; c++) h[c] = __ldg(F.Q[1][1 + c] + o + off);
+      }
       return 9.81f * ((__ldg(Vth + off) - A.x) / A.x + 0.608f * (__ldg(F.Q[1][0] + o + off) - A.y) -
-                      (__ldg(F.Q[1][1] + o + off) + __ldg(F.Q[1][2] + o + off) + __ldg(F.Q[1][3] + o + off) +
-                       __ldg(F.Q[1][4] + o + off) + __ldg(F.Q[1][5] + o + off)));
+                      (h[0] + h[1] + h[2] + h[3] + h[4]));
     };
     dw += 0.5f * (buoy(ck - 1, -g.plane) + buoy(ck, 0));
     if (BND) dw -= (LP(0) - LP(-g.plane)) / dz;
@@ -925,15 +930,20 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     const float relax = BND ? sl + l2d(F.lsfB, g, ci, cj).w * (1.f / U.cor.y) : sl;
     const float nux = __ldg(A0) * 3.f + U.turb.y, nuy = __ldg(A1) * 3.f + U.turb.y;
     float th = V[3] + dt * (nux * lapH(3, V[3]) * ix2 + nuy * lapZp(3, V[3], ck == 0, ck == nz - 1) * iz2 + (relax + spk.x) * (tth - V[3]));
-    float q1[4], q2[4];
+    // hydrometeor and spare channels: exactly +0 throughout a dry block's reach, so not read there (the sums below
+    // then see the same +0 operands the loads would have returned)
+    float q1[4] = {__ldg(F.Q[1][0] + o), 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
+    float l1[3] = {0.f, 0.f, 0.f}, l1z[3] = {0.f, 0.f, 0.f};
+    if (!dry) {
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-      q1[c] = __ldg(F.Q[1][c] + o);
-      q2[c] = __ldg(F.Q[1][4 + c] + o);
+      for (int c = 0; c < 4; c++) {
+        if (c) q1[c] = __ldg(F.Q[1][c] + o);
+        q2[c] = __ldg(F.Q[1][4 + c] + o);
+      }
     }
-    float l1[3], l1z[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
+      if (c && dry) continue;
       const float* __restrict__ q = F.Q[1][c] + o;
       l1[c] = __ldg(q + xcp) + __ldg(q + xm) + __ldg(q + ycp) + __ldg(q + ym) - 4.f * q1[c];
       l1z[c] = (ck == 0 ? q1[c] : __ldg(q + zm)) + (ck == nz - 1 ? q1[c] : __ldg(q + g.plane)) - 2.f * q1[c];
@@ -1020,7 +1030,9 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
     }
     if (!done) {
       const MCell pre = mc;
-      micro_processes(U, dt, p0, rho, spk.z, mc);
+      // with every hydrometeor exactly +0 (a dry block) each process rate is zero and the block leaves the cell as it
+      // is; the saturation adjustment below still runs (a supersaturated cell condenses)
+      if (!dry) micro_processes(U, dt, p0, rho, spk.z, mc);
       if (MM == kMicroRecord && surrogate_cell(pre) &&
           float(hash3i(ci, cj, ck ^ int(__float_as_uint(float(__ldg(F.clock))) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
         // one (state, process tendency) pair of the scheme: 12 inputs, 10 tendencies (before the saturation
@@ -1045,16 +1057,18 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       // 1 / (1 + 0) == 1 exactly: no division outside the sponge (and, in hurricane mode, the far-field decay)
       const float keep = HUR ? 1.f / (1.f + 2.f * dt * sl + dt * envDecay) : (sl > 0.f ? 1.f / (1.f + 2.f * dt * sl) : 1.f);
       qc *= keep; qi *= keep; qr *= keep; qs *= keep; qg *= keep; nr *= keep;
-      F.Q[0][0][o] = fmaxf(qv, 0.f);
-      F.Q[0][1][o] = fmaxf(qc, 0.f);
-      F.Q[0][2][o] = fmaxf(qi, 0.f);
-      F.Q[0][3][o] = fmaxf(qr, 0.f);
-      F.Q[0][4][o] = fmaxf(qs, 0.f);
-      F.Q[0][5][o] = fmaxf(qg, 0.f);
-      F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
-      F.Q[0][7][o] = q2[3];
-      out[3] = th;
       hyd = qc > 0.f || qi > 0.f || qr > 0.f || qs > 0.f || qg > 0.f || (thm ? nr : q2[2]) > 0.f || q2[3] > 0.f;
+      F.Q[0][0][o] = fmaxf(qv, 0.f);
+      if (hyd || !was0) {  // else the channels below are zero here and slot 0 already holds zeros
+        F.Q[0][1][o] = fmaxf(qc, 0.f);
+        F.Q[0][2][o] = fmaxf(qi, 0.f);
+        F.Q[0][3][o] = fmaxf(qr, 0.f);
+        F.Q[0][4][o] = fmaxf(qs, 0.f);
+        F.Q[0][5][o] = fmaxf(qg, 0.f);
+        F.Q[0][6][o] = thm ? fmaxf(nr, 0.f) : q2[2];
+        F.Q[0][7][o] = q2[3];
+      }
+      out[3] = th;
     }
   }
   const float sp = sqrtf(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
@@ -1071,12 +1085,37 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
   return hyd;
 }
 
+// The clear-air flags of a physics block (one 32 x 4 brick of cells; blocks past the last brick hold only faces, which
+// read and write no scalar), the same for all its threads: dry = Q slot 1 holds no hydrometeor and no nonzero spare in
+// the brick and its six face neighbours (ADVQ2 wrote them as zeros), which bound every scalar read of the block; was0
+// = the previous physics pass left slot 0's hydrometeor and spare channels zero in the brick (actQ0 clear), so a cell
+// whose new values there are all zero need not store them again. Hurricane mode's 2-dx filter writes slot 0 between
+// physics passes, so there was0 stays false.
+template <bool HUR>
+__device__ __forceinline__ void phys_flags(const Grid& g, const Fields& F, int BX, int BY, int ck, bool& dry, bool& was0) {
+  dry = false;
+  was0 = false;
+  if (BX >= F.nbx || BY >= F.nby || ck >= g.nz) return;
+  const int lane = threadIdx.x & 31;
+  unsigned z = 1u;
+  if (lane < 7) {
+    const int bx = BX + (lane == 1 ? -1 : lane == 2 ? 1 : 0), by = BY + (lane == 3 ? -1 : lane == 4 ? 1 : 0);
+    const int bz = ck + (lane == 5 ? -1 : lane == 6 ? 1 : 0);
+    if (bx >= 0 && bx < F.nbx && by >= 0 && by < F.nby && bz >= 0 && bz < g.nz) z = F.zeroQ1[bx + F.nbx * (by + F.nby * bz)];
+  }
+  dry = __all_sync(0xffffffffu, z != 0u);
+  if (!HUR) was0 = F.actQ0[BX + F.nbx * (BY + F.nby * ck)] == 0u;
+}
+
 template <int MM, bool HUR = false>
 __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
+  bool dry, was0;
+  phys_flags<HUR>(g, F, BX, BY, ck, dry, was0);
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
-    hyd = U.cor.z > 0.5f ? phys_texel<true, MM, HUR>(g, U, F, par, ci, cj, ck) : phys_texel<false, MM, HUR>(g, U, F, par, ci, cj, ck);
+    hyd = U.cor.z > 0.5f ? phys_texel<true, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0)
+                         : phys_texel<false, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(BX) < F.nbx && int(BY) < F.nby && ck < g.nz)
