@@ -182,7 +182,8 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "cell_steps_per_s": nsample * case.cells / el,
             "config": {"workload": "640x640x40 dx 1 km dz 500 m dt 6 s, Lin, 8 warm bubbles (Weisman-Klemp)",
-                       "parallelism": "replicas", "l2": "state 2.8 GB > L2"},
+                       "cells": case.cells, "parallelism": "replicas" if world > 1 else "single domain",
+                       "l2": "state 2.8 GB > 126 MB L2 (no flush needed)"},
             "cpu_baseline": {"value": val, "unit": "sim-s/wall-s", "cores": cores, "kind": "port",
                              "sample": "%d of the timed model steps after %d warm-up step(s); the reference's WGSL "
                                        "needs a WebGPU device (unavailable on this box), so its fp32 C++ restatement "
