@@ -39,6 +39,13 @@ extern "C" {
 #define OB_FIELD_AUX 3  /* nx*ny*nz x float2 (nu_h, nu_v) */
 #define OB_FIELD_PHI 4  /* (nx+2p)(ny+2p)nz float: the pressure solve's phi on the padded grid */
 #define OB_FIELD_RAIN 5 /* nx*ny double: accumulated surface precipitation (kg/m^2); no counterpart in the reference */
+/* Read-only diagnostics of the large-scale forcing and storm-start passes (ob_model_set_field rejects them):
+ * the per-column textures lsfA, lsfB (model.js:122-124), ciMap (model.js:277-279) and the target's hydrostatic phi
+ * phT (model.js:241), as the last LSF / CI pass left them. */
+#define OB_FIELD_LSF_A 6  /* nx*ny x float4 (dT at the ground K, air-mass depth m, qv deficit, moisture depth m) */
+#define OB_FIELD_LSF_B 7  /* nx*ny x float4 (du, dv at the ground m/s, wind-anomaly depth m, nudging weight) */
+#define OB_FIELD_CI_MAP 8 /* nx*ny x float4 (push strength 0-1, target w m/s, centre height m, half-depth m) */
+#define OB_FIELD_PHT 9    /* nx*ny*nz float: target hydrostatic phi (m^2/s^2), x fastest */
 
 /* Physics and numerics knobs: RegionalModel.params (model.js:1176-1180) with the outbreak-mode overrides of
  * app.js:1613. ob_params_default() fills the outbreak defaults. */

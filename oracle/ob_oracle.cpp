@@ -498,7 +498,9 @@ template <class R> struct Model {
   R hotSpots(int b, R s) const {
     const float* P4 = bd(b) + 16;
     R L = R(P4[2]);
-    int sd = int(R(P4[1]) * R(1000));
+    // the hash seed is an integer the reference derives in f32 (model.js:192); deriving it in double would pick
+    // another integer (5632.69f * 1000 rounds to 5632690 in f32, 5632689.94 in double) and another noise pattern
+    int sd = int(P4[1] * 1000.f);
     R ph = S.step.y / R(4800);
     int e = int(std::floor(ph));
     R fe = sstep(R(0), R(1), fractv(ph));
@@ -1515,6 +1517,10 @@ template <class R> struct Model {
       case OB_FIELD_Q2: ch = 4; return &Q2[0];
       case OB_FIELD_AUX: ch = 2; return &aux;
       case OB_FIELD_PHI: ch = 1; return &phi;
+      case OB_FIELD_LSF_A: ch = 4; return &lsfA;
+      case OB_FIELD_LSF_B: ch = 4; return &lsfB;
+      case OB_FIELD_CI_MAP: ch = 4; return &ciMap;
+      case OB_FIELD_PHT: ch = 1; return &phT;
       default: return nullptr;
     }
   }

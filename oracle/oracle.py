@@ -102,6 +102,7 @@ def _declare(L):
 
 
 FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI = 0, 1, 2, 3, 4
+FIELD_LSF_A, FIELD_LSF_B, FIELD_CI_MAP, FIELD_PHT = 6, 7, 8, 9
 
 
 def default_params() -> ObParams:
@@ -134,7 +135,9 @@ class OracleModel:
     def field_count(self, field):
         nx, ny, nz, p = self.nx, self.ny, self.nz, self.pad
         return {FIELD_V: (nx + 1) * (ny + 1) * (nz + 1) * 4, FIELD_Q1: nx * ny * nz * 4, FIELD_Q2: nx * ny * nz * 4,
-                FIELD_AUX: nx * ny * nz * 2, FIELD_PHI: (nx + 2 * p) * (ny + 2 * p) * nz}[field]
+                FIELD_AUX: nx * ny * nz * 2, FIELD_PHI: (nx + 2 * p) * (ny + 2 * p) * nz,
+                FIELD_LSF_A: nx * ny * 4, FIELD_LSF_B: nx * ny * 4, FIELD_CI_MAP: nx * ny * 4,
+                FIELD_PHT: nx * ny * nz}[field]
 
     def set_base_state(self, B):
         lib().oro_set_base_state(self.h, np.ascontiguousarray(B, np.float32))
@@ -254,10 +257,11 @@ def poisson_apply(phi, dx, dz, rhoC, rhoW):
     return out
 
 
-def setup_case(case, precision=4):
-    """Creates an oracle model for a workloads.StormCase: defaults, noise 0, scheme, base state, reset, perturbed
-    theta. Returns (model, B)."""
-    from outbreaklab_b200 import workloads
+def setup_case(case, precision=4, bounds=None, ci=None):
+    """Creates an oracle model for a workloads.StormCase: defaults, noise 0, scheme, base state, optional boundaries
+    and storm-start towers (packed by the same host code as the model's), reset, perturbed theta. Returns
+    (model, B)."""
+    from outbreaklab_b200 import workloads, boundaries, model as M
     B, _ = workloads.base_state_for(case)
     m = OracleModel(case.nx, case.ny, case.nz, case.dx, precision)
     p = default_params()
@@ -265,6 +269,11 @@ def setup_case(case, precision=4):
     p.scheme = float(case.scheme)
     m.set_params(p)
     m.set_base_state(B)
+    if bounds:
+        m.set_boundaries(*boundaries.pack_boundaries(bounds))
+    if ci:
+        f, act = M.pack_ci(ci, 0.0)
+        m.set_ci(f, len(act))
     m.reset()
     V = m.get(FIELD_V)
     m.set(FIELD_V, workloads.perturb_theta(case, V))

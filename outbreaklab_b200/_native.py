@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libob_b200.so")
 
 OB_OK, OB_ERR_OOM, OB_ERR_INVALID, OB_ERR_DEVICE, OB_ERR_TIMEOUT, OB_ERR_NAN = 0, 1, 2, 3, 4, 5
 FIELD_V, FIELD_Q1, FIELD_Q2, FIELD_AUX, FIELD_PHI, FIELD_RAIN = 0, 1, 2, 3, 4, 5
+FIELD_LSF_A, FIELD_LSF_B, FIELD_CI_MAP, FIELD_PHT = 6, 7, 8, 9
 BOUNDARY_FLOATS, MAX_BOUNDS, CI_FLOATS, MAX_CI = 148, 8, 12, 256
 OB_STATIC_POISSON_MAX_SIDE, OB_STATIC_POISSON_MAX_NZ, OB_STATIC_POISSON_MAX_CELLS = 256, 512, 1 << 20
 RADAR_MAX_RADIALS, RADAR_MAX_TORNADOES, RADAR_TORNADO_FLOATS = 720, 64, 8

@@ -669,6 +669,9 @@ static int field_layout(ObModel* m, int field, Ptr8& p, int& nch, int& X, int& Y
     case OB_FIELD_AUX:
       p.p[0] = m->F.aux[0]; p.p[1] = m->F.aux[1];
       nch = 2; X = g.nx; Y = g.ny; Z = g.nz; return OB_OK;
+    case OB_FIELD_PHT:
+      p.p[0] = m->F.phT;
+      nch = 1; X = g.nx; Y = g.ny; Z = g.nz; return OB_OK;
     default:
       set_error("unknown field %d", field);
       return OB_ERR_INVALID;
@@ -678,6 +681,14 @@ static int field_layout(ObModel* m, int field, Ptr8& p, int& nch, int& X, int& Y
 int ob_model_get_field(ObModel* m, int field, void* host, size_t bytes) {
   if (!m || !host) { set_error("ob_model_get_field: null argument"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
+  if (field == OB_FIELD_LSF_A || field == OB_FIELD_LSF_B || field == OB_FIELD_CI_MAP) {
+    const size_t need = size_t(g.nx) * g.ny * sizeof(float4);
+    if (bytes != need) { set_error("ob_model_get_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
+    const void* src = field == OB_FIELD_LSF_A ? (const void*)m->F.lsfA : field == OB_FIELD_LSF_B ? (const void*)m->F.lsfB
+                                                                                                 : (const void*)m->F.ciMap;
+    OB_TRY(cuda_status(cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, m->stream), "get field"));
+    return cuda_status(cudaStreamSynchronize(m->stream), "get field");
+  }
   if (field == OB_FIELD_PHI || field == OB_FIELD_RAIN) {
     const size_t need = field == OB_FIELD_PHI ? size_t(g.nxp) * g.nyp * g.nz * sizeof(float) : size_t(g.nx) * g.ny * sizeof(double);
     if (bytes != need) { set_error("ob_model_get_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }
@@ -698,6 +709,10 @@ int ob_model_get_field(ObModel* m, int field, void* host, size_t bytes) {
 int ob_model_set_field(ObModel* m, int field, const void* host, size_t bytes) {
   if (!m || !host) { set_error("ob_model_set_field: null argument"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
+  if (field >= OB_FIELD_LSF_A && field <= OB_FIELD_PHT) {
+    set_error("ob_model_set_field: field %d is a read-only diagnostic (the LSF and CI passes write it)", field);
+    return OB_ERR_INVALID;
+  }
   if (field == OB_FIELD_PHI || field == OB_FIELD_RAIN) {
     const size_t need = field == OB_FIELD_PHI ? size_t(g.nxp) * g.nyp * g.nz * sizeof(float) : size_t(g.nx) * g.ny * sizeof(double);
     if (bytes != need) { set_error("ob_model_set_field: %zu bytes, expected %zu", bytes, need); return OB_ERR_INVALID; }

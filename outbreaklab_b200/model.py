@@ -14,6 +14,7 @@ import math
 import numpy as np
 
 from . import _native as N
+from . import boundaries
 from . import sounding as snd_mod
 
 # grid presets (model.js:1143-1154)
@@ -113,29 +114,16 @@ class RegionalModel:
 
     def set_boundaries(self, bnds):
         """model.js:1371-1380: [{pts, motion, vel, halfW, dT, Hmax, slope, Hmin, dq, qRatio, du, dv, wRatio, nudge,
-        dFree, side, vary, seed, varyL}] in model metres and m/s."""
-        self.bounds = list(bnds)[:N.MAX_BOUNDS]
-        f = np.zeros(N.MAX_BOUNDS * N.BOUNDARY_FLOATS, np.float32)
-        for i, b in enumerate(self.bounds):
-            o = i * N.BOUNDARY_FLOATS
-            pts = list(b["pts"])[:32]
-            f[o:o + 20] = [len(pts), b["motion"][0], b["motion"][1], b["halfW"], b["dT"], b["Hmax"], b["slope"],
-                           b["Hmin"], b["dq"], b["qRatio"], b["du"], b["dv"], b["wRatio"], 1 if b.get("nudge") else 0,
-                           b["dFree"], b["side"], b.get("vary", 0) or 0, b.get("seed", 0) or 0,
-                           b.get("varyL", 60000) or 60000, 0]
-            for k, p in enumerate(pts):
-                v = (b.get("vel") or [None] * len(pts))[k] or b["motion"]
-                f[o + 20 + 4 * k:o + 24 + 4 * k] = [p[0], p[1], v[0], v[1]]
-        N.check(N.lib().ob_model_set_boundaries(self.h, N.fptr(f), len(self.bounds)))
+        dFree, side, vary, seed, varyL}] in model metres and m/s (boundaries.boundary_models builds them from the
+        boundaries drawn on the map). Like the reference, takes effect at the next reset or LSF pass."""
+        f, n = boundaries.pack_boundaries(bnds)
+        self.bounds = list(bnds)[:n]
+        N.check(N.lib().ob_model_set_boundaries(self.h, N.fptr(f), n))
 
     def set_ci(self, events):
-        """model.js:1383-1389: towers [{x, y, zc, rh, rz, wt, t0, t1, vx, vy, seed, ramp}]."""
-        act = [e for e in events if e["t1"] > self.time][-N.MAX_CI:]
-        f = np.zeros(max(1, len(act)) * N.CI_FLOATS, np.float32)
-        for i, e in enumerate(act):
-            f[i * 12:(i + 1) * 12] = [e["x"], e["y"], e["zc"], e["rh"], e["rz"], e["wt"], e["t0"], e["t1"],
-                                      e.get("vx", 0) or 0, e.get("vy", 0) or 0, e.get("seed", i * 1.37),
-                                      e.get("ramp", 150) or 150]
+        """model.js:1383-1389: towers [{x, y, zc, rh, rz, wt, t0, t1, vx, vy, seed, ramp}]; those that ended before
+        the model's time are dropped."""
+        f, act = pack_ci(events, self.time)
         self.ci_events = act
         N.check(N.lib().ob_model_set_ci(self.h, N.fptr(f), len(act)))
 
@@ -237,7 +225,9 @@ class RegionalModel:
                 N.FIELD_Q1: (nx * ny * nz * 4, np.float32), N.FIELD_Q2: (nx * ny * nz * 4, np.float32),
                 N.FIELD_AUX: (nx * ny * nz * 2, np.float32),
                 N.FIELD_PHI: ((nx + 2 * p) * (ny + 2 * p) * nz, np.float32),
-                N.FIELD_RAIN: (nx * ny, np.float64)}[field]
+                N.FIELD_RAIN: (nx * ny, np.float64),
+                N.FIELD_LSF_A: (nx * ny * 4, np.float32), N.FIELD_LSF_B: (nx * ny * 4, np.float32),
+                N.FIELD_CI_MAP: (nx * ny * 4, np.float32), N.FIELD_PHT: (nx * ny * nz, np.float32)}[field]
 
     def get_field(self, field):
         n, dt = self.field_shape(field)
@@ -302,15 +292,32 @@ class PoissonDirect:
             pass
 
 
-def setup_case(case):
-    """A RegionalModel for a workloads.StormCase: defaults, INIT noise 0, scheme, analytic sounding, reset, then the
-    bubbles and seeded theta noise. Returns (model, B)."""
+def pack_ci(events, time=0.0):
+    """setCI's record (model.js:1383-1389): the towers still active after ``time`` (at most the last OB_MAX_CI),
+    12 float32 each. Returns (array, active events)."""
+    act = [e for e in events if e["t1"] > time][-N.MAX_CI:]
+    f = np.zeros(max(1, len(act)) * N.CI_FLOATS, np.float32)
+    for i, e in enumerate(act):
+        f[i * 12:(i + 1) * 12] = [e["x"], e["y"], e["zc"], e["rh"], e["rz"], e["wt"], e["t0"], e["t1"],
+                                  e.get("vx", 0) or 0, e.get("vy", 0) or 0, e.get("seed", i * 1.37),
+                                  e.get("ramp", 150) or 150]
+    return f, act
+
+
+def setup_case(case, bounds=None, ci=None):
+    """A RegionalModel for a workloads.StormCase: defaults, INIT noise 0, scheme, analytic sounding, optional
+    boundaries (boundaries.boundary_models records) and storm-start towers, reset, then the bubbles and seeded theta
+    noise. Returns (model, B)."""
     from . import workloads
     m = RegionalModel().allocate(spec={"dx": case.dx, "n": [case.nx, case.ny, case.nz]})
     m.params["noise"] = 0.0
     m.params["scheme"] = "thompson" if case.scheme == 1 else "lin"
     B, _ = workloads.base_state_for(case)
     m.set_base_state(B)
+    if bounds:
+        m.set_boundaries(bounds)
+    if ci:
+        m.set_ci(ci)
     m.reset()
     V = m.get_field(N.FIELD_V)
     m.set_field(N.FIELD_V, workloads.perturb_theta(case, V))

@@ -10,8 +10,10 @@ bar, map painting, upload retries, the replay UI) have no counterpart here.
 
 CIScheduler mirrors scheduleCI and towerCluster (app.js:1306-1433) for outbreak mode: Poisson-drawn starts in the open
 warm sector, each a 0-4 km updraft push that moves with the storm motion (the sounding's Bunkers right mover) plus
-0-5 satellite towers, all drawn from the run's mulberry32 stream (seeded as app.js:1646). Starts along boundaries
-need the boundary geometry of the UI and are not built; without boundaries the reference draws none either.
+0-5 satellite towers, all drawn from the run's mulberry32 stream (seeded as app.js:1646), and Poisson-drawn starts
+along each boundary with a trigger rate, 6-22 km into its warm side, their satellite ellipse laid along the boundary
+(app.js:1416-1432). The warm-sector draw skips points inside any boundary's air mass (other_weight > 0.25). The
+boundaries are boundaries.boundary_models records (the run's RUN.mbs).
 """
 from __future__ import annotations
 
@@ -21,14 +23,16 @@ import time
 
 import numpy as np
 
+from . import boundaries as BND
 from . import workloads as W
 
 CI_DEFAULTS = {"warmRate": 1.2, "start": 0.25, "end": 4.5, "seed": 7, "wt": 10.0, "rh": 12000.0, "auto": True}  # app.js:27
 
 
 class CIScheduler:
-    def __init__(self, model, ci=None, motion=(0.0, 0.0), log=None):
+    def __init__(self, model, ci=None, motion=(0.0, 0.0), log=None, bounds=None):
         self.m = model
+        self.mbs = list(bounds or [])
         self.ci = dict(CI_DEFAULTS, **(ci or {}))
         self.rng = W.Mulberry32((int(self.ci["seed"]) | 0) * 7919 + 13)
         self.motion = motion
@@ -106,34 +110,66 @@ class CIScheduler:
         sub = m0[max(0, j0 - r):min(ny - 1, j0 + r) + 1:2, max(0, i0 - r):min(nx - 1, i0 + r) + 1:2, 0]
         return bool((sub > 35).any())
 
-    # app.js:1402-1433, outbreak mode, warm sector
+    # app.js:1402-1433, outbreak mode: the open warm sector, then along each boundary
     def schedule(self, t, dt_win, maps=None):
         ci = self.ci
         if not ci["auto"] or t < ci["start"] * 3600 or t > ci["end"] * 3600:
             return 0
         Lx, Ly, mar = self.m.Lx, self.m.Ly, self.margin()
-        area = max(Lx - 2 * mar, 0.0) * max(Ly - 2 * mar, 0.0) / 1e6
+        area = (Lx - 2 * mar) * (Ly - 2 * mar) / 1e6
         n = self.poisson(ci["warmRate"] * area / 1e5 * dt_win / 3600)
         added = 0
         for _ in range(n):
             for _try in range(6):
                 x = mar + self.rng() * (Lx - 2 * mar)
                 y = mar + self.rng() * (Ly - 2 * mar)
-                if self.echo_near(maps, x, y, 35000.0):   # not into another storm (its push would stir its outflow)
+                # not into another storm (its push would stir its outflow), nor into a boundary's air mass
+                if BND.other_weight(self.mbs, x, y, t) > 0.25 or self.echo_near(maps, x, y, 35000.0):
                     continue
                 self.add_event(x, y, t, "warm sector")
                 added += 1
                 break
+        for mb in self.mbs:
+            b = mb.get("b")
+            if not b or not (b.get("rate", 0) > 0):
+                continue
+            P = BND.pts_at(mb, t)
+            segs, L = [], 0.0
+            for i in range(len(P) - 1):
+                a, e = P[i], P[i + 1]
+                ln = math.hypot(e[0] - a[0], e[1] - a[1])
+                segs.append((a, e, ln))
+                L += ln
+            n = self.poisson(b["rate"] * (L / 1e6) * dt_win / 3600)
+            for _ in range(n):
+                s, seg = self.rng() * L, segs[0]
+                for sg in segs:
+                    if s <= sg[2]:
+                        seg = sg
+                        break
+                    s -= sg[2]
+                a, e, ln = seg
+                f = s / max(ln, 1)
+                ux, uy = (e[0] - a[0]) / ln, (e[1] - a[1]) / ln
+                off = (6000 + self.rng() * 16000) * -mb["side"]          # into the warm side
+                x = a[0] + (e[0] - a[0]) * f + (-uy) * off
+                y = a[1] + (e[1] - a[1]) * f + ux * off
+                if x < mar or y < mar or x > Lx - mar or y > Ly - mar:
+                    continue
+                if self.echo_near(maps, x, y, 25000.0):
+                    continue
+                self.add_event(x, y, t, BND.BND_TYPES[b["type"]]["label"].lower(), math.atan2(uy, ux))
+                added += 1
         return added
 
 
 class RunLoop:
     def __init__(self, model, dt, t_end, radar=None, ci=None, motion=(0.0, 0.0), replay_every=180.0, out_dir=None,
-                 run="run", epoch0_ms=None, pace=0.0, batch_ms=60.0, tornadoes=None):
+                 run="run", epoch0_ms=None, pace=0.0, batch_ms=60.0, tornadoes=None, bounds=None):
         self.m, self.dt, self.t_end = model, float(dt), float(t_end)
         self.radar = radar
         self.log = []
-        self.ci = CIScheduler(model, ci, motion, self.log) if ci is not None else None
+        self.ci = CIScheduler(model, ci, motion, self.log, bounds) if ci is not None else None
         # tornadoes: None, or the keyword arguments of TornadoScheme (stp, rate, on, hurricane, ...)
         self.tor = None
         if tornadoes is not None:

@@ -228,3 +228,47 @@ def hydrometeor_blob(case: StormCase, B, seed=5, thompson=False):
     if thompson:
         q2[..., 2] = q1[..., 3] * 10 ** (5 + 2 * rng.random((nz, ny, nx)))  # rain number per kg
     return q1.astype(np.float32).reshape(-1), q2.astype(np.float32).reshape(-1)
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Air-mass boundaries and storm starts (app.js:52-56, 527-545, 1321-1345; model.js:1371-1389)
+# ---------------------------------------------------------------------------------------------------------------
+TRIPLE_POINT = (36.3, -99.9)   # where the example cold front, warm front and dryline meet (app.js:53-55)
+
+
+def case_fronts(nx=96, ny=88, nz=40, dx=2000.0, scheme=0):
+    """A parity case for the large-scale forcing: the reference's example fronts over a domain centred on their
+    triple point (2 km, dt 12 s: the LSF pass reruns after 5 steps), one warm bubble in the warm sector."""
+    Lx, Ly = nx * dx, ny * dx
+    return StormCase("fronts", nx, ny, nz, dx, 12.0, 6, scheme=scheme, bubbles=[(0.7 * Lx, 0.3 * Ly)],
+                     bubble_rh=min(10000.0, Lx / 8))
+
+
+def fronts_setup(case: StormCase, n_towers=2, seed=7, t0=-300.0):
+    """The boundaries and storm-start towers of ``case_fronts``: the reference's default cold front, warm front and
+    dryline (boundaries.default_bounds) projected about their triple point at the domain centre, with the surface lows'
+    joined motion and the sounding's 150 m wind (boundaries.boundary_models), and ``n_towers`` main towers drawn by
+    the run's storm-start scheduler in the warm sector, already pushing at t = 0 (started at ``t0``, no satellites).
+    Returns (bounds, events)."""
+    from . import boundaries as BND
+    from .radar import Geo
+    from .runloop import CIScheduler
+    text = weisman_klemp_sharppy(**case.wk)
+    A = snd_mod.analyze(snd_mod.parse_sharppy(text))
+    geo = Geo(TRIPLE_POINT[0], TRIPLE_POINT[1], case.nx * case.dx, case.ny * case.dx)
+    bounds = BND.boundary_models(BND.default_bounds(), geo, A.wind_at(0.15))
+
+    class _Dom:
+        Lx, Ly = case.nx * case.dx, case.ny * case.dx
+        time = 0.0
+
+        def set_ci(self, ev):
+            pass
+
+    sch = CIScheduler(_Dom(), {"seed": seed}, motion=A.rm)
+    events = []
+    spots = [(0.72, 0.28), (0.62, 0.42), (0.80, 0.40)]   # the warm sector: south-east of the triple point
+    for k in range(n_towers):
+        x, y = spots[k % len(spots)]
+        events.append(sch.tower_cluster(x * case.nx * case.dx, y * case.ny * case.dx, t0, "warm sector")[0])
+    return bounds, events

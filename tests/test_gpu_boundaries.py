@@ -1,0 +1,92 @@
+"""GPU parity of the large-scale forcing with air-mass boundaries and of active storm starts, against the CPU oracle
+(FP32 restatement) and its FP64 instantiation, through the C ABI.
+
+The boundaries are the reference's example cold front, warm front and dryline (app.js:52-56) built by its host
+geometry (bndModel, app.js:527-541; the surface low's joined motion, app.js:495-527) and packed as setBoundaries does
+(model.js:1371-1380); the domain is centred on their triple point. Two storm-start towers drawn by the run's scheduler
+are already pushing at t = 0 (setCI, model.js:1383-1389). So the LSF pass (model.js:142-244: polyline distance,
+along-front variation, hot spots, the target's hydrostatic phi), the CI pass (model.js:249-281) and PHYS's nudging
+toward the target and updraft push (model.js:628-700) all run with nonzero weights on both sides.
+
+Bars (tests/_parity.py): one step max(1e-5, 2 x the FP32 oracle's error) per field and channel; six steps (72 s,
+through the second LSF pass at t = 60 s) max(1e-4, 3 x), as the five-step storm test.
+"""
+import numpy as np
+import pytest
+
+from outbreaklab_b200 import _native as N, model as M, workloads as W
+
+from _parity import check_field
+
+pytestmark = pytest.mark.gpu
+
+STATE = ((N.FIELD_V, 4), (N.FIELD_Q1, 4), (N.FIELD_Q2, 4), (N.FIELD_AUX, 2), (N.FIELD_PHI, 1))
+FORCING = ((N.FIELD_LSF_A, 4), (N.FIELD_LSF_B, 4), (N.FIELD_PHT, 1))
+
+
+def _setup(oracle_lib, scheme):
+    case = W.case_fronts(scheme=scheme)
+    bounds, events = W.fronts_setup(case)
+    g, _ = M.setup_case(case, bounds=bounds, ci=events)
+    f, _ = oracle_lib.setup_case(case, 4, bounds=bounds, ci=events)
+    d, _ = oracle_lib.setup_case(case, 8, bounds=bounds, ci=events)
+    return case, g, f, d
+
+
+def _compare(g, f, d, fields, tol, envelope):
+    bad = []
+    for fld, ch in fields:
+        _, b = check_field(fld, g.get_field(fld), f.get(fld), d.get(fld, f64=True), ch, tol, envelope)
+        bad += b
+    return bad
+
+
+def _active(g, d):
+    """The forcing is not trivially zero on either side: a temperature anomaly, a nudging weight and an updraft push."""
+    for name, get in (("GPU", lambda fl: g.get_field(fl)), ("FP64 oracle", lambda fl: d.get(fl, f64=True))):
+        A = get(N.FIELD_LSF_A).reshape(-1, 4)
+        B = get(N.FIELD_LSF_B).reshape(-1, 4)
+        C = get(N.FIELD_CI_MAP).reshape(-1, 4)
+        assert np.abs(A[:, 0]).max() > 1.0, name + ": no air-mass temperature anomaly"
+        assert (B[:, 3] > 0.5).sum() > 100, name + ": no nudging weight"
+        assert ((C[:, 0] * C[:, 1]) > 0.5).sum() > 10, name + ": no storm-start push"
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_forcing_fields_after_reset(oracle_lib, native, scheme):
+    """reset runs LSF (model.js:1431-1434): lsfA, lsfB and phT against the oracle."""
+    case, g, f, d = _setup(oracle_lib, scheme)
+    bad = _compare(g, f, d, FORCING, 1e-5, 2.0)
+    assert not bad, "\n".join(bad)
+    A = g.get_field(N.FIELD_LSF_A).reshape(-1, 4)
+    assert A[:, 0].min() < -5.0 and A[:, 0].max() > 1.0   # cold air behind the fronts, warm dry air behind the dryline
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_one_step_with_fronts_and_storm_starts(oracle_lib, native, scheme):
+    case, g, f, d = _setup(oracle_lib, scheme)
+    for m in (g, f, d):
+        m.step(case.dt, 1)
+    g.sync()
+    _active(g, d)
+    bad = _compare(g, f, d, STATE + FORCING + ((N.FIELD_CI_MAP, 4),), 1e-5, 2.0)
+    assert not bad, "\n".join(bad)
+    assert g.nan_count == 0
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_six_steps_through_an_lsf_cycle(oracle_lib, native, scheme):
+    """72 s: the LSF pass reruns at t = 60 s with the boundaries moved (points at p + v t, the triple point with the
+    low's mean motion)."""
+    case, g, f, d = _setup(oracle_lib, scheme)
+    A0 = g.get_field(N.FIELD_LSF_A)
+    for m in (g, f, d):
+        m.step(case.dt, 6)
+    g.sync()
+    assert abs(g.time - 72.0) < 1e-9 and abs(d.time - 72.0) < 1e-9
+    assert not np.array_equal(A0, g.get_field(N.FIELD_LSF_A)), "the LSF pass did not rerun at t = 60 s"
+    _active(g, d)
+    bad = _compare(g, f, d, FORCING + ((N.FIELD_CI_MAP, 4),), 1e-5, 2.0)
+    bad += _compare(g, f, d, STATE, 1e-4, 3.0)
+    assert not bad, "\n".join(bad)
+    assert g.nan_count == 0

@@ -85,3 +85,27 @@ def test_storm_step_at_full_size(native):
     finally:
         a.destroy()
         b.destroy()
+
+
+def test_storm_step_at_full_size_matches_the_oracle(native):
+    """One step of the 640 x 640 x 40 workload the benchmark times, every field and channel against the FP64 oracle
+    within max(1e-5, 2 x the FP32 oracle's own error) (tests/_parity.py)."""
+    from _parity import check_field
+    case = W.case_c2()
+    g, _ = M.setup_case(case)
+    f, _ = O.setup_case(case, 4)
+    d, _ = O.setup_case(case, 8)
+    try:
+        for m in (g, f, d):
+            m.step(case.dt, 1)
+        g.sync()
+        bad = []
+        for fld, ch in ((N.FIELD_V, 4), (N.FIELD_Q1, 4), (N.FIELD_Q2, 4), (N.FIELD_AUX, 2), (N.FIELD_PHI, 1)):
+            errs, b = check_field(fld, g.get_field(fld), f.get(fld), d.get(fld, f64=True), ch)
+            print("640x640x40 field %d: " % fld + ", ".join("GPU %.2e / FP32 %.2e" % e for e in errs))
+            bad += b
+        assert not bad, "\n".join(bad)
+        assert g.nan_count == 0
+    finally:
+        g.destroy()
+        del f, d
