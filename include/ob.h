@@ -204,7 +204,8 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
 int ob_model_set_graphs(ObModel* m, int on);
 /* pressure-solve precision of the model: 0 = fp32 SIMT transforms (the reference's arithmetic), 1 = bf16x3
  * tensor-core transforms, 2 = bf16x3 + one bf16x3 refinement sweep (the default where nz is 16, 40 or 80),
- * 3 = bf16x3 + one plain-bf16 refinement sweep.
+ * 3 = bf16x3 + one plain-bf16 refinement sweep, 4 = bf16x3 + two bf16x3 refinement sweeps (the residual at the
+ * floor that storing phi in fp32 sets).
  * No counterpart in the reference. */
 int ob_model_set_solver(ObModel* m, int precision);
 int ob_model_solver(ObModel* m);
@@ -214,7 +215,8 @@ void* ob_model_stream(ObModel* m);
 /* ---- PoissonDirect (solver.js:105-165) ---- */
 /* replaces new PoissonDirect(nx, ny, nz, dx, dz) (solver.js:106-137); precision 0 = FP32 SIMT transforms,
  * 1 = bf16x3 tensor-core transforms (FP32 accumulate), 2 = the same plus one iterative-refinement sweep on the
- * FP64-accumulated residual, 3 = that sweep in plain bf16 (precisions 1 to 3 need nz in {16, 40, 80}) */
+ * FP64-accumulated residual, 3 = that sweep in plain bf16, 4 = two bf16x3 refinement sweeps (precisions 1 to 4 need
+ * nz in {16, 40, 80}) */
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out);
 int ob_poisson_destroy(ObPoisson* p);
 /* replaces setDensity (solver.js:139-146): rhoC[nz] at centres, rhoW[nz+1] at bottom faces */
@@ -226,6 +228,11 @@ int ob_poisson_solve_device(ObPoisson* p, const float* d_rhs, float* d_phi, void
 /* device time of one solve on the handle's buffers (the last uploaded right-hand side), averaged over reps solves
  * bracketed by CUDA events; no counterpart in the reference */
 int ob_poisson_time(ObPoisson* p, int reps, float* ms);
+/* the residual r = rhs - A phi of the handle's last solve (the last uploaded right-hand side and its solution),
+ * accumulated in FP64 on the device, A the operator the solve inverts (solver.js:139-146: the horizontal Laplacian
+ * with phi = 0 beyond the grid, the z-operator with Neumann ends): *max_rel = max|r| / max|rhs|,
+ * *l2_rel = ||r||_2 / ||rhs||_2. A diagnostic of the solve's precision; no counterpart in the reference. */
+int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel);
 
 /* ---- RadarSim (radar.js:271-413): virtual WSR-88D gate sampling ----
  * The host keeps RadarSim's VCP tables, volume layout and scan scheduling (radar.js:289-392); the library owns each
@@ -332,8 +339,13 @@ int ob_mlp_write_pairs(ObMlp* n, const float* host, long long count);  /* replac
  * normalised units) and its gradient with respect to every parameter (OB_MLP_NPARAM floats) */
 int ob_mlp_grad(ObMlp* n, const float* pairs, int count, double* loss, float* grad);
 int ob_mlp_eval(ObMlp* n, const float* pairs, int count, float* out);  /* count x OB_MLP_NOUT tendencies */
-/* `steps` Adam steps on batches of `batch` pairs drawn from the recorded pairs; mean loss over the steps */
+/* `steps` Adam steps on batches of `batch` pairs drawn from the recorded pairs; mean loss over the steps. A seed and
+ * the recorded pairs fix the result: every batch reduction adds its partial sums in a fixed order. */
 int ob_mlp_train(ObMlp* n, int batch, int steps, float lr, unsigned seed, double* mean_loss);
+/* the arithmetic of ob_mlp_train and ob_mlp_grad: 1 (the default) = BF16 operands with FP32 accumulation on the
+ * tensor cores (tcgen05), the bias, GELU and its derivative, the loss and dY fused into the GEMM epilogues, for
+ * batches that are a multiple of 128 (others use mode 0); 0 = FP32 SIMT kernels */
+int ob_mlp_set_training(ObMlp* n, int mode);
 /* record pairs of the plain scheme into net's buffer on every following step, each candidate cell (one the scheme
  * can change) with probability rate; rate 0 stops */
 int ob_model_record_micro(ObModel* m, ObMlp* net, float rate);

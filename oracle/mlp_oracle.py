@@ -111,6 +111,45 @@ def loss_and_grad(params, pairs, norm):
     return loss, pack(g)
 
 
+def loss_and_grad_bf16(params, pairs, norm):
+    """The tensor-core training kernels' loss and gradient (ob_mlp_train_tc.cu), in float64 with bf16 rounding at the
+    same points: the normalised inputs, the weights, every hidden activation, dY and every dZ are bf16 operands; the
+    products accumulate exactly (the kernels accumulate in fp32); GELU' is taken of the unrounded pre-activation. The
+    bias gradients sum the bf16 operands (the kernels get them from a row of ones appended to the GEMM)."""
+    p = unpack(params)
+    pairs = np.asarray(pairs, np.float64)
+    n = split_norm(norm)
+    f32 = np.float32
+    raw = pairs[:, :NIN].astype(f32)
+    fe = raw.copy()
+    fe[:, 3:9] = np.log(np.maximum(fe[:, 3:9], f32(0)) + f32(1e-9))
+    fe[:, 9] = np.log(np.maximum(fe[:, 9], f32(0)) + f32(1))
+    X = bf16((fe - n["in_mean"].astype(f32)) * n["in_scale"].astype(f32))
+    sc = n["out_scale"]
+    T = np.where(sc > 0, (pairs[:, NIN:NIN + NOUT].astype(f32) / np.where(sc > 0, sc, 1.0).astype(f32)).astype(np.float64), 0.0)
+    B = X.shape[0]
+    W = {l: bf16(p["W%d" % l]) for l in (1, 2, 3, 4)}
+    hs, gs, h = [X], [], X
+    for l in (1, 2, 3):
+        z = h @ W[l].T + p["b%d" % l].astype(f32).astype(np.float64)
+        gs.append(gelu_grad(z))
+        h = bf16(gelu(z))
+        hs.append(h)
+    Y = h @ W[4].T + p["b4"]
+    D = np.zeros_like(Y)
+    D[:, :NLOSS] = Y[:, :NLOSS] - T[:, :NLOSS]
+    loss = float((D ** 2).sum() / (B * NLOSS))
+    dY = bf16(np.float32(2.0 / (B * NLOSS)) * D.astype(np.float32))
+    g = {"W4": dY.T @ hs[3], "b4": dY.sum(0)}
+    dh = dY @ W[4]
+    for l in (3, 2, 1):
+        dz = bf16(dh * gs[l - 1])
+        g["W%d" % l] = dz.T @ hs[l - 1]
+        g["b%d" % l] = dz.sum(0)
+        dh = dz @ W[l]
+    return loss, pack(g)
+
+
 CPD, RV, LV, LF, LS, T0 = 1005.7, 461.5, 2.501e6, 3.337e5, 2.834e6, 273.15
 NEW_SPECIES_FLOOR = 1e-8
 

@@ -79,6 +79,7 @@ SYMBOLS = {
     "ob_poisson_solve": (_i, [_vp, _fp, _fp]),
     "ob_poisson_solve_device": (_i, [_vp, _vp, _vp, _vp]),
     "ob_poisson_time": (_i, [_vp, _i, _fp]),
+    "ob_poisson_residual": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ob_dst_tc_selftest": (_i, [_i, _i, _i, _i, _fp, _fp, _fp]),
     "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),
     "ob_radar_create": (_i, [_vp, _sz, _i, C.POINTER(_vp)]),
@@ -103,6 +104,7 @@ SYMBOLS = {
     "ob_mlp_grad": (_i, [_vp, _fp, _i, C.POINTER(_d), _fp]),
     "ob_mlp_eval": (_i, [_vp, _fp, _i, _fp]),
     "ob_mlp_train": (_i, [_vp, _i, _i, _f, C.c_uint, C.POINTER(_d)]),
+    "ob_mlp_set_training": (_i, [_vp, _i]),
     "ob_model_record_micro": (_i, [_vp, _vp, _f]),
     "ob_model_set_graphs": (_i, [_vp, _i]),
     "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),

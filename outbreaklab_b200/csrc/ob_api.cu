@@ -867,7 +867,7 @@ int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks) 
 }
 
 int ob_model_set_solver(ObModel* m, int precision) {
-  if (!m || precision < 0 || precision > 3) { set_error("ob_model_set_solver: precision must be 0, 1, 2 or 3"); return OB_ERR_INVALID; }
+  if (!m || precision < 0 || precision > 4) { set_error("ob_model_set_solver: precision must be 0 to 4"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
   if (precision >= 1 && g.nz != 16 && g.nz != 40 && g.nz != 80) {
     set_error("ob_model_set_solver: the tensor-core solve supports nz in {16, 40, 80}");
@@ -1462,11 +1462,12 @@ struct ObPoisson {
   PoissonPlan plan;
   float* d_rhs = nullptr;
   float* d_phi = nullptr;
+  double* d_norm = nullptr;  // residual-norm scratch (ob_poisson_residual)
   cudaStream_t stream = nullptr;
 };
 
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out) {
-  if (!out || precision < 0 || precision > 3) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
+  if (!out || precision < 0 || precision > 4) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
   *out = nullptr;
   ObPoisson* p = new ObPoisson();
   int rc = p->plan.create(nx, ny, nz, dx, dz, precision);
@@ -1487,8 +1488,18 @@ int ob_poisson_destroy(ObPoisson* p) {
   p->plan.destroy();
   if (p->d_rhs) cudaFree(p->d_rhs);
   if (p->d_phi) cudaFree(p->d_phi);
+  if (p->d_norm) cudaFree(p->d_norm);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
+  return OB_OK;
+}
+int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel) {
+  if (!p || !max_rel || !l2_rel) { set_error("ob_poisson_residual: null argument"); return OB_ERR_INVALID; }
+  if (!p->d_norm) OB_TRY(cuda_status(cudaMalloc(&p->d_norm, (4 * 1024 + 4) * sizeof(double)), "poisson residual"));
+  double rel[2];
+  OB_TRY(poisson_residual(p->plan, p->d_rhs, p->d_phi, p->d_norm, rel, p->stream));
+  *max_rel = rel[0];
+  *l2_rel = rel[1];
   return OB_OK;
 }
 int ob_poisson_set_density(ObPoisson* p, const float* rhoC, const float* rhoW) {

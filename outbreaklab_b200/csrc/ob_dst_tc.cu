@@ -358,6 +358,67 @@ __global__ void k_resid(int nx, int ny, int nz, double idx2, const float4* __res
                         const float* __restrict__ phi, __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld) {
   resid_body(nx, ny, nz, idx2, zop, rhs, phi, hi, lo, ld, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+// FP64 norms of the residual r = rhs - A phi (A as in resid_body) and of rhs, over a grid-stride loop: each block
+// writes (max|r|, sum r^2, max|rhs|, sum rhs^2) to part[4 * blockIdx.x]; k_norm_final combines them in block order
+__global__ void __launch_bounds__(256) k_resid_norm(int nx, int ny, int nz, double idx2, const float4* __restrict__ zop,
+                                                    const float* __restrict__ rhs, const float* __restrict__ phi,
+                                                    double* __restrict__ part) {
+  __shared__ double red[4][8];
+  const long pl = long(nx) * ny, n = pl * nz;
+  double rmax = 0.0, rss = 0.0, bmax = 0.0, bss = 0.0;
+  for (long o = blockIdx.x * long(blockDim.x) + threadIdx.x; o < n; o += long(gridDim.x) * blockDim.x) {
+    const int k = int(o / pl);
+    const long q = o - k * pl;
+    const int j = int(q / nx), i = int(q - long(j) * nx);
+    const double p = phi[o];
+    const double xm = i > 0 ? double(phi[o - 1]) : -p, xp = i < nx - 1 ? double(phi[o + 1]) : -p;
+    const double ym = j > 0 ? double(phi[o - nx]) : -p, yp = j < ny - 1 ? double(phi[o + nx]) : -p;
+    const float4 z = __ldg(zop + k);
+    const double zm = k > 0 ? double(phi[o - pl]) : 0.0, zp = k < nz - 1 ? double(phi[o + pl]) : 0.0;
+    const double b = rhs[o];
+    const double r = b - (double(z.w) * (xm + xp + ym + yp - 4.0 * p) * idx2 + double(z.x) * zm + double(z.z) * p + double(z.y) * zp);
+    rmax = fmax(rmax, fabs(r));
+    rss += r * r;
+    bmax = fmax(bmax, fabs(b));
+    bss += b * b;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    rss += __shfl_xor_sync(0xffffffffu, rss, o);
+    bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    bss += __shfl_xor_sync(0xffffffffu, bss, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { red[0][w] = rmax; red[1][w] = rss; red[2][w] = bmax; red[3][w] = bss; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0, c = 0, d = 0;
+    for (int u = 0; u < int(blockDim.x >> 5); u++) { a = fmax(a, red[0][u]); b += red[1][u]; c = fmax(c, red[2][u]); d += red[3][u]; }
+    part[4 * blockIdx.x + 0] = a; part[4 * blockIdx.x + 1] = b; part[4 * blockIdx.x + 2] = c; part[4 * blockIdx.x + 3] = d;
+  }
+}
+__global__ void k_norm_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  double a = 0, b = 0, c = 0, d = 0;
+  for (int u = 0; u < nb; u++) { a = fmax(a, part[4 * u]); b += part[4 * u + 1]; c = fmax(c, part[4 * u + 2]); d += part[4 * u + 3]; }
+  out[0] = a; out[1] = b; out[2] = c; out[3] = d;
+}
+
+// residual of phi for rhs under the solve's operator, in FP64 on the device: rel[0] = max|r| / max|rhs|,
+// rel[1] = ||r||_2 / ||rhs||_2 (scratch: 4 * 1024 + 4 doubles)
+int poisson_residual(const PoissonPlan& P, const float* rhs, const float* phi, double* scratch, double rel[2], cudaStream_t s) {
+  constexpr int nb = 1024;
+  k_resid_norm<<<nb, 256, 0, s>>>(P.nx, P.ny, P.nz, 1.0 / (P.dx * P.dx), P.zop, rhs, phi, scratch);
+  k_norm_final<<<1, 1, 0, s>>>(scratch, nb, scratch + 4 * nb);
+  double h[4];
+  if (cudaMemcpyAsync(h, scratch + 4 * nb, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+    set_error("poisson residual: %s", cudaGetErrorString(cudaGetLastError()));
+    return OB_ERR_DEVICE;
+  }
+  rel[0] = h[2] > 0 ? h[0] / h[2] : 0.0;
+  rel[1] = h[3] > 0 ? std::sqrt(h[1] / h[3]) : 0.0;
+  return OB_OK;
+}
+
 struct ResidProb {
   int nx, ny, nz, ld;
   double idx2;
@@ -466,6 +527,127 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
     __syncthreads();
   }
 }
+// ---------------------------------------------------------------------------------------------------------------
+// The tridiagonals of one model's solve through shared memory, every transfer a TMA tile (solver.js:70-103).
+// A block takes 32 l x 8 m modes (one per thread; warp = 32 consecutive l at one m):
+//   1. one 3-D TMA load brings the block's [NZ][8][32] fp32 tile of T2[k][m][l] into shared memory (zero outside);
+//   2. each thread runs the Thomas sweep of its mode: c' in registers, d and then x updated in place in the tile
+//      (the tile row of a warp is 32 consecutive floats: no bank conflicts), the 2 x 2 lowest modes in FP64 with the
+//      host-factored coefficients;
+//   3. the tile is written out KC levels at a time, transposed: each thread reads one (level, l) column of 8 m,
+//      splits it into bf16 hi / lo and writes the two 16-byte rows back into the region of those levels (read first,
+//      then a barrier, then written), and one thread issues two 3-D TMA stores of [KC][32][8] into S_y[k][l][m].
+// About 64 registers and NZ KB of shared memory per 256-thread block, so several blocks share an SM and one block's
+// loads overlap another's sweeps and stores; the transposes cost one shared-memory read and write per element.
+// ---------------------------------------------------------------------------------------------------------------
+constexpr int TRI_TL = 32, TRI_TM = 8, TRI_KC = 8;
+template <int NZ>
+constexpr int tri_smem_bytes() { return NZ * TRI_TM * TRI_TL * 4 + 4 * NZ * 8 /*FP64 low modes*/ + 128 /*align*/ + 16 /*barrier*/; }
+
+template <int NZ>
+__global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(const __grid_constant__ CUtensorMap tIn, const __grid_constant__ CUtensorMap tHi,
+                                                          const __grid_constant__ CUtensorMap tLo, int nxp, int nyp,
+                                                          const float* __restrict__ lam, const float4* __restrict__ zop,
+                                                          const double* __restrict__ low, unsigned int* err) {
+  static_assert(NZ % TRI_KC == 0, "levels come in whole chunks");
+  extern __shared__ uint8_t smraw[];
+  float* tile = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+  double* dlow = reinterpret_cast<double*>(tile + NZ * TRI_TM * TRI_TL);   // [4][NZ]: d of the FP64 low modes
+  uint64_t* bar = reinterpret_cast<uint64_t*>(dlow + 4 * NZ);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, tid = threadIdx.x;
+  const int l0 = blockIdx.x * TRI_TL, m0 = blockIdx.y * TRI_TM;
+  if (tid == 0) {
+    tc::prefetch_tmap(&tIn);
+    tc::mbar_init(bar, 1);
+    tc::fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    tc::mbar_expect_tx(bar, NZ * TRI_TM * TRI_TL * 4);
+    tc::tma_load_3d(tile, &tIn, bar, l0, m0, 0);
+  }
+  const int l = l0 + tx, m = m0 + ty;
+  const bool act = l < nxp && m < nyp;
+  // what the sweep needs besides the tile, fetched while the tile is in flight
+  const float shift = act ? __ldg(lam + l) + __ldg(lam + nxp + m) : 0.f;
+  // one thread waits (bounded) for the tile and tells the others; if it never arrived the error word reports it and
+  // every thread leaves before touching the tile
+  __shared__ int s_ok;
+  if (tid == 0) s_ok = tc::mbar_wait(bar, 0, err, 16u) ? 1 : 0;
+  __syncthreads();
+  if (!s_ok) return;
+  float* col = tile + ty * TRI_TL + tx;           // element k of this mode: col[k * TRI_TM * TRI_TL]
+  constexpr int LS = TRI_TM * TRI_TL;
+  if (act && !(l < 2 && m < 2)) {
+    float cp[NZ];
+    float cprev = 0.f, dprev = 0.f;
+#pragma unroll
+    for (int k = 0; k < NZ; k++) {
+      const float4 o = __ldg(zop + k);
+      const float rd = __frcp_rn(o.z + shift * o.w - o.x * cprev);
+      cprev = o.y * rd;
+      dprev = (col[k * LS] - o.x * dprev) * rd;
+      cp[k] = cprev;
+      col[k * LS] = dprev;
+    }
+    float x = dprev;
+#pragma unroll
+    for (int k = NZ - 2; k >= 0; k--) {
+      x = col[k * LS] - cp[k] * x;
+      col[k * LS] = x;
+    }
+  } else if (act) {
+    // lowest modes: low[(mode*2 + 0)*NZ + k] = 1/den_k, low[(mode*2 + 1)*NZ + k] = c'_k (FP64, host-factored)
+    const int mode = m * 2 + l;
+    const double* rd = low + (mode * 2) * NZ;
+    const double* cpd = rd + NZ;
+    double* d = dlow + mode * NZ;
+    double dprev = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < NZ; k++) {
+      dprev = (double(col[k * LS]) - double(__ldg(zop + k).x) * dprev) * rd[k];
+      d[k] = dprev;
+    }
+    double x = dprev;
+    col[(NZ - 1) * LS] = float(x);
+#pragma unroll 1
+    for (int k = NZ - 2; k >= 0; k--) {
+      x = d[k] - cpd[k] * x;
+      col[k * LS] = float(x);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NZ; k++) col[k * LS] = 0.f;   // modes past the grid: zeros (the padding of the output rows)
+  }
+  __syncthreads();
+  // transposed output, TRI_KC levels at a time: thread -> (level kk of the chunk, l); its 8 m go out as one 16-byte
+  // row of hi and one of lo, at [kk][l][0..7] of the chunk's hi and lo halves
+  const int kk = tid >> 5, lx = tid & 31;
+  for (int k0 = 0; k0 < NZ; k0 += TRI_KC) {
+    float* chunk = tile + k0 * LS;
+    float v[TRI_TM];
+#pragma unroll
+    for (int u = 0; u < TRI_TM; u++) v[u] = chunk[kk * LS + u * TRI_TL + lx];
+    __align__(16) __nv_bfloat16 h16[TRI_TM], l16[TRI_TM];
+#pragma unroll
+    for (int u = 0; u < TRI_TM; u++) tc::split_bf16(v[u], h16[u], l16[u]);
+    __syncthreads();   // every read of this chunk is done before it is overwritten
+    uint4* hi = reinterpret_cast<uint4*>(chunk);
+    uint4* lo = reinterpret_cast<uint4*>(chunk) + TRI_KC * TRI_TL;
+    hi[kk * TRI_TL + lx] = *reinterpret_cast<const uint4*>(h16);
+    lo[kk * TRI_TL + lx] = *reinterpret_cast<const uint4*>(l16);
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tma_store_3d(&tHi, hi, m0, l0, k0);
+      tc::tma_store_3d(&tLo, lo, m0, l0, k0);
+      tc::bulk_commit();
+    }
+  }
+  if (tid == 0) tc::bulk_wait_read_all();   // the shared memory stays until the stores have read it
+}
+// the same solve with plain loads and stores (tri_body), for planes whose pitch a tensor map cannot describe (T2's
+// row pitch nxp * 4 bytes not a multiple of 16)
 template <int NZ>
 __global__ void __launch_bounds__(32 * tri_tm<NZ>()) k_tri_tc(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
                                                 const double* __restrict__ low, const float* __restrict__ T2,
@@ -534,6 +716,20 @@ static bool make_map_2d(CUtensorMap* m, void* base, long rows, long cols, long l
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 3-D tensor, innermost dimension first: dims[3] elements, pitches (bytes) of dimensions 1 and 2, box[3], no swizzle;
+// loads past the tensor read zeros, stores past it are dropped
+static bool make_map_3d(CUtensorMap* m, CUtensorMapDataType type, void* base, const long* dims, const long* pitch_bytes,
+                        const int* box) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t d[3] = {cuuint64_t(dims[0]), cuuint64_t(dims[1]), cuuint64_t(dims[2])};
+  cuuint64_t st[2] = {cuuint64_t(pitch_bytes[0]), cuuint64_t(pitch_bytes[1])};
+  cuuint32_t b[3] = {cuuint32_t(box[0]), cuuint32_t(box[1]), cuuint32_t(box[2])};
+  cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, type, 3, base, d, st, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // tile width for N transform outputs: the fewest tiles of at most 256, then the smallest multiple of 16 covering N
 static int pick_bn(int N, int cap = BNMAX) {
   const int nt = (N + cap - 1) / cap;
@@ -567,6 +763,9 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_tri_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
+    cudaFuncSetAttribute(k_tri_tma<80>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
     attr = true;
   }
 }
@@ -591,6 +790,8 @@ struct TcPlan {
   long qld[4] = {};
   int qdim[4] = {};
   CUtensorMap Fx[2], Fy[2], Fr[2], Frr[2];  // fields, the A operand: S_x, S_y, the split right-hand side and residual
+  CUtensorMap tri_in, tri_out[2];  // the tridiagonals' tiles: T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi / lo out
+  bool tri_tma = false;
 };
 
 static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
@@ -666,6 +867,16 @@ int PoissonPlan::tc_create() {
     set_error("poisson: tensor map encoding failed");
     return OB_ERR_DEVICE;
   }
+  // the tridiagonals' tiles (k_tri_tma); when T2's row pitch is not a multiple of 16 bytes the plain-load kernel runs
+  if ((nz == 16 || nz == 40 || nz == 80) && (long(nx) * 4) % 16 == 0) {
+    const long din[3] = {nx, ny, nz}, pin[2] = {long(nx) * 4, long(nx) * ny * 4};
+    const int bin[3] = {TRI_TL, TRI_TM, nz};
+    const long dout[3] = {T->ldy, nx, nz}, pout[2] = {T->ldy * 2, T->ldy * nx * 2};
+    const int bout[3] = {TRI_TM, TRI_TL, TRI_KC};
+    T->tri_tma = make_map_3d(&T->tri_in, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, T->t2, din, pin, bin) &&
+                 make_map_3d(&T->tri_out[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, T->sy_hi, dout, pout, bout) &&
+                 make_map_3d(&T->tri_out[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, T->sy_lo, dout, pout, bout);
+  }
   set_smem_attrs();
   return tc_factor_low();
 }
@@ -728,7 +939,14 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
   else launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
   // tridiagonals -> S_y[k][l][m]
-  switch (nz) {
+  if (T->tri_tma) {
+    const dim3 grid((nx + TRI_TL - 1) / TRI_TL, (ny + TRI_TM - 1) / TRI_TM);
+    switch (nz) {
+      case 16: k_tri_tma<16><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<16>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
+      case 40: k_tri_tma<40><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<40>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
+      default: k_tri_tma<80><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<80>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
+    }
+  } else switch (nz) {
     case 16: k_tri_tc<16><<<dim3((nx + 31) / 32, (ny + tri_tm<16>() - 1) / tri_tm<16>()), dim3(32, tri_tm<16>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
     case 40: k_tri_tc<40><<<dim3((nx + 31) / 32, (ny + tri_tm<40>() - 1) / tri_tm<40>()), dim3(32, tri_tm<40>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
     default: k_tri_tc<80><<<dim3((nx + 31) / 32, (ny + tri_tm<80>() - 1) / tri_tm<80>()), dim3(32, tri_tm<80>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
@@ -746,7 +964,8 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
 
 // precision 1: one bf16x3 pass; precision 2: a second bf16x3 pass on the FP64-accumulated residual (iterative
 // refinement); precision 3: the second pass in plain bf16 (the correction is ~5e-4 of the solution, so bf16 accuracy
-// of it leaves an error near 5e-4 x 4e-3 of the solution).
+// of it leaves an error near 5e-4 x 4e-3 of the solution); precision 4: two bf16x3 refinement sweeps, which leave the
+// solution within about an fp32 rounding of the exact one (the residual at the floor set by storing phi in fp32).
 // rhs: the fp32 right-hand side (nx*ny*nz), needed by precision 2 and by either when the split is not pre-made
 // (presplit: the model's divergence pass writes the split into rx itself).
 int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
@@ -759,8 +978,11 @@ int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
   if (!presplit) k_split_rows<<<1184, 256, 0, s>>>(rhs, long(nz) * ny, nx, T->rx_hi, T->rx_lo, int(T->ldx));
   tc_pass(*this, T, lam, zop, phi, false, s);
   if (precision >= 2) {
-    k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rr_hi, T->rr_lo, int(T->ldx));
-    tc_pass(*this, T, lam, zop, phi, true, s, precision == 3);
+    const int sweeps = precision == 4 ? 2 : 1;
+    for (int sw = 0; sw < sweeps; sw++) {
+      k_resid<<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(nx, ny, nz, 1.0 / (dx * dx), zop, rhs, phi, T->rr_hi, T->rr_lo, int(T->ldx));
+      tc_pass(*this, T, lam, zop, phi, true, s, precision == 3);
+    }
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -984,8 +1206,11 @@ static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one =
 int tc_group_solve(TcGroup* G, cudaStream_t s) {
   tc_group_pass(G, false, s);
   if (G->precision >= 2) {
-    k_resid_grp<<<dim3(G->res_blocks, 1, G->nz), 128, 0, s>>>(G->d_res, G->d_res_map);
-    tc_group_pass(G, true, s, G->precision == 3);
+    const int sweeps = G->precision == 4 ? 2 : 1;
+    for (int sw = 0; sw < sweeps; sw++) {
+      k_resid_grp<<<dim3(G->res_blocks, 1, G->nz), 128, 0, s>>>(G->d_res, G->d_res_map);
+      tc_group_pass(G, true, s, G->precision == 3);
+    }
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -1,6 +1,7 @@
-// ob_mlp.cu — training of the microphysics surrogate on the GPU (sm_100a): fp32 SIMT forward and backward kernels,
-// Adam, and the C ABI of the network (ob_mlp_*). The inference kernel that runs inside the model step is in
-// ob_mlp_tc.cu.
+// ob_mlp.cu — the C ABI of the microphysics surrogate (ob_mlp_*) and its fp32 SIMT training kernels (sm_100a):
+// forward and backward kernels and Adam, the reference arithmetic for the gradient check and the path for batches that
+// are not a multiple of 128. The default training runs on the tensor cores (ob_mlp_train_tc.cu); the inference kernel
+// that runs inside the model step is in ob_mlp_tc.cu.
 //
 // One training step on a batch of B recorded pairs: gather + normalise (k_gather), three hidden layers
 // Z = H W^T + b, H' = gelu(Z) and the output layer (k_gemm<false, true>), the mean squared error of the 8 scheme
@@ -22,17 +23,13 @@ void set_error(const char* fmt, ...);
 
 namespace mlp {
 
-// GELU, tanh form (Hendrycks and Gimpel): g(z) = z/2 (1 + tanh(c (z + a z^3))), c = sqrt(2/pi), a = 0.044715
-constexpr float GC = 0.7978845608f, GA = 0.044715f;
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + tanhf(GC * (z + GA * z * z * z))); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  const float t = tanhf(GC * (z + GA * z * z * z));
-  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * GC * (1.f + 3.f * GA * z * z);
-}
+constexpr int kMaxSplits = 64;   // batch splits of a weight-gradient GEMM (partial-sum slices of NH x NH floats)
 
-// C[M][N] (+)= op(A) op(B) (+ bias[n]) in fp32; AT: A is stored [K][M] (else [M][K]); BT: B is stored [N][K] (else
-// [K][N]). 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread; blockIdx.z splits K, and a split of more than one
-// adds its partial sum into C atomically (C zeroed by the caller).
+
+// C[M][N] = op(A) op(B) (+ bias[n]) in fp32; AT: A is stored [K][M] (else [M][K]); BT: B is stored [N][K] (else
+// [K][N]). 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread; blockIdx.z splits K: with more than one split,
+// split z writes its partial sum to its own slice C + z * M * ldc, and k_sum_slices adds the slices in split order,
+// so the result does not depend on which block finishes first.
 template <bool AT, bool BT>
 __global__ void __launch_bounds__(256) k_gemm(const float* __restrict__ A, int lda, const float* __restrict__ B, int ldb,
                                               float* __restrict__ C, int ldc, int M, int N, int K, const float* __restrict__ bias,
@@ -78,9 +75,18 @@ __global__ void __launch_bounds__(256) k_gemm(const float* __restrict__ A, int l
     for (int j = 0; j < 4; j++) {
       const int n = n0 + tx * 4 + j;
       if (n >= N) continue;
-      if (ksplit > 1) atomicAdd(C + long(m) * ldc + n, acc[i][j]);
+      if (ksplit > 1) C[long(blockIdx.z) * M * ldc + long(m) * ldc + n] = acc[i][j];
       else C[long(m) * ldc + n] = acc[i][j] + (bias ? bias[n] : 0.f);
     }
+  }
+}
+
+// out[i] = sum over z = 0 .. nsl-1 of part[z * n + i], in that order
+__global__ void k_sum_slices(const float* __restrict__ part, int nsl, long n, float* __restrict__ out) {
+  for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+    float acc = 0.f;
+    for (int z = 0; z < nsl; z++) acc += part[z * n + i];
+    out[i] = acc;
   }
 }
 
@@ -113,8 +119,11 @@ __global__ void k_gelu_back(const float* __restrict__ Z, float* __restrict__ dH,
   for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) dH[i] *= gelu_grad(Z[i]);
 }
 
-// loss = mean over the batch and the NLOSS scheme outputs of (Y - T)^2, accumulated in FP64; dY = dloss/dY
-__global__ void k_loss(const float* __restrict__ Y, const float* __restrict__ T, int B, float* __restrict__ dY, double* loss) {
+// loss = mean over the batch and the NLOSS scheme outputs of (Y - T)^2, accumulated in FP64; dY = dloss/dY. Each
+// block writes its FP64 partial sum to part[blockIdx.x]; k_loss_total adds them in block order.
+__global__ void __launch_bounds__(256) k_loss(const float* __restrict__ Y, const float* __restrict__ T, int B, float* __restrict__ dY,
+                                              double* __restrict__ part) {
+  __shared__ double red[8];
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   double l = 0.0;
   if (s < B) {
@@ -125,17 +134,30 @@ __global__ void k_loss(const float* __restrict__ Y, const float* __restrict__ T,
     }
   }
   for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-  if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l / double(B * NLOSS));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); w++) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+// loss += (sum of the nb block partials, in order) / (B * NLOSS): one thread, once per training step
+__global__ void k_loss_total(const double* __restrict__ part, int nb, int B, double* __restrict__ loss) {
+  double t = 0.0;
+  for (int b = 0; b < nb; b++) t += part[b];
+  *loss += t / double(B * NLOSS);
 }
 
-// bias gradient: column sums of dZ[B][N]
-__global__ void k_colsum(const float* __restrict__ dZ, int B, int N, float* __restrict__ g) {
+// bias gradient: column sums of dZ[B][N]; row chunk y writes its partial column sums to part[y * N + n] (summed in
+// chunk order by k_sum_slices)
+__global__ void k_colsum(const float* __restrict__ dZ, int B, int N, float* __restrict__ part) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   const int rows = (B + gridDim.y - 1) / gridDim.y, r0 = blockIdx.y * rows, r1 = min(B, r0 + rows);
   float s = 0.f;
   for (int r = r0; r < r1; r++) s += dZ[size_t(r) * N + n];
-  atomicAdd(g + n, s);
+  part[long(blockIdx.y) * N + n] = s;
 }
 
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v, int n,
@@ -158,7 +180,21 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
 using namespace ob;
 using namespace ob::mlp;
 
+namespace ob {
+struct MlpTcTrainer;
+namespace mlp {
+MlpTcTrainer* tc_trainer_new();
+void tc_trainer_delete(MlpTcTrainer* t);
+int tc_train_run(MlpTcTrainer* t, float* w, float* g, float* m, float* v, int& adam_t, const float* pairs, unsigned npairs,
+                 const Norm& nm, int batch, int steps, float lr, unsigned seed, double* d_loss, cudaStream_t s);
+int tc_grad_run(MlpTcTrainer* t, const float* w, float* g, const float* pairs, int count, const Norm& nm, double* d_loss,
+                cudaStream_t s);
+}  // namespace mlp
+}  // namespace ob
+
 struct ObMlp {
+  int train_mode = 1;    // 1: bf16 tcgen05 training kernels (batches that are multiples of 128), 0: fp32 SIMT kernels
+  ob::MlpTcTrainer* tct = nullptr;
   float* d_w = nullptr;  // fp32 master parameters
   float* d_g = nullptr;  // gradient of the last batch
   float* d_m = nullptr;  // Adam moments
@@ -172,6 +208,8 @@ struct ObMlp {
   float *X = nullptr, *T = nullptr, *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *Z3 = nullptr, *H3 = nullptr;
   float *Y = nullptr, *dY = nullptr, *dA = nullptr, *dB = nullptr, *hp = nullptr;
   unsigned* idx = nullptr;
+  float* part = nullptr;       // split-K and bias partial sums (PART_FLOATS)
+  double* lpart = nullptr;     // per-block loss partials
   double* d_loss = nullptr;
   cudaStream_t stream = nullptr;
 };
@@ -188,8 +226,12 @@ void free_scratch(ObMlp* n) {
   for (float* p : {n->X, n->T, n->Z1, n->H1, n->Z2, n->H2, n->Z3, n->H3, n->Y, n->dY, n->dA, n->dB, n->hp})
     if (p) cudaFree(p);
   if (n->idx) cudaFree(n->idx);
+  if (n->part) cudaFree(n->part);
+  if (n->lpart) cudaFree(n->lpart);
   n->X = n->T = n->Z1 = n->H1 = n->Z2 = n->H2 = n->Z3 = n->H3 = n->Y = n->dY = n->dA = n->dB = n->hp = nullptr;
   n->idx = nullptr;
+  n->part = nullptr;
+  n->lpart = nullptr;
   n->bcap = 0;
 }
 
@@ -205,9 +247,13 @@ int ensure_scratch(ObMlp* n, int B) {
   MLP_TRY(cuda_ok(cudaMalloc(&n->dY, b * NOUT * 4), "mlp scratch"));
   MLP_TRY(cuda_ok(cudaMalloc(&n->hp, b * PAIR * 4), "mlp scratch"));
   MLP_TRY(cuda_ok(cudaMalloc(&n->idx, b * 4), "mlp scratch"));
+  MLP_TRY(cuda_ok(cudaMalloc(&n->part, size_t(kMaxSplits) * NH * NH * 4), "mlp scratch"));
+  MLP_TRY(cuda_ok(cudaMalloc(&n->lpart, ((b + 255) / 256) * 8), "mlp scratch"));
   n->bcap = B;
   return OB_OK;
 }
+
+inline dim3 ew(long n) { return dim3(unsigned(std::min<long>((n + 255) / 256, 4096))); }
 
 template <bool AT, bool BT>
 void gemm(const float* A, int lda, const float* B, int ldb, float* C, int ldc, int M, int N, int K, const float* bias, int ksplit,
@@ -215,13 +261,24 @@ void gemm(const float* A, int lda, const float* B, int ldb, float* C, int ldc, i
   dim3 grid((N + 63) / 64, (M + 63) / 64, ksplit);
   k_gemm<AT, BT><<<grid, 256, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K, bias, ksplit);
 }
-// K splits of a weight-gradient GEMM (reduction over the batch): about two blocks per SM in total
+// K splits of a weight-gradient GEMM (reduction over the batch): about two blocks per SM in total, at most kMaxSplits
 int splits(int M, int N, int K) {
   const int tiles = ((M + 63) / 64) * ((N + 63) / 64);
-  return std::max(2, std::min(std::max(1, K / 256), std::max(1, 296 / tiles)));
+  return std::min(kMaxSplits, std::max(2, std::min(std::max(1, K / 256), std::max(1, 296 / tiles))));
 }
-inline dim3 ew(long n) { return dim3(unsigned(std::min<long>((n + 255) / 256, 4096))); }
-
+// weight gradient C[M][N] (pitch N) = A^T B over the batch, split over the batch into the partial-sum slices of
+// n->part and added in split order
+void weight_grad(ObMlp* n, const float* A, int lda, const float* B, int ldb, float* C, int M, int N, int K) {
+  const int ks = splits(M, N, K);
+  gemm<true, false>(A, lda, B, ldb, n->part, N, M, N, K, nullptr, ks, n->stream);
+  k_sum_slices<<<ew(long(M) * N), 256, 0, n->stream>>>(n->part, ks, long(M) * N, C);
+}
+// bias gradient g[N] = column sums of dZ[B][N], in row-chunk order
+void bias_grad(ObMlp* n, const float* dZ, int B, int N, float* g) {
+  const int chunks = std::max(1, std::min(B / 512, 64));
+  k_colsum<<<dim3((N + 127) / 128, chunks), 128, 0, n->stream>>>(dZ, B, N, n->part);
+  k_sum_slices<<<ew(N), 256, 0, n->stream>>>(n->part, chunks, N, g);
+}
 // forward of B gathered samples (n->X) to n->Y
 void forward(ObMlp* n, int B) {
   cudaStream_t s = n->stream;
@@ -240,28 +297,28 @@ void backward(ObMlp* n, int B) {
   cudaStream_t s = n->stream;
   const float* w = n->d_w;
   float* g = n->d_g;
-  cudaMemsetAsync(g, 0, NPARAM * 4, s);
-  k_loss<<<(B + 255) / 256, 256, 0, s>>>(n->Y, n->T, B, n->dY, n->d_loss);
+  const int nb = (B + 255) / 256;
+  k_loss<<<nb, 256, 0, s>>>(n->Y, n->T, B, n->dY, n->lpart);
+  k_loss_total<<<1, 1, 0, s>>>(n->lpart, nb, B, n->d_loss);
   const long bh = long(B) * NH;
-  const dim3 cs((NH + 127) / 128, std::max(1, std::min(B / 512, 64)));
   // output layer
-  gemm<true, false>(n->dY, NOUT, n->H3, NH, g + OW4, NH, NOUT, NH, B, nullptr, splits(NOUT, NH, B), s);
-  k_colsum<<<dim3(1, cs.y), 128, 0, s>>>(n->dY, B, NOUT, g + OB4);
+  weight_grad(n, n->dY, NOUT, n->H3, NH, g + OW4, NOUT, NH, B);
+  bias_grad(n, n->dY, B, NOUT, g + OB4);
   gemm<false, false>(n->dY, NOUT, w + OW4, NH, n->dA, NH, B, NH, NOUT, nullptr, 1, s);
   k_gelu_back<<<ew(bh), 256, 0, s>>>(n->Z3, n->dA, bh);
   // layer 3
-  gemm<true, false>(n->dA, NH, n->H2, NH, g + OW3, NH, NH, NH, B, nullptr, splits(NH, NH, B), s);
-  k_colsum<<<cs, 128, 0, s>>>(n->dA, B, NH, g + OB3);
+  weight_grad(n, n->dA, NH, n->H2, NH, g + OW3, NH, NH, B);
+  bias_grad(n, n->dA, B, NH, g + OB3);
   gemm<false, false>(n->dA, NH, w + OW3, NH, n->dB, NH, B, NH, NH, nullptr, 1, s);
   k_gelu_back<<<ew(bh), 256, 0, s>>>(n->Z2, n->dB, bh);
   // layer 2
-  gemm<true, false>(n->dB, NH, n->H1, NH, g + OW2, NH, NH, NH, B, nullptr, splits(NH, NH, B), s);
-  k_colsum<<<cs, 128, 0, s>>>(n->dB, B, NH, g + OB2);
+  weight_grad(n, n->dB, NH, n->H1, NH, g + OW2, NH, NH, B);
+  bias_grad(n, n->dB, B, NH, g + OB2);
   gemm<false, false>(n->dB, NH, w + OW2, NH, n->dA, NH, B, NH, NH, nullptr, 1, s);
   k_gelu_back<<<ew(bh), 256, 0, s>>>(n->Z1, n->dA, bh);
   // layer 1
-  gemm<true, false>(n->dA, NH, n->X, NIN, g + OW1, NIN, NH, NIN, B, nullptr, splits(NH, NIN, B), s);
-  k_colsum<<<cs, 128, 0, s>>>(n->dA, B, NH, g + OB1);
+  weight_grad(n, n->dA, NH, n->X, NIN, g + OW1, NH, NIN, B);
+  bias_grad(n, n->dA, B, NH, g + OB1);
 }
 }  // namespace
 
@@ -304,6 +361,7 @@ int ob_mlp_destroy(ObMlp* n) {
   if (!n) return OB_OK;
   if (n->stream) cudaStreamSynchronize(n->stream);
   free_scratch(n);
+  tc_trainer_delete(n->tct);
   for (void* p : {(void*)n->d_w, (void*)n->d_g, (void*)n->d_m, (void*)n->d_v, (void*)n->d_pairs, (void*)n->d_count, (void*)n->d_loss})
     if (p) cudaFree(p);
   if (n->stream) cudaStreamDestroy(n->stream);
@@ -372,6 +430,12 @@ int ob_mlp_write_pairs(ObMlp* n, const float* host, long long count) {
   return cuda_ok(cudaMemcpy(n->d_count, &c, 4, cudaMemcpyHostToDevice), "ob_mlp_write_pairs");
 }
 
+int ob_mlp_set_training(ObMlp* n, int mode) {
+  if (!n || (mode != 0 && mode != 1)) { set_error("ob_mlp_set_training: mode must be 0 (fp32 SIMT) or 1 (bf16 tensor cores)"); return OB_ERR_INVALID; }
+  n->train_mode = mode;
+  return OB_OK;
+}
+
 // forward + backward on `count` host pairs in order: the batch loss and the gradient of every parameter
 int ob_mlp_grad(ObMlp* n, const float* pairs, int count, double* loss, float* grad) {
   if (!n || !pairs || count < 1 || !loss || !grad) { set_error("ob_mlp_grad: bad arguments"); return OB_ERR_INVALID; }
@@ -379,9 +443,14 @@ int ob_mlp_grad(ObMlp* n, const float* pairs, int count, double* loss, float* gr
   cudaStream_t s = n->stream;
   MLP_TRY(cuda_ok(cudaMemcpyAsync(n->hp, pairs, size_t(count) * PAIR * 4, cudaMemcpyHostToDevice, s), "ob_mlp_grad"));
   cudaMemsetAsync(n->d_loss, 0, 8, s);
-  k_gather<<<(count + 127) / 128, 128, 0, s>>>(n->hp, nullptr, count, n->norm, n->X, n->T);
-  forward(n, count);
-  backward(n, count);
+  if (n->train_mode == 1 && count % 128 == 0) {
+    if (!n->tct) n->tct = tc_trainer_new();
+    MLP_TRY(tc_grad_run(n->tct, n->d_w, n->d_g, n->hp, count, n->norm, n->d_loss, s));
+  } else {
+    k_gather<<<(count + 127) / 128, 128, 0, s>>>(n->hp, nullptr, count, n->norm, n->X, n->T);
+    forward(n, count);
+    backward(n, count);
+  }
   MLP_TRY(cuda_ok(cudaMemcpyAsync(grad, n->d_g, NPARAM * 4, cudaMemcpyDeviceToHost, s), "ob_mlp_grad"));
   MLP_TRY(cuda_ok(cudaMemcpyAsync(loss, n->d_loss, 8, cudaMemcpyDeviceToHost, s), "ob_mlp_grad"));
   return cuda_ok(cudaStreamSynchronize(s), "ob_mlp_grad");
@@ -408,8 +477,19 @@ int ob_mlp_train(ObMlp* n, int batch, int steps, float lr, unsigned seed, double
   long long cnt = 0;
   MLP_TRY(ob_mlp_pair_count(n, &cnt));
   if (cnt < 1) { set_error("ob_mlp_train: no recorded pairs"); return OB_ERR_INVALID; }
-  MLP_TRY(ensure_scratch(n, batch));
   cudaStream_t s = n->stream;
+  if (n->train_mode == 1 && batch % 128 == 0) {
+    if (!n->tct) n->tct = tc_trainer_new();
+    cudaMemsetAsync(n->d_loss, 0, 8, s);
+    MLP_TRY(tc_train_run(n->tct, n->d_w, n->d_g, n->d_m, n->d_v, n->adam_t, n->d_pairs, unsigned(cnt), n->norm, batch, steps, lr,
+                         seed, n->d_loss, s));
+    double l = 0.0;
+    MLP_TRY(cuda_ok(cudaMemcpyAsync(&l, n->d_loss, 8, cudaMemcpyDeviceToHost, s), "ob_mlp_train"));
+    MLP_TRY(cuda_ok(cudaStreamSynchronize(s), "ob_mlp_train"));
+    if (mean_loss) *mean_loss = l / steps;
+    return OB_OK;
+  }
+  MLP_TRY(ensure_scratch(n, batch));
   cudaMemsetAsync(n->d_loss, 0, 8, s);
   const float b1 = 0.9f, b2 = 0.999f;
   for (int st = 0; st < steps; st++) {

@@ -26,6 +26,16 @@ struct Norm {
   float in_mean[NIN], in_scale[NIN], out_scale[NOUT], in_lo[NIN], in_hi[NIN], dt;
 };
 
+#ifdef __CUDACC__
+// GELU, tanh form (Hendrycks and Gimpel): g(z) = z/2 (1 + tanh(c (z + a z^3))), c = sqrt(2/pi), a = 0.044715
+constexpr float GC = 0.7978845608f, GA = 0.044715f;
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + tanhf(GC * (z + GA * z * z * z))); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float t = tanhf(GC * (z + GA * z * z * z));
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * GC * (1.f + 3.f * GA * z * z);
+}
+#endif
+
 __host__ __device__ inline float feature(int i, float x) {
   if (i >= 3 && i <= 8) return logf(fmaxf(x, 0.f) + QEPS);
   if (i == 9) return logf(fmaxf(x, 0.f) + 1.f);

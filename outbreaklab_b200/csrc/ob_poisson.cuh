@@ -11,7 +11,8 @@ namespace ob {
 void set_error(const char* fmt, ...);
 
 struct PoissonPlan {
-  int nx = 0, ny = 0, nz = 0, precision = 0;  // 0 fp32 SIMT, 1 bf16x3 tensor core, 2 bf16x3 + one refinement
+  int nx = 0, ny = 0, nz = 0, precision = 0;  // 0 fp32 SIMT, 1 bf16x3 tensor core, 2 bf16x3 + one refinement,
+                                              // 3 refinement in plain bf16, 4 two bf16x3 refinements
   bool presplit = false;  // precision >= 1: the caller writes the split right-hand side (tc_rhs_split) itself
   double dx = 0, dz = 0;
   float* mats = nullptr;  // qix | qx | qiy | qy (fp32, solver.js:115-125)
@@ -41,6 +42,10 @@ struct PoissonPlan {
   void tc_rhs_split(__nv_bfloat16** hi, __nv_bfloat16** lo, int* ld) const;
   void tc_destroy();
 };
+
+// FP64 residual norms of phi for rhs (device arrays) under the solve's operator: rel = {max |r| / max |rhs|,
+// ||r||_2 / ||rhs||_2}; scratch holds 4 * 1024 + 4 doubles
+int poisson_residual(const PoissonPlan& P, const float* rhs, const float* phi, double* scratch, double rel[2], cudaStream_t s);
 
 // grouped solve of an ensemble: every member's solve in the same few launches (ob_dst_tc.cu). The plans use the
 // tensor-core path with the split right-hand side written by their divergence pass, share nz and precision;

@@ -254,7 +254,8 @@ class RegionalModel:
 
 class PoissonDirect:
     """solver.js:105-165: exact solve of rho_c lap_h(phi) + d/dz(rho_w dphi/dz) = rhs on an nx x ny x nz grid.
-    precision 0: fp32 transforms; 1: bf16x3 tensor-core transforms."""
+    precision 0: fp32 transforms; 1: bf16x3 tensor-core transforms; 2: plus one bf16x3 refinement sweep on the
+    FP64-accumulated residual; 3: that sweep in plain bf16; 4: two bf16x3 refinement sweeps."""
 
     def __init__(self, nx, ny, nz, dx, dz, precision=0):
         self.nx, self.ny, self.nz, self.dx, self.dz = nx, ny, nz, dx, dz
@@ -279,6 +280,12 @@ class PoissonDirect:
         t = C.c_float()
         N.check(N.lib().ob_poisson_time(self.h, int(reps), C.byref(t)))
         return t.value
+
+    def residual(self):
+        """FP64 residual of the last solve on the device: (max|r| / max|rhs|, ||r||_2 / ||rhs||_2)."""
+        a, b = C.c_double(), C.c_double()
+        N.check(N.lib().ob_poisson_residual(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def destroy(self):
         if getattr(self, "h", None):

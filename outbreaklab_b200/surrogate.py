@@ -43,6 +43,10 @@ class MicroSurrogate:
         N.check(N.lib().ob_mlp_create(C.c_uint(seed), C.byref(h)))
         self.h = h
 
+    def set_training(self, mode: int):
+        """1 (default): BF16 tensor-core training kernels for batches that are multiples of 128; 0: FP32 SIMT."""
+        N.check(N.lib().ob_mlp_set_training(self.h, int(mode)))
+
     def close(self):
         if self.h:
             N.lib().ob_mlp_destroy(self.h)

@@ -3,7 +3,8 @@ browser sends, app.js:1743-1758) and the Archive II bytes the reference's own wr
 (l2writer.encode_volume, l2writer.py:161-182).
 
 Run in a container where the reference is mounted (it imports l2writer.py from there, read-only):
-    python tests/golden/make_level2_volume.py [/path/to/reference]
+    python tests/golden/make_level2_volume.py <path to the reference checkout>
+(or with the path in the OUTBREAKLAB_REF environment variable).
 Three sweeps cover the writer's cases: a super-resolution surveillance cut (REF, ZDR, PHI, RHO), its Doppler pair
 (VEL, SW) and a legacy-resolution cut with all six moments; gate codes are seeded, mostly zero like real volumes.
 """
@@ -13,7 +14,9 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OUTBREAKLAB_REF")
+if not ref or not os.path.isfile(os.path.join(ref, "l2writer.py")):
+    sys.exit("usage: %s <path to the reference checkout holding l2writer.py> (or set OUTBREAKLAB_REF)" % sys.argv[0])
 sys.path.insert(0, ref)
 import l2writer  # noqa: E402
 

@@ -57,6 +57,36 @@ def test_training_gradient_matches_float64_oracle(native):
     assert np.abs(y - yr).max() <= 1e-4 * np.abs(yr).max()
 
 
+def test_tensor_core_gradient_matches_bf16_oracle(native):
+    """The bf16 tensor-core training kernels (the default for batches that are multiples of 128): loss and every
+    parameter's gradient of one batch of 256 pairs against the float64 restatement that rounds to bf16 at the same
+    points (oracle/mlp_oracle.py loss_and_grad_bf16), and against the exact float64 gradient at bf16's precision."""
+    net = S.MicroSurrogate(seed=3)
+    pairs = _synthetic(11, 256)
+    norm = _norm_for(pairs)
+    net.set_norm(norm)
+    params = (np.random.default_rng(4).standard_normal(S.NPARAM) * 0.1).astype(np.float32)
+    net.set_params(params)
+    loss, g = net.grad(pairs)
+    lb, gb = MO.loss_and_grad_bf16(params.astype(np.float64), pairs.astype(np.float64), norm.astype(np.float64))
+    lr, gr = MO.loss_and_grad(params.astype(np.float64), pairs.astype(np.float64), norm.astype(np.float64))
+    assert abs(loss - lb) <= 1e-4 * abs(lb), (loss, lb)
+    assert abs(loss - lr) <= 2e-2 * abs(lr), (loss, lr)
+    o = 0
+    for name, shp in MO.SHAPES:
+        n = int(np.prod(shp))
+        a, b, r = g[o:o + n].astype(np.float64), gb[o:o + n], gr[o:o + n]
+        # fp32 accumulation against exact sums, and the odd bf16 operand rounded the other way
+        assert np.linalg.norm(a - b) <= 3e-3 * np.linalg.norm(b) + 1e-12, (name, np.linalg.norm(a - b) / np.linalg.norm(b))
+        assert np.linalg.norm(a - r) <= 5e-2 * np.linalg.norm(r) + 1e-12, (name, np.linalg.norm(a - r) / np.linalg.norm(r))
+        o += n
+    # the same batch through the fp32 SIMT kernels (mode 0) matches the exact float64 gradient, as before
+    net.set_training(0)
+    loss0, g0 = net.grad(pairs)
+    assert abs(loss0 - lr) <= 1e-5 * abs(lr)
+    assert np.linalg.norm(g0.astype(np.float64) - gr) <= 1e-4 * np.linalg.norm(gr)
+
+
 def test_adam_steps_reduce_the_loss(native):
     net = S.MicroSurrogate(seed=4)
     pairs = _synthetic(5, 20000)
@@ -73,6 +103,22 @@ def test_adam_steps_reduce_the_loss(native):
     net.train(1024, 800, 1e-3)
     last = net.train(1024, 20, 1e-4)
     assert last < 0.2 * first, (first, last)
+
+
+def test_training_is_deterministic(native):
+    """A seed fixes the trained network: two trainings from the same initial parameters on the same pairs give
+    bit-identical parameters and losses (every batch reduction adds its partial sums in a fixed order)."""
+    pairs = _synthetic(7, 6000)
+    nets = []
+    for _ in range(2):
+        net = S.MicroSurrogate(seed=9)
+        net.reserve(len(pairs))
+        net.write_pairs(pairs)
+        net.set_norm(_norm_for(pairs))
+        loss = net.train(2048, 40, 1e-3, seed=11)
+        nets.append((loss, net.params()))
+    assert nets[0][0] == nets[1][0]
+    assert np.array_equal(nets[0][1], nets[1][1])
 
 
 def _thompson_blob_model():

@@ -6,7 +6,7 @@ import struct
 
 import pytest
 
-from outbreaklab_b200 import model as M, radar as RD, runloop as RL
+from outbreaklab_b200 import _native as N, model as M, radar as RD, runloop as RL
 
 import _radar_case as RC
 
@@ -35,3 +35,23 @@ def test_run_loop_with_radar_and_storm_starts(native, tmp_path):
     assert len(meta) == 134 * 2432
     assert g.nan_count == 0
     sim.destroy()
+
+
+def test_run_loop_with_fronts_starts_storms_along_them(native):
+    """The reference's example fronts over their triple point: the run loop's scheduler starts storms along the
+    boundaries (on their warm side) as well as in the warm sector, and the model runs the nudged forcing with them."""
+    from outbreaklab_b200 import boundaries as BND, workloads as W
+    case = W.case_fronts(nx=96, ny=88, nz=40)
+    bounds, _ = W.fronts_setup(case)
+    for mb in bounds:
+        mb["b"] = dict(mb["b"], rate=400.0)        # a start on each boundary about every minute
+    g, _ = M.setup_case(case, bounds=bounds)
+    loop = RL.RunLoop(g, case.dt, 300.0, ci={"warmRate": 300.0, "start": 0.0, "rh": 6000.0}, replay_every=60.0,
+                      bounds=bounds)
+    res = loop.run()
+    labels = [s for s in res["log"] if "storm start" in s]
+    kinds = {BND.BND_TYPES[k]["label"].lower() for k in ("cold", "warm", "dry")}
+    assert any(any(k in s for k in kinds) for s in labels), labels
+    assert res["events"] > 0 and g.nan_count == 0
+    A = g.get_field(N.FIELD_LSF_A).reshape(case.ny, case.nx, 4)
+    assert A[..., 0].min() < -3.0 and A[..., 0].max() > 1.0
