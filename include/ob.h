@@ -319,7 +319,8 @@ int ob_dst_tc_selftest(int M, int N, int K, int planes, const float* A, const fl
 #define OB_MLP_NIN 12
 #define OB_MLP_NOUT 10
 #define OB_MLP_NPARAM 35978  /* W1[128][12] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[10][128] b4[10] */
-#define OB_MLP_PAIR 24       /* floats per recorded pair: 12 inputs, 10 tendencies, texel offset (uint32 bits), pad */
+#define OB_MLP_PAIR 24       /* floats per recorded pair: 12 inputs, 10 tendencies, texel offset (uint32 bits), the
+                              * model time of the recorded step */
 #define OB_MLP_NNORM 59      /* in_mean[12] in_scale[12] out_scale[10] in_lo[12] in_hi[12] dt */
 typedef struct ObMlp ObMlp;
 int ob_mlp_create(unsigned seed, ObMlp** out);  /* He-initialised weights from the seed */
@@ -335,6 +336,10 @@ int ob_mlp_reserve_pairs(ObMlp* n, long long capacity);  /* device buffer for re
 int ob_mlp_pair_count(ObMlp* n, long long* count);
 int ob_mlp_read_pairs(ObMlp* n, long long first, long long count, float* host);
 int ob_mlp_write_pairs(ObMlp* n, const float* host, long long count);  /* replaces the buffer's pairs */
+/* orders the recorded pairs by (model time of their step, texel offset), so that training on them does not depend on
+ * the order in which the physics pass appended them (an atomic counter); the pair's last two floats carry the two
+ * keys. Allocates scratch for the call (about 1.3 x the pairs' bytes). No counterpart in the reference. */
+int ob_mlp_sort_pairs(ObMlp* n);
 /* forward + backward on `count` host pairs (in order): the loss (mean squared error of the 8 scheme tendencies in
  * normalised units) and its gradient with respect to every parameter (OB_MLP_NPARAM floats) */
 int ob_mlp_grad(ObMlp* n, const float* pairs, int count, double* loss, float* grad);

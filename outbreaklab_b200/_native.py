@@ -105,6 +105,7 @@ SYMBOLS = {
     "ob_mlp_eval": (_i, [_vp, _fp, _i, _fp]),
     "ob_mlp_train": (_i, [_vp, _i, _i, _f, C.c_uint, C.POINTER(_d)]),
     "ob_mlp_set_training": (_i, [_vp, _i]),
+    "ob_mlp_sort_pairs": (_i, [_vp]),
     "ob_model_record_micro": (_i, [_vp, _vp, _f]),
     "ob_model_set_graphs": (_i, [_vp, _i]),
     "ob_model_tornado_candidates": (_i, [_vp, _f, _fp, _i, C.POINTER(_i)]),

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libob_b200.so")
-SOURCES = ["ob_api.cu", "ob_step.cu", "ob_poisson.cu", "ob_dst_tc.cu", "ob_poisson_static.cu", "ob_radar.cu", "ob_mlp.cu", "ob_mlp_tc.cu", "ob_mlp_train_tc.cu", "ob_level2.cu"]
+SOURCES = ["ob_api.cu", "ob_step.cu", "ob_poisson.cu", "ob_dst_tc.cu", "ob_poisson_static.cu", "ob_radar.cu", "ob_mlp.cu", "ob_mlp_tc.cu", "ob_mlp_train_tc.cu", "ob_mlp_sort.cu", "ob_level2.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 

@@ -603,16 +603,16 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     const double* cpd = rd + NZ;
     double* d = dlow + mode * NZ;
     double dprev = 0.0;
-#pragma unroll 1
-    for (int k = 0; k < NZ; k++) {
-      dprev = (double(col[k * LS]) - double(__ldg(zop + k).x) * dprev) * rd[k];
+#pragma unroll 8
+    for (int k = 0; k < NZ; k++) {   // the coefficient loads do not depend on the recurrence: unrolled, they overlap
+      dprev = (double(col[k * LS]) - double(__ldg(zop + k).x) * dprev) * __ldg(rd + k);
       d[k] = dprev;
     }
     double x = dprev;
     col[(NZ - 1) * LS] = float(x);
-#pragma unroll 1
+#pragma unroll 8
     for (int k = NZ - 2; k >= 0; k--) {
-      x = d[k] - cpd[k] * x;
+      x = d[k] - __ldg(cpd + k) * x;
       col[k * LS] = float(x);
     }
   } else {

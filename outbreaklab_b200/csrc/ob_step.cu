@@ -1036,13 +1036,14 @@ __device__ __forceinline__ bool phys_texel(const Grid& g, const Uni& U, const Fi
       if (MM == kMicroRecord && surrogate_cell(pre) &&
           float(hash3i(ci, cj, ck ^ int(__float_as_uint(float(__ldg(F.clock))) * 2654435761u)) >> 8u) * (1.f / 16777216.f) < F.mlp_rate) {
         // one (state, process tendency) pair of the scheme: 12 inputs, 10 tendencies (before the saturation
-        // adjustment), the cell's texel offset (as bits), 1 pad
+        // adjustment), the cell's texel offset (as bits), the model time of the step (the two order the pairs
+        // canonically: ob_mlp_sort_pairs)
         const unsigned slot = warp_append(F.mlp_count);
         if (slot < F.mlp_cap) {
           float* r = F.mlp_buf + size_t(slot) * 24;
           const float x[12] = {pre.T, p0, rho, pre.qv, pre.qc, pre.qr, pre.qi, pre.qs, pre.qg, pre.nr, q2[3], V[2]};
           const float y[12] = {mc.T - pre.T, mc.qv - pre.qv, mc.qc - pre.qc, mc.qi - pre.qi, mc.qr - pre.qr, mc.qs - pre.qs,
-                               mc.qg - pre.qg, mc.nr - pre.nr, 0.f, 0.f, __uint_as_float(unsigned(o)), 0.f};
+                               mc.qg - pre.qg, mc.nr - pre.nr, 0.f, 0.f, __uint_as_float(unsigned(o)), float(__ldg(F.clock))};
 #pragma unroll
           for (int e = 0; e < 12; e++) {
             r[e] = x[e];

@@ -43,6 +43,10 @@ class MicroSurrogate:
         N.check(N.lib().ob_mlp_create(C.c_uint(seed), C.byref(h)))
         self.h = h
 
+    def sort_pairs(self):
+        """Orders the recorded pairs by (model time of their step, texel offset) (ob_mlp_sort_pairs)."""
+        N.check(N.lib().ob_mlp_sort_pairs(self.h))
+
     def set_training(self, mode: int):
         """1 (default): BF16 tensor-core training kernels for batches that are multiples of 128; 0: FP32 SIMT."""
         N.check(N.lib().ob_mlp_set_training(self.h, int(mode)))
@@ -137,12 +141,15 @@ class MicroSurrogate:
 
 
 def record(model, net: MicroSurrogate, steps: int, dt: float, rate: float):
-    """Steps the model `steps` times with the plain scheme while recording pairs into net's buffer."""
+    """Steps the model `steps` times with the plain scheme while recording pairs into net's buffer, then puts the
+    buffer in its canonical order (model time, texel offset), so that what the network is trained on does not depend
+    on the order in which the physics pass appended the pairs."""
     N.check(N.lib().ob_model_record_micro(model.h, net.h, C.c_float(rate)))
     try:
         model.step(dt, steps)
     finally:
         N.check(N.lib().ob_model_record_micro(model.h, None, C.c_float(0.0)))
+    net.sort_pairs()
 
 
 def fit(model, net: MicroSurrogate, *, record_steps: int, dt: float, rate: float, capacity: int, batch: int = 16384,

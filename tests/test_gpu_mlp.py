@@ -138,6 +138,26 @@ def _record_one_step(rate=1.0):
     return case, a, B, net, net.read_pairs()
 
 
+def test_recorded_pairs_have_a_canonical_order(native):
+    """Two recordings of the same three steps give byte-identical pair buffers: after recording, ob_mlp_sort_pairs
+    orders the pairs by (model time of their step, texel offset), whatever order the physics pass appended them in."""
+    bufs = []
+    for _ in range(2):
+        case, a, B = _thompson_blob_model()
+        net = S.MicroSurrogate(seed=9)
+        net.reserve(3 * case.cells)
+        S.record(a, net, 3, case.dt, 0.5)
+        bufs.append(net.read_pairs())
+        net.close()
+    P, Q = bufs
+    assert len(P) > 1000 and P.shape == Q.shape
+    assert np.array_equal(P.view(np.uint32), Q.view(np.uint32))
+    t, off = P[:, 23].astype(np.float64), P[:, 22].view(np.uint32).astype(np.int64)
+    assert set(np.unique(t)) == {0.0, case.dt, 2 * case.dt}   # the model time of each recorded step
+    key = t * 2 ** 32 + off
+    assert (np.diff(key) > 0).all()                            # strictly increasing: (time, offset) is unique
+
+
 def test_recorded_pairs_are_scheme_tendencies(native):
     case, a, B, net, P = _record_one_step()
     assert len(P) > 1000
