@@ -208,6 +208,11 @@ int ob_model_set_graphs(ObModel* m, int on);
  * floor that storing phi in fp32 sets).
  * No counterpart in the reference. */
 int ob_model_set_solver(ObModel* m, int precision);
+/* tile shape of the tensor-core solve's transforms: 1 = tiles of 256 field rows computed by pairs of SMs (a cluster of
+ * two CTAs, tcgen05.mma.cta_group::2: each SM loads half of the DST-matrix tile, a third less operand traffic),
+ * 0 = tiles of 128 rows on single SMs. The results are bit-identical. Precisions 1 to 4 only (set after
+ * ob_model_set_solver, which resets it). No counterpart in the reference. */
+int ob_model_set_pair_tiles(ObModel* m, int on);
 int ob_model_solver(ObModel* m);
 /* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
 void* ob_model_stream(ObModel* m);
@@ -233,6 +238,8 @@ int ob_poisson_time(ObPoisson* p, int reps, float* ms);
  * with phi = 0 beyond the grid, the z-operator with Neumann ends): *max_rel = max|r| / max|rhs|,
  * *l2_rel = ||r||_2 / ||rhs||_2. A diagnostic of the solve's precision; no counterpart in the reference. */
 int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel);
+/* the transforms' tile shape, as ob_model_set_pair_tiles; no counterpart in the reference */
+int ob_poisson_set_pair_tiles(ObPoisson* p, int on);
 
 /* ---- RadarSim (radar.js:271-413): virtual WSR-88D gate sampling ----
  * The host keeps RadarSim's VCP tables, volume layout and scan scheduling (radar.js:289-392); the library owns each
@@ -338,7 +345,9 @@ int ob_mlp_read_pairs(ObMlp* n, long long first, long long count, float* host);
 int ob_mlp_write_pairs(ObMlp* n, const float* host, long long count);  /* replaces the buffer's pairs */
 /* orders the recorded pairs by (model time of their step, texel offset), so that training on them does not depend on
  * the order in which the physics pass appended them (an atomic counter); the pair's last two floats carry the two
- * keys. Allocates scratch for the call (about 1.3 x the pairs' bytes). No counterpart in the reference. */
+ * keys. A recording that passed the buffer's capacity holds a race-dependent subset of its last step's pairs: the sort
+ * drops that step (the count becomes the index of its first pair). Allocates scratch for the call (about 1.3 x the
+ * pairs' bytes). No counterpart in the reference. */
 int ob_mlp_sort_pairs(ObMlp* n);
 /* forward + backward on `count` host pairs (in order): the loss (mean squared error of the 8 scheme tendencies in
  * normalised units) and its gradient with respect to every parameter (OB_MLP_NPARAM floats) */

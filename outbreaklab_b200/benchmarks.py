@@ -35,11 +35,15 @@ def solve(args):
     rhs = W.gaussian_rhs(nx, ny, nz, dx, corr_len=5000.0, seed=3).astype(np.float32)
     P = M.PoissonDirect(nx, ny, nz, dx, dz, args.precision)
     P.set_density(rc, rw)
+    if args.pair_tiles is not None:
+        P.set_pair_tiles(bool(args.pair_tiles))
     P.solve(rhs)   # uploads the right-hand side that device_ms solves again
     ms = P.device_ms(args.reps)
-    # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16)
-    flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4}[args.precision]
+    # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16),
+    # 3 + 3 + 3 (two refinement sweeps)
+    flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4, 4: 9}[args.precision]
     out = {"bench": "pressure solve", "nx": nx, "ny": ny, "nz": nz, "precision": args.precision, "ms": ms,
+           "pair_tiles": args.pair_tiles,
            "dst_flops": flops, "tflops": flops / (ms * 1e-3) / 1e12}
     print(json.dumps(out), flush=True)
 
@@ -49,6 +53,8 @@ def step(args):
     m, _ = M.setup_case(case)
     if args.solver is not None:
         m.set_solver(args.solver)
+    if args.pair_tiles is not None:
+        m.set_pair_tiles(bool(args.pair_tiles))
     import ctypes as C
     from . import _native as N
     N.check(N.lib().ob_model_step(m.h, case.dt, args.warmup))
@@ -180,11 +186,14 @@ def main(argv=None):
     a.add_argument("--dx", type=float, default=1000.0)
     a.add_argument("--precision", type=int, default=2)
     a.add_argument("--reps", type=int, default=10)
+    a.add_argument("--pair-tiles", type=int, choices=[0, 1], default=None,
+                   help="1: transforms on SM pairs (256-row tiles); 0: on single SMs; default: the library's choice")
     b = sub.add_parser("step")
     b.add_argument("--case", default="c4")
     b.add_argument("--steps", type=int, default=50)
     b.add_argument("--warmup", type=int, default=5)
     b.add_argument("--solver", type=int, default=None)
+    b.add_argument("--pair-tiles", type=int, choices=[0, 1], default=None)
     c = sub.add_parser("surrogate")
     c.add_argument("--nx", type=int, default=512)
     c.add_argument("--minutes", type=float, default=60.0)

@@ -887,6 +887,13 @@ int ob_model_set_solver(ObModel* m, int precision) {
 
 int ob_model_solver(ObModel* m) { return m ? m->solver.precision : -1; }
 
+int ob_model_set_pair_tiles(ObModel* m, int on) {
+  if (!m) { set_error("ob_model_set_pair_tiles: null model"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set pair tiles"));
+  drop_graphs(m);
+  return m->solver.tc_set_pairs(on != 0);
+}
+
 unsigned ob_model_nan_count(ObModel* m) {
   unsigned h = 0;
   if (m && cudaMemcpy(&h, m->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) h = 0;
@@ -1492,6 +1499,11 @@ int ob_poisson_destroy(ObPoisson* p) {
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   return OB_OK;
+}
+int ob_poisson_set_pair_tiles(ObPoisson* p, int on) {
+  if (!p) { set_error("ob_poisson_set_pair_tiles: null handle"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(p->stream), "set pair tiles"));
+  return p->plan.tc_set_pairs(on != 0);
 }
 int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel) {
   if (!p || !max_rel || !l2_rel) { set_error("ob_poisson_residual: null argument"); return OB_ERR_INVALID; }

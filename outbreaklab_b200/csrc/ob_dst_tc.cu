@@ -321,6 +321,208 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_tc_grp(const GemmProb* __re
 // ---------------------------------------------------------------------------------------------------------------
 // fp32 field -> bf16 hi/lo planes with a padded row pitch (rows of `cols` values, pitch ld), zero in the padding
 // ---------------------------------------------------------------------------------------------------------------
+// ---------------------------------------------------------------------------------------------------------------
+// The same transform on tiles of 256 field rows x BN outputs computed by a pair of SMs (a cluster of 2 CTAs running
+// tcgen05.mma.cta_group::2, M = 256): each CTA loads its own 128 field rows and half of the DST-matrix tile (BN / 2
+// rows), the first CTA issues the MMAs, and each CTA's TMEM holds its 128 rows of the product. Per k-step a CTA then
+// loads 32 KB of field and BN x 128 bytes of matrix (60 KB at BN = 224) for the same MMA work per SM as the single-SM
+// tile that loads 88 KB: a third less operand traffic through L2, which bounds the single-SM transform. Both CTAs'
+// TMA loads (no multicast) count on the first CTA's stage barrier; the first CTA's commits release both CTAs' stages
+// and accumulators; the epilogue warps of both CTAs report a drained accumulator to the first CTA. Results equal the
+// single-SM kernel's bit for bit (the same bf16 products, accumulated over the same k-steps).
+// ---------------------------------------------------------------------------------------------------------------
+namespace {
+constexpr int STAGES2 = 3;
+constexpr int B_HALF = BNMAX / 2 * BK * 2;                   // 16 KB: half a matrix tile of 256 rows
+constexpr int STAGE2_BYTES = 2 * A_TILE + 2 * B_HALF;        // 64 KB
+constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/ + STG_BYTES;
+}  // namespace
+
+template <int MODE, bool ONE = false>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_dst_tc2(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
+              const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
+              unsigned int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES2 * STAGE2_BYTES);
+  uint64_t* empty = full + STAGES2;
+  uint64_t* tfull = empty + STAGES2;  // [2] accumulator b holds a finished tile (both CTAs)
+  uint64_t* tempty = tfull + 2;       // [2] both CTAs' epilogues have drained accumulator b (used in the first CTA)
+  uint64_t* done = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = tc::cluster_rank();
+  const bool lead = rank == 0;
+  const int ntn = (out.N + BN - 1) / BN, ntiles = ((out.M + 2 * BM - 1) / (2 * BM)) * ntn;
+  const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
+  const int bh = BN / 2;
+  const int nk = (K + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES2; s++) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      tc::mbar_init(&tfull[b], 1);
+      tc::mbar_init(&tempty[b], 8);  // four epilogue warps in each CTA
+    }
+    tc::mbar_init(done, 1);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tc::prefetch_tmap(&tF_hi);
+    tc::prefetch_tmap(&tF_lo);
+    tc::prefetch_tmap(&tQ_hi);
+    tc::prefetch_tmap(&tQ_lo);
+  }
+  if (warp == 1) {
+    tc::tmem_alloc_pair(tmem_slot, kTmemCols);
+    tc::tmem_relinquish_pair();
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();  // both CTAs' barriers exist before a load or an arrival crosses the pair
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer of this CTA's half of every stage
+      const uint32_t bytes = ONE ? 2u * uint32_t(A_TILE + bh * BK * 2) : 2u * uint32_t(2 * A_TILE + 2 * bh * BK * 2);
+      int g = 0;
+      bool ok = true;
+      for (int t = pair; t < ntiles && ok; t += npairs) {
+        const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = (t % ntn) * BN + int(rank) * bh;
+        for (int kt = 0; kt < nk; kt++, g++) {
+          const int s = g % STAGES2;
+          const uint32_t ph = (g / STAGES2) & 1;
+          if (!(ok = tc::mbar_wait(&empty[s], ph ^ 1, err, 1u))) break;
+          uint8_t* st = smem + s * STAGE2_BYTES;
+          const uint32_t fb = tc::mapa_shared(tc::smem_u32(&full[s]), 0);
+          if (lead) tc::mbar_expect_tx(&full[s], bytes);
+          tc::tma_load_2d_pair(st, &tF_hi, fb, kt * BK, m0);
+          if (!ONE) tc::tma_load_2d_pair(st + A_TILE, &tF_lo, fb, kt * BK, m0);
+          tc::tma_load_2d_pair(st + 2 * A_TILE, &tQ_hi, fb, kt * BK, n0);
+          if (!ONE) tc::tma_load_2d_pair(st + 2 * A_TILE + B_HALF, &tQ_lo, fb, kt * BK, n0);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && lead) {  // MMA issuer of the pair
+      const uint32_t idesc = tc::idesc_bf16_f32(2 * BM, BN);
+      int g = 0, it = 0;
+      bool ok = true;
+      for (int t = pair; t < ntiles && ok; t += npairs, it++) {
+        const int b = it & 1;
+        if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
+        tc::tc_fence_after();
+        const uint32_t acc = tmem + uint32_t(b * 256);
+        for (int kt = 0; kt < nk; kt++, g++) {
+          const int s = g % STAGES2;
+          const uint32_t ph = (g / STAGES2) & 1;
+          if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
+          tc::tc_fence_after();
+          const uint8_t* st = smem + s * STAGE2_BYTES;
+          const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
+          const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
+          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
+          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + B_HALF));
+          const int ksub = min(BK, K - kt * BK + 15) / 16;
+          for (int kk = 0; kk < ksub; kk++) {
+            const uint64_t o = uint64_t(kk * 2);
+            tc::mma_bf16_pair(acc, dah + o, dbh + o, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+            if (!ONE) {
+              tc::mma_bf16_pair(acc, dah + o, dbl + o, idesc, 1u);
+              tc::mma_bf16_pair(acc, dal + o, dbh + o, idesc, 1u);
+            }
+          }
+          tc::mma_commit_pair(&empty[s], 0x3);
+        }
+        if (ok) tc::mma_commit_pair(&tfull[b], 0x3);
+      }
+      tc::mma_commit_pair(done, 0x1);
+      tc::mbar_wait(done, 0, err, 4u);
+    }
+  } else {  // epilogue warps 2..5 of both CTAs: TMEM lane quadrant = warp % 4, this CTA's 128 rows of the pair tile
+    const int q = warp & 3;
+    const uint32_t tempty_lead = tc::mapa_shared(tc::smem_u32(tempty), 0);
+    int it = 0;
+    for (int t = pair; t < ntiles; t += npairs, it++) {
+      const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = (t % ntn) * BN;
+      const int b = it & 1;
+      if (!tc::mbar_wait(&tfull[b], (it >> 1) & 1, err, 8u)) break;
+      tc::tc_fence_after();
+      const int m = m0 + q * 32 + lane;
+      const bool mv = m < out.M;
+      const int cend = min(out.N, n0 + BN);
+      const int plane = m / out.R, r = m - plane * out.R;
+      for (int ch = 0; ch * 32 < BN; ch++) {
+        float v[32];
+        tc::tmem_ld32(tmem + uint32_t(b * 256) + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
+        const int c0 = n0 + ch * 32;
+        if (c0 >= cend) continue;
+        if (MODE == OUT_T_BF16X2 || MODE == OUT_T_F32) {
+          if (mv) {
+            const long base = long(plane) * out.N * out.ld + r;
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+              if (c0 + c < cend) {
+                const long a = base + long(c0 + c) * out.ld;
+                if (MODE == OUT_T_F32) {
+                  out.f[a] = v[c];
+                } else if (ONE) {
+                  out.hi[a] = __float2bfloat16_rn(v[c]);
+                } else {
+                  __nv_bfloat16 h, l;
+                  tc::split_bf16(v[c], h, l);
+                  out.hi[a] = h;
+                  out.lo[a] = l;
+                }
+              }
+            }
+          }
+        } else {
+          float* stg = reinterpret_cast<float*>(smem + STAGES2 * STAGE2_BYTES + 256) + q * 32 * STG_LD;
+#pragma unroll
+          for (int c = 0; c < 32; c++) stg[lane * STG_LD + c] = v[c];
+          __syncwarp();
+          const bool cv = c0 + lane < cend;
+          const int mrow = m0 + q * 32;
+          float old[32];
+          if (MODE == OUT_R_F32_ADD) {
+#pragma unroll
+            for (int rr = 0; rr < 32; rr++) old[rr] = (cv && mrow + rr < out.M) ? out.f[long(mrow + rr) * out.ld + c0 + lane] : 0.f;
+          }
+#pragma unroll
+          for (int rr = 0; rr < 32; rr++) {
+            if (cv && mrow + rr < out.M) {
+              const float val = stg[rr * STG_LD + lane];
+              out.f[long(mrow + rr) * out.ld + c0 + lane] = MODE == OUT_R_F32_ADD ? old[rr] + val : val;
+            }
+          }
+          __syncwarp();
+        }
+      }
+      // the accumulator is free again once both CTAs' epilogue warps have read it
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if (lead) tc::mbar_arrive(&tempty[b]);
+        else tc::mbar_arrive_cluster(tempty_lead + uint32_t(b * 8));
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();  // the second CTA's shared memory and TMEM stay until the pair's last MMA and epilogue are done
+  if (warp == 1) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc_pair(tmem, kTmemCols);
+  }
+}
+
 __global__ void k_split_rows(const float* __restrict__ src, long rows, int cols, __nv_bfloat16* __restrict__ hi,
                              __nv_bfloat16* __restrict__ lo, int ld) {
   const long n = rows * ld;
@@ -763,6 +965,13 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_T_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32_ADD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_tri_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
     cudaFuncSetAttribute(k_tri_tma<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
     cudaFuncSetAttribute(k_tri_tma<80>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
@@ -792,6 +1001,8 @@ struct TcPlan {
   CUtensorMap Fx[2], Fy[2], Fr[2], Frr[2];  // fields, the A operand: S_x, S_y, the split right-hand side and residual
   CUtensorMap tri_in, tri_out[2];  // the tridiagonals' tiles: T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi / lo out
   bool tri_tma = false;
+  CUtensorMap Qh[4][2];  // the DST matrices with boxes of half a tile's width: each CTA of a pair loads one half
+  bool pairs = false;    // transforms on SM pairs (k_dst_tc2)
 };
 
 static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
@@ -856,7 +1067,9 @@ int PoissonPlan::tc_create() {
   const int bn[4] = {T->bnx, T->bny, T->bny, T->bnx};
   ok = true;
   for (int t = 0; t < 4; t++)
-    for (int h = 0; h < 2; h++) ok = ok && make_map_2d(&T->Q[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t]);
+    for (int h = 0; h < 2; h++)
+      ok = ok && make_map_2d(&T->Q[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t]) &&
+           make_map_2d(&T->Qh[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t] / 2);
   // A operands, planes stacked: S_x and the split rhs [nz * ny][nx] pitch ldx; S_y [nz * nx][ny] pitch ldy
   ok = ok && make_map_2d(&T->Fx[0], T->sx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fx[1], T->sx_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fr[0], T->rx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fr[1], T->rx_lo, long(nz) * ny, nx, T->ldx, BM);
@@ -920,8 +1133,47 @@ void PoissonPlan::tc_destroy() {
   tc = nullptr;
 }
 
+static cudaLaunchConfig_t pair_config(int pairs, cudaStream_t s, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * pairs);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = SMEM2_BYTES;
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// pairs of SMs that can hold a k_dst_tc2 cluster at once (the GPCs' SM counts need not be even); the persistent grid
+// is no larger, so that no cluster waits for a second wave
+static int pair_slots() {
+  static int n = 0;
+  if (!n) {
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = pair_config(num_sms() / 2, nullptr, at);
+    if (cudaOccupancyMaxActiveClusters(&n, k_dst_tc2<OUT_T_F32>, &cfg) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      n = num_sms() / 2;
+    }
+    n = std::min(n, num_sms() / 2);
+  }
+  return n;
+}
+
 template <int MODE, bool ONE = false>
-static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn, const TcOut& o, unsigned int* err, cudaStream_t s) {
+static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn, const TcOut& o, unsigned int* err, cudaStream_t s,
+                      const CUtensorMap* qh = nullptr) {
+  if (qh) {  // SM pairs: tiles of 256 field rows, qh the DST matrix maps with half-width boxes
+    const int tiles = ((o.M + 2 * BM - 1) / (2 * BM)) * ((o.N + bn - 1) / bn);
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = pair_config(std::min(tiles, pair_slots()), s, at);
+    cudaLaunchKernelEx(&cfg, k_dst_tc2<MODE, ONE>, f[0], f[1], qh[0], qh[1], K, bn, o, err);
+    return;
+  }
   const int tiles = ((o.M + BM - 1) / BM) * ((o.N + bn - 1) / bn);
   k_dst_tc<MODE, ONE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
 }
@@ -930,14 +1182,15 @@ static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn,
 // (stored, or added when add)
 static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s,
                     bool one = false) {
+#define QH(t) (T->pairs ? T->Qh[t] : nullptr)
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const TcOut sy{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, t2{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny};
   // X-fwd: field rows (k, j), K = i, outputs l  -> S_y[k][l][j]
-  if (one) launch_tc<OUT_T_BF16X2, true>(T->Frr, T->Q[0], nx, T->bnx, sy, T->err, s);
-  else launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, sy, T->err, s);
+  if (one) launch_tc<OUT_T_BF16X2, true>(T->Frr, T->Q[0], nx, T->bnx, sy, T->err, s, QH(0));
+  else launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, sy, T->err, s, QH(0));
   // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
-  if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
-  else launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s);
+  if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s, QH(1));
+  else launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s, QH(1));
   // tridiagonals -> S_y[k][l][m]
   if (T->tri_tma) {
     const dim3 grid((nx + TRI_TL - 1) / TRI_TL, (ny + TRI_TM - 1) / TRI_TM);
@@ -953,13 +1206,14 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   }
   // Y-inv: field rows (k, l), K = m, outputs j  -> S_x[k][j][l]
   const TcOut sx{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny};
-  if (one) launch_tc<OUT_T_BF16X2, true>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s);
-  else launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s);
+  if (one) launch_tc<OUT_T_BF16X2, true>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s, QH(2));
+  else launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s, QH(2));
   // X-inv: field rows (k, j), K = l, outputs i  -> phi[k][j][i]
   const TcOut o{nullptr, nullptr, phi, nx, ny, nz * ny, nx};
-  if (one) launch_tc<OUT_R_F32_ADD, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
-  else if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
-  else launch_tc<OUT_R_F32>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s);
+  if (one) launch_tc<OUT_R_F32_ADD, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
+  else if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
+  else launch_tc<OUT_R_F32>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
+#undef QH
 }
 
 // precision 1: one bf16x3 pass; precision 2: a second bf16x3 pass on the FP64-accumulated residual (iterative
@@ -990,6 +1244,18 @@ int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
     return OB_ERR_DEVICE;
   }
   return OB_OK;
+}
+
+int PoissonPlan::tc_set_pairs(bool on) {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) { set_error("poisson: the SM-pair transforms need a tensor-core precision (1 to 4)"); return OB_ERR_INVALID; }
+  T->pairs = on;
+  if (on) pair_slots();   // the occupancy query runs here, outside any stream capture
+  return OB_OK;
+}
+bool PoissonPlan::tc_pairs() const {
+  const TcPlan* T = static_cast<const TcPlan*>(tc);
+  return T && T->pairs;
 }
 
 void PoissonPlan::tc_rhs_split(__nv_bfloat16** hi, __nv_bfloat16** lo, int* ld) const {

@@ -189,7 +189,7 @@ int tc_train_run(MlpTcTrainer* t, float* w, float* g, float* m, float* v, int& a
                  const Norm& nm, int batch, int steps, float lr, unsigned seed, double* d_loss, cudaStream_t s);
 int tc_grad_run(MlpTcTrainer* t, const float* w, float* g, const float* pairs, int count, const Norm& nm, double* d_loss,
                 cudaStream_t s);
-int sort_pairs(float* pairs, long n, cudaStream_t s);
+int sort_pairs(float* pairs, long n, bool overflowed, unsigned* count, cudaStream_t s);
 }  // namespace mlp
 }  // namespace ob
 
@@ -420,9 +420,11 @@ int ob_mlp_pair_count(ObMlp* n, long long* count) {
 
 int ob_mlp_sort_pairs(ObMlp* n) {
   if (!n) { set_error("ob_mlp_sort_pairs: null network"); return OB_ERR_INVALID; }
-  long long cnt = 0;
-  MLP_TRY(ob_mlp_pair_count(n, &cnt));
-  return ob::mlp::sort_pairs(n->d_pairs, long(cnt), n->stream);
+  unsigned raw = 0;
+  MLP_TRY(cuda_ok(cudaDeviceSynchronize(), "ob_mlp_sort_pairs"));
+  MLP_TRY(cuda_ok(cudaMemcpy(&raw, n->d_count, 4, cudaMemcpyDeviceToHost), "ob_mlp_sort_pairs"));
+  const long cnt = long(std::min<size_t>(raw, n->cap));
+  return ob::mlp::sort_pairs(n->d_pairs, cnt, size_t(raw) > n->cap, n->d_count, n->stream);
 }
 
 int ob_mlp_read_pairs(ObMlp* n, long long first, long long count, float* host) {

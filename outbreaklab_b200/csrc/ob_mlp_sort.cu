@@ -6,6 +6,9 @@
 // recording. ob_mlp_sort_pairs orders the buffer by (time, offset) with a stable least-significant-digit radix sort on
 // the device (8-bit digits of a 64-bit key: the time's float bits above the offset), then gathers the 96-byte pairs
 // into the new order. With it a run's recording, and so its trained network, no longer depends on the append order.
+// A recording that ran past the buffer's capacity kept an arbitrary subset of its last step's pairs (those whose
+// appends won the race); after the sort these are the tail of the buffer, and the sort drops them by setting the
+// append counter to the first pair of that step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -133,10 +136,19 @@ __global__ void k_gather_pairs(const float4* __restrict__ src, const unsigned* _
     dst[i] = src[long(order[p]) * V + (i - p * V)];
   }
 }
+// count[0] = index of the first pair whose model time is the last pair's (the pairs are in time order)
+__global__ void k_first_of_last_step(const float* __restrict__ pairs, long n, unsigned* __restrict__ count) {
+  const unsigned last = __float_as_uint(pairs[(n - 1) * PAIR + 23]);
+  for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    if (__float_as_uint(pairs[i * PAIR + 23]) == last && (i == 0 || __float_as_uint(pairs[(i - 1) * PAIR + 23]) != last))
+      count[0] = unsigned(i);
+}
 }  // namespace
 
-// sorts `n` pairs in place (`pairs` holds at least n * PAIR floats); allocates its scratch for the call
-int sort_pairs(float* pairs, long n, cudaStream_t s) {
+// sorts `n` pairs in place (`pairs` holds at least n * PAIR floats); with `overflowed` (the append counter passed the
+// capacity) it then drops the last step's pairs by setting count[0] to the first of them. Allocates its scratch for
+// the call.
+int sort_pairs(float* pairs, long n, bool overflowed, unsigned* count, cudaStream_t s) {
   if (n <= 1) return OB_OK;
   const int nb = int((n + RS_CHUNK - 1) / RS_CHUNK);
   unsigned long long *k0 = nullptr, *k1 = nullptr;
@@ -162,6 +174,7 @@ int sort_pairs(float* pairs, long n, cudaStream_t s) {
     }
     k_gather_pairs<<<2368, 256, 0, s>>>(reinterpret_cast<const float4*>(pairs), v0, n, reinterpret_cast<float4*>(tmp));
     const cudaError_t e1 = cudaMemcpyAsync(pairs, tmp, size_t(n) * PAIR * 4, cudaMemcpyDeviceToDevice, s);
+    if (overflowed && e1 == cudaSuccess) k_first_of_last_step<<<1184, 256, 0, s>>>(pairs, n, count);
     const cudaError_t e2 = cudaStreamSynchronize(s);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
       set_error("ob_mlp_sort_pairs: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));

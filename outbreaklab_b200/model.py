@@ -186,6 +186,10 @@ class RegionalModel:
         N.check(N.lib().ob_model_time(self.h, C.byref(t), C.byref(s), C.byref(p)))
         return p.value
 
+    def set_pair_tiles(self, on: bool):
+        """The solve's transforms on SM pairs (True) or single SMs (False); bit-identical results."""
+        N.check(N.lib().ob_model_set_pair_tiles(self.h, int(bool(on))))
+
     def set_solver(self, precision: int):
         """Pressure-solve precision: 0 = fp32 transforms, 1 = bf16x3 tensor-core transforms."""
         N.check(N.lib().ob_model_set_solver(self.h, int(precision)))
@@ -280,6 +284,11 @@ class PoissonDirect:
         t = C.c_float()
         N.check(N.lib().ob_poisson_time(self.h, int(reps), C.byref(t)))
         return t.value
+
+    def set_pair_tiles(self, on: bool):
+        """Transforms on tiles of 256 rows computed by SM pairs (True) or 128-row tiles on single SMs (False);
+        bit-identical results."""
+        N.check(N.lib().ob_poisson_set_pair_tiles(self.h, int(bool(on))))
 
     def residual(self):
         """FP64 residual of the last solve on the device: (max|r| / max|rhs|, ||r||_2 / ||rhs||_2)."""

@@ -158,6 +158,31 @@ def test_recorded_pairs_have_a_canonical_order(native):
     assert (np.diff(key) > 0).all()                            # strictly increasing: (time, offset) is unique
 
 
+def test_a_recording_past_capacity_drops_its_last_step(native):
+    """A buffer that fills up in the middle of a step keeps a race-dependent subset of that step's pairs; the sort
+    drops the step, so the count and the buffer are the same from run to run and end on a whole step."""
+    case, a, B = _thompson_blob_model()
+    full = S.MicroSurrogate(seed=9)
+    full.reserve(3 * case.cells)
+    S.record(a, full, 3, case.dt, 0.5)
+    ref = full.read_pairs()
+    full.close()
+    per_step = [int((ref[:, 23] == k * case.dt).sum()) for k in range(3)]
+    assert min(per_step) > 100
+    cap = per_step[0] + per_step[1] // 2          # fills up half-way through the second step
+    bufs = []
+    for _ in range(2):
+        case, a, B = _thompson_blob_model()
+        net = S.MicroSurrogate(seed=9)
+        net.reserve(cap)
+        S.record(a, net, 3, case.dt, 0.5)
+        assert net.count() == per_step[0]
+        bufs.append(net.read_pairs())
+        net.close()
+    assert np.array_equal(bufs[0].view(np.uint32), bufs[1].view(np.uint32))
+    assert np.array_equal(bufs[0].view(np.uint32), ref[:per_step[0]].view(np.uint32))
+
+
 def test_recorded_pairs_are_scheme_tendencies(native):
     case, a, B, net, P = _record_one_step()
     assert len(P) > 1000

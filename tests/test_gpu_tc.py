@@ -73,3 +73,48 @@ def test_poisson_bf16x3_vs_fp64(oracle_lib, native, shape, precision):
     else:
         assert err <= max(1e-5, 2 * err32), (err, err32)   # refined: at least as accurate as the fp32 restatement
         assert res < 3e-4, res                     # one sweep cuts the ~1e-2 residual of a single pass ~100x
+
+
+@pytest.mark.parametrize("nx,ny,nz,precision", [(656, 656, 40, 2), (656, 656, 40, 3), (336, 320, 40, 1), (1024, 1024, 80, 2),
+                                                (48, 40, 16, 2)])
+def test_pair_tiles_are_bit_identical(native, nx, ny, nz, precision):
+    """The transforms on SM pairs (tiles of 256 rows, tcgen05.mma.cta_group::2, each SM loading half of the matrix
+    tile) give the same bits as on single SMs: the same bf16 products accumulated over the same k-steps. Shapes cover
+    tile widths 224, 176 / 160, 256 and 64 (halves of 112, 88 / 80, 128 and 32 rows), the plain-bf16 correction pass
+    (precision 3) and a grid smaller than one pair tile."""
+    import numpy as np
+    from outbreaklab_b200 import model as M, workloads as W
+    dz = 20000.0 / nz
+    B, _ = W.base_state_for(W.StormCase("solve", 8, 8, nz, 1000.0, 6.0, 1))
+    Bz = B.reshape(nz + 1, 8)
+    rc, rw = Bz[:nz, 2].astype(np.float32).copy(), Bz[:, 3].astype(np.float32).copy()
+    rhs = W.gaussian_rhs(nx, ny, nz, 1000.0, corr_len=5000.0, seed=5, dtype=np.float32)
+    out = {}
+    for pairs in (False, True):
+        P = M.PoissonDirect(nx, ny, nz, 1000.0, dz, precision)
+        try:
+            P.set_density(rc, rw)
+            P.set_pair_tiles(pairs)
+            out[pairs] = P.solve(rhs)
+        finally:
+            P.destroy()
+    assert np.isfinite(out[True]).all()
+    assert np.array_equal(out[True].view(np.uint32), out[False].view(np.uint32))
+
+
+def test_pair_tiles_in_the_model_step(native):
+    import numpy as np
+    from outbreaklab_b200 import _native as N, model as M, workloads as W
+    case = W.case_small(nx=120, ny=100, nz=40, dx=1000.0, dt=6.0)
+    a, _ = M.setup_case(case)
+    b, _ = M.setup_case(case)
+    try:
+        b.set_pair_tiles(True)
+        for m in (a, b):
+            m.enc_step(case.dt, 3)
+            m.sync()
+        for f in (N.FIELD_V, N.FIELD_Q1, N.FIELD_PHI):
+            assert np.array_equal(a.get_field(f).view(np.uint32), b.get_field(f).view(np.uint32)), f
+    finally:
+        a.destroy()
+        b.destroy()
