@@ -208,11 +208,14 @@ int ob_model_set_graphs(ObModel* m, int on);
  * floor that storing phi in fp32 sets).
  * No counterpart in the reference. */
 int ob_model_set_solver(ObModel* m, int precision);
-/* tile shape of the tensor-core solve's transforms: 1 = tiles of 256 field rows computed by pairs of SMs (a cluster of
- * two CTAs, tcgen05.mma.cta_group::2: each SM loads half of the DST-matrix tile, a third less operand traffic),
- * 0 = tiles of 128 rows on single SMs. The results are bit-identical. Precisions 1 to 4 only (set after
- * ob_model_set_solver, which resets it). No counterpart in the reference. */
+/* tile shape of the tensor-core solve's transforms: 1 (the default) = tiles of 256 field rows computed by pairs of SMs
+ * (a cluster of two CTAs, tcgen05.mma.cta_group::2: each SM loads half of the DST-matrix tile and reads a third less
+ * operand data per product), 0 = tiles of 128 rows on single SMs. The results are bit-identical. Precisions 1 to 4
+ * only (ob_model_set_solver resets it to the default). No counterpart in the reference. */
 int ob_model_set_pair_tiles(ObModel* m, int on);
+/* outputs per tile of the x and y transforms (multiples of 16 in 32..256; 0 = automatic), for tuning; the results do
+ * not depend on them. Precisions 1 to 4 only (ob_model_set_solver resets them). No counterpart in the reference. */
+int ob_model_set_tile_widths(ObModel* m, int bn_x, int bn_y);
 int ob_model_solver(ObModel* m);
 /* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
 void* ob_model_stream(ObModel* m);
@@ -240,6 +243,8 @@ int ob_poisson_time(ObPoisson* p, int reps, float* ms);
 int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel);
 /* the transforms' tile shape, as ob_model_set_pair_tiles; no counterpart in the reference */
 int ob_poisson_set_pair_tiles(ObPoisson* p, int on);
+/* the transforms' tile widths, as ob_model_set_tile_widths; no counterpart in the reference */
+int ob_poisson_set_tile_widths(ObPoisson* p, int bn_x, int bn_y);
 
 /* ---- RadarSim (radar.js:271-413): virtual WSR-88D gate sampling ----
  * The host keeps RadarSim's VCP tables, volume layout and scan scheduling (radar.js:289-392); the library owns each

@@ -82,6 +82,8 @@ SYMBOLS = {
     "ob_poisson_residual": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ob_poisson_set_pair_tiles": (_i, [_vp, _i]),
     "ob_model_set_pair_tiles": (_i, [_vp, _i]),
+    "ob_poisson_set_tile_widths": (_i, [_vp, _i, _i]),
+    "ob_model_set_tile_widths": (_i, [_vp, _i, _i]),
     "ob_dst_tc_selftest": (_i, [_i, _i, _i, _i, _fp, _fp, _fp]),
     "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),
     "ob_radar_create": (_i, [_vp, _sz, _i, C.POINTER(_vp)]),

@@ -37,13 +37,15 @@ def solve(args):
     P.set_density(rc, rw)
     if args.pair_tiles is not None:
         P.set_pair_tiles(bool(args.pair_tiles))
+    if args.bn:
+        P.set_tile_widths(args.bn, args.bn)
     P.solve(rhs)   # uploads the right-hand side that device_ms solves again
     ms = P.device_ms(args.reps)
     # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16),
     # 3 + 3 + 3 (two refinement sweeps)
     flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4, 4: 9}[args.precision]
     out = {"bench": "pressure solve", "nx": nx, "ny": ny, "nz": nz, "precision": args.precision, "ms": ms,
-           "pair_tiles": args.pair_tiles,
+           "pair_tiles": args.pair_tiles, "bn": args.bn,
            "dst_flops": flops, "tflops": flops / (ms * 1e-3) / 1e12}
     print(json.dumps(out), flush=True)
 
@@ -188,6 +190,7 @@ def main(argv=None):
     a.add_argument("--reps", type=int, default=10)
     a.add_argument("--pair-tiles", type=int, choices=[0, 1], default=None,
                    help="1: transforms on SM pairs (256-row tiles); 0: on single SMs; default: the library's choice")
+    a.add_argument("--bn", type=int, default=0, help="outputs per transform tile (multiple of 16, 32..256); 0: automatic")
     b = sub.add_parser("step")
     b.add_argument("--case", default="c4")
     b.add_argument("--steps", type=int, default=50)

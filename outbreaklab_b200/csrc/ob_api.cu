@@ -264,6 +264,7 @@ static void write_uniforms(ObModel* m, double dt, cudaStream_t ts = nullptr) {
   // the same float expressions the kernels would evaluate per thread, once on the host (IEEE float arithmetic)
   const float fdt = U.step.x, fdx = U.dims.w, fdz = U.dzv.x;
   U.der = make_float4(fdt / fdx, fdt / fdz, 1.f / (fdx * fdx), 1.f / (fdz * fdz));
+  U.der2 = make_float4(1.f / fdt, 0.f, 0.f, 0.f);
   // sponge tables, remade when a uniform they read or the base state changed
   const float key[8] = {U.sponge.x, U.sponge.y, U.sponge.z, U.sponge.w, U.step.z, fdx, fdz, 0.f};
   if (m->tab_gen != m->base_gen || std::memcmp(key, m->tab_key, sizeof(key)) != 0) {
@@ -894,6 +895,13 @@ int ob_model_set_pair_tiles(ObModel* m, int on) {
   return m->solver.tc_set_pairs(on != 0);
 }
 
+int ob_model_set_tile_widths(ObModel* m, int bn_x, int bn_y) {
+  if (!m) { set_error("ob_model_set_tile_widths: null model"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "set tile widths"));
+  drop_graphs(m);
+  return m->solver.tc_set_tile_widths(bn_x, bn_y);
+}
+
 unsigned ob_model_nan_count(ObModel* m) {
   unsigned h = 0;
   if (m && cudaMemcpy(&h, m->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) h = 0;
@@ -1504,6 +1512,11 @@ int ob_poisson_set_pair_tiles(ObPoisson* p, int on) {
   if (!p) { set_error("ob_poisson_set_pair_tiles: null handle"); return OB_ERR_INVALID; }
   OB_TRY(cuda_status(cudaStreamSynchronize(p->stream), "set pair tiles"));
   return p->plan.tc_set_pairs(on != 0);
+}
+int ob_poisson_set_tile_widths(ObPoisson* p, int bn_x, int bn_y) {
+  if (!p) { set_error("ob_poisson_set_tile_widths: null handle"); return OB_ERR_INVALID; }
+  OB_TRY(cuda_status(cudaStreamSynchronize(p->stream), "set tile widths"));
+  return p->plan.tc_set_tile_widths(bn_x, bn_y);
 }
 int ob_poisson_residual(ObPoisson* p, double* max_rel, double* l2_rel) {
   if (!p || !max_rel || !l2_rel) { set_error("ob_poisson_residual: null argument"); return OB_ERR_INVALID; }

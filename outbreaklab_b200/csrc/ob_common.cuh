@@ -20,6 +20,7 @@ namespace ob {
 struct Uni {
   float4 dims, dzv, step, sponge, turb, micro, misc, cor, ci, pad, micro2, hur, hur2, hur3, hur4, hur5, vtx, vtx2, cn;
   float4 der;  // derived on the host per step: (dt/dx, dt/dz, 1/dx^2, 1/dz^2), so no thread divides uniforms
+  float4 der2; // (1/dt, 0, 0, 0), derived on the host per step
   // step.y (the model time of the reference's block) stays 0 here: the kernels read the time from Fields::clock
 };
 

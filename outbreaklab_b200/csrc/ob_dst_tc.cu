@@ -36,6 +36,12 @@ constexpr int BK = 64;                  // K per pipeline stage: one 128-byte sw
 constexpr int STAGES = 2;
 constexpr int A_TILE = BM * BK * 2;     // 16 KB per A operand tile (hi or lo)
 constexpr int B_TILE = BNMAX * BK * 2;  // 32 KB per B operand tile slot
+// the MMA's N for a tile of BN outputs of which `left` remain in its row of tiles: the multiple of 16 covering them,
+// at least 32, at most BN
+__host__ __device__ constexpr int narrow_n(int BN, int left) {
+  const int r = (left + 15) / 16 * 16;
+  return left >= BN ? BN : (r < 32 ? (BN < 32 ? BN : 32) : (r < BN ? r : BN));
+}
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int STG_LD = 33;                          // row pitch (floats) of the epilogue's transpose buffer
 constexpr int STG_BYTES = 4 * 32 * STG_LD * 4;       // 32 x 32 floats per epilogue warp
@@ -56,6 +62,15 @@ struct TcOut {
   int M;     // valid field rows (planes x R)
   int N;     // valid transform outputs
 };
+// the epilogue that adds into a row-major output reads the old rows of its tile: one thread per row brings the row's
+// [n0, n0 + BN) segment into L2, a tile ahead, so that the loads hit L2 instead of waiting on DRAM
+__device__ __forceinline__ void prefetch_rows(const TcOut& out, int m, int n0, int BN) {
+  if (m >= out.M) return;
+  const float* row = out.f + long(m) * out.ld;
+  const int c1 = min(out.N, n0 + BN) - 1;
+  for (int c = n0; c < c1; c += 32) tc::prefetch_l2(row + c);
+  tc::prefetch_l2(row + c1);
+}
 }  // namespace
 
 // one tile of a transform: its operands, sizes and output, and its corner
@@ -190,7 +205,8 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, it++) {
         TileInfo ti;
         src.tile(t, ti);
-        const uint32_t idesc = tc::idesc_bf16_f32(BM, ti.BN);
+        // the last tile of a row of tiles multiplies only the matrix rows it needs (its N narrowed to a multiple of 16)
+        const uint32_t idesc = tc::idesc_bf16_f32(BM, narrow_n(ti.BN, ti.out.N - ti.n0));
         const int nk = (ti.K + BK - 1) / BK;
         const int b = it & 1;
         if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
@@ -225,9 +241,19 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
     const int q = warp & 3;
     int it = 0;
+    if (MODE == OUT_R_F32_ADD && int(blockIdx.x) < ntiles) {
+      TileInfo tn;
+      src.tile(blockIdx.x, tn);
+      prefetch_rows(tn.out, tn.m0 + q * 32 + lane, tn.n0, tn.BN);
+    }
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
       TileInfo ti;
       src.tile(t, ti);
+      if (MODE == OUT_R_F32_ADD && t + int(gridDim.x) < ntiles) {   // the next tile's old rows, while this one drains
+        TileInfo tn;
+        src.tile(t + gridDim.x, tn);
+        prefetch_rows(tn.out, tn.m0 + q * 32 + lane, tn.n0, tn.BN);
+      }
       const TcOut& out = ti.out;
       const int BN = ti.BN, m0 = ti.m0, n0 = ti.n0;
       const int b = it & 1;
@@ -332,10 +358,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_tc_grp(const GemmProb* __re
 // single-SM kernel's bit for bit (the same bf16 products, accumulated over the same k-steps).
 // ---------------------------------------------------------------------------------------------------------------
 namespace {
-constexpr int STAGES2 = 3;
-constexpr int B_HALF = BNMAX / 2 * BK * 2;                   // 16 KB: half a matrix tile of 256 rows
-constexpr int STAGE2_BYTES = 2 * A_TILE + 2 * B_HALF;        // 64 KB
-constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 /*align*/ + 256 /*barriers*/ + STG_BYTES;
+// shared memory: the epilogue's transpose buffers, the barriers, then a ring of as many stages (field hi/lo, half the
+// matrix tile hi/lo) as the tile width leaves room for: 3 at BN = 224 or 256, 4 at BN <= 144 (every slot a multiple
+// of 1024 bytes, as the 128-byte swizzle wants)
+constexpr int MAXST2 = 6;
+constexpr int BAR2_OFF = (STG_BYTES + 1023) / 1024 * 1024;
+constexpr int RING2_OFF = BAR2_OFF + 1024;
+constexpr int SMEM2_BYTES = 227 * 1024;                      // the most a block may use
+constexpr int RING2_BYTES = SMEM2_BYTES - 1024 /*align*/ - RING2_OFF;
+__host__ __device__ constexpr int half_bytes2(int BN) { return BN / 2 * BK * 2; }
+__host__ __device__ constexpr int stage2_bytes(int BN) { return 2 * A_TILE + 2 * half_bytes2(BN); }
+__host__ __device__ constexpr int stages2(int BN) { return RING2_BYTES / stage2_bytes(BN) < MAXST2 ? RING2_BYTES / stage2_bytes(BN) : MAXST2; }
+static_assert(stages2(BNMAX) >= 3, "three stages at the widest tile");
 }  // namespace
 
 template <int MODE, bool ONE = false>
@@ -345,9 +379,9 @@ __global__ void __launch_bounds__(kThreads, 1)
               unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES2 * STAGE2_BYTES);
-  uint64_t* empty = full + STAGES2;
-  uint64_t* tfull = empty + STAGES2;  // [2] accumulator b holds a finished tile (both CTAs)
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + BAR2_OFF);
+  uint64_t* empty = full + MAXST2;
+  uint64_t* tfull = empty + MAXST2;   // [2] accumulator b holds a finished tile (both CTAs)
   uint64_t* tempty = tfull + 2;       // [2] both CTAs' epilogues have drained accumulator b (used in the first CTA)
   uint64_t* done = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -359,9 +393,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
   const int bh = BN / 2;
   const int nk = (K + BK - 1) / BK;
+  const int nst = stages2(BN), sbytes = stage2_bytes(BN), hbytes = half_bytes2(BN);
+  uint8_t* ring = smem + RING2_OFF;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES2; s++) {
+    for (int s = 0; s < MAXST2; s++) {
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
@@ -394,41 +430,43 @@ __global__ void __launch_bounds__(kThreads, 1)
       int g = 0;
       bool ok = true;
       for (int t = pair; t < ntiles && ok; t += npairs) {
-        const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = (t % ntn) * BN + int(rank) * bh;
+        // the second CTA holds the second half of the N columns the pair's MMAs use
+        const int nt0 = (t % ntn) * BN, nv = narrow_n(BN, out.N - nt0);
+        const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = nt0 + int(rank) * (nv / 2);
         for (int kt = 0; kt < nk; kt++, g++) {
-          const int s = g % STAGES2;
-          const uint32_t ph = (g / STAGES2) & 1;
+          const int s = g % nst;
+          const uint32_t ph = (g / nst) & 1;
           if (!(ok = tc::mbar_wait(&empty[s], ph ^ 1, err, 1u))) break;
-          uint8_t* st = smem + s * STAGE2_BYTES;
+          uint8_t* st = ring + s * sbytes;
           const uint32_t fb = tc::mapa_shared(tc::smem_u32(&full[s]), 0);
           if (lead) tc::mbar_expect_tx(&full[s], bytes);
           tc::tma_load_2d_pair(st, &tF_hi, fb, kt * BK, m0);
           if (!ONE) tc::tma_load_2d_pair(st + A_TILE, &tF_lo, fb, kt * BK, m0);
           tc::tma_load_2d_pair(st + 2 * A_TILE, &tQ_hi, fb, kt * BK, n0);
-          if (!ONE) tc::tma_load_2d_pair(st + 2 * A_TILE + B_HALF, &tQ_lo, fb, kt * BK, n0);
+          if (!ONE) tc::tma_load_2d_pair(st + 2 * A_TILE + hbytes, &tQ_lo, fb, kt * BK, n0);
         }
       }
     }
   } else if (warp == 1) {
     if (lane == 0 && lead) {  // MMA issuer of the pair
-      const uint32_t idesc = tc::idesc_bf16_f32(2 * BM, BN);
       int g = 0, it = 0;
       bool ok = true;
       for (int t = pair; t < ntiles && ok; t += npairs, it++) {
+        const uint32_t idesc = tc::idesc_bf16_f32(2 * BM, narrow_n(BN, out.N - (t % ntn) * BN));
         const int b = it & 1;
         if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
         tc::tc_fence_after();
         const uint32_t acc = tmem + uint32_t(b * 256);
         for (int kt = 0; kt < nk; kt++, g++) {
-          const int s = g % STAGES2;
-          const uint32_t ph = (g / STAGES2) & 1;
+          const int s = g % nst;
+          const uint32_t ph = (g / nst) & 1;
           if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
           tc::tc_fence_after();
-          const uint8_t* st = smem + s * STAGE2_BYTES;
+          const uint8_t* st = ring + s * sbytes;
           const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
           const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
           const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
-          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + B_HALF));
+          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + hbytes));
           const int ksub = min(BK, K - kt * BK + 15) / 16;
           for (int kk = 0; kk < ksub; kk++) {
             const uint64_t o = uint64_t(kk * 2);
@@ -449,8 +487,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;
     const uint32_t tempty_lead = tc::mapa_shared(tc::smem_u32(tempty), 0);
     int it = 0;
+    if (MODE == OUT_R_F32_ADD && pair < ntiles)
+      prefetch_rows(out, (pair / ntn) * 2 * BM + int(rank) * BM + q * 32 + lane, (pair % ntn) * BN, BN);
     for (int t = pair; t < ntiles; t += npairs, it++) {
       const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = (t % ntn) * BN;
+      if (MODE == OUT_R_F32_ADD && t + npairs < ntiles) {   // the next tile's old rows, while this one drains
+        const int tn = t + npairs;
+        prefetch_rows(out, (tn / ntn) * 2 * BM + int(rank) * BM + q * 32 + lane, (tn % ntn) * BN, BN);
+      }
       const int b = it & 1;
       if (!tc::mbar_wait(&tfull[b], (it >> 1) & 1, err, 8u)) break;
       tc::tc_fence_after();
@@ -484,7 +528,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
           }
         } else {
-          float* stg = reinterpret_cast<float*>(smem + STAGES2 * STAGE2_BYTES + 256) + q * 32 * STG_LD;
+          float* stg = reinterpret_cast<float*>(smem) + q * 32 * STG_LD;
 #pragma unroll
           for (int c = 0; c < 32; c++) stg[lane * STG_LD + c] = v[c];
           __syncwarp();
@@ -1002,7 +1046,7 @@ struct TcPlan {
   CUtensorMap tri_in, tri_out[2];  // the tridiagonals' tiles: T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi / lo out
   bool tri_tma = false;
   CUtensorMap Qh[4][2];  // the DST matrices with boxes of half a tile's width: each CTA of a pair loads one half
-  bool pairs = false;    // transforms on SM pairs (k_dst_tc2)
+  bool pairs = true;     // transforms on SM pairs (k_dst_tc2); single-SM tiles (k_dst_tc) when false
 };
 
 static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
@@ -1016,6 +1060,22 @@ static void split_host(const float* src, int N, long ld, std::vector<__nv_bfloat
       lo[size_t(r) * ld + c] = __float2bfloat16_rn(x - __bfloat162float(h));
     }
 }
+
+// the DST matrices' tensor maps for tiles of bnx / bny outputs: full-width boxes for single-SM tiles, half-width boxes
+// for SM pairs
+static bool matrix_maps(TcPlan* T, int bnx, int bny) {
+  T->bnx = bnx;
+  T->bny = bny;
+  const int bn[4] = {bnx, bny, bny, bnx};
+  bool ok = true;
+  for (int t = 0; t < 4; t++)
+    for (int h = 0; h < 2; h++)
+      ok = ok && make_map_2d(&T->Q[t][h], T->qmat[t][h], T->qdim[t], T->qdim[t], T->qld[t], bn[t]) &&
+           make_map_2d(&T->Qh[t][h], T->qmat[t][h], T->qdim[t], T->qdim[t], T->qld[t], bn[t] / 2);
+  return ok;
+}
+
+static int pair_slots();
 
 int PoissonPlan::tc_create() {
   if (!get_encode()) {
@@ -1062,14 +1122,7 @@ int PoissonPlan::tc_create() {
     T->qld[t] = ld[t];
     T->qdim[t] = dim[t];
   }
-  T->bnx = pick_bn(nx);
-  T->bny = pick_bn(ny);
-  const int bn[4] = {T->bnx, T->bny, T->bny, T->bnx};
-  ok = true;
-  for (int t = 0; t < 4; t++)
-    for (int h = 0; h < 2; h++)
-      ok = ok && make_map_2d(&T->Q[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t]) &&
-           make_map_2d(&T->Qh[t][h], mp[t][h], dim[t], dim[t], ld[t], bn[t] / 2);
+  ok = matrix_maps(T, pick_bn(nx), pick_bn(ny));
   // A operands, planes stacked: S_x and the split rhs [nz * ny][nx] pitch ldx; S_y [nz * nx][ny] pitch ldy
   ok = ok && make_map_2d(&T->Fx[0], T->sx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fx[1], T->sx_lo, long(nz) * ny, nx, T->ldx, BM);
   ok = ok && make_map_2d(&T->Fr[0], T->rx_hi, long(nz) * ny, nx, T->ldx, BM) && make_map_2d(&T->Fr[1], T->rx_lo, long(nz) * ny, nx, T->ldx, BM);
@@ -1091,6 +1144,7 @@ int PoissonPlan::tc_create() {
                  make_map_3d(&T->tri_out[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, T->sy_lo, dout, pout, bout);
   }
   set_smem_attrs();
+  pair_slots();   // the occupancy query of the paired transform runs here, outside any stream capture
   return tc_factor_low();
 }
 
@@ -1251,6 +1305,20 @@ int PoissonPlan::tc_set_pairs(bool on) {
   if (!T) { set_error("poisson: the SM-pair transforms need a tensor-core precision (1 to 4)"); return OB_ERR_INVALID; }
   T->pairs = on;
   if (on) pair_slots();   // the occupancy query runs here, outside any stream capture
+  return OB_OK;
+}
+int PoissonPlan::tc_set_tile_widths(int bnx, int bny) {
+  TcPlan* T = static_cast<TcPlan*>(tc);
+  if (!T) { set_error("poisson: tile widths apply to the tensor-core precisions (1 to 4)"); return OB_ERR_INVALID; }
+  for (int b : {bnx, bny})
+    if (b != 0 && (b < 32 || b > BNMAX || b % 16)) {
+      set_error("poisson: tile width %d not 0 (automatic) or a multiple of 16 in 32..%d", b, BNMAX);
+      return OB_ERR_INVALID;
+    }
+  if (!matrix_maps(T, bnx ? bnx : pick_bn(nx), bny ? bny : pick_bn(ny))) {
+    set_error("poisson: tensor map encoding failed");
+    return OB_ERR_DEVICE;
+  }
   return OB_OK;
 }
 bool PoissonPlan::tc_pairs() const {

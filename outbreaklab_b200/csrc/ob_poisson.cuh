@@ -40,6 +40,7 @@ struct PoissonPlan {
   int tc_check();  // OB_ERR_TIMEOUT if a tensor-core pipeline wait gave up since the last check
   int tc_set_pairs(bool on);  // transforms on tiles of 256 rows computed by SM pairs (bit-identical results)
   bool tc_pairs() const;
+  int tc_set_tile_widths(int bnx, int bny);  // outputs per transform tile (multiples of 16, 32..256; 0: automatic)
   // where a producer writes the split right-hand side (bf16 hi/lo, [nz][ny][ld], x fastest) for tc_solve(nullptr, ...)
   void tc_rhs_split(__nv_bfloat16** hi, __nv_bfloat16** lo, int* ld) const;
   void tc_destroy();

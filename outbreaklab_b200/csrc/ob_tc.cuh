@@ -56,6 +56,8 @@ __device__ __forceinline__ void tma_load_3d(void* smem, const void* tmap, uint64
       "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
 }
+// bring the 128-byte line holding p into L2 (a hint: no fault, no completion to wait for)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
 }

@@ -190,6 +190,10 @@ class RegionalModel:
         """The solve's transforms on SM pairs (True) or single SMs (False); bit-identical results."""
         N.check(N.lib().ob_model_set_pair_tiles(self.h, int(bool(on))))
 
+    def set_tile_widths(self, bn_x: int = 0, bn_y: int = 0):
+        """Outputs per tile of the solve's x and y transforms (multiples of 16 in 32..256; 0: automatic)."""
+        N.check(N.lib().ob_model_set_tile_widths(self.h, int(bn_x), int(bn_y)))
+
     def set_solver(self, precision: int):
         """Pressure-solve precision: 0 = fp32 transforms, 1 = bf16x3 tensor-core transforms."""
         N.check(N.lib().ob_model_set_solver(self.h, int(precision)))
@@ -289,6 +293,10 @@ class PoissonDirect:
         """Transforms on tiles of 256 rows computed by SM pairs (True) or 128-row tiles on single SMs (False);
         bit-identical results."""
         N.check(N.lib().ob_poisson_set_pair_tiles(self.h, int(bool(on))))
+
+    def set_tile_widths(self, bn_x: int = 0, bn_y: int = 0):
+        """Outputs per tile of the x and y transforms (multiples of 16 in 32..256; 0: automatic)."""
+        N.check(N.lib().ob_poisson_set_tile_widths(self.h, int(bn_x), int(bn_y)))
 
     def residual(self):
         """FP64 residual of the last solve on the device: (max|r| / max|rhs|, ||r||_2 / ||rhs||_2)."""

@@ -75,13 +75,14 @@ def test_poisson_bf16x3_vs_fp64(oracle_lib, native, shape, precision):
         assert res < 3e-4, res                     # one sweep cuts the ~1e-2 residual of a single pass ~100x
 
 
-@pytest.mark.parametrize("nx,ny,nz,precision", [(656, 656, 40, 2), (656, 656, 40, 3), (336, 320, 40, 1), (1024, 1024, 80, 2),
-                                                (48, 40, 16, 2)])
-def test_pair_tiles_are_bit_identical(native, nx, ny, nz, precision):
+@pytest.mark.parametrize("nx,ny,nz,precision,bn", [(656, 656, 40, 2, 144), (656, 656, 40, 3, 112), (336, 320, 40, 1, 64),
+                                                   (1024, 1024, 80, 2, 176), (48, 40, 16, 2, 32)])
+def test_pair_tiles_are_bit_identical(native, nx, ny, nz, precision, bn):
     """The transforms on SM pairs (tiles of 256 rows, tcgen05.mma.cta_group::2, each SM loading half of the matrix
-    tile) give the same bits as on single SMs: the same bf16 products accumulated over the same k-steps. Shapes cover
-    tile widths 224, 176 / 160, 256 and 64 (halves of 112, 88 / 80, 128 and 32 rows), the plain-bf16 correction pass
-    (precision 3) and a grid smaller than one pair tile."""
+    tile) and with other tile widths give the same bits as the automatic single-SM tiles: the same bf16 products
+    accumulated over the same k-steps. Shapes cover automatic widths 224, 176 / 160, 256 and 48, narrowed last tiles
+    (656 outputs in tiles of 144 or 112), ring depths 3 to 5, the plain-bf16 correction pass (precision 3) and a grid
+    smaller than one pair tile."""
     import numpy as np
     from outbreaklab_b200 import model as M, workloads as W
     dz = 20000.0 / nz
@@ -90,16 +91,19 @@ def test_pair_tiles_are_bit_identical(native, nx, ny, nz, precision):
     rc, rw = Bz[:nz, 2].astype(np.float32).copy(), Bz[:, 3].astype(np.float32).copy()
     rhs = W.gaussian_rhs(nx, ny, nz, 1000.0, corr_len=5000.0, seed=5, dtype=np.float32)
     out = {}
-    for pairs in (False, True):
+    for pairs, width in ((False, 0), (True, 0), (True, bn), (False, bn)):
         P = M.PoissonDirect(nx, ny, nz, 1000.0, dz, precision)
         try:
             P.set_density(rc, rw)
             P.set_pair_tiles(pairs)
-            out[pairs] = P.solve(rhs)
+            P.set_tile_widths(width, width)
+            out[pairs, width] = P.solve(rhs)
         finally:
             P.destroy()
-    assert np.isfinite(out[True]).all()
-    assert np.array_equal(out[True].view(np.uint32), out[False].view(np.uint32))
+    ref = out[False, 0]
+    assert np.isfinite(ref).all()
+    for key, phi in out.items():
+        assert np.array_equal(phi.view(np.uint32), ref.view(np.uint32)), key
 
 
 def test_pair_tiles_in_the_model_step(native):
@@ -109,7 +113,7 @@ def test_pair_tiles_in_the_model_step(native):
     a, _ = M.setup_case(case)
     b, _ = M.setup_case(case)
     try:
-        b.set_pair_tiles(True)
+        a.set_pair_tiles(False)   # single-SM tiles; b keeps the default, SM pairs
         for m in (a, b):
             m.enc_step(case.dt, 3)
             m.sync()
