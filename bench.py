@@ -10,8 +10,9 @@ Klemp analytic sounding, 8 seeded +3 K warm bubbles; synthetic inputs (no datase
 
 value  = simulated seconds per wall second over the K timed steps (device time, CUDA events, max over ranks);
 e2e    = the same metric through the public Python API (RegionalModel.enc_step) over the same K steps of a second copy
-         of the case, with the per-step forcing upload from pinned host memory and a device-to-host read of the step's
-         FP64 budgets inside the timed region (wall clock, max over ranks);
+         of the case, with the per-step forcing upload from pinned host memory and a device-to-host read of every
+         step's FP64 budgets (requested after the step, read while the next one runs) inside the timed region (wall
+         clock, max over ranks);
 roofline = the dominant kernel of the step against the measured HBM copy peak (MEASURED_PEAKS.json), and
            solve_roofline the pressure solve's MMA work against the measured bf16 peak;
 cpu_baseline = the CPU restatement of the reference step (oracle, fp32, OpenMP) on a bounded sample.
@@ -327,33 +328,44 @@ def run_ours(args, rank, world):
     cell_steps = world * args.steps * case.cells / (t_ms / 1000.0)
     # end to end through the public API, on a second copy of the case over the same steps as the timed region (the
     # storms grow, so later steps cost more): every step uploads the app's storm-start list (setCI, model.js:1383)
-    # from pinned host memory, steps, and reads back the step's FP64 water / mass / rain budgets. The list holds one
-    # event scheduled after the run (its window opens at 1e9 s), so the CI pass reads it every step while the
-    # workload stays the bubbles-only case. The untimed warm-up has as many steps as precede the device-timed region,
-    # which also captures every step graph of the list's uniforms before the timing starts.
+    # from pinned host memory, steps, and requests the step's FP64 water / mass / rain budgets, whose copy to the host
+    # is read back while the next step runs (the reference app reads its maps back the same way, double-buffered:
+    # model.js:1478-1494); the last step's budgets are read inside the timed region. The list holds one event
+    # scheduled after the run (its window opens at 1e9 s), so the CI pass reads it every step while the workload stays
+    # the bubbles-only case. The untimed warm-up has as many steps as precede the device-timed region, which also
+    # captures every step graph of the list's uniforms before the timing starts.
     import torch
     pinned_t = torch.zeros(N.CI_FLOATS, dtype=torch.float32, pin_memory=True)
     pinned = pinned_t.numpy()
     pinned[:] = [0.5 * case.nx * case.dx, 0.5 * case.ny * case.dx, 1500.0, 10000.0, 1500.0, 5.0, 1e9, 1e9 + 1800.0,
                  0.0, 0.0, 0.0, 600.0]
     h2d_bytes = int(pinned.nbytes)
-    d2h_bytes = 8 * 8   # ob_model_budgets copies back its block of 8 FP64 sums
+    d2h_bytes = 8 * 8   # each request copies back its block of 8 FP64 sums
     m2, _ = M.setup_case(case)
 
-    def e2e_step():
+    def e2e_step(prev):
         N.check(lib.ob_model_set_ci(m2.h, N.fptr(pinned), 1))
         m2.enc_step(case.dt)
-        return m2.budgets()
+        ticket = m2.request_budgets()
+        if prev is not None:
+            m2.read_budgets(prev)
+        return ticket
 
+    prev = None
     for _ in range(args.warmup + nprof):
-        e2e_step()
+        prev = e2e_step(prev)
+    m2.read_budgets(prev)
     barrier()
     m2.sync()
     ke = args.steps
     t0 = time.perf_counter()
+    prev = None
     for _ in range(ke):
-        e2e_step()
+        prev = e2e_step(prev)
+    last = m2.read_budgets(prev)
     e2e_s = allmax(time.perf_counter() - t0)
+    if not all(math.isfinite(v) for v in last.values()):
+        raise RuntimeError("end-to-end run: non-finite budgets %s" % last)
     e2e_val = world * ke * case.dt / e2e_s
     m2.destroy()
     # roofline of the dominant kernel: the pass with the longest time per kernel launch (PHYS, NUT and DIV are one

@@ -119,7 +119,9 @@ int ob_model_set_base_state(ObModel* m, const float* B, int nz);
 int ob_model_set_params(ObModel* m, const ObParams* p);
 /* replaces setBoundaries (model.js:1371); n boundaries x OB_BOUNDARY_FLOATS */
 int ob_model_set_boundaries(ObModel* m, const float* packed, int n);
-/* replaces setCI (model.js:1383); n events x OB_CI_FLOATS, already filtered to the active ones */
+/* replaces setCI (model.js:1383); n events x OB_CI_FLOATS, already filtered to the active ones. As writeBuffer, the
+ * list is copied at the call (the caller may reuse its array at once); the upload is queued on the model's stream,
+ * ordered before the steps queued after it, without waiting for the stream */
 int ob_model_set_ci(ObModel* m, const float* events, int n);
 /* replaces RegionalModel.reset (model.js:1427-1440): LSF + INIT, phi/rhs cleared, time = steps = parity = 0 */
 int ob_model_reset(ObModel* m);
@@ -189,6 +191,13 @@ int ob_model_time(ObModel* m, double* time, int* steps, int* parity);
 /* domain budgets in FP64 on the device: sum rho*q_total*dV (kg), sum rho*dV (kg), accumulated surface rain (kg);
  * no counterpart in the reference (it keeps no budgets) */
 int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain);
+/* the same budgets without waiting, in the manner of requestMaps (model.js:1478-1494): the reductions and their copy
+ * to pinned host memory are queued on the model's stream after the work queued so far, and *ticket names the result;
+ * ob_model_read_budgets waits for that copy alone (not for work queued after the request) and returns the sums. The
+ * results of the last 4 requests can be read; an older ticket fails with OB_ERR_INVALID. No counterpart in the
+ * reference. */
+int ob_model_request_budgets(ObModel* m, long long* ticket);
+int ob_model_read_budgets(ObModel* m, long long ticket, double* water, double* mass, double* rain);
 /* nsteps steps bracketed by CUDA events on the model's stream; *ms = their device time (no counterpart in the
  * reference, whose GPUProfiler (util.js:194-230) is never instantiated) */
 int ob_model_timed_steps(ObModel* m, float dt, int nsteps, float* ms);

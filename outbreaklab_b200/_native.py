@@ -83,6 +83,8 @@ SYMBOLS = {
     "ob_poisson_set_pair_tiles": (_i, [_vp, _i]),
     "ob_model_set_pair_tiles": (_i, [_vp, _i]),
     "ob_poisson_set_tile_widths": (_i, [_vp, _i, _i]),
+    "ob_model_request_budgets": (_i, [_vp, C.POINTER(C.c_longlong)]),
+    "ob_model_read_budgets": (_i, [_vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ob_model_set_tile_widths": (_i, [_vp, _i, _i]),
     "ob_dst_tc_selftest": (_i, [_i, _i, _i, _i, _fp, _fp, _fp]),
     "ob_poisson_solve_static": (_i, [_i, _i, _i, _f, _f, _vp, _vp, _vp, _vp, _vp]),

@@ -55,53 +55,77 @@ struct EventPair {
   }
 };
 
-// sum rho q_total dV and sum rho dV over the interior cells. Each block walks (y, z) rows in a grid-stride loop and
-// adds its two partial sums once: a few FP64 atomics per block rather than two per row, which on the same two
-// addresses serialise in L2 and would dominate the pass. Cells of a 32 x 4 brick whose hydrometeor flag (act, from
-// the last physics pass or the flags rebuilt after a field write) is clear hold exactly zero condensate, so they add
-// qv alone: q0 + 0 + 0 + 0 + 0 + 0 is q0, the same bits, from one array instead of six.
-constexpr int kBudgetBlocks = 1184;  // 8 blocks of 256 threads per SM of a 148-SM B200
-__global__ void __launch_bounds__(256) k_budget(Grid g, const float* __restrict__ B, float* const* q, const unsigned int* __restrict__ act,
-                                                int nbx, int nby, double dV, double* out) {
-  const float* __restrict__ q0 = q[0];
-  const float* __restrict__ q1 = q[1];
-  const float* __restrict__ q2 = q[2];
-  const float* __restrict__ q3 = q[3];
-  const float* __restrict__ q4 = q[4];
-  const float* __restrict__ q5 = q[5];
-  double w = 0.0, mass = 0.0;
-  const int nrows = g.ny * g.nz;
-  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
-    const int j = r % g.ny, k = r / g.ny;
-    const double rho = double(__ldg(B + k * 8 + 2));
-    double row = 0.0;
-    for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
-      const int o = g.at(i, j, k);
-      if (__ldg(act + (i >> 5) + nbx * ((j >> 2) + nby * k)) != 0u)
-        row += double(__ldg(q0 + o)) + double(__ldg(q1 + o)) + double(__ldg(q2 + o)) + double(__ldg(q3 + o)) +
-               double(__ldg(q4 + o)) + double(__ldg(q5 + o));
-      else
-        row += double(__ldg(q0 + o));
-    }
-    w += row * rho;
-    if (threadIdx.x == 0) mass += rho * g.nx;
-  }
-  for (int s = 16; s > 0; s >>= 1) w += __shfl_xor_sync(0xffffffffu, w, s);
-  __shared__ double part[32];
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = w;
+// sum rho q_total dV and sum rho dV over the interior cells, and the accumulated surface rain, in FP64 and in a
+// fixed order, so that the same state gives the same bits. Block b of k_budget takes rows (y, z) [R b / nb, R (b+1) /
+// nb) and reads them four cells at a time (rows start 16-byte aligned: the pitch is a multiple of 32 floats); the
+// block's sums go to part[2 b], part[2 b + 1]. Cells of a 32 x 4 brick whose hydrometeor flag (act, from the last
+// physics pass or the flags rebuilt after a field write) is clear hold exactly zero condensate, so they add qv alone:
+// q0 + 0 + 0 + 0 + 0 + 0 is q0, the same bits, from one array instead of six. k_sum_rain writes one partial per
+// block the same way, and k_budget_final adds the partials in block order.
+constexpr int kBudgetBlocks = 592;   // 4 blocks of 256 threads per SM of a 148-SM B200
+constexpr int kRainBlocks = 64;
+constexpr int kRedDoubles = 8 + 2 * kBudgetBlocks + kRainBlocks;   // results, then the partials
+__device__ __forceinline__ double block_sum(double v, double* sh) {   // fixed order: shuffle tree, then warps 0..7
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
   __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < int(blockDim.x >> 5); w++) t += sh[w];
+  return t;
+}
+__global__ void __launch_bounds__(256) k_budget(Grid g, const float* __restrict__ B, float* const* q, const unsigned int* __restrict__ act,
+                                                int nbx, int nby, double dV, double* __restrict__ part) {
+  __shared__ double sh[8];
+  const float* __restrict__ qc[6] = {q[0], q[1], q[2], q[3], q[4], q[5]};
+  const int nrows = g.ny * g.nz, nc = (g.nx + 3) >> 2;
+  const int r0 = int(long(nrows) * blockIdx.x / gridDim.x), r1 = int(long(nrows) * (blockIdx.x + 1) / gridDim.x);
+  double w = 0.0;
+  for (long t = threadIdx.x; t < long(r1 - r0) * nc; t += blockDim.x) {
+    const int r = r0 + int(t / nc), i0 = int(t % nc) << 2;
+    const int j = r % g.ny, k = r / g.ny;
+    const int o = g.at(i0, j, k);
+    const int nch = __ldg(act + (i0 >> 5) + nbx * ((j >> 2) + nby * k)) != 0u ? 6 : 1;
+    double s = 0.0;
+    if (i0 + 4 <= g.nx) {
+      for (int c = 0; c < nch; c++) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(qc[c] + o));
+        s += double(v.x) + double(v.y) + double(v.z) + double(v.w);
+      }
+    } else {
+      for (int c = 0; c < nch; c++)
+        for (int i = i0; i < g.nx; i++) s += double(__ldg(qc[c] + o + (i - i0)));
+    }
+    w += s * double(__ldg(B + k * 8 + 2));
+  }
+  double mass = 0.0;
+  if (threadIdx.x == 0)
+    for (int r = r0; r < r1; r++) mass += double(__ldg(B + (r / g.ny) * 8 + 2)) * g.nx;
+  w = block_sum(w, sh);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int i = 0; i < int(blockDim.x >> 5); i++) t += part[i];
-    atomicAdd(out, t * dV);
-    atomicAdd(out + 1, mass * dV);
+    part[2 * blockIdx.x] = w * dV;
+    part[2 * blockIdx.x + 1] = mass * dV;
   }
 }
-__global__ void k_sum_rain(const double* rain, int n, double cell_area, double* out) {
+__global__ void __launch_bounds__(256) k_sum_rain(const double* __restrict__ rain, int n, double cell_area, double* __restrict__ part) {
+  __shared__ double sh[8];
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += rain[i];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out + 2, s * cell_area);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s * cell_area;
+}
+// out[0..2] = (water, mass, rain): the partials added in block order
+__global__ void k_budget_final(const double* __restrict__ part, int nb, const double* __restrict__ rpart, int nr, double* __restrict__ out) {
+  double w = 0.0, m = 0.0, r = 0.0;
+  for (int b = 0; b < nb; b++) {
+    w += part[2 * b];
+    m += part[2 * b + 1];
+  }
+  for (int b = 0; b < nr; b++) r += rpart[b];
+  out[0] = w;
+  out[1] = m;
+  out[2] = r;
 }
 
 }  // namespace ob
@@ -130,6 +154,17 @@ struct ObModel {
   float4* d_2d = nullptr;
   double* d_red = nullptr;
   float* d_qptr = nullptr;
+  // asynchronous host hand-offs (made on first use): pinned slots for requested budgets, each with the event of its
+  // device-to-host copy and the ticket it holds; a pinned staging ring for the storm-start list, each slot with the
+  // event of its upload
+  static constexpr int kSlots = 4;
+  double* h_req = nullptr;         // [kSlots][8]
+  cudaEvent_t ev_req[kSlots] = {};
+  long long req_ticket[kSlots] = {-1, -1, -1, -1};
+  long long next_ticket = 0;
+  float* h_ci = nullptr;           // [kSlots][OB_MAX_CI * OB_CI_FLOATS]
+  cudaEvent_t ev_ci[kSlots] = {};
+  int ci_slot = 0;
   float* rhs32 = nullptr;  // the fp32 right-hand side buffer (F.rhs points here when a solver reads it)
   unsigned int* d_act = nullptr;  // 4 brick-flag arrays (clear-air skip of the scalar advection)
   float* d_tab = nullptr;          // sponge tables of the physics pass (Fields::spz/slx/sly)
@@ -211,6 +246,12 @@ static void model_free(ObModel* m) {
     if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
   }
   if (m->ev_fork) cudaEventDestroy(m->ev_fork);
+  for (int i = 0; i < ObModel::kSlots; i++) {
+    if (m->ev_req[i]) cudaEventDestroy(m->ev_req[i]);
+    if (m->ev_ci[i]) cudaEventDestroy(m->ev_ci[i]);
+  }
+  if (m->h_req) cudaFreeHost(m->h_req);
+  if (m->h_ci) cudaFreeHost(m->h_ci);
   if (m->ens) m->stream = m->own_stream;  // the ensemble's stream is not the model's to destroy
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -344,7 +385,7 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   alloc((void**)&m->d_flags, 64 * sizeof(unsigned), "flags");
   alloc((void**)&m->d_maps, n2 * 4 * sizeof(float4), "maps");
   alloc((void**)&m->d_2d, n2 * 4 * sizeof(float4), "2-D fields");
-  alloc((void**)&m->d_red, 8 * sizeof(double), "reductions");
+  alloc((void**)&m->d_red, kRedDoubles * sizeof(double), "reductions");
   alloc((void**)&m->d_clock, sizeof(double), "model clock");
   alloc((void**)&m->rhs32, np * sizeof(float), "rhs");
   alloc((void**)&m->F.phi, np * sizeof(float), "phi");
@@ -462,13 +503,32 @@ int ob_model_set_boundaries(ObModel* m, const float* packed, int n) {
   return cuda_status(cudaStreamSynchronize(m->stream), "boundaries");
 }
 
+// the pinned slots and events of the asynchronous hand-offs, made on first use
+static int async_slots(ObModel* m) {
+  if (m->h_req) return OB_OK;
+  OB_TRY(cuda_status(cudaHostAlloc(&m->h_ci, sizeof(float) * ObModel::kSlots * OB_MAX_CI * OB_CI_FLOATS, cudaHostAllocDefault), "host slots"));
+  for (int i = 0; i < ObModel::kSlots; i++) {
+    OB_TRY(cuda_status(cudaEventCreateWithFlags(&m->ev_req[i], cudaEventDisableTiming), "host slots"));
+    OB_TRY(cuda_status(cudaEventCreateWithFlags(&m->ev_ci[i], cudaEventDisableTiming), "host slots"));
+  }
+  return cuda_status(cudaHostAlloc(&m->h_req, sizeof(double) * ObModel::kSlots * 8, cudaHostAllocDefault), "host slots");
+}
+
 int ob_model_set_ci(ObModel* m, const float* ev, int n) {
   if (!m || n < 0 || (n > 0 && !ev)) { set_error("ob_model_set_ci: bad arguments"); return OB_ERR_INVALID; }
   m->nci = n < OB_MAX_CI ? n : OB_MAX_CI;
   if (m->nci) {
+    // the list is copied at the call, as queue.writeBuffer does: into a pinned staging slot, whose upload is queued
+    // on the model's stream without waiting for it (the slot is reused once its previous upload has been done)
+    OB_TRY(async_slots(m));
+    const int sl = m->ci_slot;
+    m->ci_slot = (sl + 1) % ObModel::kSlots;
+    OB_TRY(cuda_status(cudaEventSynchronize(m->ev_ci[sl]), "CI"));
+    float* stage = m->h_ci + size_t(sl) * OB_MAX_CI * OB_CI_FLOATS;
     const float* src = ev + size_t(n - m->nci) * OB_CI_FLOATS;  // the most recent MAX_CI (model.js:1384)
-    OB_TRY(cuda_status(cudaMemcpyAsync(m->d_ci, src, sizeof(float) * m->nci * OB_CI_FLOATS, cudaMemcpyHostToDevice, m->stream), "CI"));
-    OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "CI"));
+    std::memcpy(stage, src, sizeof(float) * m->nci * OB_CI_FLOATS);
+    OB_TRY(cuda_status(cudaMemcpyAsync(m->d_ci, stage, sizeof(float) * m->nci * OB_CI_FLOATS, cudaMemcpyHostToDevice, m->stream), "CI"));
+    OB_TRY(cuda_status(cudaEventRecord(m->ev_ci[sl], m->stream), "CI"));
   }
   return OB_OK;
 }
@@ -740,13 +800,53 @@ int ob_model_time(ObModel* m, double* time, int* steps, int* parity) {
   return OB_OK;
 }
 
-int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain) {
-  if (!m) { set_error("ob_model_budgets: null model"); return OB_ERR_INVALID; }
+// the budget reductions into d_red, queued on the model's stream
+static int queue_budgets(ObModel* m) {
   const Grid& g = m->g;
   OB_TRY(cuda_status(cudaMemsetAsync(m->d_red, 0, 8 * sizeof(double), m->stream), "budgets"));
-  k_budget<<<std::min(g.ny * g.nz, kBudgetBlocks), 256, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->F.actQ0,
-                                                                         m->F.nbx, m->F.nby, m->dx * m->dx * m->dz, m->d_red);
-  k_sum_rain<<<64, 256, 0, m->stream>>>(m->d_rain, g.nx * g.ny, m->dx * m->dx, m->d_red);
+  const int nb = std::min(g.ny * g.nz, kBudgetBlocks);
+  double* part = m->d_red + 8;
+  double* rpart = part + 2 * kBudgetBlocks;
+  k_budget<<<nb, 256, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->F.actQ0, m->F.nbx, m->F.nby,
+                                      m->dx * m->dx * m->dz, part);
+  k_sum_rain<<<kRainBlocks, 256, 0, m->stream>>>(m->d_rain, g.nx * g.ny, m->dx * m->dx, rpart);
+  k_budget_final<<<1, 1, 0, m->stream>>>(part, nb, rpart, kRainBlocks, m->d_red);
+  return cuda_status(cudaGetLastError(), "budgets");
+}
+
+int ob_model_request_budgets(ObModel* m, long long* ticket) {
+  if (!m || !ticket) { set_error("ob_model_request_budgets: null argument"); return OB_ERR_INVALID; }
+  OB_TRY(async_slots(m));
+  const long long t = m->next_ticket;
+  const int sl = int(t % ObModel::kSlots);
+  OB_TRY(cuda_status(cudaEventSynchronize(m->ev_req[sl]), "request budgets"));   // the slot's previous copy is done
+  OB_TRY(queue_budgets(m));
+  OB_TRY(cuda_status(cudaMemcpyAsync(m->h_req + size_t(sl) * 8, m->d_red, 8 * sizeof(double), cudaMemcpyDeviceToHost, m->stream), "request budgets"));
+  OB_TRY(cuda_status(cudaEventRecord(m->ev_req[sl], m->stream), "request budgets"));
+  m->req_ticket[sl] = t;
+  m->next_ticket = t + 1;
+  *ticket = t;
+  return OB_OK;
+}
+
+int ob_model_read_budgets(ObModel* m, long long ticket, double* water, double* mass, double* rain) {
+  if (!m) { set_error("ob_model_read_budgets: null model"); return OB_ERR_INVALID; }
+  const int sl = ticket >= 0 ? int(ticket % ObModel::kSlots) : 0;
+  if (ticket < 0 || !m->h_req || m->req_ticket[sl] != ticket) {
+    set_error("ob_model_read_budgets: ticket %lld was not requested or its slot has been reused (%d slots)", ticket, ObModel::kSlots);
+    return OB_ERR_INVALID;
+  }
+  OB_TRY(cuda_status(cudaEventSynchronize(m->ev_req[sl]), "read budgets"));
+  const double* h = m->h_req + size_t(sl) * 8;
+  if (water) *water = h[0];
+  if (mass) *mass = h[1];
+  if (rain) *rain = h[2];
+  return OB_OK;
+}
+
+int ob_model_budgets(ObModel* m, double* water, double* mass, double* rain) {
+  if (!m) { set_error("ob_model_budgets: null model"); return OB_ERR_INVALID; }
+  OB_TRY(queue_budgets(m));
   double h[8];
   OB_TRY(cuda_status(cudaMemcpyAsync(h, m->d_red, sizeof(h), cudaMemcpyDeviceToHost, m->stream), "budgets"));
   OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "budgets"));

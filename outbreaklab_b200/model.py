@@ -255,6 +255,18 @@ class RegionalModel:
         N.check(N.lib().ob_model_budgets(self.h, C.byref(w), C.byref(m), C.byref(r)))
         return {"water": w.value, "mass": m.value, "rain": r.value}
 
+    def request_budgets(self) -> int:
+        """Queues the budgets after the work queued so far and returns a ticket for read_budgets (no wait)."""
+        t = C.c_longlong()
+        N.check(N.lib().ob_model_request_budgets(self.h, C.byref(t)))
+        return t.value
+
+    def read_budgets(self, ticket: int):
+        """Waits for the budgets of a request (one of the last 4) and returns them."""
+        w, m, r = C.c_double(), C.c_double(), C.c_double()
+        N.check(N.lib().ob_model_read_budgets(self.h, C.c_longlong(ticket), C.byref(w), C.byref(m), C.byref(r)))
+        return {"water": w.value, "mass": m.value, "rain": r.value}
+
     @property
     def Vcur(self):
         return self.get_field(N.FIELD_V)
