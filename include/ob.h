@@ -212,18 +212,19 @@ int ob_model_profile_step(ObModel* m, float dt, float* ms, int max_passes);
  * launches every kernel directly. Results are identical either way. */
 int ob_model_set_graphs(ObModel* m, int on);
 /* pressure-solve precision of the model: 0 = fp32 SIMT transforms (the reference's arithmetic), 1 = bf16x3
- * tensor-core transforms, 2 = bf16x3 + one bf16x3 refinement sweep (the default where nz is 16, 40 or 80),
+ * tensor-core transforms, 2 = bf16x3 + one bf16x3 refinement sweep,
  * 3 = bf16x3 + one plain-bf16 refinement sweep, 4 = bf16x3 + two bf16x3 refinement sweeps (the residual at the
- * floor that storing phi in fp32 sets).
+ * floor that storing phi in fp32 sets), 5 = a plain-bf16 pass + one bf16x3 refinement sweep (the default where nz is
+ * 16, 40 or 80: within 1.5 x the floor, as precision 2 is, for 4 products per transform element instead of 6).
  * No counterpart in the reference. */
 int ob_model_set_solver(ObModel* m, int precision);
 /* tile shape of the tensor-core solve's transforms: 1 (the default) = tiles of 256 field rows computed by pairs of SMs
  * (a cluster of two CTAs, tcgen05.mma.cta_group::2: each SM loads half of the DST-matrix tile and reads a third less
- * operand data per product), 0 = tiles of 128 rows on single SMs. The results are bit-identical. Precisions 1 to 4
+ * operand data per product), 0 = tiles of 128 rows on single SMs. The results are bit-identical. Precisions 1 to 5
  * only (ob_model_set_solver resets it to the default). No counterpart in the reference. */
 int ob_model_set_pair_tiles(ObModel* m, int on);
 /* outputs per tile of the x and y transforms (multiples of 16 in 32..256; 0 = automatic), for tuning; the results do
- * not depend on them. Precisions 1 to 4 only (ob_model_set_solver resets them). No counterpart in the reference. */
+ * not depend on them. Precisions 1 to 5 only (ob_model_set_solver resets them). No counterpart in the reference. */
 int ob_model_set_tile_widths(ObModel* m, int bn_x, int bn_y);
 int ob_model_solver(ObModel* m);
 /* CUDA stream of the model (cudaStream_t) for zero-copy hand-off */
@@ -232,7 +233,8 @@ void* ob_model_stream(ObModel* m);
 /* ---- PoissonDirect (solver.js:105-165) ---- */
 /* replaces new PoissonDirect(nx, ny, nz, dx, dz) (solver.js:106-137); precision 0 = FP32 SIMT transforms,
  * 1 = bf16x3 tensor-core transforms (FP32 accumulate), 2 = the same plus one iterative-refinement sweep on the
- * FP64-accumulated residual, 3 = that sweep in plain bf16, 4 = two bf16x3 refinement sweeps (precisions 1 to 4 need
+ * FP64-accumulated residual, 3 = that sweep in plain bf16, 4 = two bf16x3 refinement sweeps, 5 = a plain-bf16 pass
+ * refined by one bf16x3 sweep (precisions 1 to 5 need
  * nz in {16, 40, 80}) */
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out);
 int ob_poisson_destroy(ObPoisson* p);

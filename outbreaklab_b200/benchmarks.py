@@ -43,7 +43,7 @@ def solve(args):
     ms = P.device_ms(args.reps)
     # MMAs per transform element: 1 (fp32 SIMT), 3 (bf16x3), 3 + 3 (refined), 3 + 1 (refined in plain bf16),
     # 3 + 3 + 3 (two refinement sweeps)
-    flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4, 4: 9}[args.precision]
+    flops = 4.0 * nx * ny * nz * (nx + ny) * {0: 1, 1: 3, 2: 6, 3: 4, 4: 9, 5: 4}[args.precision]
     out = {"bench": "pressure solve", "nx": nx, "ny": ny, "nz": nz, "precision": args.precision, "ms": ms,
            "pair_tiles": args.pair_tiles, "bn": args.bn,
            "dst_flops": flops, "tflops": flops / (ms * 1e-3) / 1e12}

@@ -63,7 +63,7 @@ struct EventPair {
 // q0 + 0 + 0 + 0 + 0 + 0 is q0, the same bits, from one array instead of six. k_sum_rain writes one partial per
 // block the same way, and k_budget_final adds the partials in block order.
 constexpr int kBudgetBlocks = 592;   // 4 blocks of 256 threads per SM of a 148-SM B200
-constexpr int kRainBlocks = 64;
+constexpr int kRainBlocks = 296;  // 2 blocks of 256 threads per SM
 constexpr int kRedDoubles = 8 + 2 * kBudgetBlocks + kRainBlocks;   // results, then the partials
 __device__ __forceinline__ double block_sum(double v, double* sh) {   // fixed order: shuffle tree, then warps 0..7
   for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
@@ -115,17 +115,25 @@ __global__ void __launch_bounds__(256) k_sum_rain(const double* __restrict__ rai
   s = block_sum(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = s * cell_area;
 }
-// out[0..2] = (water, mass, rain): the partials added in block order
-__global__ void k_budget_final(const double* __restrict__ part, int nb, const double* __restrict__ rpart, int nr, double* __restrict__ out) {
+// out[0..2] = (water, mass, rain) from the partials, in a fixed order: thread t adds partials t, t + 256, ... in
+// turn, then block_sum adds the threads' sums in its fixed tree
+__global__ void __launch_bounds__(256) k_budget_final(const double* __restrict__ part, int nb, const double* __restrict__ rpart, int nr,
+                                                      double* __restrict__ out) {
+  __shared__ double sh[8];
   double w = 0.0, m = 0.0, r = 0.0;
-  for (int b = 0; b < nb; b++) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     w += part[2 * b];
     m += part[2 * b + 1];
   }
-  for (int b = 0; b < nr; b++) r += rpart[b];
-  out[0] = w;
-  out[1] = m;
-  out[2] = r;
+  for (int b = threadIdx.x; b < nr; b += blockDim.x) r += rpart[b];
+  w = block_sum(w, sh);
+  m = block_sum(m, sh);
+  r = block_sum(r, sh);
+  if (threadIdx.x == 0) {
+    out[0] = w;
+    out[1] = m;
+    out[2] = r;
+  }
 }
 
 }  // namespace ob
@@ -397,8 +405,9 @@ int ob_model_create(const ObGrid* grid, ObModel** out) {
   alloc((void**)&m->d_act, 4 * nbr * sizeof(unsigned int), "activity flags");
   const size_t ntab = size_t(4) * (nz + 1) + 2 * size_t(nx + 1) + 2 * size_t(ny + 1);
   alloc((void**)&m->d_tab, ntab * sizeof(float), "sponge tables");
-  // the refined bf16x3 tensor-core solve where its tridiagonal kernel is specialised, else fp32
-  const int prec = (nz == 16 || nz == 40 || nz == 80) ? 2 : 0;
+  // the refined tensor-core solve (a plain-bf16 pass refined by a bf16x3 sweep) where its tridiagonal kernel is
+  // specialised, else fp32
+  const int prec = (nz == 16 || nz == 40 || nz == 80) ? 5 : 0;
   if (rc == OB_OK) rc = m->solver.create(g.nxp, g.nyp, nz, m->dx, m->dz, prec);
   if (rc != OB_OK) {
     if (rc == OB_ERR_OOM) {
@@ -810,7 +819,7 @@ static int queue_budgets(ObModel* m) {
   k_budget<<<nb, 256, 0, m->stream>>>(g, m->d_B, reinterpret_cast<float* const*>(m->d_qptr), m->F.actQ0, m->F.nbx, m->F.nby,
                                       m->dx * m->dx * m->dz, part);
   k_sum_rain<<<kRainBlocks, 256, 0, m->stream>>>(m->d_rain, g.nx * g.ny, m->dx * m->dx, rpart);
-  k_budget_final<<<1, 1, 0, m->stream>>>(part, nb, rpart, kRainBlocks, m->d_red);
+  k_budget_final<<<1, 256, 0, m->stream>>>(part, nb, rpart, kRainBlocks, m->d_red);
   return cuda_status(cudaGetLastError(), "budgets");
 }
 
@@ -968,7 +977,7 @@ int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks) 
 }
 
 int ob_model_set_solver(ObModel* m, int precision) {
-  if (!m || precision < 0 || precision > 4) { set_error("ob_model_set_solver: precision must be 0 to 4"); return OB_ERR_INVALID; }
+  if (!m || precision < 0 || precision > 5) { set_error("ob_model_set_solver: precision must be 0 to 5"); return OB_ERR_INVALID; }
   const Grid& g = m->g;
   if (precision >= 1 && g.nz != 16 && g.nz != 40 && g.nz != 80) {
     set_error("ob_model_set_solver: the tensor-core solve supports nz in {16, 40, 80}");
@@ -1582,7 +1591,7 @@ struct ObPoisson {
 };
 
 int ob_poisson_create(int nx, int ny, int nz, float dx, float dz, int precision, ObPoisson** out) {
-  if (!out || precision < 0 || precision > 4) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
+  if (!out || precision < 0 || precision > 5) { set_error("ob_poisson_create: bad arguments"); return OB_ERR_INVALID; }
   *out = nullptr;
   ObPoisson* p = new ObPoisson();
   int rc = p->plan.create(nx, ny, nz, dx, dz, precision);

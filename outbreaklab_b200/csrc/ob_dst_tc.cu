@@ -1006,9 +1006,11 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc<OUT_R_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_dst_tc_grp<OUT_R_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_T_BF16X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_T_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
@@ -1016,6 +1018,7 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc2<OUT_T_BF16X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
+    cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_tri_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
     cudaFuncSetAttribute(k_tri_tma<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
     cudaFuncSetAttribute(k_tri_tma<80>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
@@ -1240,7 +1243,7 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const TcOut sy{T->sy_hi, T->sy_lo, nullptr, T->ldy, ny, nz * ny, nx}, t2{nullptr, nullptr, T->t2, nx, nx, nz * nx, ny};
   // X-fwd: field rows (k, j), K = i, outputs l  -> S_y[k][l][j]
-  if (one) launch_tc<OUT_T_BF16X2, true>(T->Frr, T->Q[0], nx, T->bnx, sy, T->err, s, QH(0));
+  if (one) launch_tc<OUT_T_BF16X2, true>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, sy, T->err, s, QH(0));
   else launch_tc<OUT_T_BF16X2>(add ? T->Frr : T->Fr, T->Q[0], nx, T->bnx, sy, T->err, s, QH(0));
   // Y-fwd: field rows (k, l), K = j, outputs m  -> T2[k][m][l] fp32
   if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s, QH(1));
@@ -1264,7 +1267,8 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   else launch_tc<OUT_T_BF16X2>(T->Fy, T->Q[2], ny, T->bny, sx, T->err, s, QH(2));
   // X-inv: field rows (k, j), K = l, outputs i  -> phi[k][j][i]
   const TcOut o{nullptr, nullptr, phi, nx, ny, nz * ny, nx};
-  if (one) launch_tc<OUT_R_F32_ADD, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
+  if (one && add) launch_tc<OUT_R_F32_ADD, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
+  else if (one) launch_tc<OUT_R_F32, true>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
   else if (add) launch_tc<OUT_R_F32_ADD>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
   else launch_tc<OUT_R_F32>(T->Fx, T->Q[3], nx, T->bnx, o, T->err, s, QH(3));
 #undef QH
@@ -1284,7 +1288,7 @@ int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
     if (!rhs) { set_error("poisson: right-hand side missing"); return OB_ERR_INVALID; }
   }
   if (!presplit) k_split_rows<<<1184, 256, 0, s>>>(rhs, long(nz) * ny, nx, T->rx_hi, T->rx_lo, int(T->ldx));
-  tc_pass(*this, T, lam, zop, phi, false, s);
+  tc_pass(*this, T, lam, zop, phi, false, s, precision == 5);
   if (precision >= 2) {
     const int sweeps = precision == 4 ? 2 : 1;
     for (int sw = 0; sw < sweeps; sw++) {
@@ -1302,14 +1306,14 @@ int PoissonPlan::tc_solve(const float* rhs, float* phi, cudaStream_t s) {
 
 int PoissonPlan::tc_set_pairs(bool on) {
   TcPlan* T = static_cast<TcPlan*>(tc);
-  if (!T) { set_error("poisson: the SM-pair transforms need a tensor-core precision (1 to 4)"); return OB_ERR_INVALID; }
+  if (!T) { set_error("poisson: the SM-pair transforms need a tensor-core precision (1 to 5)"); return OB_ERR_INVALID; }
   T->pairs = on;
   if (on) pair_slots();   // the occupancy query runs here, outside any stream capture
   return OB_OK;
 }
 int PoissonPlan::tc_set_tile_widths(int bnx, int bny) {
   TcPlan* T = static_cast<TcPlan*>(tc);
-  if (!T) { set_error("poisson: tile widths apply to the tensor-core precisions (1 to 4)"); return OB_ERR_INVALID; }
+  if (!T) { set_error("poisson: tile widths apply to the tensor-core precisions (1 to 5)"); return OB_ERR_INVALID; }
   for (int b : {bnx, bny})
     if (b != 0 && (b < 32 || b > BNMAX || b % 16)) {
       set_error("poisson: tile width %d not 0 (automatic) or a multiple of 16 in 32..%d", b, BNMAX);
@@ -1515,7 +1519,7 @@ static void launch_tc_grp(const TcGroup* G, int t, cudaStream_t s) {
 static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one = false) {
   const int n = G->n;
   if (one) {
-    launch_tc_grp<OUT_T_BF16X2, true>(G, 4, s);
+    launch_tc_grp<OUT_T_BF16X2, true>(G, add ? 4 : 0, s);
     launch_tc_grp<OUT_T_F32, true>(G, 1, s);
   } else {
     launch_tc_grp<OUT_T_BF16X2>(G, add ? 4 : 0, s);
@@ -1529,7 +1533,8 @@ static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one =
   }
   if (one) {
     launch_tc_grp<OUT_T_BF16X2, true>(G, 2, s);
-    launch_tc_grp<OUT_R_F32_ADD, true>(G, 3, s);
+    if (add) launch_tc_grp<OUT_R_F32_ADD, true>(G, 3, s);
+    else launch_tc_grp<OUT_R_F32, true>(G, 3, s);
   } else {
     launch_tc_grp<OUT_T_BF16X2>(G, 2, s);
     if (add) launch_tc_grp<OUT_R_F32_ADD>(G, 3, s);
@@ -1538,7 +1543,7 @@ static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one =
 }
 
 int tc_group_solve(TcGroup* G, cudaStream_t s) {
-  tc_group_pass(G, false, s);
+  tc_group_pass(G, false, s, G->precision == 5);
   if (G->precision >= 2) {
     const int sweeps = G->precision == 4 ? 2 : 1;
     for (int sw = 0; sw < sweeps; sw++) {

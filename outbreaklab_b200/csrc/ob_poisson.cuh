@@ -12,7 +12,8 @@ void set_error(const char* fmt, ...);
 
 struct PoissonPlan {
   int nx = 0, ny = 0, nz = 0, precision = 0;  // 0 fp32 SIMT, 1 bf16x3 tensor core, 2 bf16x3 + one refinement,
-                                              // 3 refinement in plain bf16, 4 two bf16x3 refinements
+                                              // 3 refinement in plain bf16, 4 two bf16x3 refinements,
+                                              // 5 a plain-bf16 pass refined by one bf16x3 sweep
   bool presplit = false;  // precision >= 1: the caller writes the split right-hand side (tc_rhs_split) itself
   double dx = 0, dz = 0;
   float* mats = nullptr;  // qix | qx | qiy | qy (fp32, solver.js:115-125)

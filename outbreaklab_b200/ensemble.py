@@ -357,5 +357,5 @@ def _run_grouped(ens, models, cases, steps, warmup, tune, cache, reps, lanes):
            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
            "latency_ms_all": lat.tolist(), "nan_guard_count": int(sum(m.nan_count for m in models)),
            "tiles": ens.tiles(), "tiles_source": tiles_src, "tune_ms": tune_ms, "lanes": ens.lanes, "lane_step_ms": lane_ms,
-           "launches_per_step": ens.lanes * (11 + (11 if models[0].solver == 2 else 5) + (1 if getattr(models[0], "surrogate", False) else 0))}
+           "launches_per_step": ens.lanes * (11 + {1: 5, 4: 17}.get(models[0].solver, 11) + (1 if getattr(models[0], "surrogate", False) else 0))}
     return out

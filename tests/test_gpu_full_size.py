@@ -112,7 +112,8 @@ def test_storm_step_at_full_size_matches_the_oracle(native):
 
 
 def test_refined_solves_reach_the_fp32_floor(native):
-    """Precisions 2 (one bf16x3 refinement sweep) and 4 (two) at 656 x 656 x 40: their residuals are within twice the
+    """Precisions 2 (one bf16x3 refinement sweep), 4 (two) and 5 (a plain-bf16 pass refined by one bf16x3 sweep) at
+    656 x 656 x 40: their residuals are within twice the
     floor that storing phi in fp32 sets (the FP64 oracle's solution rounded to fp32, under the FP64 operator), in both
     norms. The device's own FP64 residual (ob_poisson_residual) applies the solve's operator, whose coefficients are
     fp32: it must lie within the same floor."""
@@ -122,7 +123,7 @@ def test_refined_solves_reach_the_fp32_floor(native):
     rc, rw = _density(nz)
     rhs = W.gaussian_rhs(nx, ny, nz, dx, corr_len=5000.0, seed=3, dtype=np.float32)
     phis, dev, ms = {}, {}, {}
-    for prec in (2, 4):
+    for prec in (2, 4, 5):
         P = M.PoissonDirect(nx, ny, nz, dx, dz, prec)
         try:
             P.set_density(rc, rw)
@@ -139,7 +140,7 @@ def test_refined_solves_reach_the_fp32_floor(native):
 
     exact = O.poisson_solve(rhs, dx, dz, rc, rw, 8)
     f_inf, f_l2 = residual(exact.astype(np.float32))
-    for prec in (2, 4):
+    for prec in (2, 4, 5):
         r_inf, r_l2 = residual(phis[prec])
         d_inf, d_l2 = dev[prec]
         print("precision %d at 656x656x40: %.3f ms, residual %.3g (max) %.3g (L2); fp32 floor %.3g / %.3g; device %.3g / %.3g"

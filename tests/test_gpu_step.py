@@ -44,11 +44,11 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("solver", [2, 3, 0])
+@pytest.mark.parametrize("solver", [2, 3, 5, 0])
 @pytest.mark.parametrize("name", list(CASES))
 def test_one_step_parity(oracle_lib, native, name, solver):
-    """Solvers 2 (bf16x3 solve refined in bf16x3), 3 (refined in plain bf16) and 0 (fp32 transforms) all within the
-    envelope."""
+    """Solvers 2 (bf16x3 solve refined in bf16x3), 3 (refined in plain bf16), 5 (a plain-bf16 solve refined in
+    bf16x3) and 0 (fp32 transforms) all within the envelope."""
     case = CASES[name]()
     g, f, d = _setup(oracle_lib, case, blob="blob" in name)
     g.set_solver(solver)

@@ -48,7 +48,7 @@ def _density(nz, dz):
     return rc.astype(np.float32), rw.astype(np.float32)
 
 
-@pytest.mark.parametrize("precision", [1, 2, 3])
+@pytest.mark.parametrize("precision", [1, 2, 3, 5])
 @pytest.mark.parametrize("shape", [(96, 80, 40), (150, 130, 16), (256, 200, 80)])
 def test_poisson_bf16x3_vs_fp64(oracle_lib, native, shape, precision):
     nx, ny, nz = shape
