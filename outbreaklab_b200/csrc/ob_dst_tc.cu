@@ -137,9 +137,13 @@ template <int MODE, bool ONE, class Src>
 __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // the plain-bf16 pass loads hi planes only: its stages are 48 KB, four of them in the two 96 KB stages' space
+  constexpr int NST = ONE ? (STAGES * STAGE_BYTES) / (A_TILE + B_TILE) : STAGES;
+  constexpr int SB = ONE ? A_TILE + B_TILE : STAGE_BYTES;
+  constexpr int BOFF = ONE ? A_TILE : 2 * A_TILE;   // the matrix tile's place in a stage
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* empty = full + STAGES;
-  uint64_t* tfull = empty + STAGES;  // [2] accumulator b holds a finished tile
+  uint64_t* empty = full + NST;
+  uint64_t* tfull = empty + NST;     // [2] accumulator b holds a finished tile
   uint64_t* tempty = tfull + 2;      // [2] the epilogue has drained accumulator b
   uint64_t* done = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -148,7 +152,7 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
   const int ntiles = src.total();
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) {
+    for (int s = 0; s < NST; s++) {
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
@@ -186,15 +190,15 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
         const uint32_t bytes = ONE ? uint32_t(A_TILE + ti.BN * BK * 2) : uint32_t(2 * A_TILE + 2 * ti.BN * BK * 2);
         const int nk = (ti.K + BK - 1) / BK;
         for (int kt = 0; kt < nk; kt++, g++) {
-          const int s = g % STAGES;
-          const uint32_t ph = (g / STAGES) & 1;
+          const int s = g % NST;
+          const uint32_t ph = (g / NST) & 1;
           if (!(ok = tc::mbar_wait(&empty[s], ph ^ 1, err, 1u))) break;
-          uint8_t* st = smem + s * STAGE_BYTES;
+          uint8_t* st = smem + s * SB;
           tc::mbar_expect_tx(&full[s], bytes);
           tc::tma_load_2d(st, ti.f_hi, &full[s], kt * BK, ti.m0);
           if (!ONE) tc::tma_load_2d(st + A_TILE, ti.f_lo, &full[s], kt * BK, ti.m0);
-          tc::tma_load_2d(st + 2 * A_TILE, ti.q_hi, &full[s], kt * BK, ti.n0);
-          if (!ONE) tc::tma_load_2d(st + 2 * A_TILE + B_TILE, ti.q_lo, &full[s], kt * BK, ti.n0);
+          tc::tma_load_2d(st + BOFF, ti.q_hi, &full[s], kt * BK, ti.n0);
+          if (!ONE) tc::tma_load_2d(st + BOFF + B_TILE, ti.q_lo, &full[s], kt * BK, ti.n0);
         }
       }
     }
@@ -213,15 +217,15 @@ __device__ __forceinline__ void dst_tc_run(const Src& src, unsigned int* err) {
         tc::tc_fence_after();
         const uint32_t acc = tmem + uint32_t(b * 256);
         for (int kt = 0; kt < nk; kt++, g++) {
-          const int s = g % STAGES;
-          const uint32_t ph = (g / STAGES) & 1;
+          const int s = g % NST;
+          const uint32_t ph = (g / NST) & 1;
           if (!(ok = tc::mbar_wait(&full[s], ph, err, 2u))) break;
           tc::tc_fence_after();
-          const uint8_t* st = smem + s * STAGE_BYTES;
+          const uint8_t* st = smem + s * SB;
           const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
           const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
-          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
-          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + B_TILE));
+          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + BOFF));
+          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + BOFF + B_TILE));
           const int ksub = min(BK, ti.K - kt * BK + 15) / 16;  // 16-wide steps holding data (the rest is zero fill)
           for (int kk = 0; kk < ksub; kk++) {
             const uint64_t o = uint64_t(kk * 2);  // 16 bf16 = 32 bytes, >> 4
@@ -361,15 +365,20 @@ namespace {
 // shared memory: the epilogue's transpose buffers, the barriers, then a ring of as many stages (field hi/lo, half the
 // matrix tile hi/lo) as the tile width leaves room for: 3 at BN = 224 or 256, 4 at BN <= 144 (every slot a multiple
 // of 1024 bytes, as the 128-byte swizzle wants)
-constexpr int MAXST2 = 6;
+constexpr int MAXST2 = 8;
 constexpr int BAR2_OFF = (STG_BYTES + 1023) / 1024 * 1024;
 constexpr int RING2_OFF = BAR2_OFF + 1024;
 constexpr int SMEM2_BYTES = 227 * 1024;                      // the most a block may use
 constexpr int RING2_BYTES = SMEM2_BYTES - 1024 /*align*/ - RING2_OFF;
 __host__ __device__ constexpr int half_bytes2(int BN) { return BN / 2 * BK * 2; }
-__host__ __device__ constexpr int stage2_bytes(int BN) { return 2 * A_TILE + 2 * half_bytes2(BN); }
-__host__ __device__ constexpr int stages2(int BN) { return RING2_BYTES / stage2_bytes(BN) < MAXST2 ? RING2_BYTES / stage2_bytes(BN) : MAXST2; }
-static_assert(stages2(BNMAX) >= 3, "three stages at the widest tile");
+// a stage holds the field's hi (and lo) tile, then the matrix half's hi (and lo): the plain-bf16 pass (ONE) loads hi
+// planes only, so its stages are half as large and twice as many fit
+__host__ __device__ constexpr int stage2_bytes(int BN, bool one) { return one ? A_TILE + half_bytes2(BN) : 2 * A_TILE + 2 * half_bytes2(BN); }
+__host__ __device__ constexpr int b_off2(bool one) { return one ? A_TILE : 2 * A_TILE; }
+__host__ __device__ constexpr int stages2(int BN, bool one) {
+  return RING2_BYTES / stage2_bytes(BN, one) < MAXST2 ? RING2_BYTES / stage2_bytes(BN, one) : MAXST2;
+}
+static_assert(stages2(BNMAX, false) >= 3, "three stages at the widest tile");
 }  // namespace
 
 template <int MODE, bool ONE = false>
@@ -393,7 +402,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
   const int bh = BN / 2;
   const int nk = (K + BK - 1) / BK;
-  const int nst = stages2(BN), sbytes = stage2_bytes(BN), hbytes = half_bytes2(BN);
+  const int nst = stages2(BN, ONE), sbytes = stage2_bytes(BN, ONE), hbytes = half_bytes2(BN);
+  constexpr int BOFF = b_off2(ONE);
   uint8_t* ring = smem + RING2_OFF;
 
   if (threadIdx.x == 0) {
@@ -442,8 +452,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (lead) tc::mbar_expect_tx(&full[s], bytes);
           tc::tma_load_2d_pair(st, &tF_hi, fb, kt * BK, m0);
           if (!ONE) tc::tma_load_2d_pair(st + A_TILE, &tF_lo, fb, kt * BK, m0);
-          tc::tma_load_2d_pair(st + 2 * A_TILE, &tQ_hi, fb, kt * BK, n0);
-          if (!ONE) tc::tma_load_2d_pair(st + 2 * A_TILE + hbytes, &tQ_lo, fb, kt * BK, n0);
+          tc::tma_load_2d_pair(st + BOFF, &tQ_hi, fb, kt * BK, n0);
+          if (!ONE) tc::tma_load_2d_pair(st + BOFF + hbytes, &tQ_lo, fb, kt * BK, n0);
         }
       }
     }
@@ -465,8 +475,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint8_t* st = ring + s * sbytes;
           const uint64_t dah = tc::desc_k_sw128(tc::smem_u32(st));
           const uint64_t dal = tc::desc_k_sw128(tc::smem_u32(st + A_TILE));
-          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE));
-          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + 2 * A_TILE + hbytes));
+          const uint64_t dbh = tc::desc_k_sw128(tc::smem_u32(st + BOFF));
+          const uint64_t dbl = tc::desc_k_sw128(tc::smem_u32(st + BOFF + hbytes));
           const int ksub = min(BK, K - kt * BK + 15) / 16;
           for (int kk = 0; kk < ksub; kk++) {
             const uint64_t o = uint64_t(kk * 2);
