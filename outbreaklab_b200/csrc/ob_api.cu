@@ -476,6 +476,9 @@ int ob_model_destroy(ObModel* m) {
 
 int ob_model_set_base_state(ObModel* m, const float* B, int nz) {
   if (!m || !B || nz != m->g.nz) { set_error("ob_model_set_base_state: expected nz = %d", m ? m->g.nz : -1); return OB_ERR_INVALID; }
+  // captured steps hold the solve's z-operator by value (the tridiagonal's kernel parameters): recapture after it
+  OB_TRY(cuda_status(cudaStreamSynchronize(m->stream), "base state"));
+  drop_graphs(m);
   m->Bh.assign(B, B + size_t(nz + 1) * 8);
   m->rhoSfc = B[2];
   m->base_gen++;

@@ -702,6 +702,16 @@ __global__ void k_resid_grp(const ResidProb* __restrict__ probs, const uint2* __
 // of a 512-thread block, else 8
 template <int NZ>
 constexpr int tri_tm() { return NZ > 40 ? 8 : 16; }
+// the reciprocal of a mode's pivot at one level, den = diag + shift * rhoC - lower * c'_{k-1} (solver.js:88-90), with
+// c'_{k-1} in the innermost product so that nothing of it is computed ahead of the recurrence; rcp.approx is one
+// MUFU instruction, at most 1 ulp from the rounded reciprocal (the pivots are normal numbers: |den| >= the diagonal's
+// 1/dz^2 scale)
+__device__ __forceinline__ float tri_pivot_rcp(const float4& o, float shift, float cprev) {
+  const float den = fmaf(shift, o.w, fmaf(-o.x, cprev, o.z));
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(den));
+  return r;
+}
 template <int NZ>
 __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float* __restrict__ lam, const float4* __restrict__ zop,
                                          const double* __restrict__ low, const float* __restrict__ T2,
@@ -726,14 +736,14 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
 #pragma unroll
     for (int k = 0; k < NZ; k++) {
       const float4 o = __ldg(zop + k);
-      const float rd = __frcp_rn(o.z + shift * o.w - o.x * cprev);
+      const float rd = tri_pivot_rcp(o, shift, cprev);
       cprev = o.y * rd;
-      dprev = (rhs[k] - o.x * dprev) * rd;
+      dprev = fmaf(-o.x, dprev, rhs[k]) * rd;
       cp[k] = cprev;
       x[k] = dprev;
     }
 #pragma unroll
-    for (int k = NZ - 2; k >= 0; k--) x[k] = x[k] - cp[k] * x[k + 1];
+    for (int k = NZ - 2; k >= 0; k--) x[k] = fmaf(-cp[k], x[k + 1], x[k]);
   } else if (act) {
     // low mode: low[(mode*2 + 0)*NZ + k] = 1/den_k, low[(mode*2 + 1)*NZ + k] = c'_k (FP64, host-factored)
     const int mode = m * 2 + l;
@@ -776,7 +786,7 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
         for (int h = 0; h < TRI_TM / 8; h++)
           if (BY * TRI_TM + h * 8 + 8 <= ldy) {
             *reinterpret_cast<uint4*>(ohi + o + h * 8) = *reinterpret_cast<const uint4*>(h16 + h * 8);
-            *reinterpret_cast<uint4*>(olo + o + h * 8) = *reinterpret_cast<const uint4*>(l16 + h * 8);
+            if (olo) *reinterpret_cast<uint4*>(olo + o + h * 8) = *reinterpret_cast<const uint4*>(l16 + h * 8);
           }
       }
     }
@@ -785,32 +795,42 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
 }
 // ---------------------------------------------------------------------------------------------------------------
 // The tridiagonals of one model's solve through shared memory, every transfer a TMA tile (solver.js:70-103).
-// A block takes 32 l x 8 m modes (one per thread; warp = 32 consecutive l at one m):
-//   1. one 3-D TMA load brings the block's [NZ][8][32] fp32 tile of T2[k][m][l] into shared memory (zero outside);
+// A block takes 16 l x 16 m modes (one per thread; warp = 16 consecutive l at two m):
+//   1. one 3-D TMA load brings the block's [NZ][16][16] fp32 tile of T2[k][m][l] into shared memory (zero outside);
 //   2. each thread runs the Thomas sweep of its mode: c' in registers, d and then x updated in place in the tile
-//      (the tile row of a warp is 32 consecutive floats: no bank conflicts), the 2 x 2 lowest modes in FP64 with the
-//      host-factored coefficients;
-//   3. the tile is written out KC levels at a time, transposed: each thread reads one (level, l) column of 8 m,
-//      splits it into bf16 hi / lo and writes the two 16-byte rows back into the region of those levels (read first,
-//      then a barrier, then written), and one thread issues two 3-D TMA stores of [KC][32][8] into S_y[k][l][m].
-// About 64 registers and NZ KB of shared memory per 256-thread block, so several blocks share an SM and one block's
-// loads overlap another's sweeps and stores; the transposes cost one shared-memory read and write per element.
+//      (a warp's tile row is 32 consecutive floats: no bank conflicts), the 2 x 2 lowest modes in FP64 with the
+//      host-factored coefficients. The z-operator (lower, upper, diagonal, rhoC per level) is a kernel parameter,
+//      so every coefficient is a constant-bank operand of the instruction that uses it (no load in the recurrence),
+//      and the reciprocal of each pivot is the hardware's rcp.approx (at most 1 ulp from the rounded quotient);
+//   3. one barrier later every thread reads the NZ/8 half rows (level, l, 8 m) it will write, splits them into bf16
+//      hi / lo (hi alone for a plain-bf16 pass, HI_ONLY) and holds them in registers; after a second barrier they go
+//      back into the tile as [NZ][16][16] hi and lo rows, and one thread stores each with one 3-D TMA store into
+//      S_y[k][l][m]: 32-byte rows, whole DRAM sectors (rows of 8 m left each sector half written by two blocks, which
+//      doubled the L2 write transactions and made L2 fetch sectors back from DRAM).
+// 64 registers and NZ KB of shared memory per 256-thread block (NZ <= 40: four blocks per SM), so one block's loads
+// overlap another's sweeps and stores.
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int TRI_TL = 32, TRI_TM = 8, TRI_KC = 8;
+constexpr int TRI_TL = 16, TRI_TM = 16;
 template <int NZ>
 constexpr int tri_smem_bytes() { return NZ * TRI_TM * TRI_TL * 4 + 4 * NZ * 8 /*FP64 low modes*/ + 128 /*align*/ + 16 /*barrier*/; }
-
+// the z-operator by value: (lower, upper, diagonal, rhoC) of each level (solver.js:139-146)
 template <int NZ>
+struct TriZ {
+  float4 z[NZ];
+};
+
+template <int NZ, bool HI_ONLY>
 __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(const __grid_constant__ CUtensorMap tIn, const __grid_constant__ CUtensorMap tHi,
                                                           const __grid_constant__ CUtensorMap tLo, int nxp, int nyp,
-                                                          const float* __restrict__ lam, const float4* __restrict__ zop,
+                                                          const float* __restrict__ lam, const __grid_constant__ TriZ<NZ> Z,
                                                           const double* __restrict__ low, unsigned int* err) {
-  static_assert(NZ % TRI_KC == 0, "levels come in whole chunks");
+  static_assert(NZ % 8 == 0, "levels come in whole groups of 8");
   extern __shared__ uint8_t smraw[];
   float* tile = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
   double* dlow = reinterpret_cast<double*>(tile + NZ * TRI_TM * TRI_TL);   // [4][NZ]: d of the FP64 low modes
   uint64_t* bar = reinterpret_cast<uint64_t*>(dlow + 4 * NZ);
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, tid = threadIdx.x;
+  static_assert(TRI_TL == 16 && TRI_TM == 16, "thread and output mappings below assume 16 x 16 modes");
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4, tid = threadIdx.x;
   const int l0 = blockIdx.x * TRI_TL, m0 = blockIdx.y * TRI_TM;
   if (tid == 0) {
     tc::prefetch_tmap(&tIn);
@@ -839,18 +859,22 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     float cprev = 0.f, dprev = 0.f;
 #pragma unroll
     for (int k = 0; k < NZ; k++) {
-      const float4 o = __ldg(zop + k);
-      const float rd = __frcp_rn(o.z + shift * o.w - o.x * cprev);
+      const float4 o = Z.z[k];
+      const float rd = tri_pivot_rcp(o, shift, cprev);
       cprev = o.y * rd;
-      dprev = (col[k * LS] - o.x * dprev) * rd;
+      dprev = fmaf(-o.x, dprev, col[k * LS]) * rd;
       cp[k] = cprev;
       col[k * LS] = dprev;
+      // a compiler fence every 8 levels: the tile reads of later levels (which do not depend on the recurrence) are
+      // not all hoisted ahead of it, which would hold NZ more values in registers next to c'
+      if ((k & 7) == 7) asm volatile("" ::: "memory");
     }
     float x = dprev;
 #pragma unroll
     for (int k = NZ - 2; k >= 0; k--) {
-      x = col[k * LS] - cp[k] * x;
+      x = fmaf(-cp[k], x, col[k * LS]);
       col[k * LS] = x;
+      if ((k & 7) == 0) asm volatile("" ::: "memory");
     }
   } else if (act) {
     // lowest modes: low[(mode*2 + 0)*NZ + k] = 1/den_k, low[(mode*2 + 1)*NZ + k] = c'_k (FP64, host-factored)
@@ -861,7 +885,7 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     double dprev = 0.0;
 #pragma unroll 8
     for (int k = 0; k < NZ; k++) {   // the coefficient loads do not depend on the recurrence: unrolled, they overlap
-      dprev = (double(col[k * LS]) - double(__ldg(zop + k).x) * dprev) * __ldg(rd + k);
+      dprev = (double(col[k * LS]) - double(Z.z[k].x) * dprev) * __ldg(rd + k);
       d[k] = dprev;
     }
     double x = dprev;
@@ -876,31 +900,52 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     for (int k = 0; k < NZ; k++) col[k * LS] = 0.f;   // modes past the grid: zeros (the padding of the output rows)
   }
   __syncthreads();
-  // transposed output, TRI_KC levels at a time: thread -> (level kk of the chunk, l); its 8 m go out as one 16-byte
-  // row of hi and one of lo, at [kk][l][0..7] of the chunk's hi and lo halves
-  const int kk = tid >> 5, lx = tid & 31;
-  for (int k0 = 0; k0 < NZ; k0 += TRI_KC) {
-    float* chunk = tile + k0 * LS;
-    float v[TRI_TM];
+  // transposed output: in group g, warp kk writes level 8 g + kk; lane -> (l = lx, half of the 16 m); a lane reads
+  // its 8 m with the pairs of the second half-warp swapped (m ^ 1), so that the two halves hit different banks, and
+  // packs them back in order; the split rows are held as packed bf16 pairs until every thread has read the tile
+  const int kk = tid >> 5, lx = tid & 15, half = (tid >> 4) & 1;
+  constexpr int NG = NZ / 8;
+  uint4 ph[NG], pl[HI_ONLY ? 1 : NG];
 #pragma unroll
-    for (int u = 0; u < TRI_TM; u++) v[u] = chunk[kk * LS + u * TRI_TL + lx];
-    __align__(16) __nv_bfloat16 h16[TRI_TM], l16[TRI_TM];
+  for (int g = 0; g < NG; g++) {
+    const float* src = tile + (g * 8 + kk) * LS + half * 8 * TRI_TL + lx;
+    const float* se = src + half * TRI_TL;   // even u reads m = u + half
+    const float* so = src - half * TRI_TL;   // odd u reads m = u - half
+    float v[8];
 #pragma unroll
-    for (int u = 0; u < TRI_TM; u++) tc::split_bf16(v[u], h16[u], l16[u]);
-    __syncthreads();   // every read of this chunk is done before it is overwritten
-    uint4* hi = reinterpret_cast<uint4*>(chunk);
-    uint4* lo = reinterpret_cast<uint4*>(chunk) + TRI_KC * TRI_TL;
-    hi[kk * TRI_TL + lx] = *reinterpret_cast<const uint4*>(h16);
-    lo[kk * TRI_TL + lx] = *reinterpret_cast<const uint4*>(l16);
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc::tma_store_3d(&tHi, hi, m0, l0, k0);
-      tc::tma_store_3d(&tLo, lo, m0, l0, k0);
-      tc::bulk_commit();
+    for (int u = 0; u < 8; u++) v[u] = (u & 1) ? so[u * TRI_TL] : se[u * TRI_TL];
+    uint32_t h[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const float a = half ? v[2 * u + 1] : v[2 * u], b = half ? v[2 * u] : v[2 * u + 1];
+      const __nv_bfloat162 hh = __floats2bfloat162_rn(a, b);
+      h[u] = *reinterpret_cast<const uint32_t*>(&hh);
+      if (!HI_ONLY) {
+        const float2 hf = __bfloat1622float2(hh);
+        const __nv_bfloat162 ll = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+        lo[u] = *reinterpret_cast<const uint32_t*>(&ll);
+      }
     }
+    ph[g] = make_uint4(h[0], h[1], h[2], h[3]);
+    if (!HI_ONLY) pl[g] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
   }
-  if (tid == 0) tc::bulk_wait_read_all();   // the shared memory stays until the stores have read it
+  __syncthreads();   // every read of the tile is done before it is overwritten
+  uint4* hi = reinterpret_cast<uint4*>(tile);            // [NZ][16 l][16 m] bf16: two uint4 per (level, l)
+  uint4* lo = hi + NZ * TRI_TL * 2;
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    const int o = ((g * 8 + kk) * TRI_TL + lx) * 2 + half;
+    hi[o] = ph[g];
+    if (!HI_ONLY) lo[o] = pl[g];
+  }
+  tc::fence_proxy_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tc::tma_store_3d(&tHi, hi, m0, l0, 0);
+    if (!HI_ONLY) tc::tma_store_3d(&tLo, lo, m0, l0, 0);
+    tc::bulk_commit();
+    tc::bulk_wait_read_all();   // the shared memory stays until the stores have read it
+  }
 }
 // the same solve with plain loads and stores (tri_body), for planes whose pitch a tensor map cannot describe (T2's
 // row pitch nxp * 4 bytes not a multiple of 16)
@@ -1029,9 +1074,12 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_dst_tc2<OUT_T_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32_ADD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
     cudaFuncSetAttribute(k_dst_tc2<OUT_R_F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES);
-    cudaFuncSetAttribute(k_tri_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
-    cudaFuncSetAttribute(k_tri_tma<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
-    cudaFuncSetAttribute(k_tri_tma<80>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
+    cudaFuncSetAttribute(k_tri_tma<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma<40, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
+    cudaFuncSetAttribute(k_tri_tma<80, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
+    cudaFuncSetAttribute(k_tri_tma<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma<40, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
+    cudaFuncSetAttribute(k_tri_tma<80, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
     attr = true;
   }
 }
@@ -1058,6 +1106,7 @@ struct TcPlan {
   CUtensorMap Fx[2], Fy[2], Fr[2], Frr[2];  // fields, the A operand: S_x, S_y, the split right-hand side and residual
   CUtensorMap tri_in, tri_out[2];  // the tridiagonals' tiles: T2[k][m][l] fp32 in, S_y[k][l][m] bf16 hi / lo out
   bool tri_tma = false;
+  float4 zh[80] = {};    // the z-operator on the host: the by-value coefficients of k_tri_tma (nz <= 80)
   CUtensorMap Qh[4][2];  // the DST matrices with boxes of half a tile's width: each CTA of a pair loads one half
   bool pairs = true;     // transforms on SM pairs (k_dst_tc2); single-SM tiles (k_dst_tc) when false
 };
@@ -1151,7 +1200,7 @@ int PoissonPlan::tc_create() {
     const long din[3] = {nx, ny, nz}, pin[2] = {long(nx) * 4, long(nx) * ny * 4};
     const int bin[3] = {TRI_TL, TRI_TM, nz};
     const long dout[3] = {T->ldy, nx, nz}, pout[2] = {T->ldy * 2, T->ldy * nx * 2};
-    const int bout[3] = {TRI_TM, TRI_TL, TRI_KC};
+    const int bout[3] = {TRI_TM, TRI_TL, nz};
     T->tri_tma = make_map_3d(&T->tri_in, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, T->t2, din, pin, bin) &&
                  make_map_3d(&T->tri_out[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, T->sy_hi, dout, pout, bout) &&
                  make_map_3d(&T->tri_out[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, T->sy_lo, dout, pout, bout);
@@ -1169,6 +1218,7 @@ int PoissonPlan::tc_factor_low() {
   std::vector<float4> zo(nz);
   cudaMemcpy(lamh.data(), lam, lamh.size() * 4, cudaMemcpyDeviceToHost);
   cudaMemcpy(zo.data(), zop, zo.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+  for (int k = 0; k < nz && k < 80; k++) T->zh[k] = zo[k];
   std::vector<double> f(size_t(8) * nz);
   for (int mode = 0; mode < 4; mode++) {
     const int l = mode & 1, m = mode >> 1;
@@ -1245,6 +1295,16 @@ static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn,
   k_dst_tc<MODE, ONE><<<std::min(tiles, num_sms()), kThreads, SMEM_BYTES, s>>>(f[0], f[1], q[0], q[1], K, bn, o, err);
 }
 
+// the TMA tridiagonals of one pass: the z-operator goes by value (the host copy of set_density's coefficients)
+template <int NZ>
+static void launch_tri_tma(const TcPlan* T, const float* lam, bool hi_only, cudaStream_t s) {
+  TriZ<NZ> Z;
+  for (int k = 0; k < NZ; k++) Z.z[k] = T->zh[k];
+  const dim3 grid((T->nx + TRI_TL - 1) / TRI_TL, (T->ny + TRI_TM - 1) / TRI_TM);
+  if (hi_only) k_tri_tma<NZ, true><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<NZ>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], T->nx, T->ny, lam, Z, T->low, T->err);
+  else k_tri_tma<NZ, false><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<NZ>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], T->nx, T->ny, lam, Z, T->low, T->err);
+}
+
 // the four transforms and the tridiagonals from a split right-hand side (rx, or the residual rr when add) to phi
 // (stored, or added when add)
 static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const float4* zop, float* phi, bool add, cudaStream_t s,
@@ -1259,17 +1319,20 @@ static void tc_pass(const PoissonPlan& P, TcPlan* T, const float* lam, const flo
   if (one) launch_tc<OUT_T_F32, true>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s, QH(1));
   else launch_tc<OUT_T_F32>(T->Fy, T->Q[1], ny, T->bny, t2, T->err, s, QH(1));
   // tridiagonals -> S_y[k][l][m]
+  // (a plain-bf16 pass writes the hi plane alone: its y-inverse transform reads nothing else)
   if (T->tri_tma) {
-    const dim3 grid((nx + TRI_TL - 1) / TRI_TL, (ny + TRI_TM - 1) / TRI_TM);
     switch (nz) {
-      case 16: k_tri_tma<16><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<16>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
-      case 40: k_tri_tma<40><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<40>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
-      default: k_tri_tma<80><<<grid, TRI_TL * TRI_TM, tri_smem_bytes<80>(), s>>>(T->tri_in, T->tri_out[0], T->tri_out[1], nx, ny, lam, zop, T->low, T->err); break;
+      case 16: launch_tri_tma<16>(T, lam, one, s); break;
+      case 40: launch_tri_tma<40>(T, lam, one, s); break;
+      default: launch_tri_tma<80>(T, lam, one, s); break;
     }
-  } else switch (nz) {
-    case 16: k_tri_tc<16><<<dim3((nx + 31) / 32, (ny + tri_tm<16>() - 1) / tri_tm<16>()), dim3(32, tri_tm<16>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
-    case 40: k_tri_tc<40><<<dim3((nx + 31) / 32, (ny + tri_tm<40>() - 1) / tri_tm<40>()), dim3(32, tri_tm<40>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
-    default: k_tri_tc<80><<<dim3((nx + 31) / 32, (ny + tri_tm<80>() - 1) / tri_tm<80>()), dim3(32, tri_tm<80>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, T->sy_lo); break;
+  } else {
+    __nv_bfloat16* lo = one ? nullptr : T->sy_lo;
+    switch (nz) {
+      case 16: k_tri_tc<16><<<dim3((nx + 31) / 32, (ny + tri_tm<16>() - 1) / tri_tm<16>()), dim3(32, tri_tm<16>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, lo); break;
+      case 40: k_tri_tc<40><<<dim3((nx + 31) / 32, (ny + tri_tm<40>() - 1) / tri_tm<40>()), dim3(32, tri_tm<40>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, lo); break;
+      default: k_tri_tc<80><<<dim3((nx + 31) / 32, (ny + tri_tm<80>() - 1) / tri_tm<80>()), dim3(32, tri_tm<80>()), 0, s>>>(nx, ny, int(T->ldy), lam, zop, T->low, T->t2, T->sy_hi, lo); break;
+    }
   }
   // Y-inv: field rows (k, l), K = m, outputs j  -> S_x[k][j][l]
   const TcOut sx{T->sx_hi, T->sx_lo, nullptr, T->ldx, nx, nz * nx, ny};
