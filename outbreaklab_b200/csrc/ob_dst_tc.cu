@@ -381,10 +381,35 @@ __host__ __device__ constexpr int stages2(int BN, bool one) {
 static_assert(stages2(BNMAX, false) >= 3, "three stages at the widest tile");
 }  // namespace
 
+// The pair kernel's tile list. Tiles t < base are whole tiles of BN outputs (n fastest); when the persistent grid's
+// last round would be at most half full, the tiles of that round are split along N into S sub-tiles of w outputs each
+// (tile tt = base + u / S, sub-tile u % S), so that more pairs share the round. A sub-tile multiplies the same bf16
+// products over the same k-steps as the whole tile (the same bits); it stops at its tile's last column, so no output
+// is written twice.
+struct PairSched {
+  int ntn, BN, N, base, S, w, total;
+  // row tile, first output, MMA width (a multiple of 16) and end of the outputs this tile writes
+  __device__ __forceinline__ void at(int t, int& mt, int& n0, int& nv, int& ce) const {
+    if (t < base) {
+      mt = t / ntn;
+      n0 = (t % ntn) * BN;
+      ce = min(N, n0 + BN);
+      nv = narrow_n(BN, N - n0);
+      return;
+    }
+    const int u = t - base, tt = base + u / S, sub = u - (u / S) * S;
+    mt = tt / ntn;
+    const int nt0 = (tt % ntn) * BN;
+    n0 = nt0 + sub * w;
+    ce = min(min(N, nt0 + BN), n0 + w);
+    nv = narrow_n(w, ce - n0);
+  }
+};
+
 template <int MODE, bool ONE = false>
 __global__ void __launch_bounds__(kThreads, 1)
     k_dst_tc2(const __grid_constant__ CUtensorMap tF_hi, const __grid_constant__ CUtensorMap tF_lo,
-              const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, int BN, TcOut out,
+              const __grid_constant__ CUtensorMap tQ_hi, const __grid_constant__ CUtensorMap tQ_lo, int K, PairSched sc, TcOut out,
               unsigned int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -398,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = tc::cluster_rank();
   const bool lead = rank == 0;
-  const int ntn = (out.N + BN - 1) / BN, ntiles = ((out.M + 2 * BM - 1) / (2 * BM)) * ntn;
+  const int BN = sc.BN, ntiles = sc.total;
   const int pair = int(blockIdx.x >> 1), npairs = int(gridDim.x >> 1);
   const int bh = BN / 2;
   const int nk = (K + BK - 1) / BK;
@@ -441,8 +466,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int t = pair; t < ntiles && ok; t += npairs) {
         // the second CTA holds the second half of the N columns the pair's MMAs use
-        const int nt0 = (t % ntn) * BN, nv = narrow_n(BN, out.N - nt0);
-        const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = nt0 + int(rank) * (nv / 2);
+        int mt, nt0, nv, ce;
+        sc.at(t, mt, nt0, nv, ce);
+        const int m0 = mt * 2 * BM + int(rank) * BM, n0 = nt0 + int(rank) * (nv / 2);
         for (int kt = 0; kt < nk; kt++, g++) {
           const int s = g % nst;
           const uint32_t ph = (g / nst) & 1;
@@ -462,7 +488,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       int g = 0, it = 0;
       bool ok = true;
       for (int t = pair; t < ntiles && ok; t += npairs, it++) {
-        const uint32_t idesc = tc::idesc_bf16_f32(2 * BM, narrow_n(BN, out.N - (t % ntn) * BN));
+        int mt, n0, nv, ce;
+        sc.at(t, mt, n0, nv, ce);
+        const uint32_t idesc = tc::idesc_bf16_f32(2 * BM, nv);
         const int b = it & 1;
         if (!(ok = tc::mbar_wait(&tempty[b], ((it >> 1) & 1) ^ 1, err, 2u))) break;
         tc::tc_fence_after();
@@ -497,22 +525,27 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;
     const uint32_t tempty_lead = tc::mapa_shared(tc::smem_u32(tempty), 0);
     int it = 0;
-    if (MODE == OUT_R_F32_ADD && pair < ntiles)
-      prefetch_rows(out, (pair / ntn) * 2 * BM + int(rank) * BM + q * 32 + lane, (pair % ntn) * BN, BN);
+    if (MODE == OUT_R_F32_ADD && pair < ntiles) {
+      int mt, n0, nv, ce;
+      sc.at(pair, mt, n0, nv, ce);
+      prefetch_rows(out, mt * 2 * BM + int(rank) * BM + q * 32 + lane, n0, ce - n0);
+    }
     for (int t = pair; t < ntiles; t += npairs, it++) {
-      const int m0 = (t / ntn) * 2 * BM + int(rank) * BM, n0 = (t % ntn) * BN;
+      int mt, n0, nv, cend;
+      sc.at(t, mt, n0, nv, cend);
+      const int m0 = mt * 2 * BM + int(rank) * BM;
       if (MODE == OUT_R_F32_ADD && t + npairs < ntiles) {   // the next tile's old rows, while this one drains
-        const int tn = t + npairs;
-        prefetch_rows(out, (tn / ntn) * 2 * BM + int(rank) * BM + q * 32 + lane, (tn % ntn) * BN, BN);
+        int mtn, n0n, nvn, cen;
+        sc.at(t + npairs, mtn, n0n, nvn, cen);
+        prefetch_rows(out, mtn * 2 * BM + int(rank) * BM + q * 32 + lane, n0n, cen - n0n);
       }
       const int b = it & 1;
       if (!tc::mbar_wait(&tfull[b], (it >> 1) & 1, err, 8u)) break;
       tc::tc_fence_after();
       const int m = m0 + q * 32 + lane;
       const bool mv = m < out.M;
-      const int cend = min(out.N, n0 + BN);
       const int plane = m / out.R, r = m - plane * out.R;
-      for (int ch = 0; ch * 32 < BN; ch++) {
+      for (int ch = 0; ch * 32 < BN; ch++) {   // a sub-tile's chunks past its end are skipped below
         float v[32];
         tc::tmem_ld32(tmem + uint32_t(b * 256) + (uint32_t(q * 32) << 16) + uint32_t(ch * 32), v);
         const int c0 = n0 + ch * 32;
@@ -549,13 +582,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int rr = 0; rr < 32; rr++) old[rr] = (cv && mrow + rr < out.M) ? out.f[long(mrow + rr) * out.ld + c0 + lane] : 0.f;
           }
+          // every staged value read before the first store, so that the 32 row stores issue back to back
+          float val[32];
 #pragma unroll
-          for (int rr = 0; rr < 32; rr++) {
-            if (cv && mrow + rr < out.M) {
-              const float val = stg[rr * STG_LD + lane];
-              out.f[long(mrow + rr) * out.ld + c0 + lane] = MODE == OUT_R_F32_ADD ? old[rr] + val : val;
-            }
-          }
+          for (int rr = 0; rr < 32; rr++) val[rr] = stg[rr * STG_LD + lane];
+#pragma unroll
+          for (int rr = 0; rr < 32; rr++)
+            if (cv && mrow + rr < out.M) out.f[long(mrow + rr) * out.ld + c0 + lane] = MODE == OUT_R_F32_ADD ? old[rr] + val[rr] : val[rr];
           __syncwarp();
         }
       }
@@ -728,9 +761,8 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
   if (act && !lowm) {
     const float shift = __ldg(lam + l) + __ldg(lam + nxp + m);
     const float* h = T2 + long(m) * nxp + l;
-    float rhs[NZ];
 #pragma unroll
-    for (int k = 0; k < NZ; k++) rhs[k] = __ldg(h + sxy * k);  // all loads issued up front
+    for (int k = 0; k < NZ; k++) x[k] = __ldg(h + sxy * k);  // all loads issued up front; d and then x replace them
     float cp[NZ];
     float cprev = 0.f, dprev = 0.f;
 #pragma unroll
@@ -738,7 +770,7 @@ __device__ __forceinline__ void tri_body(int nxp, int nyp, int ldy, const float*
       const float4 o = __ldg(zop + k);
       const float rd = tri_pivot_rcp(o, shift, cprev);
       cprev = o.y * rd;
-      dprev = fmaf(-o.x, dprev, rhs[k]) * rd;
+      dprev = fmaf(-o.x, dprev, x[k]) * rd;
       cp[k] = cprev;
       x[k] = dprev;
     }
@@ -1281,14 +1313,44 @@ static int pair_slots() {
   return n;
 }
 
+// the pair kernel's tiles for M field rows and N outputs at width BN over at most max_pairs pairs (the grid, in
+// pairs): whole tiles, except that a last round at most half full is split into sub-tiles (2 to 4 per tile, each at
+// least 32 outputs wide, none empty)
+static PairSched pair_sched(int M, int N, int BN, int max_pairs, int& pairs) {
+  PairSched sc{};
+  sc.ntn = (N + BN - 1) / BN;
+  sc.BN = BN;
+  sc.N = N;
+  const int T = ((M + 2 * BM - 1) / (2 * BM)) * sc.ntn;
+  pairs = std::max(1, std::min(T, max_pairs));
+  sc.base = sc.total = T;
+  sc.S = 1;
+  sc.w = BN;
+  const int R = T % pairs, wlast = N - (sc.ntn - 1) * BN;   // tiles of the last round; the narrowest tile's width
+  if (R > 0 && 2 * R <= pairs) {
+    for (int S = std::min(4, pairs / R); S >= 2; S--) {
+      const int w = std::max(32, ((BN + S - 1) / S + 15) / 16 * 16);
+      if ((S - 1) * w < wlast) {
+        sc.base = T - R;
+        sc.S = S;
+        sc.w = w;
+        sc.total = T - R + R * S;
+        break;
+      }
+    }
+  }
+  return sc;
+}
+
 template <int MODE, bool ONE = false>
 static void launch_tc(const CUtensorMap* f, const CUtensorMap* q, int K, int bn, const TcOut& o, unsigned int* err, cudaStream_t s,
                       const CUtensorMap* qh = nullptr) {
   if (qh) {  // SM pairs: tiles of 256 field rows, qh the DST matrix maps with half-width boxes
-    const int tiles = ((o.M + 2 * BM - 1) / (2 * BM)) * ((o.N + bn - 1) / bn);
+    int pairs = 0;
+    const PairSched sc = pair_sched(o.M, o.N, bn, pair_slots(), pairs);
     cudaLaunchAttribute at[1];
-    const cudaLaunchConfig_t cfg = pair_config(std::min(tiles, pair_slots()), s, at);
-    cudaLaunchKernelEx(&cfg, k_dst_tc2<MODE, ONE>, f[0], f[1], qh[0], qh[1], K, bn, o, err);
+    const cudaLaunchConfig_t cfg = pair_config(pairs, s, at);
+    cudaLaunchKernelEx(&cfg, k_dst_tc2<MODE, ONE>, f[0], f[1], qh[0], qh[1], K, sc, o, err);
     return;
   }
   const int tiles = ((o.M + BM - 1) / BM) * ((o.N + bn - 1) / bn);
