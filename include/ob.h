@@ -385,8 +385,9 @@ int ob_model_set_surrogate(ObModel* m, const ObMlp* net);
 int ob_model_surrogate_stats(ObModel* m, unsigned* queued, unsigned* fallbacks);
 
 /* ---- the pressure solve for callers that cannot allocate device memory ----
- * No counterpart in the reference. For a host that may not call cudaMalloc (work recorded into a CUDA graph while
- * the capture is live, or a plugin living inside another runtime's fixed GPU memory budget): one fp32 solve of
+ * No counterpart in the reference. For a host that may not call cudaMalloc: a plugin that lives inside another
+ * runtime which owns the GPU's memory and hands out only its own fixed budget, or a host whose rules forbid device
+ * allocation after start-up. One fp32 solve of
  * rhoC lap_h(phi) + d/dz(rhoW dphi/dz) = rhs on nx*ny*nz with every working buffer in a fixed file-scope device array
  * (about 14 MB, held by each GPU that loads the library until the process exits). All pointers are device pointers
  * owned by the caller: rhoC[nz], rhoW[nz+1], rhs and phi (nx*ny*nz, x fastest); the work is queued on `stream`

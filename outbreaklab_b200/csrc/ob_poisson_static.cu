@@ -1,8 +1,8 @@
 // ob_poisson_static.cu — the pressure solve without any device allocation.
 //
-// Some hosts cannot call cudaMalloc: a caller that records its work into a CUDA graph while the capture is live
-// (allocation is not a capturable operation), or a plugin that runs inside another runtime's memory budget and has
-// no right to grow it (a JavaScript engine's GPU process, a real-time loop that must never block on the allocator).
+// Some hosts cannot call cudaMalloc: a plugin that runs inside another runtime's memory budget and has no right to
+// grow it (a JavaScript engine's GPU process), or a real-time loop whose rules forbid blocking on the allocator once
+// it has started.
 // For them this file keeps the solver's working memory — the sine-transform matrices, eigenvalues, z-operator and
 // the two intermediate spectra — in one file-scope device array of fixed size, and the entry point only launches
 // kernels into it. The caller still owns and passes the right-hand side, the solution and the densities.

@@ -1,10 +1,11 @@
 """The allocation-free pressure solve (ob_poisson_solve_static) against the handle-based one (ob_poisson_solve).
 
-Some callers cannot allocate GPU memory: code recording into a CUDA graph while the capture is live, or a plugin
-bound to another runtime's fixed memory budget. ob_poisson_solve_static serves them from a fixed device array; this
-test calls it through the C ABI twice in a row (the array keeps the previous call's contents) and checks each result
-against the allocating entry point within the tests' one-step tolerance (1e-5 relative). It sits in its own file,
-collected last, and works both alone in a fresh process and after the other tests.
+Some callers cannot allocate GPU memory: a plugin bound to another runtime that owns the GPU's memory and hands out
+only its own fixed budget, or a host that forbids device allocation after start-up. ob_poisson_solve_static serves
+them from a fixed device array; this test calls it through the C ABI twice in a row (the array keeps the previous
+call's contents) and checks each result against the allocating entry point within the tests' one-step tolerance
+(1e-5 relative). It sits in its own file, collected last, and works both alone in a fresh process and after the other
+tests.
 """
 import ctypes as C
 
