@@ -1108,22 +1108,28 @@ __device__ __forceinline__ void phys_flags(const Grid& g, const Fields& F, int B
   if (!HUR) was0 = F.actQ0[BX + F.nbx * (BY + F.nby * ck)] == 0u;
 }
 
-template <int MM, bool HUR = false>
+// BND: 1 = boundary air masses present, 0 = none, -1 = decided per launch from the uniforms (U.cor.z)
+template <int MM, bool HUR = false, int BND = -1>
 __device__ __forceinline__ void phys_body(const Grid& g, const Uni& U, const Fields& F, int par, const int BX, const int BY, const int BZ) {
   const int ci = BX * blockDim.x + threadIdx.x, cj = BY * blockDim.y + threadIdx.y, ck = BZ;
   bool dry, was0;
   phys_flags<HUR>(g, F, BX, BY, ck, dry, was0);
   bool hyd = false;
   if (ci <= g.nx && cj <= g.ny && ck <= g.nz)
-    hyd = U.cor.z > 0.5f ? phys_texel<true, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0)
-                         : phys_texel<false, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0);
+    hyd = (BND == 1 || (BND < 0 && U.cor.z > 0.5f)) ? phys_texel<BND != 0, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0)
+                                                    : phys_texel<false, MM, HUR>(g, U, F, par, ci, cj, ck, dry, was0);
   // hydrometeor flag of this block's brick for the next step's scalar advection
   const bool any = __syncthreads_or(hyd) != 0;
   if (threadIdx.x == 0 && threadIdx.y == 0 && int(BX) < F.nbx && int(BY) < F.nby && ck < g.nz)
     F.actQ0[BX + F.nbx * (BY + F.nby * ck)] = any ? 1u : 0u;
 }
-template <int MM>
-__global__ void __launch_bounds__(128, 9) k_phys(Grid g, Uni U, Fields F, int par) { phys_body<MM>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z); }
+// one kernel per microphysics mode and per presence of boundary air masses: with one texel body per kernel, ten
+// 128-thread blocks fit on an SM at 48 registers without spilling (the surrogate with boundaries keeps nine), where the
+// kernel holding both bodies needed 56 registers at nine blocks; 0.64 -> 0.61 ms at 640 x 640 x 40
+template <int MM, int BND>
+__global__ void __launch_bounds__(128, (MM == kMicroSurrogate && BND == 1) ? 9 : 10) k_phys(Grid g, Uni U, Fields F, int par) {
+  phys_body<MM, false, BND>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 __global__ void __launch_bounds__(128) k_phys_hur(Grid g, Uni U, Fields F, int par) {
   phys_body<kMicroPlain, true>(g, U, F, par, blockIdx.x, blockIdx.y, blockIdx.z);
 }
@@ -1558,9 +1564,18 @@ void launch_phys(const Grid& g, const Uni& U, const Fields& F, int par, cudaStre
     k_phys_hur<<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
     return;
   }
-  if (micro_mode == kMicroRecord) k_phys<kMicroRecord><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
-  else if (micro_mode == kMicroSurrogate) k_phys<kMicroSurrogate><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
-  else k_phys<kMicroPlain><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3), kB3, 0, s>>>(g, U, F, par);
+  const dim3 grid = grid3(g.nx + 1, g.ny + 1, g.nz + 1, kB3);
+  const bool bnd = U.cor.z > 0.5f;
+  if (micro_mode == kMicroRecord) {
+    if (bnd) k_phys<kMicroRecord, 1><<<grid, kB3, 0, s>>>(g, U, F, par);
+    else k_phys<kMicroRecord, 0><<<grid, kB3, 0, s>>>(g, U, F, par);
+  } else if (micro_mode == kMicroSurrogate) {
+    if (bnd) k_phys<kMicroSurrogate, 1><<<grid, kB3, 0, s>>>(g, U, F, par);
+    else k_phys<kMicroSurrogate, 0><<<grid, kB3, 0, s>>>(g, U, F, par);
+  } else {
+    if (bnd) k_phys<kMicroPlain, 1><<<grid, kB3, 0, s>>>(g, U, F, par);
+    else k_phys<kMicroPlain, 0><<<grid, kB3, 0, s>>>(g, U, F, par);
+  }
 }
 void launch_div(const Grid& g, const Uni& U, const Fields& F, int par, cudaStream_t s) {
   k_div<<<grid3(g.nx, g.ny, g.nz, kB3), kB3, 0, s>>>(g, U, F, par);
