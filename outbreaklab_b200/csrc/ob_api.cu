@@ -229,6 +229,9 @@ static void model_bind_solver(ObModel* m) {
     m->solver.tc_rhs_split(&m->F.rhs_hi, &m->F.rhs_lo, &m->F.rhs_ld);
     m->solver.presplit = true;
     if (m->solver.precision == 1) m->F.rhs = nullptr;  // no fp32 copy needed
+    // precision 5's first pass is plain bf16 (the hi plane alone) and its refinement starts from the fp32 residual:
+    // the lo plane of the right-hand side is never read
+    if (m->solver.precision == 5) m->F.rhs_lo = nullptr;
   }
 }
 

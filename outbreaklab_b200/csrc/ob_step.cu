@@ -1160,7 +1160,7 @@ __device__ __forceinline__ void div_body(const Grid& g, const Uni& U, const Fiel
     const long o2 = (long(ck) * g.nyp + (cj + g.pad)) * F.rhs_ld + (ci + g.pad);
     const __nv_bfloat16 h = __float2bfloat16_rn(r);
     F.rhs_hi[o2] = h;
-    F.rhs_lo[o2] = __float2bfloat16_rn(r - __bfloat162float(h));
+    if (F.rhs_lo) F.rhs_lo[o2] = __float2bfloat16_rn(r - __bfloat162float(h));   // none when no pass reads it
   }
   if (F.rhs) F.rhs[g.pidx(ci, cj, ck)] = r;  // fp32 solve, or the residual of the refined solve
 }
