@@ -55,3 +55,64 @@ def test_run_loop_with_fronts_starts_storms_along_them(native):
     assert res["events"] > 0 and g.nan_count == 0
     A = g.get_field(N.FIELD_LSF_A).reshape(case.ny, case.nx, 4)
     assert A[..., 0].min() < -3.0 and A[..., 0].max() > 1.0
+
+
+class _Recorder:
+    """The GPU model as the run loop sees it, recording every storm-start list the scheduler sends (setCI) with the
+    number of steps taken before it, packed as the model packs it."""
+
+    def __init__(self, model):
+        self._m = model
+        self.calls = []
+
+    def __getattr__(self, name):
+        return getattr(self._m, name)
+
+    def set_ci(self, events):
+        f, act = M.pack_ci(events, self._m.time)
+        self.calls.append((self._m.steps, f.copy(), len(act)))
+        self._m.set_ci(events)
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_run_loop_storm_starts_match_the_oracle(oracle_lib, native, scheme):
+    """The run loop's scheduler (warm sector and along the reference's example fronts) drives the GPU model for 132 s
+    (11 steps through the LSF pass at t = 60 s, scheduler windows at t = 0, 60 and 120 s); every storm-start list it
+    sent, at the step it was sent, is replayed on the FP32 oracle and its FP64 instantiation, and the state is held
+    to the five-step bar: max(1e-4, 3 x the FP32 oracle's error) per field and channel against FP64."""
+    from outbreaklab_b200 import workloads as W
+    from _parity import check_field
+    case = W.case_fronts(scheme=scheme)
+    bounds, _ = W.fronts_setup(case)
+    for mb in bounds:
+        mb["b"] = dict(mb["b"], rate=400.0)
+    g, _ = M.setup_case(case, bounds=bounds)
+    rec = _Recorder(g)
+    loop = RL.RunLoop(rec, case.dt, 132.0, ci={"warmRate": 3000.0, "start": 0.0, "rh": 6000.0}, replay_every=60.0,
+                      bounds=bounds)
+    res = loop.run()
+    g.sync()
+    assert res["steps"] == 11 and res["events"] > 0 and rec.calls, res
+    f, _ = oracle_lib.setup_case(case, 4, bounds=bounds)
+    d, _ = oracle_lib.setup_case(case, 8, bounds=bounds)
+    calls = list(rec.calls)
+    for step in range(res["steps"]):
+        while calls and calls[0][0] == step:
+            _, packed, n = calls.pop(0)
+            for o in (f, d):
+                o.set_ci(packed, n)
+        for o in (f, d):
+            o.step(case.dt, 1)
+    assert not calls
+    assert abs(d.time - g.time) < 1e-9
+    C = d.get(N.FIELD_CI_MAP, f64=True).reshape(-1, 4)
+    assert ((C[:, 0] * C[:, 1]) > 0.5).sum() > 10, "no storm-start push on the oracle side"
+    bad = []
+    for fld, ch in ((N.FIELD_V, 4), (N.FIELD_Q1, 4), (N.FIELD_Q2, 4), (N.FIELD_PHI, 1)):
+        errs, b = check_field(fld, g.get_field(fld), f.get(fld), d.get(fld, f64=True), ch, 1e-4, 3.0)
+        print(fld, ["%.2e/%.2e" % e for e in errs])
+        bad += b
+    bad += check_field(N.FIELD_CI_MAP, g.get_field(N.FIELD_CI_MAP), f.get(N.FIELD_CI_MAP),
+                       d.get(N.FIELD_CI_MAP, f64=True), 4, 1e-5, 2.0)[1]
+    assert not bad, "\n".join(bad)
+    assert g.nan_count == 0
