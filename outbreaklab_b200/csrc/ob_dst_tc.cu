@@ -851,28 +851,27 @@ struct TriZ {
   float4 z[NZ];
 };
 
-template <int NZ, bool HI_ONLY>
-__global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(const __grid_constant__ CUtensorMap tIn, const __grid_constant__ CUtensorMap tHi,
-                                                          const __grid_constant__ CUtensorMap tLo, int nxp, int nyp,
-                                                          const float* __restrict__ lam, const __grid_constant__ TriZ<NZ> Z,
-                                                          const double* __restrict__ low, unsigned int* err) {
+// One block's tile (modes l0 .. l0 + 15, m0 .. m0 + 15) given its tensor maps (kernel parameters, or a member's maps
+// in global memory) and zop(k), the z-operator of level k (a constant-bank parameter, or a copy in shared memory).
+template <int NZ, bool HI_ONLY, class Zop>
+__device__ __forceinline__ void tri_tma_tile(const CUtensorMap* tIn, const CUtensorMap* tHi, const CUtensorMap* tLo, int nxp, int nyp,
+                                             const float* __restrict__ lam, const Zop& zop, const double* __restrict__ low,
+                                             unsigned int* err, const int l0, const int m0, uint8_t* smraw) {
   static_assert(NZ % 8 == 0, "levels come in whole groups of 8");
-  extern __shared__ uint8_t smraw[];
   float* tile = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
   double* dlow = reinterpret_cast<double*>(tile + NZ * TRI_TM * TRI_TL);   // [4][NZ]: d of the FP64 low modes
   uint64_t* bar = reinterpret_cast<uint64_t*>(dlow + 4 * NZ);
   static_assert(TRI_TL == 16 && TRI_TM == 16, "thread and output mappings below assume 16 x 16 modes");
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4, tid = threadIdx.x;
-  const int l0 = blockIdx.x * TRI_TL, m0 = blockIdx.y * TRI_TM;
   if (tid == 0) {
-    tc::prefetch_tmap(&tIn);
+    tc::prefetch_tmap(tIn);
     tc::mbar_init(bar, 1);
     tc::fence_mbar_init();
   }
   __syncthreads();
   if (tid == 0) {
     tc::mbar_expect_tx(bar, NZ * TRI_TM * TRI_TL * 4);
-    tc::tma_load_3d(tile, &tIn, bar, l0, m0, 0);
+    tc::tma_load_3d(tile, tIn, bar, l0, m0, 0);
   }
   const int l = l0 + tx, m = m0 + ty;
   const bool act = l < nxp && m < nyp;
@@ -891,7 +890,7 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     float cprev = 0.f, dprev = 0.f;
 #pragma unroll
     for (int k = 0; k < NZ; k++) {
-      const float4 o = Z.z[k];
+      const float4 o = zop(k);
       const float rd = tri_pivot_rcp(o, shift, cprev);
       cprev = o.y * rd;
       dprev = fmaf(-o.x, dprev, col[k * LS]) * rd;
@@ -917,7 +916,7 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
     double dprev = 0.0;
 #pragma unroll 8
     for (int k = 0; k < NZ; k++) {   // the coefficient loads do not depend on the recurrence: unrolled, they overlap
-      dprev = (double(col[k * LS]) - double(Z.z[k].x) * dprev) * __ldg(rd + k);
+      dprev = (double(col[k * LS]) - double(zop(k).x) * dprev) * __ldg(rd + k);
       d[k] = dprev;
     }
     double x = dprev;
@@ -973,11 +972,56 @@ __global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(co
   tc::fence_proxy_async_smem();
   __syncthreads();
   if (tid == 0) {
-    tc::tma_store_3d(&tHi, hi, m0, l0, 0);
-    if (!HI_ONLY) tc::tma_store_3d(&tLo, lo, m0, l0, 0);
+    tc::tma_store_3d(tHi, hi, m0, l0, 0);
+    if (!HI_ONLY) tc::tma_store_3d(tLo, lo, m0, l0, 0);
     tc::bulk_commit();
     tc::bulk_wait_read_all();   // the shared memory stays until the stores have read it
   }
+}
+
+template <int NZ, bool HI_ONLY>
+__global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma(const __grid_constant__ CUtensorMap tIn, const __grid_constant__ CUtensorMap tHi,
+                                                          const __grid_constant__ CUtensorMap tLo, int nxp, int nyp,
+                                                          const float* __restrict__ lam, const __grid_constant__ TriZ<NZ> Z,
+                                                          const double* __restrict__ low, unsigned int* err) {
+  extern __shared__ uint8_t smraw[];
+  tri_tma_tile<NZ, HI_ONLY>(&tIn, &tHi, &tLo, nxp, nyp, lam, [&](int k) { return Z.z[k]; }, low, err, blockIdx.x * TRI_TL,
+                            blockIdx.y * TRI_TM, smraw);
+}
+
+// The same tiles for every member of an ensemble: member p owns the blocks [start[p], start[p+1]) of its gx x gy
+// tiles; its tensor maps live in global memory (written by the host before any launch that reads them), and its
+// z-operator is copied into shared memory for the sweeps (the members' densities differ, so it cannot be a parameter)
+struct alignas(64) TriTmaProb {
+  CUtensorMap in, hi, lo;
+  const float* lam;
+  const float4* zop;
+  const double* low;
+  int nxp, nyp, gx, pad;
+};
+template <int NZ, bool HI_ONLY>
+__global__ void __launch_bounds__(TRI_TL * TRI_TM, NZ > 40 ? 2 : 4) k_tri_tma_grp(const TriTmaProb* __restrict__ probs, const int* __restrict__ start,
+                                                                              int n, unsigned int* err) {
+  extern __shared__ uint8_t smraw[];
+  __shared__ float4 zs[NZ];
+  __shared__ int s_mem, s_r;
+  if (threadIdx.x == 0) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    s_mem = lo;
+    s_r = b - __ldg(start + lo);
+  }
+  __syncthreads();
+  const TriTmaProb* P = probs + s_mem;
+  for (int k = threadIdx.x; k < NZ; k += blockDim.x) zs[k] = __ldg(P->zop + k);   // read after the tile's first barrier
+  const int r = s_r, gx = P->gx;
+  tri_tma_tile<NZ, HI_ONLY>(&P->in, &P->hi, &P->lo, P->nxp, P->nyp, P->lam, [&](int k) { return zs[k]; }, P->low, err,
+                            (r % gx) * TRI_TL, (r / gx) * TRI_TM, smraw);
 }
 // the same solve with plain loads and stores (tri_body), for planes whose pitch a tensor map cannot describe (T2's
 // row pitch nxp * 4 bytes not a multiple of 16)
@@ -1110,6 +1154,12 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_tri_tma<40, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
     cudaFuncSetAttribute(k_tri_tma<80, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
     cudaFuncSetAttribute(k_tri_tma<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma_grp<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma_grp<40, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
+    cudaFuncSetAttribute(k_tri_tma_grp<80, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
+    cudaFuncSetAttribute(k_tri_tma_grp<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<16>());
+    cudaFuncSetAttribute(k_tri_tma_grp<40, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
+    cudaFuncSetAttribute(k_tri_tma_grp<80, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
     cudaFuncSetAttribute(k_tri_tma<40, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<40>());
     cudaFuncSetAttribute(k_tri_tma<80, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri_smem_bytes<80>());
     attr = true;
@@ -1497,6 +1547,9 @@ struct TcGroup {
   GemmProb* d_probs = nullptr;  // [5][n]: x-fwd, y-fwd, y-inv, x-inv, x-fwd of the residual
   int* d_start = nullptr;       // [5][n + 1] tile starts, [n + 1] tridiagonal block starts, [n + 1] residual block starts
   TriProb* d_tri = nullptr;
+  TriTmaProb* d_tri_tma = nullptr;  // the TMA tridiagonals' per-member maps, when every member has them
+  bool tri_tma = false;
+  int tri_tma_blocks = 0;
   ResidProb* d_res = nullptr;
   uint2* d_res_map = nullptr;  // block map of the residual launch
   unsigned int* err = nullptr;
@@ -1509,7 +1562,9 @@ static int tc_group_build(TcGroup* G) {
   const int n = G->n;
   constexpr int NT = 5;  // transform lists
   std::vector<GemmProb> probs(size_t(NT) * n);
-  std::vector<int> start(size_t(NT + 2) * (n + 1), 0);
+  std::vector<int> start(size_t(NT + 3) * (n + 1), 0);
+  std::vector<TriTmaProb> trit(n);
+  bool all_tma = true;
   std::vector<TriProb> tri(n);
   std::vector<ResidProb> res(n);
   std::vector<uint2> res_map;
@@ -1542,6 +1597,24 @@ static int tc_group_build(TcGroup* G) {
       const int nt = ((out[t].M + BM - 1) / BM) * g.ntn;
       start[size_t(t) * (n + 1) + i + 1] = start[size_t(t) * (n + 1) + i] + nt;
     }
+    {  // the TMA tiles of 16 x 16 modes (k_tri_tma_grp), when this member's plan has their maps
+      const int tx16 = (nx + TRI_TL - 1) / TRI_TL, ty16 = (ny + TRI_TM - 1) / TRI_TM;
+      all_tma = all_tma && T->tri_tma;
+      TriTmaProb& q = trit[i];
+      std::memset(&q, 0, sizeof(q));
+      if (T->tri_tma) {
+        q.in = T->tri_in;
+        q.hi = T->tri_out[0];
+        q.lo = T->tri_out[1];
+      }
+      q.lam = P->lam;
+      q.zop = P->zop;
+      q.low = T->low;
+      q.nxp = nx;
+      q.nyp = ny;
+      q.gx = tx16;
+      start[size_t(NT + 2) * (n + 1) + i + 1] = start[size_t(NT + 2) * (n + 1) + i] + tx16 * ty16;
+    }
     const int gx = (nx + 31) / 32, gy = (ny + tm - 1) / tm;
     tri[i] = TriProb{nx, ny, int(T->ldy), gx, P->lam, P->zop, T->low, T->t2, T->sy_hi, T->sy_lo};
     start[size_t(NT) * (n + 1) + i + 1] = start[size_t(NT) * (n + 1) + i] + gx * gy;
@@ -1554,9 +1627,12 @@ static int tc_group_build(TcGroup* G) {
   for (int t = 0; t < NT; t++) G->tiles[t] = start[size_t(t) * (n + 1) + n];
   G->tri_blocks = start[size_t(NT) * (n + 1) + n];
   G->res_blocks = start[size_t(NT + 1) * (n + 1) + n];
+  G->tri_tma = all_tma;
+  G->tri_tma_blocks = start[size_t(NT + 2) * (n + 1) + n];
   const bool ok = cudaMemcpy(G->d_probs, probs.data(), probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_tri, tri.data(), tri.size() * sizeof(TriProb), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(G->d_tri_tma, trit.data(), trit.size() * sizeof(TriTmaProb), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_res, res.data(), res.size() * sizeof(ResidProb), cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(G->d_res_map, res_map.data(), res_map.size() * sizeof(uint2), cudaMemcpyHostToDevice) == cudaSuccess;
   if (!ok) {
@@ -1568,7 +1644,7 @@ static int tc_group_build(TcGroup* G) {
 
 void tc_group_destroy(TcGroup* G) {
   if (!G) return;
-  for (void* p : {(void*)G->d_probs, (void*)G->d_start, (void*)G->d_tri, (void*)G->d_res, (void*)G->d_res_map, (void*)G->err})
+  for (void* p : {(void*)G->d_probs, (void*)G->d_start, (void*)G->d_tri, (void*)G->d_tri_tma, (void*)G->d_res, (void*)G->d_res_map, (void*)G->err})
     if (p) cudaFree(p);
   delete G;
 }
@@ -1613,8 +1689,9 @@ int tc_group_create(PoissonPlan* const* plans, float* const* phi, const float* c
     return OB_ERR_INVALID;
   }
   const bool ok = cudaMalloc(&G->d_probs, size_t(5) * n * sizeof(GemmProb)) == cudaSuccess &&
-                  cudaMalloc(&G->d_start, size_t(7) * (n + 1) * sizeof(int)) == cudaSuccess &&
+                  cudaMalloc(&G->d_start, size_t(8) * (n + 1) * sizeof(int)) == cudaSuccess &&
                   cudaMalloc(&G->d_tri, size_t(n) * sizeof(TriProb)) == cudaSuccess &&
+                  cudaMalloc(&G->d_tri_tma, size_t(n) * sizeof(TriTmaProb)) == cudaSuccess &&
                   cudaMalloc(&G->d_res, size_t(n) * sizeof(ResidProb)) == cudaSuccess && cudaMalloc(&G->err, 16) == cudaSuccess &&
                   cudaMalloc(&G->d_res_map, res_map_blocks(plans, n) * sizeof(uint2)) == cudaSuccess &&
                   cudaMemset(G->err, 0, 16) == cudaSuccess;
@@ -1661,7 +1738,19 @@ static void tc_group_pass(const TcGroup* G, bool add, cudaStream_t s, bool one =
     launch_tc_grp<OUT_T_F32>(G, 1, s);
   }
   const int* ts = G->d_start + size_t(5) * (n + 1);
-  switch (G->nz) {
+  if (G->tri_tma) {   // TMA tiles; a plain-bf16 pass writes the hi plane alone
+    const int* tt = G->d_start + size_t(7) * (n + 1);
+    const int nb = G->tri_tma_blocks, th = TRI_TL * TRI_TM;
+#define OB_TRI_GRP(NZ)                                                                                        \
+    if (one) k_tri_tma_grp<NZ, true><<<nb, th, tri_smem_bytes<NZ>(), s>>>(G->d_tri_tma, tt, n, G->err);      \
+    else k_tri_tma_grp<NZ, false><<<nb, th, tri_smem_bytes<NZ>(), s>>>(G->d_tri_tma, tt, n, G->err);
+    switch (G->nz) {
+      case 16: OB_TRI_GRP(16) break;
+      case 40: OB_TRI_GRP(40) break;
+      default: OB_TRI_GRP(80) break;
+    }
+#undef OB_TRI_GRP
+  } else switch (G->nz) {
     case 16: k_tri_tc_grp<16><<<G->tri_blocks, dim3(32, tri_tm<16>()), 0, s>>>(G->d_tri, ts, n); break;
     case 40: k_tri_tc_grp<40><<<G->tri_blocks, dim3(32, tri_tm<40>()), 0, s>>>(G->d_tri, ts, n); break;
     default: k_tri_tc_grp<80><<<G->tri_blocks, dim3(32, tri_tm<80>()), 0, s>>>(G->d_tri, ts, n); break;
