@@ -86,3 +86,16 @@ def test_perturb_theta_touches_interior_only():
     assert np.all(P[..., :3] == 0)
     assert np.all(P[case.nz, :, :, 3] == 0) and np.all(P[:, case.ny, :, 3] == 0) and np.all(P[:, :, case.nx, 3] == 0)
     assert np.abs(P[:case.nz, :case.ny, :case.nx, 3]).max() > 1.0
+
+
+def test_traffic_table_covers_the_bench_passes():
+    """bench.py's roofline traffic comes from profiles/ncu_traffic.json: every pass with algorithmic bytes but LSF+CI
+    (a few 2-D columns) has a positive entry with its captured cell count, and the solve's entry is the sum of its
+    kernels' captures (transforms 622 MB, tridiagonals 73 + 89 MB, residual 181 MB per precision-5 solve)."""
+    import json
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(root, "profiles", "ncu_traffic.json")) as f:
+        table = json.load(f)
+    for name in ("NUT", "ADVV", "ADVQ", "PHYS", "DIV", "SOLVE", "PROJ+RAIN"):
+        assert table[name]["bytes"] > 0 and table[name]["cells"] > 0, name
+    assert abs(table["SOLVE"]["bytes"] - (622 + 73 + 89 + 181) * 1e6) < 1e6
